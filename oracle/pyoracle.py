@@ -1,0 +1,304 @@
+"""Test infrastructure, not product code.
+
+ctypes bindings for the two CPU checkers:
+  * ``Restatement`` - oracle/rq_oracle.c, the per-ray C restatement of the
+    reference's ray-query path (builds anywhere gcc exists);
+  * ``Reference``   - oracle/_ref/libmanta_ref.so, the reference's own classes
+    compiled from its sources by oracle/ref.mk, driven by
+    oracle/ref_harness.cc.  Present only where that library was built.
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmanta_ref.so")
+REF_SSE_SO = os.path.join(HERE, "_ref", "libmanta_ref_sse.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C")
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+@dataclass
+class Tree:
+    """Reference DynBVH node array, field by field (DynBVH.h:37-79)."""
+
+    bounds: np.ndarray  # (N, 6) float32: min xyz, max xyz
+    child: np.ndarray  # (N,) int32
+    children: np.ndarray  # (N,) int32, leaf iff != 0
+    axis: np.ndarray  # (N,) uint8
+    left_cheaper: np.ndarray  # (N,) uint8
+    ids: np.ndarray  # (T,) int32
+
+    def arrays(self):
+        return (np.ascontiguousarray(self.bounds, np.float32),
+                np.ascontiguousarray(self.child, np.int32),
+                np.ascontiguousarray(self.children, np.int32),
+                np.ascontiguousarray(self.axis, np.uint8),
+                np.ascontiguousarray(self.left_cheaper, np.uint8),
+                np.ascontiguousarray(self.ids, np.int32))
+
+    def save_npz(self, path):
+        np.savez_compressed(path, bounds=self.bounds, child=self.child,
+                            children=self.children, axis=self.axis,
+                            left_cheaper=self.left_cheaper, ids=self.ids)
+
+    @staticmethod
+    def load_npz(path) -> "Tree":
+        z = np.load(path)
+        return Tree(z["bounds"], z["child"], z["children"], z["axis"],
+                    z["left_cheaper"], z["ids"])
+
+
+def build_restatement() -> str:
+    if not os.path.exists(ORACLE_SO) or (
+            os.path.getmtime(ORACLE_SO) < os.path.getmtime(os.path.join(HERE, "rq_oracle.c"))):
+        subprocess.check_call(["make", "-s", "-f", os.path.join(HERE, "Makefile")],
+                              cwd=os.path.dirname(HERE))
+    return ORACLE_SO
+
+
+class Restatement:
+    """oracle/rq_oracle.c through ctypes."""
+
+    def __init__(self):
+        self.lib = C.CDLL(build_restatement())
+        L = self.lib
+        L.orq_wald_setup.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.orq_trace.argtypes = [C.c_void_p] * 10 + [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 7
+        L.orq_trace.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 3 +
+                                [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 7)
+        L.orq_top2.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 3 +
+                               [C.c_int] + [C.c_void_p] * 7)
+        L.orq_sah_cost.argtypes = [C.c_void_p] * 3
+        L.orq_sah_cost.restype = C.c_double
+        L.orq_camera_basis.argtypes = [C.c_void_p] * 3 + [C.c_float, C.c_float, C.c_void_p]
+        L.orq_primary_rays.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.orq_render_whitted.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 6 +
+                                         [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 4)
+        L.orq_render_whitted.restype = C.c_longlong
+
+    def wald_setup(self, mesh) -> np.ndarray:
+        v = np.ascontiguousarray(mesh.vertices, np.float32)
+        i = np.ascontiguousarray(mesh.indices, np.uint32)
+        out = np.zeros((mesh.n_tris, 12), np.float32)
+        self.lib.orq_wald_setup(_ptr(v), _ptr(i), mesh.n_tris, _ptr(out))
+        return out
+
+    def _scene_args(self, tree: Tree, mesh, tri_kind, wald):
+        b, c, ch, ax, lc, ids = tree.arrays()
+        v = np.ascontiguousarray(mesh.vertices, np.float32)
+        ix = np.ascontiguousarray(mesh.indices, np.uint32)
+        if wald is None and tri_kind == 0:
+            wald = self.wald_setup(mesh)
+        keep = (b, c, ch, ax, lc, ids, v, ix, wald)
+        args = [_ptr(b), _ptr(c), _ptr(ch), _ptr(ax), _ptr(lc), _ptr(ids), tri_kind,
+                _ptr(v), _ptr(ix), _ptr(wald) if wald is not None else None]
+        return keep, args
+
+    def trace(self, tree, mesh, org, dir, tmax, anyhit=False, tri_kind=0,
+              wald=None, counts=False):
+        n = int(tmax.shape[0])
+        org = np.ascontiguousarray(org, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        keep, args = self._scene_args(tree, mesh, tri_kind, wald)
+        hit = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        nt = np.zeros(n, np.int32) if counts else None
+        tt = np.zeros(n, np.int32) if counts else None
+        self.lib.orq_trace(*args, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
+                           _ptr(hit), _ptr(t), _ptr(prim), _ptr(u), _ptr(v),
+                           _ptr(nt), _ptr(tt))
+        out = dict(hit=hit, t=t, prim=prim, u=u, v=v)
+        if counts:
+            out["node_tests"] = nt
+            out["tri_tests"] = tt
+        return out
+
+    def top2(self, tree, mesh, org, dir, tmax, tri_kind=0, wald=None):
+        n = int(tmax.shape[0])
+        org = np.ascontiguousarray(org, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        keep, args = self._scene_args(tree, mesh, tri_kind, wald)
+        t1 = np.zeros(n, np.float32)
+        t2 = np.zeros(n, np.float32)
+        p1 = np.zeros(n, np.int32)
+        p2 = np.zeros(n, np.int32)
+        self.lib.orq_top2(*args, n, _ptr(org), _ptr(dir), _ptr(tmax),
+                          _ptr(t1), _ptr(t2), _ptr(p1), _ptr(p2))
+        return t1, t2, p1, p2
+
+    def sah_cost(self, tree: Tree) -> float:
+        b, c, ch, *_ = tree.arrays()
+        return float(self.lib.orq_sah_cost(_ptr(b), _ptr(c), _ptr(ch)))
+
+    def camera_basis(self, cam) -> np.ndarray:
+        e = np.asarray(cam.eye, np.float32)
+        la = np.asarray(cam.lookat, np.float32)
+        up = np.asarray(cam.up, np.float32)
+        out = np.zeros(12, np.float32)
+        self.lib.orq_camera_basis(_ptr(e), _ptr(la), _ptr(up), cam.hfov, cam.vfov, _ptr(out))
+        return out
+
+    def primary_rays(self, basis, xres, yres):
+        n = xres * yres
+        org = np.zeros((3, n), np.float32)
+        dir = np.zeros((3, n), np.float32)
+        b = np.ascontiguousarray(basis, np.float32)
+        self.lib.orq_primary_rays(_ptr(b), xres, yres, _ptr(org), _ptr(dir))
+        return org, dir
+
+    def render_whitted(self, tree, scene, tri_kind=0, wald=None, rows=None):
+        mesh = scene.mesh
+        keep, args = self._scene_args(tree, mesh, tri_kind, wald)
+        basis = self.camera_basis(scene.camera)
+        xres, yres = scene.xres, scene.yres
+        y0, y1 = rows if rows else (0, yres)
+        lights = np.array([list(l.position) + list(l.color) for l in scene.lights], np.float32)
+        amb = np.asarray(scene.ambient, np.float32)
+        bg = np.asarray(scene.background, np.float32)
+        fm = np.ascontiguousarray(mesh.face_material, np.uint32)
+        mats = np.ascontiguousarray(mesh.materials, np.float32)
+        npx = xres * yres
+        rgb = np.zeros((npx, 3), np.float32)
+        tp = np.zeros(npx, np.float32)
+        pr = np.full(npx, -1, np.int32)
+        lit = np.zeros(npx, np.int32)
+        ns = self.lib.orq_render_whitted(*args, _ptr(fm), _ptr(mats), _ptr(basis), xres, yres,
+                                         _ptr(lights), len(scene.lights), _ptr(amb), _ptr(bg),
+                                         y0, y1, _ptr(rgb), _ptr(tp), _ptr(pr), _ptr(lit))
+        return dict(rgb=rgb, t=tp, prim=pr, lit=lit, shadow_rays=int(ns))
+
+
+class Reference:
+    """The reference's own classes (oracle/_ref), through ref_harness.cc."""
+
+    def __init__(self, sse: bool = False):
+        path = REF_SSE_SO if sse else REF_SO
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.mref_scene_create.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                        C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.mref_scene_create.restype = C.c_void_p
+        L.mref_scene_destroy.argtypes = [C.c_void_p]
+        L.mref_tree_count.argtypes = [C.c_void_p] * 4
+        L.mref_tree_export.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 6
+        L.mref_tree_save.argtypes = [C.c_void_p, C.c_char_p]
+        L.mref_tree_cost.argtypes = [C.c_void_p]
+        L.mref_tree_cost.restype = C.c_double
+        L.mref_intersect.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
+                                     [C.c_int, C.c_int] + [C.c_void_p] * 5)
+        L.mref_camera_basis.argtypes = [C.c_void_p] * 3 + [C.c_float, C.c_float, C.c_void_p]
+        L.mref_render.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] +
+                                  [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 5)
+        L.mref_node_size.restype = C.c_int
+
+    @staticmethod
+    def available(sse: bool = False) -> bool:
+        return os.path.exists(REF_SSE_SO if sse else REF_SO)
+
+    def scene(self, mesh, tri_kind=0) -> "RefScene":
+        return RefScene(self, mesh, tri_kind)
+
+    def camera_basis(self, cam) -> np.ndarray:
+        e = np.asarray(cam.eye, np.float32)
+        la = np.asarray(cam.lookat, np.float32)
+        up = np.asarray(cam.up, np.float32)
+        out = np.zeros(12, np.float32)
+        self.lib.mref_camera_basis(_ptr(e), _ptr(la), _ptr(up), cam.hfov, cam.vfov, _ptr(out))
+        return out
+
+
+class RefScene:
+    def __init__(self, ref: Reference, mesh, tri_kind=0):
+        self.ref = ref
+        self.mesh = mesh
+        v = np.ascontiguousarray(mesh.vertices, np.float32)
+        ix = np.ascontiguousarray(mesh.indices, np.uint32)
+        fm = np.ascontiguousarray(mesh.face_material, np.uint32)
+        mats = np.ascontiguousarray(mesh.materials, np.float32)
+        self._keep = (v, ix, fm, mats)
+        self.h = ref.lib.mref_scene_create(_ptr(v), v.shape[0], _ptr(ix), mesh.n_tris,
+                                           _ptr(fm), _ptr(mats), mats.shape[0], tri_kind)
+        if not self.h:
+            raise RuntimeError("reference scene build failed")
+
+    def close(self):
+        if self.h:
+            self.ref.lib.mref_scene_destroy(self.h)
+            self.h = None
+
+    def tree(self) -> Tree:
+        used, alloc, nids = C.c_int(), C.c_int(), C.c_int()
+        self.ref.lib.mref_tree_count(self.h, C.byref(used), C.byref(alloc), C.byref(nids))
+        n = used.value
+        b = np.zeros((n, 6), np.float32)
+        c = np.zeros(n, np.int32)
+        ch = np.zeros(n, np.int32)
+        ax = np.zeros(n, np.uint8)
+        lc = np.zeros(n, np.uint8)
+        ids = np.zeros(nids.value, np.int32)
+        self.ref.lib.mref_tree_export(self.h, n, _ptr(b), _ptr(c), _ptr(ch), _ptr(ax),
+                                      _ptr(lc), _ptr(ids))
+        return Tree(b, c, ch, ax, lc, ids)
+
+    def save_blob(self, path: str):
+        if self.ref.lib.mref_tree_save(self.h, path.encode()) != 0:
+            raise RuntimeError("saveToFile failed")
+
+    def sah_cost(self) -> float:
+        return float(self.ref.lib.mref_tree_cost(self.h))
+
+    def intersect(self, org, dir, tmax, anyhit=False, packet=64):
+        n = int(tmax.shape[0])
+        org = np.ascontiguousarray(org, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        hit = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        self.ref.lib.mref_intersect(self.h, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
+                                    packet, _ptr(hit), _ptr(t), _ptr(prim), _ptr(u), _ptr(v))
+        return dict(hit=hit, t=t, prim=prim, u=u, v=v)
+
+    def render(self, scene, nthreads=1, want_ids=True):
+        cam = scene.camera
+        args = np.array(list(cam.eye) + list(cam.lookat) + list(cam.up) +
+                        [cam.hfov, cam.vfov, 0.0], np.float32)
+        lights = np.array([list(l.position) + list(l.color) for l in scene.lights], np.float32)
+        amb = np.asarray(scene.ambient, np.float32)
+        bg = np.asarray(scene.background, np.float32)
+        npx = scene.xres * scene.yres
+        rgb = np.zeros((npx, 3), np.float32)
+        tp = np.zeros(npx, np.float32) if want_ids else None
+        pr = np.zeros(npx, np.int32) if want_ids else None
+        secs = C.c_double()
+        nsr = C.c_longlong()
+        self.ref.lib.mref_render(self.h, scene.xres, scene.yres, _ptr(args), _ptr(lights),
+                                 len(scene.lights), _ptr(amb), _ptr(bg), nthreads, _ptr(rgb),
+                                 _ptr(tp), _ptr(pr), C.byref(secs), C.byref(nsr))
+        return dict(rgb=rgb, t=tp, prim=pr, seconds=secs.value, shadow_rays=nsr.value)

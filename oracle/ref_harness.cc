@@ -1,0 +1,438 @@
+// Test infrastructure, not product code.
+//
+// Harness that drives the reference's own classes (compiled from the
+// reference sources by oracle/ref.mk) through a small extern "C" surface so
+// the Python tests and the CPU-baseline leg of bench.py can call them with
+// plain arrays.  Nothing here restates an algorithm: every result comes out
+// of the reference's code path.
+//
+//   scene      Mesh (Model/Groups/Mesh.h:27-102) of WaldTriangle
+//              (Model/Primitives/WaldTriangle.cc:13-126) or
+//              KenslerShirleyTriangle primitives, one Lambertian
+//              (Model/Materials/Lambertian.cc) per material id, under a
+//              DynBVH (Model/Groups/DynBVH.cc:1699 rebuild).
+//   intersect  DynBVH::intersect (DynBVH.cc:101-272) over 64-ray packets
+//              (Interface/RayPacket.h:58-130), closest hit or AnyHit.
+//   render     Raytracer::traceEyeRays (Engine/Renderers/Raytracer.cc:41-97)
+//              with PinholeCamera(-normalizeRays), Lambertian, HardShadows
+//              (Engine/Shadows/HardShadows.cc:46), PointLight,
+//              ConstantAmbient and ConstantBackground, on N pthreads that
+//              take image rows from an atomic counter (the role of
+//              Core/Thread/WorkQueue.cc:61-69 in the reference's frame loop).
+//
+// Compiled as C++98 (the reference's dialect).
+
+#include <Core/Color/Color.h>
+#include <Core/Exceptions/Exception.h>
+#include <Core/Color/RGBColor.h>
+#include <Core/Geometry/BBox.h>
+#include <Core/Geometry/Vector.h>
+#include <Engine/Renderers/Raytracer.h>
+#include <Engine/SampleGenerators/ConstantSampleGenerator.h>
+#include <Engine/Shadows/HardShadows.h>
+#include <Interface/Context.h>
+#include <Interface/LightSet.h>
+#include <Interface/RayPacket.h>
+#include <Interface/Scene.h>
+#include <Model/AmbientLights/ConstantAmbient.h>
+#include <Model/Backgrounds/ConstantBackground.h>
+#include <Model/Cameras/PinholeCamera.h>
+#include <Model/Groups/DynBVH.h>
+#include <Model/Groups/Mesh.h>
+#include <Model/Lights/PointLight.h>
+#include <Model/Materials/Lambertian.h>
+#include <Model/Primitives/KenslerShirleyTriangle.h>
+#include <Model/Primitives/MeshTriangle.h>
+#include <Model/Primitives/WaldTriangle.h>
+
+#include <pthread.h>
+#include <stdio.h>
+#include <string.h>
+#include <sys/time.h>
+#include <string>
+#include <vector>
+
+using namespace Manta;
+
+namespace {
+
+// Exposes the protected tree arrays and the SAH cost routine of the
+// reference DynBVH (DynBVH.h:88-89, DynBVH.cc:3389-3416).
+class ExposedBVH : public DynBVH {
+public:
+  ExposedBVH() : DynBVH(false) {}
+  const std::vector<BVHNode>& treeNodes() const { return nodes; }
+  const std::vector<int>& treeIds() const { return object_ids; }
+  float sahCost() { return computeCost<true>(0); }
+};
+
+// Reads MeshTriangle::myID (protected, Model/Primitives/MeshTriangle.h:63).
+class TriId : public MeshTriangle {
+public:
+  static unsigned int of(const Primitive* p) {
+    return static_cast<const TriId*>(static_cast<const MeshTriangle*>(p))->myID;
+  }
+};
+
+// Exposes the camera basis set up by PinholeCamera::setup
+// (Model/Cameras/PinholeCamera.cc:167-198).
+class ExposedCamera : public PinholeCamera {
+public:
+  ExposedCamera(const std::vector<std::string>& args) : PinholeCamera(args) {}
+  void basis(float* out) const {
+    for (int i = 0; i < 3; ++i) {
+      out[0 + i] = eye[i];
+      out[3 + i] = direction[i];
+      out[6 + i] = u[i];
+      out[9 + i] = v[i];
+    }
+  }
+};
+
+// HardShadows that also counts the shadow rays it sends into the scene.
+class CountingShadows : public HardShadows {
+public:
+  CountingShadows() : HardShadows(false) {}
+  long long* counter;  // per-thread slot, set before each use
+  void computeShadows(const RenderContext& context, StateBuffer& state,
+                      const LightSet* lights, RayPacket& source,
+                      RayPacket& shadow) {
+    HardShadows::computeShadows(context, state, lights, source, shadow);
+    for (int i = shadow.begin(); i < shadow.end(); ++i)
+      if (!shadow.rayIsMasked(i)) ++*counter;
+  }
+};
+
+struct RefScene {
+  Mesh* mesh;
+  ExposedBVH* bvh;
+  std::vector<Material*> materials;
+  LightSet* lights;
+  Scene* scene;
+};
+
+double now_s() {
+  struct timeval tv;
+  gettimeofday(&tv, 0);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Builds Mesh + triangles + DynBVH.  tri_kind 0 = WaldTriangle,
+// 1 = KenslerShirleyTriangle.  mat_rgb holds nmat diffuse colours.
+void* mref_scene_create(const float* verts, int nverts, const unsigned* idx,
+                        int ntris, const unsigned* face_mat,
+                        const float* mat_rgb, int nmat, int tri_kind) {
+  try {
+    RefScene* s = new RefScene();
+    s->mesh = new Mesh();
+    Mesh* m = s->mesh;
+    m->vertices.resize(nverts);
+    for (int i = 0; i < nverts; ++i)
+      m->vertices[i] = Vector(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+    m->vertex_indices.assign(idx, idx + 3 * (size_t)ntris);
+    m->face_material.assign(face_mat, face_mat + ntris);
+    for (int k = 0; k < nmat; ++k) {
+      Material* mat = new Lambertian(
+          Color(RGB(mat_rgb[3 * k], mat_rgb[3 * k + 1], mat_rgb[3 * k + 2])));
+      m->materials.push_back(mat);
+      s->materials.push_back(mat);
+    }
+    for (int t = 0; t < ntris; ++t) {
+      if (tri_kind == 0)
+        m->addTriangle(new WaldTriangle(m, t));
+      else
+        m->addTriangle(new KenslerShirleyTriangle(m, t));
+    }
+    s->lights = new LightSet();
+    s->lights->setAmbientLight(new ConstantAmbient(Color(RGB(0, 0, 0))));
+    s->scene = 0;
+    PreprocessContext ctx;
+    ctx.globalLights = s->lights;
+    m->preprocess(ctx);
+    s->bvh = new ExposedBVH();
+    s->bvh->setGroup(m);
+    s->bvh->rebuild(0, 1);
+    return s;
+  } catch (...) {
+    return 0;
+  }
+}
+
+void mref_scene_destroy(void* h) {
+  // The reference never frees scene objects (Scene/Mesh own raw pointers);
+  // only the harness record is released.
+  delete static_cast<RefScene*>(h);
+}
+
+// Number of nodes the builder used (reachable from the root), the size of
+// the node vector saveToFile writes, and the object_ids count.
+int mref_tree_count(void* h, int* nodes_used, int* nodes_alloc, int* nids) {
+  RefScene* s = static_cast<RefScene*>(h);
+  const std::vector<DynBVH::BVHNode>& n = s->bvh->treeNodes();
+  int maxIdx = 0;
+  std::vector<int> stack(1, 0);
+  while (!stack.empty()) {
+    int i = stack.back();
+    stack.pop_back();
+    if (i > maxIdx) maxIdx = i;
+    if (!n[i].isLeaf()) {
+      stack.push_back(n[i].child);
+      stack.push_back(n[i].child + 1);
+    }
+  }
+  *nodes_used = maxIdx + 1;
+  *nodes_alloc = (int)n.size();
+  *nids = (int)s->bvh->treeIds().size();
+  return 0;
+}
+
+// Field-wise export of the first nodes_used nodes plus object_ids.
+int mref_tree_export(void* h, int nodes_used, float* bounds, int* child,
+                     int* children, unsigned char* axis,
+                     unsigned char* left_cheaper, int* ids) {
+  RefScene* s = static_cast<RefScene*>(h);
+  const std::vector<DynBVH::BVHNode>& n = s->bvh->treeNodes();
+  for (int i = 0; i < nodes_used; ++i) {
+    for (int c = 0; c < 3; ++c) {
+      bounds[6 * i + c] = n[i].bounds[0][c];
+      bounds[6 * i + 3 + c] = n[i].bounds[1][c];
+    }
+    child[i] = n[i].child;
+    children[i] = n[i].children;
+    axis[i] = n[i].axis;
+    left_cheaper[i] = n[i].isLeftCheaper;
+  }
+  const std::vector<int>& o = s->bvh->treeIds();
+  for (size_t i = 0; i < o.size(); ++i) ids[i] = o[i];
+  return 0;
+}
+
+// DynBVH::saveToFile (DynBVH.cc:2479-2501) byte stream.
+int mref_tree_save(void* h, const char* path) {
+  RefScene* s = static_cast<RefScene*>(h);
+  return s->bvh->saveToFile(std::string(path)) ? 0 : 1;
+}
+
+// sizeof(DynBVH::BVHNode) as compiled here (the saveToFile record size).
+int mref_node_size() { return (int)sizeof(DynBVH::BVHNode); }
+
+double mref_tree_cost(void* h) {
+  return static_cast<RefScene*>(h)->bvh->sahCost();
+}
+
+// DynBVH::intersect over packets of `packet` consecutive rays.  org/dir are
+// SoA ([x0..xn-1, y0.., z0..]).  Per ray: hit flag, t, triangle id, scratch
+// u/v (WaldTriangle lambda/mue, KS uoverd/voverd).  anyhit sets
+// RayPacket::AnyHit (HardShadows.cc:79).
+int mref_intersect(void* h, int n, const float* org, const float* dir,
+                   const float* tmax, int anyhit, int packet, int* hit,
+                   float* t, int* prim, float* u, float* v) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (packet < 1 || packet > RayPacket::MaxSize) packet = RayPacket::MaxSize;
+  RenderContext ctx(0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+  for (int base = 0; base < n; base += packet) {
+    int cnt = n - base < packet ? n - base : packet;
+    RayPacketData data;
+    RayPacket rays(data, RayPacket::UnknownShape, 0, cnt, 0,
+                   anyhit ? RayPacket::AnyHit : 0);
+    for (int i = 0; i < cnt; ++i) {
+      int r = base + i;
+      rays.setRay(i, Vector(org[r], org[n + r], org[2 * n + r]),
+                  Vector(dir[r], dir[n + r], dir[2 * n + r]));
+      rays.resetHit(i, tmax[r]);
+    }
+    s->bvh->intersect(ctx, rays);
+    for (int i = 0; i < cnt; ++i) {
+      int r = base + i;
+      hit[r] = rays.wasHit(i) ? 1 : 0;
+      t[r] = rays.getMinT(i);
+      if (hit[r]) {
+        prim[r] = (int)TriId::of(rays.getHitPrimitive(i));
+        u[r] = rays.getScratchpad<Real>(WaldTriangle::SCRATCH_U)[i];
+        v[r] = rays.getScratchpad<Real>(WaldTriangle::SCRATCH_V)[i];
+      } else {
+        prim[r] = -1;
+        u[r] = 0.f;
+        v[r] = 0.f;
+      }
+    }
+  }
+  return 0;
+}
+
+// Camera basis (eye, lookat-eye, u, v) of PinholeCamera with the given
+// eye/lookat/up/hfov/vfov and -normalizeRays.
+int mref_camera_basis(const float* eye, const float* lookat, const float* up,
+                      float hfov, float vfov, float* out12) {
+  char buf[16][32];
+  std::vector<std::string> args;
+  args.push_back("-eye");
+  for (int i = 0; i < 3; ++i) { snprintf(buf[i], 32, "%.9g", eye[i]); args.push_back(buf[i]); }
+  args.push_back("-lookat");
+  for (int i = 0; i < 3; ++i) { snprintf(buf[3 + i], 32, "%.9g", lookat[i]); args.push_back(buf[3 + i]); }
+  args.push_back("-up");
+  for (int i = 0; i < 3; ++i) { snprintf(buf[6 + i], 32, "%.9g", up[i]); args.push_back(buf[6 + i]); }
+  args.push_back("-hfov"); snprintf(buf[9], 32, "%.9g", hfov); args.push_back(buf[9]);
+  args.push_back("-vfov"); snprintf(buf[10], 32, "%.9g", vfov); args.push_back(buf[10]);
+  args.push_back("-normalizeRays");
+  try {
+    ExposedCamera cam(args);
+    cam.basis(out12);
+  } catch (Exception& e) {
+    fprintf(stderr, "mref_camera_basis: %s\n", e.message());
+    return 1;
+  } catch (...) {
+    return 1;
+  }
+  return 0;
+}
+
+struct RenderJob {
+  RefScene* s;
+  Raytracer* renderer;
+  CountingShadows* shadows;
+  ExposedCamera* camera;
+  ConstantSampleGenerator* sampler;
+  int xres, yres;
+  float xscale, yscale, xoffset, yoffset;
+  float* rgb;
+  float* tprim;
+  int* prim;
+  volatile int next_row;
+  pthread_mutex_t lock;
+  long long shadow_rays[256];
+  int nthreads;
+};
+
+struct RenderArg {
+  RenderJob* job;
+  int proc;
+};
+
+static void* render_worker(void* p) {
+  RenderArg* a = static_cast<RenderArg*>(p);
+  RenderJob* j = a->job;
+  CountingShadows shadows;  // per-thread (it carries the counter slot)
+  shadows.counter = &j->shadow_rays[a->proc];
+  RenderContext ctx(0, 0, a->proc, j->nthreads, 0, 0, 0, j->renderer, &shadows,
+                    j->camera, j->s->scene, 0, 0, j->sampler);
+  for (;;) {
+    pthread_mutex_lock(&j->lock);
+    int y = j->next_row++;
+    pthread_mutex_unlock(&j->lock);
+    if (y >= j->yres) break;
+    for (int x0 = 0; x0 < j->xres; x0 += RayPacket::MaxSize) {
+      int cnt = j->xres - x0 < RayPacket::MaxSize ? j->xres - x0 : (int)RayPacket::MaxSize;
+      RayPacketData data;
+      RayPacket rays(data, RayPacket::UnknownShape, 0, cnt, 0,
+                     RayPacket::HaveImageCoordinates | RayPacket::ConstantEye);
+      for (int i = 0; i < cnt; ++i) {
+        // Image coordinates per pixel in closed form (SingleSampler.cc:38-41
+        // scale/offset); the reference's frame loop accumulates px instead.
+        Real px = (Real)(x0 + i) * j->xscale + j->xoffset;
+        Real py = (Real)y * j->yscale + j->yoffset;
+        rays.setPixel(i, 0, px, py);
+      }
+      j->renderer->traceEyeRays(ctx, rays);
+      for (int i = 0; i < cnt; ++i) {
+        size_t pix = (size_t)y * j->xres + x0 + i;
+        Color c = rays.getColor(i);
+        j->rgb[3 * pix + 0] = c[0];
+        j->rgb[3 * pix + 1] = c[1];
+        j->rgb[3 * pix + 2] = c[2];
+        if (j->prim) {
+          bool h = rays.wasHit(i);
+          j->prim[pix] = h ? (int)TriId::of(rays.getHitPrimitive(i)) : -1;
+          j->tprim[pix] = rays.getMinT(i);
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+// Whitted frame through Raytracer::traceEyeRays.  lights: nlights x
+// (px,py,pz, r,g,b).  ambient/background: RGB.  Returns wall seconds of the
+// frame loop in *seconds and the shadow-ray count in *shadow_rays.
+int mref_render(void* h, int xres, int yres, const float* cam12_args,
+                const float* lights, int nlights, const float* ambient,
+                const float* background, int nthreads, float* rgb,
+                float* tprim, int* prim, double* seconds,
+                long long* shadow_rays) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  // cam12_args: eye[3], lookat[3], up[3], hfov, vfov, unused
+  char buf[16][32];
+  std::vector<std::string> args;
+  const char* names[3] = {"-eye", "-lookat", "-up"};
+  for (int k = 0; k < 3; ++k) {
+    args.push_back(names[k]);
+    for (int i = 0; i < 3; ++i) {
+      snprintf(buf[3 * k + i], 32, "%.9g", cam12_args[3 * k + i]);
+      args.push_back(buf[3 * k + i]);
+    }
+  }
+  args.push_back("-hfov"); snprintf(buf[9], 32, "%.9g", cam12_args[9]); args.push_back(buf[9]);
+  args.push_back("-vfov"); snprintf(buf[10], 32, "%.9g", cam12_args[10]); args.push_back(buf[10]);
+  args.push_back("-normalizeRays");
+  ExposedCamera camera(args);
+
+  LightSet* ls = new LightSet();
+  ls->setAmbientLight(new ConstantAmbient(Color(RGB(ambient[0], ambient[1], ambient[2]))));
+  for (int k = 0; k < nlights; ++k) {
+    const float* L = lights + 6 * k;
+    ls->add(new PointLight(Vector(L[0], L[1], L[2]), Color(RGB(L[3], L[4], L[5]))));
+  }
+  PreprocessContext pctx;
+  pctx.globalLights = ls;
+  for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
+  if (!s->scene) s->scene = new Scene();
+  s->scene->setObject(s->bvh);
+  s->scene->setBackground(new ConstantBackground(
+      Color(RGB(background[0], background[1], background[2]))));
+  s->scene->setLights(ls);
+
+  Raytracer renderer;
+  ConstantSampleGenerator sampler(0.f);
+  RenderJob job;
+  job.s = s;
+  job.renderer = &renderer;
+  job.camera = &camera;
+  job.sampler = &sampler;
+  job.xres = xres;
+  job.yres = yres;
+  job.xscale = (Real)2 / xres;
+  job.yscale = (Real)2 / yres;
+  job.xoffset = (-xres / (Real)2 + (Real)0.5) * job.xscale;
+  job.yoffset = (-yres / (Real)2 + (Real)0.5) * job.yscale;
+  job.rgb = rgb;
+  job.tprim = tprim;
+  job.prim = prim;
+  job.next_row = 0;
+  job.nthreads = nthreads;
+  memset(job.shadow_rays, 0, sizeof(job.shadow_rays));
+  pthread_mutex_init(&job.lock, 0);
+  std::vector<pthread_t> th(nthreads);
+  std::vector<RenderArg> ar(nthreads);
+  double t0 = now_s();
+  for (int p = 0; p < nthreads; ++p) {
+    ar[p].job = &job;
+    ar[p].proc = p;
+    pthread_create(&th[p], 0, render_worker, &ar[p]);
+  }
+  for (int p = 0; p < nthreads; ++p) pthread_join(th[p], 0);
+  double t1 = now_s();
+  pthread_mutex_destroy(&job.lock);
+  long long total = 0;
+  for (int p = 0; p < nthreads; ++p) total += job.shadow_rays[p];
+  if (seconds) *seconds = t1 - t0;
+  if (shadow_rays) *shadow_rays = total;
+  return 0;
+}
+
+}  // extern "C"

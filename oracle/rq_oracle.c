@@ -1,0 +1,589 @@
+/*
+ * Test infrastructure, not product code: the CPU restatement ("oracle") of
+ * Manta's ray-query hot path, used only by tests/, the smoke check and the
+ * CPU-baseline leg of bench.py to check the device path.
+ *
+ * It restates, one ray at a time and in the reference's float operation
+ * order (x86-64 SSE scalar float, no FMA contraction: compile with
+ * -ffp-contract=off), what the reference computes:
+ *
+ *   orq_wald_setup    WaldTriangle::setPoints
+ *                     (Model/Primitives/WaldTriangle.cc:64-126)
+ *   box test          DynBVH::firstIntersects scalar branch
+ *                     (Model/Groups/DynBVH.cc:657-681)
+ *   traversal order   DynBVH::intersectNode (DynBVH.cc:274-404): closest
+ *                     hit visits child (dir[axis] > 0 ? 0 : 1) first, AnyHit
+ *                     visits (isLeftCheaper ? 0 : 1) first
+ *   Wald test         WaldTriangle::intersect scalar (WaldTriangle.cc:489-555)
+ *   KS test           KenslerShirleyTriangle::intersect scalar
+ *                     (Model/Primitives/KenslerShirleyTriangle.cc:336-378)
+ *   hit acceptance    RayPacket::hit (Interface/RayPacket.h:531-543)
+ *   SAH tree cost     DynBVH::computeCost (DynBVH.cc:3389-3416) with
+ *                     BBox::computeArea (Core/Geometry/BBox.h:117-121)
+ *   camera            PinholeCamera::setup / makeRaysSpecialized scalar
+ *                     (Model/Cameras/PinholeCamera.cc:167-198, 356-366) and
+ *                     the SingleSampler pixel scale/offset
+ *                     (Engine/PixelSamplers/SingleSampler.cc:38-41)
+ *   shading           Raytracer::traceRays (Engine/Renderers/Raytracer.cc:49-97),
+ *                     Lambertian::shade (Model/Materials/Lambertian.cc:63-246,
+ *                     scalar branches), HardShadows::computeShadows
+ *                     (Engine/Shadows/HardShadows.cc:46-360, scalar branch),
+ *                     PointLight::computeLight (Model/Lights/PointLight.cc:31-79),
+ *                     RayPacket normalizeDirections / computeHitPositions /
+ *                     computeFFNormals / computeFFGeometricNormals
+ *                     (Interface/RayPacket.cc:8-79, 114-146, 205-310).
+ *
+ * A packet traversal and this per-ray traversal test the same (ray, box) and
+ * (ray, triangle) pairs with the same float operations; they can disagree
+ * only where two candidate hits tie (which one the traversal order meets
+ * first) or where rounding puts a hit within an ulp of a box face.
+ * orq_top2 reports the two nearest candidate distances so such rays can be
+ * identified.
+ *
+ * Tree format: the reference DynBVH node array, field by field (DynBVH.h:37-79):
+ * bounds[6*i] = min xyz, max xyz; child; children (leaf iff != 0); axis;
+ * isLeftCheaper; plus object_ids.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define T_EPSILON 1.e-4f
+#define MAXT 1.e19f
+
+typedef struct {
+  const float* bounds;
+  const int* child;
+  const int* children;
+  const unsigned char* axis;
+  const unsigned char* left_cheaper;
+  const int* ids;
+  int tri_kind; /* 0 Wald, 1 Kensler-Shirley */
+  const float* verts;
+  const unsigned* idx;
+  const float* wald; /* 12 floats per triangle, see orq_wald_setup */
+} Tree;
+
+typedef struct {
+  float o[3], d[3], inv[3];
+  float minT;
+  int hit;  /* reference: hitMatl != 0 */
+  int prim;
+  float u, v;
+  long node_tests, tri_tests;
+  int anyhit;
+} Ray;
+
+/* ---------------------------------------------------------------- Wald --- */
+
+static float f_abs(float x) { return x < 0.f ? -x : x; }
+
+/* WaldTriangle::setPoints (WaldTriangle.cc:64-126).  Record layout:
+ * [n_u, n_v, n_d, k(bits), b_nu, b_nv, b_d, n_k, c_nu, c_nv, c_d, 0]. */
+void orq_wald_setup(const float* verts, const unsigned* idx, int ntris,
+                    float* rec) {
+  for (int t = 0; t < ntris; ++t) {
+    const float* p1 = verts + 3 * idx[3 * t + 0];
+    const float* p2 = verts + 3 * idx[3 * t + 1];
+    const float* p3 = verts + 3 * idx[3 * t + 2];
+    float e1[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+    float e2[3] = {p3[0] - p1[0], p3[1] - p1[1], p3[2] - p1[2]};
+    float nrm[3] = {e1[1] * e2[2] - e1[2] * e2[1],
+                    e1[2] * e2[0] - e1[0] * e2[2],
+                    e1[0] * e2[1] - e1[1] * e2[0]};
+    /* Vector::normalize (Core/Geometry/Vector.h:322-331) */
+    float l = sqrtf(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+    float scale = 1 / l;
+    nrm[0] *= scale;
+    nrm[1] *= scale;
+    nrm[2] *= scale;
+    unsigned n = 0, u, v;
+    if (f_abs(nrm[1]) > f_abs(nrm[n])) n = 1;
+    if (f_abs(nrm[2]) > f_abs(nrm[n])) n = 2;
+    switch (n) {
+      case 0: u = 1; v = 2; break;
+      case 1: u = 2; v = 0; break;
+      default: u = 0; v = 1; break;
+    }
+    unsigned k = n;
+    float inv_normalk = 1 / nrm[k];
+    float n_u = nrm[u] * inv_normalk;
+    float n_v = nrm[v] * inv_normalk;
+    float n_d = p1[u] * n_u + p1[v] * n_v + p1[k];
+    float s;
+    float c_nu = +p2[v] - p1[v];
+    float c_nv = -p2[u] + p1[u];
+    float c_d = -(p1[u] * c_nu + p1[v] * c_nv);
+    s = 1.f / (p3[u] * c_nu + p3[v] * c_nv + c_d);
+    c_nu *= s;
+    c_nv *= s;
+    c_d *= s;
+    float b_nu = +p3[v] - p1[v];
+    float b_nv = -p3[u] + p1[u];
+    float b_d = -(p1[u] * b_nu + p1[v] * b_nv);
+    s = 1.f / (p2[u] * b_nu + p2[v] * b_nv + b_d);
+    b_nu *= s;
+    b_nv *= s;
+    b_d *= s;
+    float* r = rec + 12 * (size_t)t;
+    r[0] = n_u;
+    r[1] = n_v;
+    r[2] = n_d;
+    memcpy(&r[3], &k, 4);
+    r[4] = b_nu;
+    r[5] = b_nv;
+    r[6] = b_d;
+    r[7] = nrm[k];
+    r[8] = c_nu;
+    r[9] = c_nv;
+    r[10] = c_d;
+    r[11] = 0.f;
+  }
+}
+
+/* RayPacket::hit (RayPacket.h:531-543). */
+static int ray_hit(Ray* r, float t, int prim) {
+  if (t > T_EPSILON && t < r->minT) {
+    r->minT = t;
+    r->hit = 1;
+    r->prim = prim;
+    return 1;
+  }
+  return 0;
+}
+
+/* WaldTriangle::intersect scalar (WaldTriangle.cc:489-555), one ray. */
+static void wald_test(const Tree* T, int tri, Ray* r) {
+  const float* w = T->wald + 12 * (size_t)tri;
+  unsigned k;
+  memcpy(&k, &w[3], 4);
+  const int axis = (int)k;
+  const int ku = (k == 2) ? 0 : (int)k + 1;
+  const int kv = (k == 0) ? 2 : (int)k - 1;
+  const float n_u = w[0], n_v = w[1], n_d = w[2];
+  const float nd0 = n_u * r->d[ku] + n_v * r->d[kv] + r->d[axis];
+  const float nd = 1.f / nd0;
+  const float org_k = r->o[axis], org_ku = r->o[ku], org_kv = r->o[kv];
+  const float f0 = n_d - (org_k + n_u * org_ku + n_v * org_kv);
+  const float f = f0 * nd;
+  if (f < T_EPSILON || f > r->minT) return;
+  const float hu = org_ku + f * r->d[ku];
+  const float hv = org_kv + f * r->d[kv];
+  const float lambda = w[6] + hu * w[4] + hv * w[5];
+  if (lambda < 0.f) return;
+  const float mue = w[10] + hu * w[8] + hv * w[9];
+  if (mue < 0.f || mue + lambda > 1.f) return;
+  if (ray_hit(r, f, tri)) {
+    r->u = lambda;
+    r->v = mue;
+  }
+}
+
+/* KenslerShirleyTriangle::intersect scalar (KenslerShirleyTriangle.cc:336-378). */
+static void ks_test(const Tree* T, int tri, Ray* r) {
+  const float* p0 = T->verts + 3 * T->idx[3 * tri + 0];
+  const float* p1 = T->verts + 3 * T->idx[3 * tri + 1];
+  const float* p2 = T->verts + 3 * T->idx[3 * tri + 2];
+  const float e0[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+  const float e1[3] = {p0[0] - p2[0], p0[1] - p2[1], p0[2] - p2[2]};
+  const float n[3] = {e0[1] * e1[2] - e0[2] * e1[1],
+                      e0[2] * e1[0] - e0[0] * e1[2],
+                      e0[0] * e1[1] - e0[1] * e1[0]};
+  const float oldt = r->minT;
+  const float rcp = 1.0f / (n[0] * r->d[0] + n[1] * r->d[1] + n[2] * r->d[2]);
+  const float e2[3] = {p0[0] - r->o[0], p0[1] - r->o[1], p0[2] - r->o[2]};
+  const float toverd = (n[0] * e2[0] + n[1] * e2[1] + n[2] * e2[2]) * rcp;
+  if (toverd > oldt - T_EPSILON || toverd < T_EPSILON) return;
+  const float im[3] = {e2[1] * r->d[2] - e2[2] * r->d[1],
+                       e2[2] * r->d[0] - e2[0] * r->d[2],
+                       e2[0] * r->d[1] - e2[1] * r->d[0]};
+  const float uoverd = (im[0] * e1[0] + im[1] * e1[1] + im[2] * e1[2]) * rcp;
+  if (uoverd < 0.0f) return;
+  const float voverd = (im[0] * e0[0] + im[1] * e0[1] + im[2] * e0[2]) * rcp;
+  if (uoverd + voverd > 1.0f || voverd < 0.0f) return;
+  if (ray_hit(r, toverd, tri)) {
+    r->u = uoverd;
+    r->v = voverd;
+  }
+}
+
+/* DynBVH::firstIntersects scalar box test (DynBVH.cc:666-681). */
+static int box_test(const float* b, const Ray* r) {
+  float tmin = T_EPSILON;
+  float tmax = r->minT;
+  for (int c = 0; c < 3; c++) {
+    float t0 = (b[c] - r->o[c]) * r->inv[c];
+    float t1 = (b[3 + c] - r->o[c]) * r->inv[c];
+    float near = (t0 < t1) ? t0 : t1;
+    float far = (t0 < t1) ? t1 : t0;
+    tmin = (tmin < near) ? near : tmin;
+    tmax = (far < tmax) ? far : tmax;
+  }
+  return tmin <= tmax;
+}
+
+/* DynBVH::intersectNode (DynBVH.cc:274-404) for one ray. */
+static void visit(const Tree* T, int node, Ray* r) {
+  if (r->anyhit && r->hit) return; /* firstIntersects skips hit rays */
+  r->node_tests++;
+  if (!box_test(T->bounds + 6 * (size_t)node, r)) return;
+  const int nch = T->children[node];
+  const int first = T->child[node];
+  if (nch != 0) {
+    for (int i = 0; i < nch; ++i) {
+      const int obj = T->ids[first + i];
+      r->tri_tests++;
+      if (T->tri_kind == 0)
+        wald_test(T, obj, r);
+      else
+        ks_test(T, obj, r);
+      if (r->anyhit && r->hit) {
+        /* OpaqueShadower terminates the ray (DynBVH.cc:331-349) */
+        r->minT = T_EPSILON;
+        return;
+      }
+    }
+    return;
+  }
+  int front;
+  if (r->anyhit)
+    front = T->left_cheaper[node] ? 0 : 1;
+  else
+    front = r->d[T->axis[node]] > 0 ? 0 : 1;
+  visit(T, first + front, r);
+  visit(T, first + 1 - front, r);
+}
+
+static void ray_init(Ray* r, const float* org, const float* dir, int n, int i,
+                     float tmax, int anyhit) {
+  for (int c = 0; c < 3; ++c) {
+    r->o[c] = org[c * n + i];
+    r->d[c] = dir[c * n + i];
+    /* RayPacket::actualComputeInverseDirections (RayPacket.cc:106-110) */
+    r->inv[c] = (float)1 / r->d[c];
+  }
+  r->minT = tmax;
+  r->hit = 0;
+  r->prim = -1;
+  r->u = r->v = 0.f;
+  r->node_tests = r->tri_tests = 0;
+  r->anyhit = anyhit;
+}
+
+/* Closest-hit / any-hit query of n rays (SoA org/dir).  Outputs hit flag,
+ * t (minT after the query), triangle id, u, v; optional per-ray node and
+ * triangle test counts. */
+int orq_trace(const float* bounds, const int* child, const int* children,
+              const unsigned char* axis, const unsigned char* left_cheaper,
+              const int* ids, int tri_kind, const float* verts,
+              const unsigned* idx, const float* wald, int n, const float* org,
+              const float* dir, const float* tmax, int anyhit, int* hit,
+              float* t, int* prim, float* u, float* v, int* node_tests,
+              int* tri_tests) {
+  Tree T = {bounds, child, children, axis, left_cheaper, ids,
+            tri_kind, verts, idx, wald};
+  for (int i = 0; i < n; ++i) {
+    Ray r;
+    ray_init(&r, org, dir, n, i, tmax[i], anyhit);
+    visit(&T, 0, &r);
+    hit[i] = r.hit;
+    t[i] = r.minT;
+    prim[i] = r.hit ? r.prim : -1;
+    u[i] = r.u;
+    v[i] = r.v;
+    if (node_tests) node_tests[i] = (int)r.node_tests;
+    if (tri_tests) tri_tests[i] = (int)r.tri_tests;
+  }
+  return 0;
+}
+
+/* -------------------------------------------------- near-tie detection --- */
+
+typedef struct {
+  float t1, t2;
+  int p1, p2;
+} Top2;
+
+static void top2_visit(const Tree* T, int node, Ray* r, Top2* k) {
+  /* cull against the second-nearest candidate */
+  r->minT = k->t2;
+  if (!box_test(T->bounds + 6 * (size_t)node, r)) return;
+  const int nch = T->children[node];
+  const int first = T->child[node];
+  if (nch != 0) {
+    for (int i = 0; i < nch; ++i) {
+      const int obj = T->ids[first + i];
+      r->minT = k->t2;
+      r->hit = 0;
+      if (T->tri_kind == 0)
+        wald_test(T, obj, r);
+      else
+        ks_test(T, obj, r);
+      if (r->hit) {
+        float tt = r->minT;
+        if (tt < k->t1) {
+          k->t2 = k->t1;
+          k->p2 = k->p1;
+          k->t1 = tt;
+          k->p1 = obj;
+        } else {
+          k->t2 = tt;
+          k->p2 = obj;
+        }
+      }
+    }
+    return;
+  }
+  top2_visit(T, first, r, k);
+  top2_visit(T, first + 1, r, k);
+}
+
+/* Nearest and second-nearest candidate hit distance per ray (MAXT/tmax when
+ * absent) over all triangles the ray hits in (T_EPSILON, tmax). */
+int orq_top2(const float* bounds, const int* child, const int* children,
+             const unsigned char* axis, const unsigned char* left_cheaper,
+             const int* ids, int tri_kind, const float* verts,
+             const unsigned* idx, const float* wald, int n, const float* org,
+             const float* dir, const float* tmax, float* t1, float* t2,
+             int* p1, int* p2) {
+  Tree T = {bounds, child, children, axis, left_cheaper, ids,
+            tri_kind, verts, idx, wald};
+  for (int i = 0; i < n; ++i) {
+    Ray r;
+    ray_init(&r, org, dir, n, i, tmax[i], 0);
+    Top2 k = {tmax[i], tmax[i], -1, -1};
+    top2_visit(&T, 0, &r, &k);
+    t1[i] = k.t1;
+    t2[i] = k.t2;
+    p1[i] = k.p1;
+    p2[i] = k.p2;
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------- SAH cost --- */
+
+static float box_area(const float* b) {
+  /* BBox::computeArea: 2 * (dx*dy + dy*dz + dx*dz) in float */
+  float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+  return 2 * (dx * dy + dy * dz + dx * dz);
+}
+
+static float cost_rec(const float* bounds, const int* child,
+                      const int* children, int node) {
+  if (children[node] != 0) return children[node] * 1.f;
+  const int l = child[node], r = child[node] + 1;
+  float lc = cost_rec(bounds, child, children, l);
+  float rc = cost_rec(bounds, child, children, r);
+  float area = box_area(bounds + 6 * (size_t)node);
+  float la = box_area(bounds + 6 * (size_t)l);
+  float ra = box_area(bounds + 6 * (size_t)r);
+  return 1.f + (la * lc + ra * rc) / area;
+}
+
+/* DynBVH::computeCost<>(0) (DynBVH.cc:3389-3416), C_isec = C_trav = 1. */
+double orq_sah_cost(const float* bounds, const int* child, const int* children) {
+  return cost_rec(bounds, child, children, 0);
+}
+
+/* ------------------------------------------------------------ camera --- */
+
+static void v_normalize(float* a) {
+  float l = sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  float s = 1 / l;
+  a[0] *= s;
+  a[1] *= s;
+  a[2] *= s;
+}
+
+static void v_cross(const float* a, const float* b, float* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* PinholeCamera::setup (PinholeCamera.cc:167-198): out = eye, direction, u, v. */
+void orq_camera_basis(const float* eye, const float* lookat, const float* up_in,
+                      float hfov, float vfov, float* out12) {
+  float dir[3] = {lookat[0] - eye[0], lookat[1] - eye[1], lookat[2] - eye[2]};
+  float nearZ = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+  float up[3] = {up_in[0], up_in[1], up_in[2]};
+  v_normalize(up);
+  float v[3], u[3];
+  v_cross(dir, up, v);
+  v_normalize(v);
+  v_cross(v, dir, u);
+  v_normalize(u);
+  const double pi = 3.14159265358979323846;
+  float height = (float)(nearZ * tan((0.5 * vfov) * (pi / 180.)));
+  u[0] *= height;
+  u[1] *= height;
+  u[2] *= height;
+  float width = (float)(nearZ * tan((0.5 * hfov) * (pi / 180.)));
+  v[0] *= width;
+  v[1] *= width;
+  v[2] *= width;
+  for (int i = 0; i < 3; ++i) {
+    out12[i] = eye[i];
+    out12[3 + i] = dir[i];
+    out12[6 + i] = u[i];
+    out12[9 + i] = v[i];
+  }
+}
+
+/* SingleSampler scale/offset + PinholeCamera::makeRaysSpecialized<true,false>
+ * scalar branch: o = eye, d = normalize(v*px + u*py + direction). */
+static void primary_ray(const float* cam, int xres, int yres, int x, int y,
+                        float* o, float* d) {
+  const float xscale = (float)2 / xres;
+  const float yscale = (float)2 / yres;
+  const float xoffset = (-xres / (float)2 + (float)0.5) * xscale;
+  const float yoffset = (-yres / (float)2 + (float)0.5) * yscale;
+  const float px = (float)x * xscale + xoffset;
+  const float py = (float)y * yscale + yoffset;
+  const float* dir = cam + 3;
+  const float* u = cam + 6;
+  const float* v = cam + 9;
+  for (int c = 0; c < 3; ++c) {
+    o[c] = cam[c];
+    d[c] = v[c] * px + u[c] * py + dir[c];
+  }
+  v_normalize(d);
+}
+
+/* Primary rays of an xres x yres frame, SoA. */
+void orq_primary_rays(const float* cam, int xres, int yres, float* org,
+                      float* dir) {
+  const int n = xres * yres;
+  for (int y = 0; y < yres; ++y)
+    for (int x = 0; x < xres; ++x) {
+      float o[3], d[3];
+      primary_ray(cam, xres, yres, x, y, o, d);
+      const int i = y * xres + x;
+      for (int c = 0; c < 3; ++c) {
+        org[c * n + i] = o[c];
+        dir[c * n + i] = d[c];
+      }
+    }
+}
+
+/* Unit geometric normal of triangle `tri`: WaldTriangle::computeNormal
+ * without vertex normals (WaldTriangle.cc:578-590) or the normalised
+ * KenslerShirleyTriangle::computeNormal cross product
+ * (KenslerShirleyTriangle.cc:396-405, normalised by RayPacket.cc:177-186). */
+static void tri_normal(const Tree* T, int tri, float* nrm) {
+  if (T->tri_kind == 0) {
+    const float* w = T->wald + 12 * (size_t)tri;
+    unsigned k;
+    memcpy(&k, &w[3], 4);
+    const int ku = (k == 2) ? 0 : (int)k + 1;
+    const int kv = (k == 0) ? 2 : (int)k - 1;
+    const float n_k = w[7];
+    nrm[k] = n_k;
+    nrm[ku] = n_k * w[0];
+    nrm[kv] = n_k * w[1];
+  } else {
+    const float* p0 = T->verts + 3 * T->idx[3 * tri + 0];
+    const float* p1 = T->verts + 3 * T->idx[3 * tri + 1];
+    const float* p2 = T->verts + 3 * T->idx[3 * tri + 2];
+    const float e0[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    const float e1[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+    v_cross(e0, e1, nrm);
+    float sum = 0;
+    for (int j = 0; j < 3; ++j) sum += nrm[j] * nrm[j];
+    float scale = 1 / sqrtf(sum);
+    for (int j = 0; j < 3; ++j) nrm[j] *= scale;
+  }
+}
+
+/* Whitted frame: Raytracer + Lambertian + HardShadows(point lights).
+ * lights: nl x (pos xyz, rgb).  mat_rgb/face_mat: diffuse colour per
+ * material.  Outputs rgb (3 per pixel), primary t and triangle id, the
+ * number of shadow rays sent, and optional per-pixel occlusion bits
+ * (bit j set = light j unshadowed). */
+long long orq_render_whitted(const float* bounds, const int* child,
+                             const int* children, const unsigned char* axis,
+                             const unsigned char* left_cheaper, const int* ids,
+                             int tri_kind, const float* verts,
+                             const unsigned* idx, const float* wald,
+                             const unsigned* face_mat, const float* mat_rgb,
+                             const float* cam, int xres, int yres,
+                             const float* lights, int nl, const float* ambient,
+                             const float* background, int y0, int y1,
+                             float* rgb, float* tprim, int* prim,
+                             int* lit_bits) {
+  Tree T = {bounds, child, children, axis, left_cheaper, ids,
+            tri_kind, verts, idx, wald};
+  long long shadow_rays = 0;
+  for (int y = y0; y < y1; ++y) {
+    for (int x = 0; x < xres; ++x) {
+      const size_t pix = (size_t)y * xres + x;
+      Ray r;
+      primary_ray(cam, xres, yres, x, y, r.o, r.d);
+      for (int c = 0; c < 3; ++c) r.inv[c] = (float)1 / r.d[c];
+      r.minT = MAXT;
+      r.hit = 0;
+      r.prim = -1;
+      r.u = r.v = 0.f;
+      r.anyhit = 0;
+      r.node_tests = r.tri_tests = 0;
+      visit(&T, 0, &r);
+      tprim[pix] = r.minT;
+      prim[pix] = r.hit ? r.prim : -1;
+      if (lit_bits) lit_bits[pix] = 0;
+      if (!r.hit) {
+        /* ConstantBackground::shade */
+        for (int c = 0; c < 3; ++c) rgb[3 * pix + c] = background[c];
+        continue;
+      }
+      /* Lambertian::shade.  Directions are already unit length
+       * (NormalizedDirections set by the camera), so normalizeDirections is
+       * a no-op here. */
+      const float* kd = mat_rgb + 3 * face_mat[r.prim];
+      float nrm[3];
+      tri_normal(&T, r.prim, nrm);
+      float ffn[3];
+      const float dn = nrm[0] * r.d[0] + nrm[1] * r.d[1] + nrm[2] * r.d[2];
+      for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0) ? nrm[c] : -nrm[c];
+      /* geometric normal == shading normal for both triangle kinds here */
+      const float* ffg = ffn;
+      float total[3] = {ambient[0], ambient[1], ambient[2]};
+      float hp[3];
+      for (int c = 0; c < 3; ++c) hp[c] = r.o[c] + r.d[c] * r.minT;
+      for (int j = 0; j < nl; ++j) {
+        const float* L = lights + 6 * j;
+        float sd[3] = {L[0] - hp[0], L[1] - hp[1], L[2] - hp[2]};
+        if (!(sd[0] * ffg[0] + sd[1] * ffg[1] + sd[2] * ffg[2] > 0))
+          continue; /* masked: counts as shadowed */
+        Ray s;
+        for (int c = 0; c < 3; ++c) {
+          s.o[c] = hp[c];
+          s.d[c] = sd[c];
+          s.inv[c] = (float)1 / sd[c];
+        }
+        s.minT = 1 - T_EPSILON;
+        s.hit = 0;
+        s.prim = -1;
+        s.u = s.v = 0.f;
+        s.anyhit = 1;
+        s.node_tests = s.tri_tests = 0;
+        shadow_rays++;
+        visit(&T, 0, &s);
+        if (s.hit) continue;
+        if (lit_bits) lit_bits[pix] |= 1 << j;
+        /* shadowRays.normalizeDirections (RayPacket.cc:61-71) */
+        float sum = 0;
+        for (int c = 0; c < 3; ++c) sum += sd[c] * sd[c];
+        float length = sqrtf(sum);
+        float scale = 1 / length;
+        for (int c = 0; c < 3; ++c) sd[c] *= scale;
+        const float cos_theta = sd[0] * ffn[0] + sd[1] * ffn[1] + sd[2] * ffn[2];
+        for (int c = 0; c < 3; ++c) total[c] += L[3 + c] * cos_theta;
+      }
+      for (int c = 0; c < 3; ++c) rgb[3 * pix + c] = total[c] * kd[c];
+    }
+  }
+  return shadow_rays;
+}

@@ -1,0 +1,269 @@
+"""Seeded synthetic scenes for the ray-query path.
+
+The reference renders triangle meshes handed to a ``Mesh`` group
+(Model/Groups/Mesh.h:27-50): a float vertex array, three vertex indices per
+triangle and one material index per triangle.  The generators here produce
+exactly those three arrays (float32 / uint32) so that the device path, the
+CPU restatement and the reference's own classes all read identical bytes.
+
+Shapes follow the workloads this project measures:
+  * displaced icosphere: subdivided icosahedron, vertices pushed along the
+    radius by seeded 3-D value noise;
+  * ground quad grid: a flat grid of quads split into two triangles each;
+  * heightfield: an nx x nz grid whose heights are seeded fractal (fBm)
+    2-D value noise.
+All arithmetic before the final float32 cast is float64 numpy, which is
+IEEE-deterministic, so a seed always yields the same bytes.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Mesh:
+    """Triangle soup in the reference's Mesh layout."""
+
+    vertices: np.ndarray  # (V, 3) float32
+    indices: np.ndarray  # (T, 3) uint32
+    face_material: np.ndarray  # (T,) uint32
+    materials: np.ndarray = field(default_factory=lambda: np.zeros((1, 3), np.float32))
+
+    @property
+    def n_tris(self) -> int:
+        return int(self.indices.shape[0])
+
+    def bounds(self) -> tuple[np.ndarray, np.ndarray]:
+        return self.vertices.min(axis=0), self.vertices.max(axis=0)
+
+
+def merge(meshes: list[Mesh], materials: np.ndarray) -> Mesh:
+    """Concatenates meshes; each keeps its own face_material values."""
+    verts, idx, mats = [], [], []
+    base = 0
+    for m in meshes:
+        verts.append(m.vertices)
+        idx.append(m.indices + np.uint32(base))
+        mats.append(m.face_material)
+        base += m.vertices.shape[0]
+    return Mesh(
+        np.ascontiguousarray(np.concatenate(verts).astype(np.float32)),
+        np.ascontiguousarray(np.concatenate(idx).astype(np.uint32)),
+        np.ascontiguousarray(np.concatenate(mats).astype(np.uint32)),
+        np.ascontiguousarray(np.asarray(materials, np.float32).reshape(-1, 3)),
+    )
+
+
+# ---------------------------------------------------------------- noise ----
+
+class ValueNoise:
+    """Seeded lattice value noise with smoothstep interpolation."""
+
+    def __init__(self, seed: int, size: int = 256):
+        rng = np.random.default_rng(seed)
+        self.size = size
+        self.perm = rng.permutation(size).astype(np.int64)
+        self.vals = rng.random(size)
+
+    def _hash(self, *coords: np.ndarray) -> np.ndarray:
+        h = np.zeros_like(coords[0])
+        for c in coords:
+            h = self.perm[(h + c) % self.size]
+        return h
+
+    def noise3(self, p: np.ndarray) -> np.ndarray:
+        """p: (N, 3) float64 -> (N,) in [0, 1)."""
+        fl = np.floor(p)
+        i = fl.astype(np.int64)
+        f = p - fl
+        s = f * f * (3.0 - 2.0 * f)
+        out = np.zeros(p.shape[0])
+        for dz in (0, 1):
+            wz = s[:, 2] if dz else 1.0 - s[:, 2]
+            for dy in (0, 1):
+                wy = s[:, 1] if dy else 1.0 - s[:, 1]
+                for dx in (0, 1):
+                    wx = s[:, 0] if dx else 1.0 - s[:, 0]
+                    v = self.vals[self._hash(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz)]
+                    out += wx * wy * wz * v
+        return out
+
+    def noise2(self, p: np.ndarray) -> np.ndarray:
+        """p: (N, 2) float64 -> (N,) in [0, 1)."""
+        fl = np.floor(p)
+        i = fl.astype(np.int64)
+        f = p - fl
+        s = f * f * (3.0 - 2.0 * f)
+        out = np.zeros(p.shape[0])
+        for dy in (0, 1):
+            wy = s[:, 1] if dy else 1.0 - s[:, 1]
+            for dx in (0, 1):
+                wx = s[:, 0] if dx else 1.0 - s[:, 0]
+                out += wx * wy * self.vals[self._hash(i[:, 0] + dx, i[:, 1] + dy)]
+        return out
+
+
+# ------------------------------------------------------------ primitives ---
+
+def icosphere(level: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit icosphere: 20 * 4**level triangles (level 6 -> 81,920)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array(
+        [[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0],
+         [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+         [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array(
+        [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11],
+         [1, 5, 9], [5, 11, 4], [11, 10, 2], [10, 7, 6], [7, 1, 8],
+         [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9],
+         [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    for _ in range(level):
+        edges = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        key = np.sort(edges, axis=1)
+        uniq, inv = np.unique(key, axis=0, return_inverse=True)
+        inv = inv.reshape(-1)
+        mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = v.shape[0]
+        v = np.concatenate([v, mid])
+        nf = f.shape[0]
+        m01 = base + inv[:nf]
+        m12 = base + inv[nf:2 * nf]
+        m20 = base + inv[2 * nf:]
+        f = np.concatenate([
+            np.stack([f[:, 0], m01, m20], 1),
+            np.stack([f[:, 1], m12, m01], 1),
+            np.stack([f[:, 2], m20, m12], 1),
+            np.stack([m01, m12, m20], 1)])
+    return v, f
+
+
+def displaced_icosphere(level: int = 6, seed: int = 1, amplitude: float = 0.05,
+                        frequency: float = 4.0, center=(0.0, 0.0, 0.0),
+                        radius: float = 1.0, material: int = 0) -> Mesh:
+    """Icosphere with radius r * (1 + amplitude * (2 * noise(freq * p) - 1))."""
+    v, f = icosphere(level)
+    n = ValueNoise(seed).noise3(v * frequency + 17.0)
+    r = radius * (1.0 + amplitude * (2.0 * n - 1.0))
+    pos = v * r[:, None] + np.asarray(center, np.float64)
+    return Mesh(pos.astype(np.float32), f.astype(np.uint32),
+                np.full(f.shape[0], material, np.uint32))
+
+
+def quad_grid(n_quads_x: int, n_quads_z: int, x0: float, x1: float,
+              z0: float, z1: float, heights: np.ndarray | None = None,
+              y: float = 0.0, material: int = 0) -> Mesh:
+    """(nx x nz) quads, two triangles each; optional per-vertex heights."""
+    xs = np.linspace(x0, x1, n_quads_x + 1)
+    zs = np.linspace(z0, z1, n_quads_z + 1)
+    gx, gz = np.meshgrid(xs, zs, indexing="xy")
+    gy = np.full_like(gx, y) if heights is None else y + heights.reshape(gx.shape)
+    verts = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], 1)
+    w = n_quads_x + 1
+    iz, ix = np.meshgrid(np.arange(n_quads_z), np.arange(n_quads_x), indexing="ij")
+    a = (iz * w + ix).ravel()
+    b = a + 1
+    c = a + w
+    d = c + 1
+    tris = np.concatenate([np.stack([a, c, b], 1), np.stack([b, c, d], 1)])
+    # interleave the two triangles of each quad
+    tris = tris.reshape(2, -1, 3).transpose(1, 0, 2).reshape(-1, 3)
+    return Mesh(verts.astype(np.float32), tris.astype(np.uint32),
+                np.full(tris.shape[0], material, np.uint32))
+
+
+def fbm_heights(nx: int, nz: int, seed: int, octaves: int = 5,
+                amplitude: float = 0.2, base_frequency: float = 4.0) -> np.ndarray:
+    """(nz+1, nx+1) fractal value-noise heights in [-amplitude, amplitude]."""
+    noise = ValueNoise(seed)
+    u = np.linspace(0.0, 1.0, nx + 1)
+    w = np.linspace(0.0, 1.0, nz + 1)
+    gu, gw = np.meshgrid(u, w, indexing="xy")
+    p = np.stack([gu.ravel(), gw.ravel()], 1)
+    h = np.zeros(p.shape[0])
+    a, fr, norm = 1.0, base_frequency, 0.0
+    for o in range(octaves):
+        h += a * (2.0 * noise.noise2(p * fr + 31.0 * o) - 1.0)
+        norm += a
+        a *= 0.5
+        fr *= 2.0
+    return (amplitude * h / norm).reshape(nz + 1, nx + 1)
+
+
+def heightfield(nx: int, nz: int, seed: int, extent: float = 4.0,
+                octaves: int = 5, amplitude: float = 0.2, y: float = -1.1,
+                material: int = 0) -> Mesh:
+    """nx x nz heightfield grid (2*nx*nz triangles) of fBm heights."""
+    h = fbm_heights(nx, nz, seed, octaves, amplitude)
+    e = extent / 2.0
+    return quad_grid(nx, nz, -e, e, -e, e, heights=h, y=y, material=material)
+
+
+# ------------------------------------------------------------ workloads ---
+
+@dataclass
+class Camera:
+    eye: tuple
+    lookat: tuple
+    up: tuple
+    hfov: float
+    vfov: float
+
+
+@dataclass
+class PointLightSpec:
+    position: tuple
+    color: tuple
+
+
+@dataclass
+class WhittedScene:
+    mesh: Mesh
+    camera: Camera
+    lights: list
+    ambient: tuple
+    background: tuple
+    xres: int
+    yres: int
+
+
+def small_frame_scene(level: int = 6, grid: int = 100, xres: int = 512,
+                      yres: int = 512, seed: int = 7) -> WhittedScene:
+    """512x512 primary + hard-shadow frame over a displaced icosphere
+    (level 6: 81,920 tris, amplitude 0.05, frequency 4) and a 2x2 ground grid
+    of 2*grid*grid tris (grid=100: 20,000), one point light at (2,3,2),
+    pinhole camera at (0,0,3) looking at the origin, fov 60 degrees."""
+    sphere = displaced_icosphere(level, seed=seed, material=0)
+    ground = quad_grid(grid, grid, -1.0, 1.0, -1.0, 1.0, y=-1.1, material=1)
+    mats = np.array([[0.8, 0.3, 0.2], [0.6, 0.6, 0.6]], np.float32)
+    mesh = merge([sphere, ground], mats)
+    cam = Camera((0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 60.0, 60.0)
+    lights = [PointLightSpec((2.0, 3.0, 2.0), (0.9, 0.9, 0.9))]
+    return WhittedScene(mesh, cam, lights, (0.1, 0.1, 0.1), (0.2, 0.3, 0.5), xres, yres)
+
+
+def tiny_frame_scene(xres: int = 48, yres: int = 40, seed: int = 3) -> WhittedScene:
+    """The small-frame layout scaled down (level-2 icosphere, 6x6 grid) for
+    committed fixtures."""
+    s = small_frame_scene(level=2, grid=6, xres=xres, yres=yres, seed=seed)
+    s.lights.append(PointLightSpec((-2.0, 1.5, 2.5), (0.3, 0.35, 0.4)))
+    return s
+
+
+def random_rays(n: int, lo: np.ndarray, hi: np.ndarray, seed: int,
+                anyhit_fraction: float = 0.0):
+    """Origins uniform in [lo, hi], directions uniform on the sphere, tmax
+    uniform in [0.1, |hi-lo|] (for the any-hit share) or 1e19 (closest)."""
+    rng = np.random.default_rng(seed)
+    o = lo + (hi - lo) * rng.random((n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    diag = float(np.linalg.norm(hi - lo))
+    anyhit = rng.random(n) < anyhit_fraction
+    tmax = np.where(anyhit, rng.uniform(0.1, max(diag, 0.1000001), n), 1e19)
+    return (np.ascontiguousarray(o.T.astype(np.float32)),
+            np.ascontiguousarray(d.T.astype(np.float32)),
+            tmax.astype(np.float32), anyhit)

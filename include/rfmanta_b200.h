@@ -1,0 +1,167 @@
+/*
+ * rfmanta_b200 - B200 (sm_100a) ray-query path for the Manta ray tracer.
+ *
+ * Plain C ABI: opaque handles, plain pointers and sizes, int status codes.
+ * No exception and no C++ or torch type crosses it.  A Manta build binds it
+ * through the C++ drop-in classes in rfmanta_b200/manta/ (GpuDynBVH as the
+ * AccelerationStructure, GpuHardShadows as the ShadowAlgorithm); Python binds
+ * it through ctypes (rfmanta_b200/_lib.py).
+ *
+ * Arithmetic is IEEE float32 in the reference's operation order, so results
+ * match the reference's MANTA_SSE=OFF build.
+ *
+ * Ray arrays are structure-of-arrays: org = [x0..x(n-1), y0.., z0..], the
+ * same for dir.  "t" is in units of the direction vector as passed in.
+ *
+ * Thread safety: calls on different scenes may run concurrently.  Calls on
+ * one scene may run concurrently from several host threads (the reference
+ * calls DynBVH::intersect from every render worker); each call then uses its
+ * own staging buffers and stream.
+ */
+#ifndef RFMANTA_B200_H
+#define RFMANTA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RQ_API __attribute__((visibility("default")))
+#else
+#define RQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (every entry point returns one). */
+enum {
+  RQ_OK = 0,
+  RQ_ERR_ARG = 1,      /* bad argument (null pointer, bad size, bad flag) */
+  RQ_ERR_CUDA = 2,     /* a CUDA call failed; see rq_last_error() */
+  RQ_ERR_OOM = 3,      /* device allocation failed */
+  RQ_ERR_FORMAT = 4,   /* malformed tree import (bad index, cycle, ...) */
+  RQ_ERR_STATE = 5,    /* scene has no acceleration structure yet */
+  RQ_ERR_CAPACITY = 6, /* tree deeper than the traversal stack supports */
+  RQ_ERR_TIMEOUT = 7,  /* a bounded device wait gave up */
+  RQ_ERR_NODEV = 8     /* no usable sm_100 device */
+};
+
+/* Triangle intersection kernels of the reference. */
+enum {
+  RQ_TRI_WALD = 0, /* WaldTriangle (Model/Primitives/WaldTriangle.cc) */
+  RQ_TRI_KS = 1    /* KenslerShirleyTriangle (Model/Primitives/KenslerShirleyTriangle.cc) */
+};
+
+/* Query flags. */
+enum {
+  RQ_CLOSEST = 0, /* closest hit: Raytracer::traceRays -> DynBVH::intersect */
+  RQ_ANYHIT = 1   /* occlusion: RayPacket::AnyHit set by HardShadows.cc:79 */
+};
+
+typedef struct rq_scene rq_scene;
+
+/* Message of the last failed call on this host thread ("" if none). */
+RQ_API const char* rq_last_error(void);
+
+/* Library build identification: "rfmanta_b200 <version> sm_100a". */
+RQ_API const char* rq_version(void);
+
+/*
+ * Uploads a triangle mesh (Mesh::vertices / vertex_indices / face_material,
+ * Model/Groups/Mesh.h:27-50) to device `device`.  Replaces constructing the
+ * Mesh + WaldTriangle/KenslerShirleyTriangle objects and
+ * DynBVH::setGroup(Group*) (Model/Groups/DynBVH.h:150).  The scene has no
+ * tree until one of the rq_scene_import_* / rq_scene_build calls.
+ */
+RQ_API int rq_scene_create(const float* vertices, int n_vertices,
+                    const uint32_t* indices, int n_tris,
+                    const uint32_t* face_material, int tri_kind, int device,
+                    rq_scene** out);
+
+RQ_API int rq_scene_destroy(rq_scene* scene);
+
+/*
+ * Imports a DynBVH tree in the reference's own byte format, the stream
+ * DynBVH::saveToFile writes (Model/Groups/DynBVH.cc:2479-2501):
+ *   u32 n_ids, int32 object_ids[n_ids], u32 n_nodes, BVHNode nodes[n_nodes]
+ * with the x86-64 32-byte BVHNode (DynBVH.h:37-52: BBox at 0, int child at
+ * 24, u8 axis at 28, isLeftCheaper bit 0 of byte 29, short children at 30).
+ * Replaces DynBVH::buildFromFile (DynBVH.cc:2442-2476).  Nodes not reachable
+ * from the root are ignored.
+ */
+RQ_API int rq_scene_import_dynbvh(rq_scene* scene, const void* blob, size_t bytes);
+
+/*
+ * Same tree given field by field: bounds[6*i] = min xyz, max xyz;
+ * child[i]; children[i] (leaf iff != 0); axis[i]; left_cheaper[i];
+ * object_ids[n_tris].
+ */
+RQ_API int rq_scene_import_tree(rq_scene* scene, int n_nodes, const float* bounds,
+                         const int32_t* child, const int32_t* children,
+                         const uint8_t* axis, const uint8_t* left_cheaper,
+                         const int32_t* object_ids);
+
+/*
+ * Builds the tree on the GPU with a binned SAH builder (`bins` bins per
+ * axis, 0 = default 32).  Replaces DynBVH::rebuild (DynBVH.cc:1699-1802);
+ * reaches an SAH cost (DynBVH::computeCost, DynBVH.cc:3389-3416) within a
+ * few percent of the reference's exact sweep build.
+ */
+RQ_API int rq_scene_build(rq_scene* scene, int bins);
+
+/* SAH cost of the scene's tree, DynBVH::computeCost<>(0) with C_isec=C_trav=1. */
+RQ_API int rq_scene_sah_cost(const rq_scene* scene, double* cost);
+
+/* Counts: internal records, leaves, maximum traversal depth. */
+RQ_API int rq_scene_info(const rq_scene* scene, int* n_records, int* n_leaves,
+                  int* depth, size_t* device_bytes);
+
+/*
+ * Exports the tree in the saveToFile byte format (DynBVH::saveToFile).
+ * With blob == NULL only *bytes is set.
+ */
+RQ_API int rq_scene_export_dynbvh(const rq_scene* scene, void* blob, size_t* bytes);
+
+/*
+ * Ray query over HOST arrays (copies in, traces, copies out): the per-call
+ * drop-in for DynBVH::intersect(const RenderContext&, RayPacket&) const
+ * (Model/Groups/DynBVH.cc:101-272).  flags = RQ_CLOSEST or RQ_ANYHIT.
+ * tmax[i] is the ray's minT on entry (RayPacket::resetHit).
+ * Outputs (any may be NULL): t[i] = minT on exit (closest: hit distance or
+ * tmax; any-hit: occluder distance or tmax), prim[i] = triangle index or -1,
+ * u[i], v[i] = the triangle's scratchpad pair (Wald lambda/mue, KS
+ * uoverd/voverd).
+ */
+RQ_API int rq_trace(rq_scene* scene, int n, const float* org, const float* dir,
+             const float* tmax, int flags, float* t, int32_t* prim, float* u,
+             float* v);
+
+/*
+ * Same query over DEVICE arrays already resident in HBM, enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream); returns without
+ * synchronising.
+ */
+RQ_API int rq_trace_device(rq_scene* scene, int n, const float* d_org,
+                    const float* d_dir, const float* d_tmax, int flags,
+                    float* d_t, int32_t* d_prim, float* d_u, float* d_v,
+                    void* stream);
+
+/* Traversal launch parameters (persistent kernel, warp-ballot ray fetch). */
+typedef struct {
+  int block_threads;    /* threads per block (multiple of 32) */
+  int blocks_per_sm;    /* resident blocks per SM, 0 = occupancy maximum */
+  int refill_threshold; /* idle lanes in a warp before it fetches new rays */
+  int persistent;       /* 0 = one thread per ray, 1 = persistent */
+} rq_launch_config;
+
+RQ_API int rq_set_launch_config(rq_scene* scene, int flags,
+                         const rq_launch_config* cfg);
+RQ_API int rq_get_launch_config(const rq_scene* scene, int flags,
+                         rq_launch_config* cfg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RFMANTA_B200_H */

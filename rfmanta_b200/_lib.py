@@ -1,0 +1,94 @@
+"""ctypes binding of the C ABI in include/rfmanta_b200.h.
+
+The CUDA library must have been built (``python -m rfmanta_b200.build``);
+there is no fallback path: importing this module without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librfmanta_b200.so")
+
+RQ_OK = 0
+RQ_ERR_ARG = 1
+RQ_ERR_CUDA = 2
+RQ_ERR_OOM = 3
+RQ_ERR_FORMAT = 4
+RQ_ERR_STATE = 5
+RQ_ERR_CAPACITY = 6
+RQ_ERR_TIMEOUT = 7
+RQ_ERR_NODEV = 8
+
+RQ_TRI_WALD = 0
+RQ_TRI_KS = 1
+RQ_CLOSEST = 0
+RQ_ANYHIT = 1
+
+ERROR_NAMES = {
+    RQ_ERR_ARG: "RQ_ERR_ARG", RQ_ERR_CUDA: "RQ_ERR_CUDA", RQ_ERR_OOM: "RQ_ERR_OOM",
+    RQ_ERR_FORMAT: "RQ_ERR_FORMAT", RQ_ERR_STATE: "RQ_ERR_STATE",
+    RQ_ERR_CAPACITY: "RQ_ERR_CAPACITY", RQ_ERR_TIMEOUT: "RQ_ERR_TIMEOUT",
+    RQ_ERR_NODEV: "RQ_ERR_NODEV",
+}
+
+
+class RQError(RuntimeError):
+    """A C-ABI call returned a non-zero status (the C++ shim maps these to
+    Manta's InternalError)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class LaunchConfig(C.Structure):
+    _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
+                ("refill_threshold", C.c_int), ("persistent", C.c_int)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m rfmanta_b200.build` "
+            "(the ray-query path has no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    vp, i, sz = C.c_void_p, C.c_int, C.c_size_t
+    sig = {
+        "rq_last_error": ([], C.c_char_p),
+        "rq_version": ([], C.c_char_p),
+        "rq_scene_create": ([vp, i, vp, i, vp, i, i, C.POINTER(vp)], i),
+        "rq_scene_destroy": ([vp], i),
+        "rq_scene_import_dynbvh": ([vp, vp, sz], i),
+        "rq_scene_import_tree": ([vp, i, vp, vp, vp, vp, vp, vp], i),
+        "rq_scene_build": ([vp, i], i),
+        "rq_scene_sah_cost": ([vp, C.POINTER(C.c_double)], i),
+        "rq_scene_info": ([vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz)], i),
+        "rq_scene_export_dynbvh": ([vp, vp, C.POINTER(sz)], i),
+        "rq_trace": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp], i),
+        "rq_trace_device": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp, vp], i),
+        "rq_set_launch_config": ([vp, i, C.POINTER(LaunchConfig)], i),
+        "rq_get_launch_config": ([vp, i, C.POINTER(LaunchConfig)], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+lib = _load()
+
+
+def check(rc: int) -> None:
+    if rc != RQ_OK:
+        raise RQError(rc, lib.rq_last_error().decode(errors="replace"))
+
+
+def declared_symbols(header: str | None = None) -> list[str]:
+    """Entry points declared in include/rfmanta_b200.h."""
+    import re
+    header = header or os.path.join(os.path.dirname(HERE), "include", "rfmanta_b200.h")
+    text = open(header).read()
+    return sorted(set(re.findall(r"RQ_API\s+[\w\s\*]+?\b(rq_\w+)\s*\(", text)))

@@ -1,0 +1,83 @@
+// Host-side scene object behind the opaque rq_scene handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "../../include/rfmanta_b200.h"
+#include "rq_device.cuh"
+#include "rq_internal.h"
+
+namespace rq {
+
+// The reference DynBVH tree, field by field (Model/Groups/DynBVH.h:37-79).
+struct HostTree {
+  std::vector<float> bounds;  // 6 per node: min xyz, max xyz
+  std::vector<int32_t> child;
+  std::vector<int32_t> children;
+  std::vector<uint8_t> axis;
+  std::vector<uint8_t> left_cheaper;
+  std::vector<int32_t> ids;  // object_ids, one per triangle
+};
+
+double tree_sah_cost(const HostTree& t);
+
+// Per-call resources for the host-array entry point.
+struct Staging {
+  cudaStream_t stream = nullptr;
+  void* h_buf = nullptr;  // pinned
+  void* d_buf = nullptr;
+  int* d_counter = nullptr;
+  size_t cap = 0;
+  ~Staging();
+};
+
+struct Scene {
+  int device = 0;
+  int tri_kind = 0;
+  int n_tris = 0;
+  int n_verts = 0;
+  int num_sms = 148;
+  std::vector<float> verts;
+  std::vector<uint32_t> idx;
+  std::vector<uint32_t> face_mat;
+  float* d_verts = nullptr;
+  uint32_t* d_idx = nullptr;
+  uint32_t* d_face_mat = nullptr;
+
+  // tree
+  bool has_tree = false;
+  HostTree tree;
+  float4* d_nodes = nullptr;
+  float4* d_tris = nullptr;
+  int n_records = 0;
+  int n_leaves = 0;
+  int n_leaf_tris = 0;
+  int depth = 0;
+  int root_ref = 0;
+  float root_lo[3] = {0, 0, 0};
+  float root_hi[3] = {0, 0, 0};
+
+  rq_launch_config cfg[2];
+  int* d_counter = nullptr;  // persistent-launch counters for rq_trace_device
+
+  std::mutex mu;
+  std::vector<std::unique_ptr<Staging>> staging;
+
+  ~Scene();
+  void free_tree();
+  int set_tree(const HostTree& t);
+  DevScene dev() const;
+  Staging* acquire(size_t bytes_in, size_t bytes_out);
+  void release(Staging* s);
+  LaunchPlan plan(bool anyhit, int n, int* counter) const;
+  int trace_device(int n, const float* org, const float* dir, const float* tmax,
+                   bool anyhit, float* t, int32_t* prim, float* u, float* v,
+                   cudaStream_t st, int* counter);
+};
+
+}  // namespace rq

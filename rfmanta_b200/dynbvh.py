@@ -1,0 +1,221 @@
+"""Python host mirror of the reference's ray-query interfaces.
+
+``GpuDynBVH`` mirrors Manta's ``DynBVH : AccelerationStructure``
+(Interface/AccelerationStructure.h:11-66, Model/Groups/DynBVH.h:151-224):
+``setGroup``, ``groupDirty``, ``getGroup``, ``rebuild``, ``buildFromFile``,
+``saveToFile``, ``computeBounds`` and ``intersect``.  ``RayBatch`` plays the
+role of ``RayPacket`` (Interface/RayPacket.h:58-130) for any number of rays:
+structure-of-arrays origins/directions, ``minT`` in and out, hit primitive,
+scratchpad u/v and the ``AnyHit`` flag.  Every call goes through the C ABI
+into the CUDA library; errors surface as ``RQError`` (the reference throws
+``InternalError``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import RQ_ANYHIT, RQ_CLOSEST, RQ_TRI_KS, RQ_TRI_WALD, check, lib
+from .scenes import Mesh
+
+T_EPSILON = np.float32(1.e-4)
+MAXT = np.float32(1.e19)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class RayBatch:
+    """Host-side ray batch (RayPacket semantics, any size).
+
+    org, dir: (3, n) float32 SoA.  minT: (n,) float32, the query's upper
+    bound on entry (RayPacket::resetHit) and the hit distance on exit.
+    """
+
+    AnyHit = RQ_ANYHIT
+
+    def __init__(self, org, dir, minT=None, flags: int = 0):
+        self.org = np.ascontiguousarray(org, np.float32).reshape(3, -1)
+        self.dir = np.ascontiguousarray(dir, np.float32).reshape(3, -1)
+        n = self.org.shape[1]
+        self.minT = (np.full(n, MAXT, np.float32) if minT is None
+                     else np.ascontiguousarray(minT, np.float32).copy())
+        self.flags = flags
+        self.hitPrim = np.full(n, -1, np.int32)
+        self.u = np.zeros(n, np.float32)
+        self.v = np.zeros(n, np.float32)
+
+    def __len__(self):
+        return self.org.shape[1]
+
+    def getFlag(self, f: int) -> bool:
+        return bool(self.flags & f)
+
+    def setFlag(self, f: int) -> None:
+        self.flags |= f
+
+    def resetHits(self, maxt=MAXT) -> None:
+        self.minT[:] = maxt
+        self.hitPrim[:] = -1
+
+    def wasHit(self) -> np.ndarray:
+        return self.hitPrim >= 0
+
+
+@dataclass
+class SceneInfo:
+    n_records: int
+    n_leaves: int
+    depth: int
+    device_bytes: int
+
+
+class GpuDynBVH:
+    """AccelerationStructure over one triangle Mesh, on one GPU."""
+
+    def __init__(self, tri_kind: int = RQ_TRI_WALD, device: int = 0):
+        self.tri_kind = tri_kind
+        self.device = device
+        self._h = C.c_void_p()
+        self._group: Mesh | None = None
+        self._dirty = False
+
+    # -- AccelerationStructure surface -------------------------------------
+    def setGroup(self, group: Mesh) -> None:
+        if group is not self._group:
+            self._dirty = True
+        self._group = group
+
+    def getGroup(self) -> Mesh | None:
+        return self._group
+
+    def groupDirty(self) -> None:
+        self._dirty = True
+
+    def _upload(self) -> None:
+        if self._group is None:
+            raise _lib.RQError(_lib.RQ_ERR_STATE, "setGroup was not called")
+        self.close()
+        m = self._group
+        v = np.ascontiguousarray(m.vertices, np.float32)
+        ix = np.ascontiguousarray(m.indices, np.uint32)
+        fm = np.ascontiguousarray(m.face_material, np.uint32)
+        check(lib.rq_scene_create(_p(v), v.shape[0], _p(ix), m.n_tris, _p(fm),
+                                  self.tri_kind, self.device, C.byref(self._h)))
+        self._dirty = False
+
+    def rebuild(self, bins: int = 0) -> None:
+        """DynBVH::rebuild, done by the GPU binned-SAH builder."""
+        if self._dirty or not self._h:
+            self._upload()
+        check(lib.rq_scene_build(self._h, bins))
+
+    def importTree(self, tree) -> None:
+        """Reference tree given field by field (oracle Tree or compatible)."""
+        if self._dirty or not self._h:
+            self._upload()
+        b = np.ascontiguousarray(tree.bounds, np.float32)
+        c = np.ascontiguousarray(tree.child, np.int32)
+        ch = np.ascontiguousarray(tree.children, np.int32)
+        ax = np.ascontiguousarray(tree.axis, np.uint8)
+        lc = np.ascontiguousarray(tree.left_cheaper, np.uint8)
+        ids = np.ascontiguousarray(tree.ids, np.int32)
+        check(lib.rq_scene_import_tree(self._h, ch.shape[0], _p(b), _p(c), _p(ch), _p(ax),
+                                       _p(lc), _p(ids)))
+
+    def importBlob(self, blob: bytes) -> None:
+        if self._dirty or not self._h:
+            self._upload()
+        buf = C.create_string_buffer(blob, len(blob))
+        check(lib.rq_scene_import_dynbvh(self._h, buf, len(blob)))
+
+    def buildFromFile(self, path: str) -> bool:
+        """DynBVH::buildFromFile: the saveToFile byte stream."""
+        try:
+            with open(path, "rb") as f:
+                blob = f.read()
+        except OSError:
+            return False
+        self.importBlob(blob)
+        return True
+
+    def exportBlob(self) -> bytes:
+        n = C.c_size_t()
+        check(lib.rq_scene_export_dynbvh(self._h, None, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        check(lib.rq_scene_export_dynbvh(self._h, buf, C.byref(n)))
+        return buf.raw[: n.value]
+
+    def saveToFile(self, path: str) -> bool:
+        with open(path, "wb") as f:
+            f.write(self.exportBlob())
+        return True
+
+    def computeBounds(self):
+        return self._group.bounds()
+
+    def sahCost(self) -> float:
+        c = C.c_double()
+        check(lib.rq_scene_sah_cost(self._h, C.byref(c)))
+        return c.value
+
+    def info(self) -> SceneInfo:
+        a, b, d = C.c_int(), C.c_int(), C.c_int()
+        nb = C.c_size_t()
+        check(lib.rq_scene_info(self._h, C.byref(a), C.byref(b), C.byref(d), C.byref(nb)))
+        return SceneInfo(a.value, b.value, d.value, nb.value)
+
+    def intersect(self, rays: RayBatch) -> None:
+        """DynBVH::intersect over a host batch (copies in and out)."""
+        n = len(rays)
+        flags = RQ_ANYHIT if rays.getFlag(RQ_ANYHIT) else RQ_CLOSEST
+        t = np.empty(n, np.float32)
+        check(lib.rq_trace(self._h, n, _p(rays.org), _p(rays.dir), _p(rays.minT), flags,
+                           _p(t), _p(rays.hitPrim), _p(rays.u), _p(rays.v)))
+        rays.minT[:] = t
+
+    def intersect_device(self, n: int, org_ptr: int, dir_ptr: int, tmax_ptr: int,
+                         anyhit: bool, t_ptr: int, prim_ptr: int, u_ptr: int = 0,
+                         v_ptr: int = 0, stream: int = 0) -> None:
+        """Query over device arrays already in HBM (raw pointers), enqueued on
+        `stream` without synchronising."""
+        check(lib.rq_trace_device(self._h, n, C.c_void_p(org_ptr), C.c_void_p(dir_ptr),
+                                  C.c_void_p(tmax_ptr), RQ_ANYHIT if anyhit else RQ_CLOSEST,
+                                  C.c_void_p(t_ptr), C.c_void_p(prim_ptr),
+                                  C.c_void_p(u_ptr or None), C.c_void_p(v_ptr or None),
+                                  C.c_void_p(stream or None)))
+
+    def set_launch_config(self, anyhit: bool, block_threads=128, blocks_per_sm=0,
+                          refill_threshold=8, persistent=True) -> None:
+        cfg = _lib.LaunchConfig(block_threads, blocks_per_sm, refill_threshold, int(persistent))
+        check(lib.rq_set_launch_config(self._h, RQ_ANYHIT if anyhit else RQ_CLOSEST,
+                                       C.byref(cfg)))
+
+    def get_launch_config(self, anyhit: bool) -> dict:
+        cfg = _lib.LaunchConfig()
+        check(lib.rq_get_launch_config(self._h, RQ_ANYHIT if anyhit else RQ_CLOSEST,
+                                       C.byref(cfg)))
+        return dict(block_threads=cfg.block_threads, blocks_per_sm=cfg.blocks_per_sm,
+                    refill_threshold=cfg.refill_threshold, persistent=bool(cfg.persistent))
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib.rq_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["GpuDynBVH", "RayBatch", "RQ_TRI_WALD", "RQ_TRI_KS", "T_EPSILON", "MAXT"]

@@ -1,0 +1,89 @@
+"""Generates the committed golden fixtures from the reference's own code.
+
+    make -f oracle/ref.mk REF=/path/to/rfManta -j8 oracle/_ref/libmanta_ref.so
+    python tests/golden/make_golden.py
+
+For each triangle kind (WaldTriangle, KenslerShirleyTriangle) it builds the
+small seeded frame scene (level-2 displaced icosphere + 6x6 ground grid, 392
+triangles, 48x40 pixels, two point lights) with the reference's Mesh +
+DynBVH::rebuild, and records what the reference computes:
+  * the tree (field by field) and the DynBVH::saveToFile byte stream;
+  * DynBVH::computeCost of that tree;
+  * the PinholeCamera basis;
+  * DynBVH::intersect results (hit, t, triangle id, u, v) for the frame's
+    primary rays, for seeded random closest-hit rays and for seeded random
+    any-hit rays;
+  * the Raytracer::traceEyeRays frame (RGB, primary t and triangle id) and
+    the number of shadow rays HardShadows sent.
+The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
+path to the reference without needing the reference at test time.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle.pyoracle import Reference, Restatement  # noqa: E402
+from rfmanta_b200 import scenes  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def main() -> None:
+    ref = Reference()
+    restated = Restatement()
+    sc = scenes.tiny_frame_scene()
+    mesh = sc.mesh
+    lo, hi = mesh.bounds()
+    pad = 0.25 * (hi - lo)
+    o_r, d_r, _, _ = scenes.random_rays(4096, lo - pad, hi + pad, seed=11)
+    o_a, d_a, tm_a, _ = scenes.random_rays(4096, lo - pad, hi + pad, seed=12,
+                                           anyhit_fraction=1.0)
+    for kind, name in ((0, "wald"), (1, "ks")):
+        rs = ref.scene(mesh, kind)
+        tree = rs.tree()
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "tree.bvh")
+            rs.save_blob(path)
+            blob = np.frombuffer(open(path, "rb").read(), np.uint8)
+        basis = ref.camera_basis(sc.camera)
+        org, dir = restated.primary_rays(basis, sc.xres, sc.yres)
+        n = org.shape[1]
+        prim_q = rs.intersect(org, dir, np.full(n, 1e19, np.float32))
+        rnd_q = rs.intersect(o_r, d_r, np.full(o_r.shape[1], 1e19, np.float32))
+        any_q = rs.intersect(o_a, d_a, tm_a, anyhit=True)
+        img = rs.render(sc, nthreads=1)
+        out = dict(
+            vertices=mesh.vertices, indices=mesh.indices, face_material=mesh.face_material,
+            materials=mesh.materials,
+            bounds=tree.bounds, child=tree.child, children=tree.children, axis=tree.axis,
+            left_cheaper=tree.left_cheaper, ids=tree.ids, blob=blob,
+            node_size=np.int32(ref.lib.mref_node_size()),
+            sah_cost=np.float64(rs.sah_cost()), camera_basis=basis,
+            xres=np.int32(sc.xres), yres=np.int32(sc.yres),
+            lights=np.array([list(l.position) + list(l.color) for l in sc.lights], np.float32),
+            ambient=np.asarray(sc.ambient, np.float32),
+            background=np.asarray(sc.background, np.float32),
+            cam=np.array(list(sc.camera.eye) + list(sc.camera.lookat) + list(sc.camera.up) +
+                         [sc.camera.hfov, sc.camera.vfov], np.float32),
+            primary_org=org, primary_dir=dir,
+            **{f"primary_{k}": v for k, v in prim_q.items()},
+            rand_org=o_r, rand_dir=d_r, **{f"rand_{k}": v for k, v in rnd_q.items()},
+            any_org=o_a, any_dir=d_a, any_tmax=tm_a, **{f"any_{k}": v for k, v in any_q.items()},
+            img_rgb=img["rgb"], img_t=img["t"], img_prim=img["prim"],
+            img_shadow_rays=np.int64(img["shadow_rays"]),
+        )
+        path = os.path.join(OUT, f"tiny_{name}.npz")
+        np.savez_compressed(path, **out)
+        rs.close()
+        print(path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

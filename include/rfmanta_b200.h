@@ -160,6 +160,62 @@ RQ_API int rq_set_launch_config(rq_scene* scene, int flags,
 RQ_API int rq_get_launch_config(const rq_scene* scene, int flags,
                          rq_launch_config* cfg);
 
+/*
+ * Whitted frame (Raytracer::traceEyeRays, Engine/Renderers/Raytracer.cc:41-97,
+ * with PinholeCamera -normalizeRays, Lambertian, HardShadows and point
+ * lights): the frame the reference's render workers produce tile by tile,
+ * here as one device wavefront.
+ */
+typedef struct {
+  float eye[3], lookat[3], up[3]; /* PinholeCamera -eye -lookat -up */
+  float hfov, vfov;               /* degrees */
+  int xres, yres;
+  int n_lights;                   /* point lights, 0..16 */
+  const float* lights;            /* host: n_lights x (x, y, z, r, g, b) */
+  float ambient[3];               /* ConstantAmbient colour */
+  float background[3];            /* ConstantBackground colour */
+  int n_materials;                /* Lambertian diffuse colours by material id */
+  const float* material_rgb;      /* host: n_materials x (r, g, b) */
+} rq_whitted_params;
+
+/* PinholeCamera::setup basis (Model/Cameras/PinholeCamera.cc:167-198):
+ * out12 = eye, lookat-eye, u, v.  Host-only, needs no device. */
+RQ_API int rq_camera_basis(const float* eye, const float* lookat, const float* up,
+                           float hfov, float vfov, float* out12);
+
+/* Renders into HOST buffers: rgb (3 per pixel, row-major from y = 0), primary
+ * hit distance t and triangle id prim (-1 = miss); shadow_rays = number of
+ * shadow rays sent.  t, prim, shadow_rays may be NULL. */
+RQ_API int rq_render_whitted(rq_scene* scene, const rq_whitted_params* params,
+                             float* rgb, float* t, int32_t* prim,
+                             uint64_t* shadow_rays);
+
+/* Same into DEVICE buffers, enqueued on `stream` without synchronising.
+ * d_shadow_rays (device, may be NULL) receives the shadow-ray count. */
+RQ_API int rq_render_whitted_device(rq_scene* scene, const rq_whitted_params* params,
+                                    float* d_rgb, float* d_t, int32_t* d_prim,
+                                    uint64_t* d_shadow_rays, void* stream);
+
+/*
+ * Profiling hook (the role of DynBVH's COLLECT_STATS counters,
+ * Model/Groups/DynBVH.h:314-374): when `events` (n cudaEvent_t handles
+ * created by the caller) is set, the frame paths record events[0] before
+ * their first stage and events[k] after stage k.  NULL turns it off.
+ */
+RQ_API int rq_set_stage_events(rq_scene* scene, void* events, int n);
+
+/*
+ * Traversal statistics (DynBVH COLLECT_STATS: node traversals and
+ * intersections per ray).  d_counters is a device array of 4 uint64 the
+ * frame paths add to: box tests and triangle tests of primary (or bounce)
+ * rays, then of shadow rays.  The caller zeroes it.  NULL turns counting off
+ * (the default; counting builds use separate kernels).
+ */
+RQ_API int rq_set_stats(rq_scene* scene, uint64_t* d_counters);
+
+/* Device time in seconds of the last rq_scene_build. */
+RQ_API int rq_scene_build_seconds(const rq_scene* scene, double* seconds);
+
 #ifdef __cplusplus
 }
 #endif

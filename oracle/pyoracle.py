@@ -90,7 +90,7 @@ class Restatement:
         L.orq_primary_rays.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.orq_render_whitted.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 6 +
                                          [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
-                                          C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 4)
+                                          C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5)
         L.orq_render_whitted.restype = C.c_longlong
 
     def wald_setup(self, mesh) -> np.ndarray:
@@ -184,10 +184,14 @@ class Restatement:
         tp = np.zeros(npx, np.float32)
         pr = np.full(npx, -1, np.int32)
         lit = np.zeros(npx, np.int32)
+        counts = np.zeros(4, np.int64)
         ns = self.lib.orq_render_whitted(*args, _ptr(fm), _ptr(mats), _ptr(basis), xres, yres,
                                          _ptr(lights), len(scene.lights), _ptr(amb), _ptr(bg),
-                                         y0, y1, _ptr(rgb), _ptr(tp), _ptr(pr), _ptr(lit))
-        return dict(rgb=rgb, t=tp, prim=pr, lit=lit, shadow_rays=int(ns))
+                                         y0, y1, _ptr(rgb), _ptr(tp), _ptr(pr), _ptr(lit),
+                                         _ptr(counts))
+        return dict(rgb=rgb, t=tp, prim=pr, lit=lit, shadow_rays=int(ns),
+                    primary_node_tests=int(counts[0]), primary_tri_tests=int(counts[1]),
+                    shadow_node_tests=int(counts[2]), shadow_tri_tests=int(counts[3]))
 
 
 class Reference:

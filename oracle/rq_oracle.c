@@ -501,8 +501,9 @@ static void tri_normal(const Tree* T, int tri, float* nrm) {
 /* Whitted frame: Raytracer + Lambertian + HardShadows(point lights).
  * lights: nl x (pos xyz, rgb).  mat_rgb/face_mat: diffuse colour per
  * material.  Outputs rgb (3 per pixel), primary t and triangle id, the
- * number of shadow rays sent, and optional per-pixel occlusion bits
- * (bit j set = light j unshadowed). */
+ * number of shadow rays sent, optional per-pixel occlusion bits (bit j set =
+ * light j unshadowed) and optional traversal counts: counts[0..3] = node
+ * tests and triangle tests of the primary rays, then of the shadow rays. */
 long long orq_render_whitted(const float* bounds, const int* child,
                              const int* children, const unsigned char* axis,
                              const unsigned char* left_cheaper, const int* ids,
@@ -513,7 +514,7 @@ long long orq_render_whitted(const float* bounds, const int* child,
                              const float* lights, int nl, const float* ambient,
                              const float* background, int y0, int y1,
                              float* rgb, float* tprim, int* prim,
-                             int* lit_bits) {
+                             int* lit_bits, long long* counts) {
   Tree T = {bounds, child, children, axis, left_cheaper, ids,
             tri_kind, verts, idx, wald};
   long long shadow_rays = 0;
@@ -530,6 +531,10 @@ long long orq_render_whitted(const float* bounds, const int* child,
       r.anyhit = 0;
       r.node_tests = r.tri_tests = 0;
       visit(&T, 0, &r);
+      if (counts) {
+        counts[0] += r.node_tests;
+        counts[1] += r.tri_tests;
+      }
       tprim[pix] = r.minT;
       prim[pix] = r.hit ? r.prim : -1;
       if (lit_bits) lit_bits[pix] = 0;
@@ -571,6 +576,10 @@ long long orq_render_whitted(const float* bounds, const int* child,
         s.node_tests = s.tri_tests = 0;
         shadow_rays++;
         visit(&T, 0, &s);
+        if (counts) {
+          counts[2] += s.node_tests;
+          counts[3] += s.tri_tests;
+        }
         if (s.hit) continue;
         if (lit_bits) lit_bits[pix] |= 1 << j;
         /* shadowRays.normalizeDirections (RayPacket.cc:61-71) */

@@ -43,6 +43,14 @@ class RQError(RuntimeError):
         self.code = code
 
 
+class WhittedParams(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("lookat", C.c_float * 3), ("up", C.c_float * 3),
+                ("hfov", C.c_float), ("vfov", C.c_float), ("xres", C.c_int), ("yres", C.c_int),
+                ("n_lights", C.c_int), ("lights", C.c_void_p), ("ambient", C.c_float * 3),
+                ("background", C.c_float * 3), ("n_materials", C.c_int),
+                ("material_rgb", C.c_void_p)]
+
+
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
                 ("refill_threshold", C.c_int), ("persistent", C.c_int)]
@@ -70,6 +78,13 @@ def _load():
         "rq_trace_device": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp, vp], i),
         "rq_set_launch_config": ([vp, i, C.POINTER(LaunchConfig)], i),
         "rq_get_launch_config": ([vp, i, C.POINTER(LaunchConfig)], i),
+        "rq_camera_basis": ([vp, vp, vp, C.c_float, C.c_float, vp], i),
+        "rq_render_whitted": ([vp, C.POINTER(WhittedParams), vp, vp, vp,
+                               C.POINTER(C.c_uint64)], i),
+        "rq_render_whitted_device": ([vp, C.POINTER(WhittedParams), vp, vp, vp, vp, vp], i),
+        "rq_set_stage_events": ([vp, vp, i], i),
+        "rq_set_stats": ([vp, vp], i),
+        "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -78,12 +78,18 @@ __device__ __forceinline__ bool box_test(const Ray& r, float lx, float ly,
 
 struct Hit {
   float t;
-  int id;  // original triangle index, -1 = none
+  int id;   // original triangle index, -1 = none
+  int pos;  // triangle record index (leaf order) of the hit
   float u, v;
 };
 
+__device__ __forceinline__ float pick3(const float* a, int k) {
+  return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]);
+}
+
 // WaldTriangle::intersect scalar branch (WaldTriangle.cc:489-555) for one
-// ray, followed by RayPacket::hit (Interface/RayPacket.h:531-543).
+// ray, followed by RayPacket::hit (Interface/RayPacket.h:531-543).  The
+// projection axes are chosen with selects so the ray stays in registers.
 __device__ __forceinline__ bool wald_test(Ray& r, const float4 q0,
                                           const float4 q1, const float4 q2,
                                           Hit& h) {
@@ -91,8 +97,8 @@ __device__ __forceinline__ bool wald_test(Ray& r, const float4 q0,
   const int ku = (k == 2) ? 0 : k + 1;
   const int kv = (k == 0) ? 2 : k - 1;
   const float n_u = q0.x, n_v = q0.y, n_d = q0.z;
-  const float dk = r.d[k], dku = r.d[ku], dkv = r.d[kv];
-  const float ok = r.o[k], oku = r.o[ku], okv = r.o[kv];
+  const float dk = pick3(r.d, k), dku = pick3(r.d, ku), dkv = pick3(r.d, kv);
+  const float ok = pick3(r.o, k), oku = pick3(r.o, ku), okv = pick3(r.o, kv);
   const float nd0 = fadd(fadd(fmul(n_u, dku), fmul(n_v, dkv)), dk);
   const float nd = fdiv(1.f, nd0);
   const float f0 = fsub(n_d, fadd(fadd(ok, fmul(n_u, oku)), fmul(n_v, okv)));

@@ -1,0 +1,51 @@
+// Frame-level (wavefront) rendering on the device: parameters and buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rq_device.cuh"
+
+namespace rq {
+
+constexpr int kMaxLights = 16;
+
+enum FrameCounter { kCntQueue = 0, kCntWork = 1, kNumCounters = 4 };
+
+// Per-frame constants (passed by value as a kernel parameter).
+struct FrameParams {
+  float cam[12];  // eye, lookat-eye, u, v (PinholeCamera::setup basis)
+  int xres, yres;
+  int n_lights;
+  float lights[6 * kMaxLights];  // position xyz, colour rgb
+  float ambient[3];
+  float background[3];
+  const float* materials;  // device, 3 floats per material id
+};
+
+// Device buffers of one frame.  rgb/t/prim are outputs; pos, queue and the
+// counters are scratch.
+struct FrameBuffers {
+  float* rgb;       // 3 per pixel
+  float* t;         // primary hit distance per pixel
+  int32_t* prim;    // primary triangle id per pixel (-1 = miss)
+  int32_t* pos;     // scratch: triangle record index of the primary hit
+  int32_t* queue;   // scratch: compacted hit pixels
+  int32_t* counters;                 // scratch: kNumCounters ints
+  unsigned long long* shadow_rays_ptr;  // shadow rays sent this frame
+  // optional statistics (NULL = off): box tests and triangle tests of the
+  // primary rays, then of the shadow rays
+  unsigned long long* stats;
+};
+
+cudaError_t launch_whitted(const DevScene& S, const FrameParams& P,
+                           const FrameBuffers& B, int grid1, int grid2,
+                           cudaStream_t st, const cudaEvent_t* ev, int nev);
+int whitted_blocks_per_sm(int tri_kind, size_t smem);
+
+// PinholeCamera::setup (Model/Cameras/PinholeCamera.cc:167-198) on the host.
+void camera_basis(const float* eye, const float* lookat, const float* up,
+                  float hfov, float vfov, float* out12);
+
+}  // namespace rq

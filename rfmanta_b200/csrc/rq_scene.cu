@@ -61,6 +61,7 @@ Scene::~Scene() {
   if (d_idx) cudaFree(d_idx);
   if (d_face_mat) cudaFree(d_face_mat);
   if (d_counter) cudaFree(d_counter);
+  if (frame) destroy_frame(frame);
   staging.clear();
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -554,6 +555,25 @@ int rq_trace(rq_scene* s, int n, const float* org, const float* dir,
   }
   s->release(st);
   return rc;
+}
+
+int rq_set_stats(rq_scene* s, uint64_t* d_counters) {
+  if (!s) return fail(RQ_ERR_ARG, "NULL scene");
+  s->stats = reinterpret_cast<unsigned long long*>(d_counters);
+  return RQ_OK;
+}
+
+int rq_scene_build_seconds(const rq_scene* s, double* seconds) {
+  if (!s || !seconds) return fail(RQ_ERR_ARG, "NULL argument");
+  *seconds = s->last_build_seconds;
+  return RQ_OK;
+}
+
+int rq_set_stage_events(rq_scene* s, void* events, int n) {
+  if (!s || n < 0 || n > 8 || (n > 0 && !events)) return fail(RQ_ERR_ARG, "0..8 events");
+  s->n_stage_events = n;
+  for (int i = 0; i < n; ++i) s->stage_events[i] = static_cast<cudaEvent_t*>(events)[i];
+  return RQ_OK;
 }
 
 int rq_set_launch_config(rq_scene* s, int flags, const rq_launch_config* cfg) {

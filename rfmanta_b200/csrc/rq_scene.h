@@ -14,6 +14,9 @@
 
 namespace rq {
 
+struct FrameScratch;
+void destroy_frame(FrameScratch* f);
+
 // The reference DynBVH tree, field by field (Model/Groups/DynBVH.h:37-79).
 struct HostTree {
   std::vector<float> bounds;  // 6 per node: min xyz, max xyz
@@ -67,6 +70,13 @@ struct Scene {
 
   std::mutex mu;
   std::vector<std::unique_ptr<Staging>> staging;
+
+  FrameScratch* frame = nullptr;  // frame-path scratch (rq_frame.cu)
+  double last_build_seconds = 0;
+  unsigned long long* stats = nullptr;  // device counters, NULL = off
+  cudaEvent_t stage_events[8] = {};
+  int n_stage_events = 0;
+  std::mutex frame_mu;
 
   ~Scene();
   void free_tree();

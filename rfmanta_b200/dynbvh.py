@@ -202,6 +202,67 @@ class GpuDynBVH:
         return dict(block_threads=cfg.block_threads, blocks_per_sm=cfg.blocks_per_sm,
                     refill_threshold=cfg.refill_threshold, persistent=bool(cfg.persistent))
 
+    # -- frame path -----------------------------------------------------------
+    @staticmethod
+    def whitted_params(scene, materials=None) -> "_lib.WhittedParams":
+        """rq_whitted_params for a scenes.WhittedScene (arrays kept alive on
+        the returned object)."""
+        p = _lib.WhittedParams()
+        cam = scene.camera
+        p.eye[:] = cam.eye
+        p.lookat[:] = cam.lookat
+        p.up[:] = cam.up
+        p.hfov, p.vfov = cam.hfov, cam.vfov
+        p.xres, p.yres = scene.xres, scene.yres
+        lights = np.array([list(l.position) + list(l.color) for l in scene.lights],
+                          np.float32).reshape(-1, 6)
+        mats = np.ascontiguousarray(scene.mesh.materials if materials is None else materials,
+                                    np.float32)
+        p.n_lights = lights.shape[0]
+        p.lights = lights.ctypes.data
+        p.ambient[:] = scene.ambient
+        p.background[:] = scene.background
+        p.n_materials = mats.shape[0]
+        p.material_rgb = mats.ctypes.data
+        p._keep = (lights, mats)
+        return p
+
+    def render_whitted(self, scene):
+        """Raytracer::traceEyeRays over a whole frame; host outputs."""
+        p = self.whitted_params(scene)
+        npx = scene.xres * scene.yres
+        rgb = np.zeros((npx, 3), np.float32)
+        t = np.zeros(npx, np.float32)
+        prim = np.zeros(npx, np.int32)
+        ns = C.c_uint64()
+        check(lib.rq_render_whitted(self._h, C.byref(p), _p(rgb), _p(t), _p(prim), C.byref(ns)))
+        return dict(rgb=rgb, t=t, prim=prim, shadow_rays=int(ns.value))
+
+    def render_whitted_device(self, params, rgb_ptr: int, t_ptr: int, prim_ptr: int,
+                              shadow_ptr: int = 0, stream: int = 0) -> None:
+        check(lib.rq_render_whitted_device(self._h, C.byref(params), C.c_void_p(rgb_ptr),
+                                           C.c_void_p(t_ptr), C.c_void_p(prim_ptr),
+                                           C.c_void_p(shadow_ptr or None),
+                                           C.c_void_p(stream or None)))
+
+    def set_stage_events(self, events) -> None:
+        """events: list of torch.cuda.Event (created with timing enabled) or []."""
+        if not events:
+            check(lib.rq_set_stage_events(self._h, None, 0))
+            return
+        arr = (C.c_void_p * len(events))(*[e.cuda_event for e in events])
+        self._events_keep = (arr, events)
+        check(lib.rq_set_stage_events(self._h, arr, len(events)))
+
+    def set_stats(self, counters_ptr: int) -> None:
+        """Device uint64[4] receiving box/triangle test counts (0 = off)."""
+        check(lib.rq_set_stats(self._h, C.c_void_p(counters_ptr or None)))
+
+    def build_seconds(self) -> float:
+        s = C.c_double()
+        check(lib.rq_scene_build_seconds(self._h, C.byref(s)))
+        return s.value
+
     @property
     def handle(self) -> C.c_void_p:
         return self._h
@@ -216,6 +277,16 @@ class GpuDynBVH:
             self.close()
         except Exception:
             pass
+
+
+def camera_basis(cam) -> np.ndarray:
+    """PinholeCamera::setup basis (host-only C-ABI call)."""
+    e = np.asarray(cam.eye, np.float32)
+    la = np.asarray(cam.lookat, np.float32)
+    up = np.asarray(cam.up, np.float32)
+    out = np.zeros(12, np.float32)
+    check(lib.rq_camera_basis(_p(e), _p(la), _p(up), cam.hfov, cam.vfov, _p(out)))
+    return out
 
 
 __all__ = ["GpuDynBVH", "RayBatch", "RQ_TRI_WALD", "RQ_TRI_KS", "T_EPSILON", "MAXT"]

@@ -15,6 +15,8 @@ DynBVH::rebuild, and records what the reference computes:
     any-hit rays;
   * the Raytracer::traceEyeRays frame (RGB, primary t and triangle id) and
     the number of shadow rays HardShadows sent.
+It also records DynBVH::computeCost of the reference's own tree for a few
+larger seeded scenes (sah_costs.json), the bound for the GPU builder.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -85,5 +87,36 @@ def main() -> None:
         print(path, os.path.getsize(path), "bytes")
 
 
+def sah_scenes():
+    """Scenes whose reference SAH cost pins the GPU builder (2% bound)."""
+    out = {"small_frame": scenes.small_frame_scene().mesh,
+           "heightfield_256": scenes.merge(
+               [scenes.heightfield(256, 256, seed=21, extent=4.0, y=-1.1),
+                scenes.displaced_icosphere(4, seed=22, center=(0.5, 0.0, -0.5), radius=0.6)],
+               np.array([[0.5, 0.5, 0.5]], np.float32))}
+    rng = np.random.default_rng(23)
+    n = 20000
+    c = rng.uniform(-2, 2, (n, 1, 3))
+    tri = (c + rng.normal(scale=0.05, size=(n, 3, 3))).reshape(-1, 3).astype(np.float32)
+    out["random_soup"] = scenes.Mesh(tri, np.arange(3 * n, dtype=np.uint32).reshape(-1, 3),
+                                     np.zeros(n, np.uint32), np.ones((1, 3), np.float32))
+    return out
+
+
+def write_sah_costs() -> None:
+    import json
+    ref = Reference()
+    costs = {}
+    for name, mesh in sah_scenes().items():
+        rs = ref.scene(mesh, 0)
+        costs[name] = rs.sah_cost()
+        rs.close()
+    path = os.path.join(OUT, "sah_costs.json")
+    with open(path, "w") as f:
+        json.dump(costs, f, indent=1, sort_keys=True)
+    print(path, costs)
+
+
 if __name__ == "__main__":
     main()
+    write_sah_costs()

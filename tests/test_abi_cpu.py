@@ -44,3 +44,14 @@ def test_treeio_roundtrip(golden):
     t2 = parse_dynbvh_blob(write_dynbvh_blob(t))
     for f in ("bounds", "child", "children", "axis", "left_cheaper", "ids"):
         assert np.array_equal(getattr(t, f), getattr(t2, f))
+
+
+def test_camera_basis_matches_reference(golden):
+    """rq_camera_basis (host-only) equals the reference PinholeCamera basis."""
+    from rfmanta_b200.dynbvh import camera_basis
+    from rfmanta_b200.scenes import Camera
+    _, g = golden
+    c = g["cam"]
+    cam = Camera(tuple(c[0:3]), tuple(c[3:6]), tuple(c[6:9]), float(c[9]), float(c[10]))
+    assert np.array_equal(camera_basis(cam).view(np.uint32),
+                          g["camera_basis"].view(np.uint32))

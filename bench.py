@@ -237,6 +237,8 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
 
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    for e in ev:  # torch creates the CUDA event on first record
+        e.record(stream)
     pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
              for _ in range(args.steps)]
     stage = np.zeros((args.steps, 2))

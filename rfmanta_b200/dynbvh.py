@@ -246,7 +246,9 @@ class GpuDynBVH:
                                            C.c_void_p(stream or None)))
 
     def set_stage_events(self, events) -> None:
-        """events: list of torch.cuda.Event (created with timing enabled) or []."""
+        """events: list of torch.cuda.Event (created with timing enabled and
+        recorded at least once, which is when torch creates the CUDA event),
+        or []."""
         if not events:
             check(lib.rq_set_stage_events(self._h, None, 0))
             return

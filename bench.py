@@ -1,42 +1,49 @@
 """Benchmark of the ray-query path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload small_frame]
+                    [--workload path_frame|small_frame]
 
 Prints ONE JSON line (rank 0).  A step is one frame of the named workload:
 
-  small_frame  512x512, 1 spp pinhole primary rays + hard-shadow rays from
-               one point light over a displaced level-6 icosphere (81,920
-               triangles, seeded value noise, amplitude 0.05, frequency 4)
-               and a 2x2 ground grid of 20,000 triangles; Lambertian
-               shading; Wald triangles.  Rays per step = primary rays +
-               shadow rays actually sent (the reference culls back-facing
-               ones).
+  path_frame   (default) incoherent path tracing: 1280x720, 16 spp
+               stratified jitter, diffuse bounces to depth 4 with cosine
+               hemisphere sampling from per-path PCG32 streams, Russian
+               roulette from bounce 2, one parallelogram area light sampled
+               with a shadow ray at every bounce, over a 512x1024 fBm
+               heightfield (1,048,576 triangles) plus 32 displaced level-4
+               icospheres (163,840 triangles).  Rays per step = camera +
+               bounce rays + shadow rays traced.
+  small_frame  512x512, 1 spp primary + hard-shadow rays from one point
+               light over a displaced level-6 icosphere (81,920 triangles)
+               and a 2x2 ground grid of 20,000 triangles.
 
 value     Mrays/s with the scene and frame buffers resident in HBM, device
           time from CUDA events around each frame, L2 flushed (a 256 MiB
           write) before every timed frame; whole job = sum over ranks.
-e2e       Same metric through the host-buffer call rq_render_whitted (camera
-          parameters in, RGB + primary t + triangle id copied back every
-          frame), host wall clock per frame.
-roofline  The dominant stage kernel: algorithmic bytes per launch
-          (rays x (32 + 16|4 + 32 x box tests/ray + 48 x triangle tests/ray),
+e2e       Same metric through the host-buffer call (rq_render_path /
+          rq_render_whitted: parameters in, the image copied back to host
+          memory every frame), host wall clock per frame.
+roofline  The dominant kernel of the frame: algorithmic bytes (rays x
+          (32 + 16|4 + 32 x box tests per ray + 48 x triangle tests per ray),
           test counts from the library's statistics mode on the same frame)
-          over its CUDA-event duration, against the measured HBM copy peak.
+          over its CUDA-event time, against the measured HBM copy peak.
 cpu_baseline / --impl reference
-          The reference's own CPU renderer for the same frame
-          (Raytracer + DynBVH + WaldTriangle + Lambertian + HardShadows,
-          MANTA_SSE build, compiled from the reference sources into
-          oracle/_ref by oracle/ref.mk) on all host cores.
+          The reference's own CPU renderer on the same scene and camera
+          (KajiyaPathtracer or Raytracer, DynBVH, WaldTriangle, Lambertian,
+          HardShadows; MANTA_SSE build compiled from the reference sources
+          into oracle/_ref by oracle/ref.mk) on all host cores, on a bounded
+          sample of the frame.
 
 With --gpus N (torchrun) every rank renders the same frame on its own GPU:
-the path has no exchange step, so the ranks are independent replicas
-(weak scaling) and the only collectives are the timing barrier and the
-max-over-ranks reduction.
+the path has no exchange step, so ranks are independent replicas (weak
+scaling); the only collectives are the timing barrier and the max-over-ranks
+reduction.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
+import datetime
 import json
 import os
 import statistics
@@ -82,6 +89,7 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)
         except Exception:
             self.proc = None
         return self
@@ -127,70 +135,175 @@ def _dist():
     return world, rank, local
 
 
-def _workload(name):
-    from rfmanta_b200 import scenes
-    if name == "small_frame":
-        return scenes.small_frame_scene()
-    raise SystemExit(f"unknown workload {name}")
+# ------------------------------------------------------------- workloads ---
+
+class PathFrame:
+    name = "path_frame"
+
+    def __init__(self):
+        from rfmanta_b200 import scenes
+        self.sc = scenes.path_scene()
+
+    def config(self):
+        sc = self.sc
+        return {"workload": self.name, "resolution": [sc.xres, sc.yres], "spp": sc.spp,
+                "max_depth": sc.max_depth, "russian_roulette_from": sc.rr_depth,
+                "triangles": int(sc.mesh.n_tris), "lights": "1 parallelogram area light",
+                "triangle_kind": "wald", "tree": "gpu binned SAH",
+                "l2": "flushed before every timed frame (256 MiB write)"}
+
+    def setup(self, bvh, dev):
+        import torch
+        self.bvh = bvh
+        self.params = bvh.path_params(self.sc, chunk_paths=self.sc.xres * self.sc.yres * self.sc.spp)
+        npx = self.sc.xres * self.sc.yres
+        self.rgb = torch.empty(npx * 3, device=dev)
+        self.counts = torch.zeros(2, dtype=torch.int64, device=dev)
+        self.n_events = 2 + 2 * self.sc.max_depth
+        self.stage_names = []
+        for d in range(self.sc.max_depth):
+            self.stage_names += [f"path_extend_kernel[{d}]", f"path_shade_kernel[{d}]"]
+        self.stage_names.append("path_resolve_kernel")
+        self.launches = 1 + 3 * self.sc.max_depth + 1
+
+    def frame(self, stream_ptr):
+        self.bvh.render_path_device(self.params, self.rgb.data_ptr(), self.counts.data_ptr(),
+                                    stream_ptr)
+
+    def rays(self):
+        c = self.counts.cpu().numpy()
+        return int(c[0]), int(c[1])
+
+    def host_frame(self):
+        """One frame through the host-buffer call; returns bytes in/out."""
+        from rfmanta_b200 import _lib
+        sc = self.sc
+        if not hasattr(self, "_host_rgb"):
+            self._host_rgb = np.empty((sc.xres * sc.yres, 3), np.float32)
+            self._host_counts = (C.c_uint64 * 2)()
+        _lib.check(_lib.lib.rq_render_path(self.bvh.handle, C.byref(self.params),
+                                           self._host_rgb.ctypes.data, self._host_counts))
+        return C.sizeof(self.params), self._host_rgb.nbytes + 16
+
+    def roofline_bytes(self, stats, rays):
+        """Algorithmic bytes of the extend stage (all bounces) and of the
+        fused shade stage (its shadow rays)."""
+        ext, shadow = rays
+        b_e, t_e = stats[0] / max(ext, 1), stats[1] / max(ext, 1)
+        b_s, t_s = stats[2] / max(shadow, 1), stats[3] / max(shadow, 1)
+        per_ray = {"extension_box_tests": round(b_e, 3), "extension_tri_tests": round(t_e, 3),
+                   "shadow_box_tests": round(b_s, 3), "shadow_tri_tests": round(t_s, 3)}
+        return (ext * (32 + 16 + 32 * b_e + 48 * t_e),
+                shadow * (32 + 4 + 32 * b_s + 48 * t_s)), per_ray
+
+    def group_stages(self, stage_ms):
+        D = self.sc.max_depth
+        ext = sum(stage_ms[2 * d] for d in range(D))
+        shade = sum(stage_ms[2 * d + 1] for d in range(D))
+        return ["path_extend_kernel", "path_shade_kernel"], [ext, shade]
+
+    def cpu_reference(self, seconds_budget, threads):
+        """Reference KajiyaPathtracer on a 1 spp sample of the same frame."""
+        from dataclasses import replace
+        from oracle.pyoracle import Reference
+        sse = Reference.available(sse=True)
+        ref = Reference(sse=sse)
+        rs = ref.scene(self.sc.mesh, 0)
+        sample = replace(self.sc, spp=1)
+        frames, secs, rays = 0, 0.0, 0
+        while frames < 1 or secs < seconds_budget:
+            out = rs.render_path(sample, nthreads=threads)
+            secs += out["seconds"]
+            rays += out["rays"]
+            frames += 1
+        rs.close()
+        text = (f"{frames} frame(s) of {sample.xres}x{sample.yres} at 1 spp (1/{self.sc.spp} of "
+                f"a step), depth {sample.max_depth}, reference KajiyaPathtracer/DynBVH/"
+                f"WaldTriangle/Lambertian/HardShadows/AreaLight "
+                f"({'MANTA_SSE' if sse else 'scalar'} build), rays counted at DynBVH::intersect")
+        return rays / secs / 1e6, threads, text, secs
 
 
-def _workload_config(name, sc):
-    return {"workload": name, "resolution": [sc.xres, sc.yres], "spp": 1,
-            "triangles": int(sc.mesh.n_tris), "lights": len(sc.lights),
-            "triangle_kind": "wald", "tree": "gpu binned SAH",
-            "l2": "flushed before every timed frame (256 MiB write)"}
+class SmallFrame:
+    name = "small_frame"
+
+    def __init__(self):
+        from rfmanta_b200 import scenes
+        self.sc = scenes.small_frame_scene()
+
+    def config(self):
+        sc = self.sc
+        return {"workload": self.name, "resolution": [sc.xres, sc.yres], "spp": 1,
+                "triangles": int(sc.mesh.n_tris), "lights": len(sc.lights),
+                "triangle_kind": "wald", "tree": "gpu binned SAH",
+                "l2": "flushed before every timed frame (256 MiB write)"}
+
+    def setup(self, bvh, dev):
+        import torch
+        self.bvh = bvh
+        self.params = bvh.whitted_params(self.sc)
+        npx = self.sc.xres * self.sc.yres
+        self.rgb = torch.empty(npx * 3, device=dev)
+        self.t = torch.empty(npx, device=dev)
+        self.prim = torch.empty(npx, dtype=torch.int32, device=dev)
+        self.nshadow = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.n_events = 3
+        self.stage_names = ["whitted_primary_kernel", "whitted_shade_kernel"]
+        self.launches = 2
+
+    def frame(self, stream_ptr):
+        self.bvh.render_whitted_device(self.params, self.rgb.data_ptr(), self.t.data_ptr(),
+                                       self.prim.data_ptr(), self.nshadow.data_ptr(), stream_ptr)
+
+    def rays(self):
+        return self.sc.xres * self.sc.yres, int(self.nshadow.item())
+
+    def host_frame(self):
+        from rfmanta_b200 import _lib
+        npx = self.sc.xres * self.sc.yres
+        if not hasattr(self, "_h"):
+            self._h = (np.empty((npx, 3), np.float32), np.empty(npx, np.float32),
+                       np.empty(npx, np.int32), C.c_uint64())
+        rgb, t, p, ns = self._h
+        _lib.check(_lib.lib.rq_render_whitted(self.bvh.handle, C.byref(self.params),
+                                              rgb.ctypes.data, t.ctypes.data, p.ctypes.data,
+                                              C.byref(ns)))
+        return C.sizeof(self.params) + 24 * len(self.sc.lights), npx * 20 + 8
+
+    def roofline_bytes(self, stats, rays):
+        prim, shadow = rays
+        b_p, t_p = stats[0] / max(prim, 1), stats[1] / max(prim, 1)
+        b_s, t_s = stats[2] / max(shadow, 1), stats[3] / max(shadow, 1)
+        per_ray = {"primary_box_tests": round(b_p, 3), "primary_tri_tests": round(t_p, 3),
+                   "shadow_box_tests": round(b_s, 3), "shadow_tri_tests": round(t_s, 3)}
+        return (prim * (32 + 16 + 32 * b_p + 48 * t_p),
+                shadow * (32 + 4 + 32 * b_s + 48 * t_s)), per_ray
+
+    def group_stages(self, stage_ms):
+        return self.stage_names, [stage_ms[0], stage_ms[1]]
+
+    def cpu_reference(self, seconds_budget, threads):
+        from oracle.pyoracle import Reference
+        sse = Reference.available(sse=True)
+        ref = Reference(sse=sse)
+        rs = ref.scene(self.sc.mesh, 0)
+        frames, secs, rays = 0, 0.0, 0
+        while frames < 1 or secs < seconds_budget:
+            out = rs.render(self.sc, nthreads=threads, want_ids=False)
+            secs += out["seconds"]
+            rays += self.sc.xres * self.sc.yres + out["shadow_rays"]
+            frames += 1
+        rs.close()
+        text = (f"{frames} full {self.sc.xres}x{self.sc.yres} frame(s), reference Raytracer/"
+                f"DynBVH/WaldTriangle/Lambertian/HardShadows "
+                f"({'MANTA_SSE' if sse else 'scalar'} build)")
+        return rays / secs / 1e6, threads, text, secs
 
 
-def reference_frames(sc, seconds_budget: float, threads: int):
-    """The reference's CPU renderer on the same frame, repeated within a
-    time budget.  Returns (Mrays/s, frames, threads, kind, sample text)."""
-    from oracle.pyoracle import Reference
-    sse = Reference.available(sse=True)
-    ref = Reference(sse=sse)
-    rs = ref.scene(sc.mesh, 0)
-    frames, secs, rays = 0, 0.0, 0
-    while frames < 1 or secs < seconds_budget:
-        out = rs.render(sc, nthreads=threads, want_ids=False)
-        secs += out["seconds"]
-        rays += sc.xres * sc.yres + out["shadow_rays"]
-        frames += 1
-    rs.close()
-    kind = "reference"
-    sample = (f"{frames} full {sc.xres}x{sc.yres} frame(s), reference Raytracer/DynBVH/"
-              f"WaldTriangle/Lambertian/HardShadows ({'MANTA_SSE' if sse else 'scalar'} build)")
-    return rays / secs / 1e6, frames, threads, kind, sample, secs
+WORKLOADS = {"path_frame": PathFrame, "small_frame": SmallFrame}
 
 
-def run_reference(args):
-    world, rank, _ = _dist()
-    if rank != 0:
-        return
-    sc = _workload(args.workload)
-    threads = os.cpu_count() or 1
-    from oracle.pyoracle import Reference
-    if not Reference.available():
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "oracle/_ref/libmanta_ref.so was not built (needs the reference sources)"}))
-        return
-    per_step = []
-    for k in range(args.warmup + args.steps):
-        v, frames, threads, kind, sample, secs = reference_frames(sc, 0.0, threads)
-        if k >= args.warmup:
-            per_step.append((v, secs))
-    value = statistics.median([p[0] for p in per_step])
-    ms = statistics.median([p[1] for p in per_step]) * 1e3
-    print(json.dumps({
-        "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded scene generators)", "impl": "reference",
-        "config": _workload_config(args.workload, sc),
-        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads,
-                         "kind": kind, "sample": f"one frame per step: {sample}"},
-        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-    }))
-
+# ----------------------------------------------------------------- runs ----
 
 def run_ours(args):
     import torch
@@ -199,49 +312,39 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", init_method="env://",
-                                timeout=__import__("datetime").timedelta(seconds=120))
+                                timeout=datetime.timedelta(seconds=120))
     from rfmanta_b200.dynbvh import GpuDynBVH
-    sc = _workload(args.workload)
+    wl = WORKLOADS[args.workload]()
+    dev = torch.device("cuda", local)
     bvh = GpuDynBVH(tri_kind=0, device=local)
-    bvh.setGroup(sc.mesh)
+    bvh.setGroup(wl.sc.mesh)
     bvh.rebuild()
     build_s = bvh.build_seconds()
-    params = bvh.whitted_params(sc)
-    npx = sc.xres * sc.yres
-    dev = torch.device("cuda", local)
-    rgb = torch.empty(npx * 3, device=dev)
-    tbuf = torch.empty(npx, device=dev)
-    prim = torch.empty(npx, dtype=torch.int32, device=dev)
-    nshadow = torch.zeros(1, dtype=torch.int64, device=dev)
+    wl.setup(bvh, dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
 
-    def frame():
-        bvh.render_whitted_device(params, rgb.data_ptr(), tbuf.data_ptr(), prim.data_ptr(),
-                                  nshadow.data_ptr(), sptr)
-
     # statistics frame (untimed): box / triangle tests per ray
     stats = torch.zeros(4, dtype=torch.int64, device=dev)
     bvh.set_stats(stats.data_ptr())
-    frame()
+    wl.frame(sptr)
     torch.cuda.synchronize(dev)
     bvh.set_stats(0)
     st = stats.cpu().numpy().astype(np.float64)
-    n_shadow = int(nshadow.item())
-    boxes_p, tris_p = st[0] / npx, st[1] / npx
-    boxes_s, tris_s = st[2] / max(n_shadow, 1), st[3] / max(n_shadow, 1)
+    rays = wl.rays()
+    rays_per_step = sum(rays)
 
     for _ in range(args.warmup):
-        frame()
+        wl.frame(sptr)
     torch.cuda.synchronize(dev)
 
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(wl.n_events)]
     for e in ev:  # torch creates the CUDA event on first record
         e.record(stream)
     pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
              for _ in range(args.steps)]
-    stage = np.zeros((args.steps, 2))
+    stage = np.zeros((args.steps, wl.n_events - 1))
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -250,11 +353,11 @@ def run_ours(args):
         for k in range(args.steps):
             flush.fill_(k & 0xff)
             pairs[k][0].record(stream)
-            frame()
+            wl.frame(sptr)
             pairs[k][1].record(stream)
             torch.cuda.synchronize(dev)
-            stage[k, 0] = ev[0].elapsed_time(ev[1])
-            stage[k, 1] = ev[1].elapsed_time(ev[2])
+            for j in range(wl.n_events - 1):
+                stage[k, j] = ev[j].elapsed_time(ev[j + 1])
         bvh.set_stage_events([])
         torch.cuda.synchronize(dev)
     if world > 1:
@@ -264,42 +367,31 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
     total_ms = float(t_max.item())
-    rays_per_step = npx + n_shadow
     value = rays_per_step * args.steps * world / (total_ms * 1e-3) / 1e6
 
-    # e2e through the host-buffer public call
-    out_rgb = np.empty((npx, 3), np.float32)
-    e2e_times = []
-    from rfmanta_b200 import _lib
-    import ctypes as C
-    t_host = np.empty(npx, np.float32)
-    p_host = np.empty(npx, np.int32)
-    ns = C.c_uint64()
+    # end to end through the host-buffer public call
+    e2e = []
+    bin_ = bout = 0
     for k in range(args.warmup + args.steps):
         flush.fill_(k & 0xff)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        _lib.check(_lib.lib.rq_render_whitted(bvh.handle, C.byref(params),
-                                              out_rgb.ctypes.data, t_host.ctypes.data,
-                                              p_host.ctypes.data, C.byref(ns)))
+        bin_, bout = wl.host_frame()
         t1 = time.perf_counter()
         if k >= args.warmup:
-            e2e_times.append(t1 - t0)
-    e2e_secs = sum(e2e_times)
-    e2e_t = torch.tensor([e2e_secs], dtype=torch.float64, device=dev)
+            e2e.append(t1 - t0)
+    e2e_t = torch.tensor([sum(e2e)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = rays_per_step * args.steps * world / float(e2e_t.item()) / 1e6
 
-    # roofline of the dominant stage
+    # roofline of the dominant kernel
     hbm, peak_kind = _peaks()
     mean_stage = stage.mean(axis=0)
-    bytes_primary = npx * (32 + 16 + 32 * boxes_p + 48 * tris_p)
-    bytes_shadow = n_shadow * (32 + 4 + 32 * boxes_s + 48 * tris_s)
-    dom = int(np.argmax(mean_stage))
-    alg = [bytes_primary, bytes_shadow][dom]
-    achieved = alg / (mean_stage[dom] * 1e-3) / 1e9
-    names = ["whitted_primary_kernel", "whitted_shade_kernel"]
+    names, kms = wl.group_stages(mean_stage)
+    alg, per_ray = wl.roofline_bytes(st, rays)
+    dom = int(np.argmax(kms))
+    achieved = alg[dom] / (kms[dom] * 1e-3) / 1e9
 
     if rank == 0:
         line = {
@@ -308,45 +400,71 @@ def run_ours(args):
             "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene generators)",
-            "config": dict(_workload_config(args.workload, sc), parallelism=f"replicas x{world}",
-                           rays_per_step=rays_per_step, shadow_rays=n_shadow,
+            "config": dict(wl.config(), parallelism=f"replicas x{world}",
+                           rays_per_step=rays_per_step, rays_split=list(rays),
                            build_ms=round(build_s * 1e3, 2)),
             "clocks": clk.summary(),
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
-                    "h2d_bytes_per_step": int(C.sizeof(params) + 4 * 6 * len(sc.lights)),
-                    "d2h_bytes_per_step": int(npx * 20 + 8)},
-            "gpu_launches": 2 * args.steps,
+                    "h2d_bytes_per_step": int(bin_), "d2h_bytes_per_step": int(bout)},
+            "gpu_launches": wl.launches * args.steps,
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1),
                          "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": None,
-                         "stage_ms": [round(x, 4) for x in mean_stage],
-                         "per_ray": {"primary_box_tests": round(boxes_p, 3),
-                                     "primary_tri_tests": round(tris_p, 3),
-                                     "shadow_box_tests": round(boxes_s, 3),
-                                     "shadow_tri_tests": round(tris_s, 3)}},
+                         "kernel_ms_per_step": {n: round(v, 4) for n, v in zip(names, kms)},
+                         "per_ray": per_ray},
         }
         if not args.no_cpu_baseline:
-            v, frames, threads, kind, sample, secs = reference_frames(sc, args.cpu_seconds,
-                                                                      os.cpu_count() or 1)
+            v, threads, text, _ = wl.cpu_reference(args.cpu_seconds, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mrays/s", "cores": threads,
-                                    "kind": kind, "sample": sample}
+                                    "kind": "reference", "sample": text}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    from oracle.pyoracle import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libmanta_ref.so was not built (needs the reference sources)"}))
+        return
+    wl = WORKLOADS[args.workload]()
+    threads = os.cpu_count() or 1
+    per_step = []
+    text = ""
+    for k in range(args.warmup + args.steps):
+        v, threads, text, secs = wl.cpu_reference(0.0, threads)
+        if k >= args.warmup:
+            per_step.append((v, secs))
+    value = statistics.median([p[0] for p in per_step])
+    ms = statistics.median([p[1] for p in per_step]) * 1e3
+    print(json.dumps({
+        "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene generators)", "impl": "reference",
+        "config": wl.config(),
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads,
+                         "kind": "reference", "sample": f"one sample per step: {text}"},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="small_frame")
-    ap.add_argument("--cpu-seconds", type=float, default=5.0)
+    ap.add_argument("--workload", default="path_frame", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -197,10 +197,57 @@ RQ_API int rq_render_whitted_device(rq_scene* scene, const rq_whitted_params* pa
                                     uint64_t* d_shadow_rays, void* stream);
 
 /*
+ * Path-traced frame: KajiyaPathtracer::traceEyeRays
+ * (Engine/Renderers/KajiyaPathtracer.cc:113-302) with Lambertian materials,
+ * one parallelogram AreaLight sampled with HardShadows shadow rays, cosine
+ * hemisphere bounces and Russian roulette, run as a device wavefront with
+ * stream compaction.  Each path draws from its own PCG32 stream keyed by
+ * (seed, pixel * spp + sample), so results do not depend on batching.
+ */
+typedef struct {
+  float eye[3], lookat[3], up[3]; /* PinholeCamera */
+  float hfov, vfov;
+  int xres, yres;
+  int spp;                        /* 1, 4, 16, ... (stratified jitter) */
+  int max_depth;                  /* bounces, primary hit = depth 0 */
+  int rr_depth;                   /* Russian roulette from this depth on */
+  uint64_t seed;
+  float light_anchor[3];          /* Parallelogram anchor, v1, v2 */
+  float light_v1[3];
+  float light_v2[3];
+  float light_color[3];
+  float background[3];
+  int n_materials;
+  const float* material_rgb;      /* host: n_materials x (r, g, b) */
+  int chunk_paths;                /* paths per wavefront pass, 0 = 4Mi */
+} rq_path_params;
+
+/* Renders into HOST rgb (3 per pixel); ray_counts[0] = camera + bounce rays
+ * traced, ray_counts[1] = shadow rays traced (may be NULL). */
+RQ_API int rq_render_path(rq_scene* scene, const rq_path_params* params,
+                          float* rgb, uint64_t* ray_counts);
+
+/* Same into DEVICE rgb on `stream`, counts into d_ray_counts (2 x uint64,
+ * device, may be NULL); returns without synchronising. */
+RQ_API int rq_render_path_device(rq_scene* scene, const rq_path_params* params,
+                                 float* d_rgb, uint64_t* d_ray_counts,
+                                 void* stream);
+
+/* Parity aid: when d_prim is set, the next path-traced frames write, per
+ * bounce and path, the ray (d_org / d_dir: [3][max_depth][capacity]) and the
+ * triangle it hit (d_prim: [max_depth][capacity], untouched for paths that
+ * already ended).  capacity_paths must cover xres*yres*spp.  NULL turns it off. */
+RQ_API int rq_set_path_debug(rq_scene* scene, int32_t* d_prim, float* d_org,
+                             float* d_dir, int64_t capacity_paths);
+
+/*
  * Profiling hook (the role of DynBVH's COLLECT_STATS counters,
  * Model/Groups/DynBVH.h:314-374): when `events` (n cudaEvent_t handles
- * created by the caller) is set, the frame paths record events[0] before
- * their first stage and events[k] after stage k.  NULL turns it off.
+ * created by the caller, up to 16) is set, the frame paths record events[0]
+ * before their first stage and events[k] after stage k: Whitted frames have
+ * two stages (primary, shade); path-traced frames record, for their last
+ * chunk, extend and shade of every bounce (events[1 + 2d], events[2 + 2d])
+ * and the resolve after them.  NULL turns it off.
  */
 RQ_API int rq_set_stage_events(rq_scene* scene, void* events, int n);
 

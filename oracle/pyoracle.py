@@ -92,6 +92,49 @@ class Restatement:
                                          [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                           C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5)
         L.orq_render_whitted.restype = C.c_longlong
+        L.orq_sincos_2pi.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.orq_render_path.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 7 +
+                                      [C.c_uint64, C.c_longlong, C.c_longlong] +
+                                      [C.c_void_p] * 3)
+
+    def sincos_2pi(self, u):
+        u = np.ascontiguousarray(u, np.float32)
+        c = np.zeros_like(u)
+        s = np.zeros_like(u)
+        self.lib.orq_sincos_2pi(_ptr(u), u.shape[0], _ptr(c), _ptr(s))
+        return c, s
+
+    def render_path(self, tree, scene, tri_kind=0, paths=None, debug=False):
+        """Path-traced frame (restatement of the device wavefront).  Returns
+        per-path radiance for paths [p0, p1), the pixel image when all paths
+        are traced, ray counts and optionally per-bounce hit ids."""
+        mesh = scene.mesh
+        keep, args = self._scene_args(tree, mesh, tri_kind, None)
+        basis = self.camera_basis(scene.camera)
+        L = scene.light
+        fp = np.concatenate([basis, np.asarray(L.anchor, np.float32),
+                             np.asarray(L.v1, np.float32), np.asarray(L.v2, np.float32),
+                             np.asarray(L.color, np.float32),
+                             np.asarray(scene.background, np.float32)]).astype(np.float32)
+        ip = np.array([scene.xres, scene.yres, scene.spp, scene.max_depth, scene.rr_depth],
+                      np.int32)
+        total = scene.xres * scene.yres * scene.spp
+        p0, p1 = paths if paths else (0, total)
+        rad = np.zeros((p1 - p0, 3), np.float32)
+        counts = np.zeros(2, np.int64)
+        dbg = np.full((scene.max_depth, total), -2, np.int32) if debug else None
+        fm = np.ascontiguousarray(mesh.face_material, np.uint32)
+        mats = np.ascontiguousarray(mesh.materials, np.float32)
+        self.lib.orq_render_path(*args, _ptr(fm), _ptr(mats), _ptr(fp), _ptr(ip),
+                                 int(scene.seed), p0, p1, _ptr(rad), _ptr(counts), _ptr(dbg))
+        out = dict(rad=rad, rays=int(counts[0]), shadow_rays=int(counts[1]), prim=dbg)
+        if paths is None:
+            r = rad.reshape(-1, scene.spp, 3)
+            acc = np.zeros((r.shape[0], 3), np.float32)
+            for s_ in range(scene.spp):
+                acc = (acc + r[:, s_]).astype(np.float32)
+            out["rgb"] = (acc * np.float32(np.float32(1.0) / np.float32(scene.spp))).astype(np.float32)
+        return out
 
     def wald_setup(self, mesh) -> np.ndarray:
         v = np.ascontiguousarray(mesh.vertices, np.float32)
@@ -218,6 +261,9 @@ class Reference:
         L.mref_render.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] +
                                   [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 5)
         L.mref_node_size.restype = C.c_int
+        L.mref_render_path.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                        C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_uint,
+                                        C.c_void_p, C.c_void_p, C.c_void_p])
 
     @staticmethod
     def available(sse: bool = False) -> bool:
@@ -306,3 +352,19 @@ class RefScene:
                                  len(scene.lights), _ptr(amb), _ptr(bg), nthreads, _ptr(rgb),
                                  _ptr(tp), _ptr(pr), C.byref(secs), C.byref(nsr))
         return dict(rgb=rgb, t=tp, prim=pr, seconds=secs.value, shadow_rays=nsr.value)
+
+    def render_path(self, scene, nthreads=1):
+        """KajiyaPathtracer frame (reference defaults) over this scene."""
+        cam = scene.camera
+        args = np.array(list(cam.eye) + list(cam.lookat) + list(cam.up) +
+                        [cam.hfov, cam.vfov], np.float32)
+        L = scene.light
+        light = np.array(list(L.anchor) + list(L.v1) + list(L.v2) + list(L.color), np.float32)
+        bg = np.asarray(scene.background, np.float32)
+        rgb = np.zeros((scene.xres * scene.yres, 3), np.float32)
+        secs = C.c_double()
+        rays = C.c_longlong()
+        self.ref.lib.mref_render_path(self.h, scene.xres, scene.yres, _ptr(args), scene.spp,
+                                      scene.max_depth, _ptr(light), _ptr(bg), nthreads,
+                                      int(scene.seed), _ptr(rgb), C.byref(secs), C.byref(rays))
+        return dict(rgb=rgb, seconds=secs.value, rays=rays.value)

@@ -67,11 +67,15 @@ MODEL_SRC := \
   Model/Lights/PointLight.cc \
   Model/AmbientLights/ConstantAmbient.cc \
   Model/Backgrounds/ConstantBackground.cc \
-  Model/Cameras/PinholeCamera.cc
+  Model/Cameras/PinholeCamera.cc \
+  Model/Lights/AreaLight.cc Model/Primitives/Parallelogram.cc \
+  Model/Primitives/PrimitiveCommon.cc Model/TexCoordMappers/UniformMapper.cc
 
 ENGINE_SRC := \
   Engine/Shadows/HardShadows.cc Engine/Renderers/Raytracer.cc \
-  Engine/SampleGenerators/ConstantSampleGenerator.cc
+  Engine/SampleGenerators/ConstantSampleGenerator.cc \
+  Engine/SampleGenerators/UniformRandomGenerator.cc \
+  Engine/Renderers/KajiyaPathtracer.cc Engine/Shadows/NoDirect.cc
 
 SRC := $(CORE_SRC) $(IFACE_SRC) $(MODEL_SRC) $(ENGINE_SRC)
 

@@ -27,7 +27,12 @@
 #include <Core/Color/RGBColor.h>
 #include <Core/Geometry/BBox.h>
 #include <Core/Geometry/Vector.h>
+#include <Core/Math/CheapRNG.h>
+#include <Engine/Renderers/KajiyaPathtracer.h>
 #include <Engine/Renderers/Raytracer.h>
+#include <Engine/SampleGenerators/UniformRandomGenerator.h>
+#include <Model/Lights/AreaLight.h>
+#include <Model/Primitives/Parallelogram.h>
 #include <Engine/SampleGenerators/ConstantSampleGenerator.h>
 #include <Engine/Shadows/HardShadows.h>
 #include <Interface/Context.h>
@@ -60,7 +65,19 @@ namespace {
 // reference DynBVH (DynBVH.h:88-89, DynBVH.cc:3389-3416).
 class ExposedBVH : public DynBVH {
 public:
-  ExposedBVH() : DynBVH(false) {}
+  ExposedBVH() : DynBVH(false), ray_counters(0) {}
+  // When set, counts the unmasked rays of every intersect call per worker
+  // (counters[16 * proc]) before handing the packet to DynBVH::intersect.
+  long long* ray_counters;
+  void intersect(const RenderContext& context, RayPacket& rays) const {
+    if (ray_counters) {
+      long long n = 0;
+      for (int i = rays.begin(); i < rays.end(); ++i)
+        if (!rays.rayIsMasked(i)) ++n;
+      ray_counters[16 * context.proc] += n;
+    }
+    DynBVH::intersect(context, rays);
+  }
   const std::vector<BVHNode>& treeNodes() const { return nodes; }
   const std::vector<int>& treeIds() const { return object_ids; }
   float sahCost() { return computeCost<true>(0); }
@@ -432,6 +449,150 @@ int mref_render(void* h, int xres, int yres, const float* cam12_args,
   for (int p = 0; p < nthreads; ++p) total += job.shadow_rays[p];
   if (seconds) *seconds = t1 - t0;
   if (shadow_rays) *shadow_rays = total;
+  return 0;
+}
+
+struct PathJob {
+  RefScene* s;
+  KajiyaPathtracer* renderer;
+  ExposedCamera* camera;
+  int xres, yres, spp;
+  float xscale, yscale, xoff, yoff;
+  float* rgb;
+  volatile int next_row;
+  pthread_mutex_t lock;
+  int nthreads;
+  unsigned seed;
+};
+
+struct PathArg {
+  PathJob* job;
+  int proc;
+};
+
+static void* path_worker(void* p) {
+  PathArg* a = static_cast<PathArg*>(p);
+  PathJob* j = a->job;
+  HardShadows shadows(false);
+  CheapRNG rng;
+  rng.seed(j->seed + 7919u * (unsigned)a->proc);
+  UniformRandomGenerator sampler;
+  RenderContext ctx(0, 0, a->proc, j->nthreads, 0, 0, 0, j->renderer, &shadows, j->camera,
+                    j->s->scene, 0, &rng, &sampler);
+  int strata = 1;
+  while (strata * strata < j->spp) ++strata;
+  for (;;) {
+    pthread_mutex_lock(&j->lock);
+    int y = j->next_row++;
+    pthread_mutex_unlock(&j->lock);
+    if (y >= j->yres) break;
+    for (int x0 = 0; x0 < j->xres; x0 += RayPacket::MaxSize) {
+      int cnt = j->xres - x0 < RayPacket::MaxSize ? j->xres - x0 : (int)RayPacket::MaxSize;
+      float acc[3][RayPacket::MaxSize];
+      memset(acc, 0, sizeof(acc));
+      for (int sidx = 0; sidx < j->spp; ++sidx) {
+        RayPacketData data;
+        RayPacket rays(data, RayPacket::UnknownShape, 0, cnt, 0,
+                       RayPacket::HaveImageCoordinates | RayPacket::ConstantEye);
+        const int sx = sidx % strata, sy = sidx / strata;
+        for (int i = 0; i < cnt; ++i) {
+          // stratified jitter inside the pixel
+          float jx = j->spp > 1 ? (sx + rng.nextFloat()) / strata : 0.5f;
+          float jy = j->spp > 1 ? (sy + rng.nextFloat()) / strata : 0.5f;
+          rays.setPixel(i, 0, (x0 + i + jx) * j->xscale + j->xoff, (y + jy) * j->yscale + j->yoff);
+        }
+        j->renderer->traceEyeRays(ctx, rays);
+        for (int i = 0; i < cnt; ++i) {
+          Color c = rays.getColor(i);
+          for (int k = 0; k < 3; ++k) acc[k][i] += c[k];
+        }
+      }
+      for (int i = 0; i < cnt; ++i) {
+        size_t pix = (size_t)y * j->xres + x0 + i;
+        for (int k = 0; k < 3; ++k) j->rgb[3 * pix + k] = acc[k][i] / j->spp;
+      }
+    }
+  }
+  return 0;
+}
+
+// Path-traced frame through KajiyaPathtracer::traceEyeRays
+// (Engine/Renderers/KajiyaPathtracer.cc:113-302) with its default modes,
+// HardShadows and one Parallelogram AreaLight; rows of 64-ray packets on N
+// pthreads, spp stratified-jitter packets per pixel row segment.  *rays =
+// every unmasked ray handed to DynBVH::intersect (camera, bounce, shadow).
+int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
+                     int max_depth, const float* light12, const float* background,
+                     int nthreads, unsigned seed, float* rgb, double* seconds,
+                     long long* rays) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  char buf[16][32];
+  std::vector<std::string> args;
+  const char* names[3] = {"-eye", "-lookat", "-up"};
+  for (int k = 0; k < 3; ++k) {
+    args.push_back(names[k]);
+    for (int i = 0; i < 3; ++i) {
+      snprintf(buf[3 * k + i], 32, "%.9g", cam11[3 * k + i]);
+      args.push_back(buf[3 * k + i]);
+    }
+  }
+  args.push_back("-hfov"); snprintf(buf[9], 32, "%.9g", cam11[9]); args.push_back(buf[9]);
+  args.push_back("-vfov"); snprintf(buf[10], 32, "%.9g", cam11[10]); args.push_back(buf[10]);
+  args.push_back("-normalizeRays");
+  ExposedCamera camera(args);
+  LightSet* ls = new LightSet();
+  ls->setAmbientLight(new ConstantAmbient(Color(RGB(0, 0, 0))));
+  Parallelogram* emitter = new Parallelogram(s->materials[0],
+      Vector(light12[0], light12[1], light12[2]), Vector(light12[3], light12[4], light12[5]),
+      Vector(light12[6], light12[7], light12[8]));
+  ls->add(new AreaLight(emitter, Color(RGB(light12[9], light12[10], light12[11]))));
+  PreprocessContext pctx;
+  pctx.globalLights = ls;
+  for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
+  if (!s->scene) s->scene = new Scene();
+  s->scene->setObject(s->bvh);
+  s->scene->setBackground(new ConstantBackground(
+      Color(RGB(background[0], background[1], background[2]))));
+  s->scene->setLights(ls);
+  s->scene->getRenderParameters().maxDepth = max_depth;
+  std::vector<std::string> none;
+  KajiyaPathtracer renderer(none);
+  std::vector<long long> counters(16 * nthreads, 0);
+  s->bvh->ray_counters = &counters[0];
+  PathJob job;
+  job.s = s;
+  job.renderer = &renderer;
+  job.camera = &camera;
+  job.xres = xres;
+  job.yres = yres;
+  job.spp = spp;
+  job.xscale = (Real)2 / xres;
+  job.yscale = (Real)2 / yres;
+  job.xoff = (-xres / (Real)2) * job.xscale;
+  job.yoff = (-yres / (Real)2) * job.yscale;
+  job.rgb = rgb;
+  job.next_row = 0;
+  job.nthreads = nthreads;
+  job.seed = seed;
+  pthread_mutex_init(&job.lock, 0);
+  std::vector<pthread_t> th(nthreads);
+  std::vector<PathArg> ar(nthreads);
+  double t0 = now_s();
+  for (int p = 0; p < nthreads; ++p) {
+    ar[p].job = &job;
+    ar[p].proc = p;
+    pthread_create(&th[p], 0, path_worker, &ar[p]);
+  }
+  for (int p = 0; p < nthreads; ++p) pthread_join(th[p], 0);
+  double t1 = now_s();
+  pthread_mutex_destroy(&job.lock);
+  s->bvh->ray_counters = 0;
+  long long total = 0;
+  for (int p = 0; p < nthreads; ++p) total += counters[16 * p];
+  if (seconds) *seconds = t1 - t0;
+  if (rays) *rays = total;
   return 0;
 }
 

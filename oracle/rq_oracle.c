@@ -596,3 +596,224 @@ long long orq_render_whitted(const float* bounds, const int* child,
   }
   return shadow_rays;
 }
+
+/* ------------------------------------------------------ path tracing --- */
+/* Restatement of the device path-tracing wavefront (rfmanta_b200/csrc/
+ * rq_path.cu), which follows KajiyaPathtracer::traceEyeRays
+ * (Engine/Renderers/KajiyaPathtracer.cc:113-302), Lambertian::sampleBSDF
+ * (Model/Materials/Lambertian.cc:248-280), AreaLight::computeLight
+ * (Model/Lights/AreaLight.cc:25-54) with Parallelogram::getRandomPoints
+ * (Model/Primitives/Parallelogram.cc:569-614), HardShadows' cull and
+ * russian_roulette_full (KajiyaPathtracer.cc:389-478), one path at a time.
+ * Random numbers: PCG32 (O'Neill 2014); sin/cos: quadrant reduction of
+ * 2*pi*u plus Taylor polynomials, evaluated with the same separately
+ * rounded float operations as the device. */
+
+typedef struct {
+  uint64_t state, inc;
+} Pcg32;
+
+static uint32_t pcg_next(Pcg32* g) {
+  uint64_t old = g->state;
+  g->state = old * 6364136223846793005ULL + g->inc;
+  uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+  uint32_t rot = (uint32_t)(old >> 59u);
+  return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+
+static void pcg_seed(Pcg32* g, uint64_t initstate, uint64_t initseq) {
+  g->state = 0u;
+  g->inc = (initseq << 1u) | 1u;
+  pcg_next(g);
+  g->state += initstate;
+  pcg_next(g);
+}
+
+static float pcg_float(Pcg32* g) {
+  return (float)(pcg_next(g) >> 8) * (1.0f / 16777216.0f);
+}
+
+static void sincos_2pi(float u, float* c, float* s) {
+  const float u4 = u * 4.f;
+  const float qf = floorf(u4);
+  const int q = (int)qf & 3;
+  const float f = u4 - qf;
+  const float y = f * 1.57079632679489662f;
+  const float y2 = y * y;
+  float ps = 1.f - y2 * (1.f / 110.f);
+  ps = 1.f - (y2 * (1.f / 72.f)) * ps;
+  ps = 1.f - (y2 * (1.f / 42.f)) * ps;
+  ps = 1.f - (y2 * (1.f / 20.f)) * ps;
+  ps = 1.f - (y2 * (1.f / 6.f)) * ps;
+  const float sy = y * ps;
+  float pc = 1.f - y2 * (1.f / 132.f);
+  pc = 1.f - (y2 * (1.f / 90.f)) * pc;
+  pc = 1.f - (y2 * (1.f / 56.f)) * pc;
+  pc = 1.f - (y2 * (1.f / 30.f)) * pc;
+  pc = 1.f - (y2 * (1.f / 12.f)) * pc;
+  const float cy = 1.f - (y2 * 0.5f) * pc;
+  switch (q) {
+    case 0: *c = cy; *s = sy; break;
+    case 1: *c = -sy; *s = cy; break;
+    case 2: *c = -cy; *s = -sy; break;
+    default: *c = sy; *s = -cy; break;
+  }
+}
+
+void orq_sincos_2pi(const float* u, int n, float* c, float* s) {
+  for (int i = 0; i < n; ++i) sincos_2pi(u[i], &c[i], &s[i]);
+}
+
+/* params (float): cam[12], light_anchor[3], light_v1[3], light_v2[3],
+ * light_color[3], background[3]; iparams: xres, yres, spp, max_depth,
+ * rr_depth.  Writes rgb per pixel, ray counts[2] (extension, shadow), and
+ * optionally prim[max_depth][n_paths] (-2 where a path had ended). */
+void orq_render_path(const float* bounds, const int* child, const int* children,
+                     const unsigned char* axis, const unsigned char* left_cheaper,
+                     const int* ids, int tri_kind, const float* verts,
+                     const unsigned* idx, const float* wald, const unsigned* face_mat,
+                     const float* mat_rgb, const float* fp, const int* ip,
+                     unsigned long long seed, long long p0, long long p1, float* rad_out,
+                     long long* counts, int* dbg_prim) {
+  Tree T = {bounds, child, children, axis, left_cheaper, ids,
+            tri_kind, verts, idx, wald};
+  const float* cam = fp;
+  const float* la = fp + 12;
+  const float* lv1 = fp + 15;
+  const float* lv2 = fp + 18;
+  const float* lcol = fp + 21;
+  const float* bg = fp + 24;
+  const int xres = ip[0], yres = ip[1], spp = ip[2], maxd = ip[3], rrd = ip[4];
+  int strata = 1;
+  while (strata * strata < spp) ++strata;
+  const long long npaths = (long long)xres * yres * spp;
+  /* Parallelogram (Parallelogram.cc:26-35) */
+  float ln[3];
+  v_cross(lv1, lv2, ln);
+  const float ll = sqrtf(ln[0] * ln[0] + ln[1] * ln[1] + ln[2] * ln[2]);
+  const float lsc = 1 / ll;
+  for (int c = 0; c < 3; ++c) ln[c] = ln[c] * lsc;
+  const float inv_area = (float)1 / ll;
+  const float xscale = 2.f / (float)xres, yscale = 2.f / (float)yres;
+  const float xo = ((float)(-xres) / 2.f) * xscale, yo = ((float)(-yres) / 2.f) * yscale;
+  for (long long g = p0; g < p1; ++g) {
+    Pcg32 rng;
+    pcg_seed(&rng, seed ^ ((unsigned long long)g * 0x9E3779B97F4A7C15ULL),
+             (unsigned long long)g);
+    const long long pix = g / spp;
+    const int s = (int)(g - pix * spp);
+    const int x = (int)(pix % xres), y = (int)(pix / xres);
+    float jx = 0.5f, jy = 0.5f;
+    if (spp > 1) {
+      const int sx = s % strata, sy = s / strata;
+      jx = ((float)sx + pcg_float(&rng)) / (float)strata;
+      jy = ((float)sy + pcg_float(&rng)) / (float)strata;
+    }
+    const float px = ((float)x + jx) * xscale + xo;
+    const float py = ((float)y + jy) * yscale + yo;
+    Ray r;
+    float d[3];
+    for (int c = 0; c < 3; ++c) {
+      r.o[c] = cam[c];
+      d[c] = cam[9 + c] * px + cam[6 + c] * py + cam[3 + c];
+    }
+    v_normalize(d);
+    for (int c = 0; c < 3; ++c) r.d[c] = d[c];
+    float imp[3] = {1.f, 1.f, 1.f}, rad[3] = {0.f, 0.f, 0.f};
+    for (int depth = 0; depth < maxd; ++depth) {
+      for (int c = 0; c < 3; ++c) r.inv[c] = (float)1 / r.d[c];
+      r.minT = MAXT;
+      r.hit = 0;
+      r.prim = -1;
+      r.anyhit = 0;
+      visit(&T, 0, &r);
+      counts[0]++;
+      if (dbg_prim) dbg_prim[(size_t)depth * npaths + g] = r.hit ? r.prim : -1;
+      if (!r.hit) {
+        for (int c = 0; c < 3; ++c) rad[c] = rad[c] + bg[c] * imp[c];
+        break;
+      }
+      float hp[3], ng[3], ffn[3];
+      for (int c = 0; c < 3; ++c) hp[c] = r.o[c] + r.d[c] * r.minT;
+      tri_normal(&T, r.prim, ng);
+      const float dn = ng[0] * r.d[0] + ng[1] * r.d[1] + ng[2] * r.d[2];
+      for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0.f) ? ng[c] : -ng[c];
+      const float r1 = pcg_float(&rng);
+      const float r2 = pcg_float(&rng);
+      const float sintheta = sqrtf(r1);
+      const float costheta = sqrtf(1.f - r1);
+      float cph, sph;
+      sincos_2pi(r2, &cph, &sph);
+      const float cosphi = cph * sintheta;
+      const float sinphi = sph * sintheta;
+      float v1[3];
+      {
+        const float d2 = ffn[2] * ffn[2];
+        const float d1 = ffn[1] * ffn[1];
+        if (d2 + d1 < 1e-4f) {
+          v1[0] = -ffn[2];
+          v1[1] = 0.f;
+          v1[2] = ffn[0];
+        } else {
+          v1[0] = 0.f;
+          v1[1] = ffn[2];
+          v1[2] = -ffn[1];
+        }
+        v_normalize(v1);
+      }
+      float v2[3];
+      v_cross(v1, ffn, v2);
+      float nd[3];
+      for (int c = 0; c < 3; ++c) nd[c] = ffn[c] * costheta + v1[c] * cosphi + v2[c] * sinphi;
+      const float* kd = mat_rgb + 3 * face_mat[r.prim];
+      for (int c = 0; c < 3; ++c) imp[c] = imp[c] * kd[c];
+      const float lr1 = pcg_float(&rng);
+      const float lr2 = pcg_float(&rng);
+      float ld[3];
+      for (int c = 0; c < 3; ++c) ld[c] = (la[c] + lr1 * lv1[c] + lr2 * lv2[c]) - hp[c];
+      const float len = sqrtf(ld[0] * ld[0] + ld[1] * ld[1] + ld[2] * ld[2]);
+      {
+        const float sc = 1.f / len;
+        for (int c = 0; c < 3; ++c) ld[c] = ld[c] * sc;
+      }
+      const float cosine = -(ld[0] * ln[0] + ld[1] * ln[1] + ld[2] * ln[2]);
+      if (cosine > 0.f && ld[0] * ffn[0] + ld[1] * ffn[1] + ld[2] * ffn[2] > 0.f) {
+        Ray sr;
+        for (int c = 0; c < 3; ++c) {
+          sr.o[c] = hp[c];
+          sr.d[c] = ld[c];
+          sr.inv[c] = (float)1 / ld[c];
+        }
+        sr.minT = len - T_EPSILON;
+        sr.hit = 0;
+        sr.prim = -1;
+        sr.anyhit = 1;
+        counts[1]++;
+        visit(&T, 0, &sr);
+        if (!sr.hit) {
+          const float solid_pdf = inv_area * (len * len);
+          const float f = cosine / solid_pdf;
+          const float sum = ld[0] * ld[0] + ld[1] * ld[1] + ld[2] * ld[2];
+          const float sc = 1.f / sqrtf(sum);
+          float ldn[3];
+          for (int c = 0; c < 3; ++c) ldn[c] = ld[c] * sc;
+          const float w = ffn[0] * ldn[0] + ffn[1] * ldn[1] + ffn[2] * ldn[2];
+          for (int c = 0; c < 3; ++c) rad[c] = rad[c] + (imp[c] * (f * lcol[c])) * w;
+        }
+      }
+      if (depth + 1 >= maxd) break;
+      if (depth >= rrd && depth != maxd - 1) {
+        const float rr = pcg_float(&rng);
+        const float mx = fmaxf(fmaxf(kd[0], kd[1]), kd[2]);
+        if (rr > mx) break;
+        const float sc = 1.f / mx;
+        for (int c = 0; c < 3; ++c) imp[c] = imp[c] * sc;
+      }
+      for (int c = 0; c < 3; ++c) {
+        r.o[c] = hp[c];
+        r.d[c] = nd[c];
+      }
+    }
+    for (int c = 0; c < 3; ++c) rad_out[3 * (g - p0) + c] = rad[c];
+  }
+}

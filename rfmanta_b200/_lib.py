@@ -51,6 +51,17 @@ class WhittedParams(C.Structure):
                 ("material_rgb", C.c_void_p)]
 
 
+class PathParams(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("lookat", C.c_float * 3), ("up", C.c_float * 3),
+                ("hfov", C.c_float), ("vfov", C.c_float), ("xres", C.c_int), ("yres", C.c_int),
+                ("spp", C.c_int), ("max_depth", C.c_int), ("rr_depth", C.c_int),
+                ("seed", C.c_uint64), ("light_anchor", C.c_float * 3),
+                ("light_v1", C.c_float * 3), ("light_v2", C.c_float * 3),
+                ("light_color", C.c_float * 3), ("background", C.c_float * 3),
+                ("n_materials", C.c_int), ("material_rgb", C.c_void_p),
+                ("chunk_paths", C.c_int)]
+
+
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
                 ("refill_threshold", C.c_int), ("persistent", C.c_int)]
@@ -84,6 +95,9 @@ def _load():
         "rq_render_whitted_device": ([vp, C.POINTER(WhittedParams), vp, vp, vp, vp, vp], i),
         "rq_set_stage_events": ([vp, vp, i], i),
         "rq_set_stats": ([vp, vp], i),
+        "rq_render_path": ([vp, C.POINTER(PathParams), vp, vp], i),
+        "rq_render_path_device": ([vp, C.POINTER(PathParams), vp, vp, vp], i),
+        "rq_set_path_debug": ([vp, vp, vp, vp, C.c_int64], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
     }
     for name, (args, res) in sig.items():

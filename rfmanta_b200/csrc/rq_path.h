@@ -1,0 +1,56 @@
+// Path-tracing wavefront: parameters and buffers (see rq_path.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rq_device.cuh"
+
+namespace rq {
+
+constexpr int kMaxPathDepth = 16;
+constexpr int kPathCounters = kMaxPathDepth + 2;
+
+struct PathParams {
+  float cam[12];  // eye, lookat-eye, u, v
+  int xres, yres;
+  int spp, strata;  // strata * strata == spp
+  int max_depth;    // bounces (primary hit = depth 0)
+  int rr_depth;     // Russian roulette from this depth on
+  unsigned long long seed;
+  float light_anchor[3], light_v1[3], light_v2[3];
+  float light_normal[3];  // Parallelogram: unit Cross(v1, v2)
+  float light_inv_area;   // 1 / |Cross(v1, v2)|
+  float light_color[3];
+  float background[3];
+  const float* materials;  // device, rgb per material id
+};
+
+struct PathBuffers {
+  size_t capacity;      // paths per chunk
+  long long g0;         // global id of the chunk's first path
+  float* o;             // 3 * capacity
+  float* d;
+  float* imp;
+  float* rad;
+  unsigned long long* rng;  // PCG32 state per path
+  float* t;
+  int32_t* pos;
+  int32_t* prim;
+  int32_t* queue[2];
+  int32_t* counters;            // kPathCounters: live paths per depth
+  unsigned long long* ray_counts;  // [0] extension rays, [1] shadow rays
+  unsigned long long* stats;       // optional box/tri test counters (4)
+  // optional per-bounce dump for parity checks: [depth][path]
+  int32_t* dbg_prim;
+  float* dbg_org;  // [3][depth][path]
+  float* dbg_dir;
+};
+
+cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffers B,
+                              long long g0, int n, float* rgb, int grid, cudaStream_t st,
+                              const cudaEvent_t* ev, int nev);
+int path_blocks_per_sm(int tri_kind, size_t smem);
+
+}  // namespace rq

@@ -62,6 +62,7 @@ Scene::~Scene() {
   if (d_face_mat) cudaFree(d_face_mat);
   if (d_counter) cudaFree(d_counter);
   if (frame) destroy_frame(frame);
+  if (paths) destroy_path_scratch(paths);
   staging.clear();
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -570,7 +571,7 @@ int rq_scene_build_seconds(const rq_scene* s, double* seconds) {
 }
 
 int rq_set_stage_events(rq_scene* s, void* events, int n) {
-  if (!s || n < 0 || n > 8 || (n > 0 && !events)) return fail(RQ_ERR_ARG, "0..8 events");
+  if (!s || n < 0 || n > 16 || (n > 0 && !events)) return fail(RQ_ERR_ARG, "0..16 events");
   s->n_stage_events = n;
   for (int i = 0; i < n; ++i) s->stage_events[i] = static_cast<cudaEvent_t*>(events)[i];
   return RQ_OK;

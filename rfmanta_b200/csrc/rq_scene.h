@@ -16,6 +16,8 @@ namespace rq {
 
 struct FrameScratch;
 void destroy_frame(FrameScratch* f);
+struct PathScratch;
+void destroy_path_scratch(PathScratch* p);
 
 // The reference DynBVH tree, field by field (Model/Groups/DynBVH.h:37-79).
 struct HostTree {
@@ -72,9 +74,14 @@ struct Scene {
   std::vector<std::unique_ptr<Staging>> staging;
 
   FrameScratch* frame = nullptr;  // frame-path scratch (rq_frame.cu)
+  PathScratch* paths = nullptr;   // path-tracing scratch (rq_pathhost.cu)
+  int32_t* path_dbg_prim = nullptr;
+  float* path_dbg_org = nullptr;
+  float* path_dbg_dir = nullptr;
+  long long path_dbg_capacity = 0;
   double last_build_seconds = 0;
   unsigned long long* stats = nullptr;  // device counters, NULL = off
-  cudaEvent_t stage_events[8] = {};
+  cudaEvent_t stage_events[16] = {};
   int n_stage_events = 0;
   std::mutex frame_mu;
 

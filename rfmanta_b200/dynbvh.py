@@ -256,6 +256,49 @@ class GpuDynBVH:
         self._events_keep = (arr, events)
         check(lib.rq_set_stage_events(self._h, arr, len(events)))
 
+    @staticmethod
+    def path_params(scene, chunk_paths: int = 0) -> "_lib.PathParams":
+        """rq_path_params for a scenes.PathScene."""
+        p = _lib.PathParams()
+        cam = scene.camera
+        p.eye[:] = cam.eye
+        p.lookat[:] = cam.lookat
+        p.up[:] = cam.up
+        p.hfov, p.vfov = cam.hfov, cam.vfov
+        p.xres, p.yres, p.spp = scene.xres, scene.yres, scene.spp
+        p.max_depth, p.rr_depth, p.seed = scene.max_depth, scene.rr_depth, scene.seed
+        L = scene.light
+        p.light_anchor[:] = L.anchor
+        p.light_v1[:] = L.v1
+        p.light_v2[:] = L.v2
+        p.light_color[:] = L.color
+        p.background[:] = scene.background
+        mats = np.ascontiguousarray(scene.mesh.materials, np.float32)
+        p.n_materials = mats.shape[0]
+        p.material_rgb = mats.ctypes.data
+        p.chunk_paths = chunk_paths
+        p._keep = (mats,)
+        return p
+
+    def render_path(self, scene, chunk_paths: int = 0):
+        """KajiyaPathtracer frame; host outputs (rgb per pixel, ray counts)."""
+        p = self.path_params(scene, chunk_paths)
+        rgb = np.zeros((scene.xres * scene.yres, 3), np.float32)
+        counts = (C.c_uint64 * 2)()
+        check(lib.rq_render_path(self._h, C.byref(p), _p(rgb), counts))
+        return dict(rgb=rgb, rays=int(counts[0]), shadow_rays=int(counts[1]))
+
+    def render_path_device(self, params, rgb_ptr: int, counts_ptr: int = 0,
+                           stream: int = 0) -> None:
+        check(lib.rq_render_path_device(self._h, C.byref(params), C.c_void_p(rgb_ptr),
+                                        C.c_void_p(counts_ptr or None),
+                                        C.c_void_p(stream or None)))
+
+    def set_path_debug(self, prim_ptr: int, org_ptr: int, dir_ptr: int, capacity: int) -> None:
+        check(lib.rq_set_path_debug(self._h, C.c_void_p(prim_ptr or None),
+                                    C.c_void_p(org_ptr or None), C.c_void_p(dir_ptr or None),
+                                    capacity))
+
     def set_stats(self, counters_ptr: int) -> None:
         """Device uint64[4] receiving box/triangle test counts (0 = off)."""
         check(lib.rq_set_stats(self._h, C.c_void_p(counters_ptr or None)))

@@ -267,3 +267,62 @@ def random_rays(n: int, lo: np.ndarray, hi: np.ndarray, seed: int,
     return (np.ascontiguousarray(o.T.astype(np.float32)),
             np.ascontiguousarray(d.T.astype(np.float32)),
             tmax.astype(np.float32), anyhit)
+
+
+@dataclass
+class AreaLightSpec:
+    """Parallelogram emitter: anchor + u*v1 + w*v2, u, w in [0, 1)."""
+
+    anchor: tuple
+    v1: tuple
+    v2: tuple
+    color: tuple
+
+
+@dataclass
+class PathScene:
+    mesh: Mesh
+    camera: Camera
+    light: AreaLightSpec
+    background: tuple
+    xres: int
+    yres: int
+    spp: int
+    max_depth: int
+    rr_depth: int
+    seed: int = 1
+
+
+def path_scene(hf_nx: int = 512, hf_nz: int = 1024, n_spheres: int = 32,
+               sphere_level: int = 4, xres: int = 1280, yres: int = 720, spp: int = 16,
+               max_depth: int = 4, rr_depth: int = 2, seed: int = 17) -> PathScene:
+    """Incoherent path-tracing frame: an hf_nx x hf_nz fBm heightfield
+    (2*hf_nx*hf_nz triangles, 5 octaves, amplitude 0.2) plus n_spheres
+    displaced icospheres at seeded positions on it, one parallelogram area
+    light above, diffuse bounces to max_depth with Russian roulette from
+    rr_depth on.  Defaults: 1280x720, 16 spp, depth 4, RR after bounce 2,
+    1,048,576 + 32 x 5,120 = 1,212,416 triangles."""
+    rng = np.random.default_rng(seed)
+    ext = 8.0
+    parts = [heightfield(hf_nx, hf_nz, seed=seed + 1, extent=ext, y=0.0, material=0)]
+    for k in range(n_spheres):
+        c = (float(rng.uniform(-3.0, 3.0)), float(rng.uniform(0.3, 0.7)),
+             float(rng.uniform(-3.0, 3.0)))
+        parts.append(displaced_icosphere(sphere_level, seed=seed + 10 + k, center=c,
+                                         radius=float(rng.uniform(0.25, 0.5)),
+                                         material=1 + (k % 3)))
+    mats = np.array([[0.7, 0.7, 0.65], [0.8, 0.3, 0.2], [0.2, 0.6, 0.3],
+                     [0.3, 0.4, 0.8]], np.float32)
+    mesh = merge(parts, mats)
+    cam = Camera((0.0, 3.5, 7.5), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 60.0,
+                 float(2.0 * np.degrees(np.arctan(np.tan(np.radians(30.0)) * yres / xres))))
+    light = AreaLightSpec((-1.0, 5.0, -1.0), (2.0, 0.0, 0.0), (0.0, 0.0, 2.0),
+                          (30.0, 28.0, 25.0))
+    return PathScene(mesh, cam, light, (0.15, 0.2, 0.3), xres, yres, spp, max_depth,
+                     rr_depth, seed)
+
+
+def tiny_path_scene(xres: int = 40, yres: int = 30, spp: int = 4) -> PathScene:
+    """The path-tracing layout scaled down for committed checks."""
+    return path_scene(hf_nx=16, hf_nz=16, n_spheres=3, sphere_level=2, xres=xres,
+                      yres=yres, spp=spp, max_depth=4, rr_depth=2, seed=5)

@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmanta_ref.so")
 REF_SSE_SO = os.path.join(HERE, "_ref", "libmanta_ref_sse.so")
+DROPIN_SO = os.path.join(HERE, "_ref", "libmanta_dropin.so")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
@@ -240,8 +241,8 @@ class Restatement:
 class Reference:
     """The reference's own classes (oracle/_ref), through ref_harness.cc."""
 
-    def __init__(self, sse: bool = False):
-        path = REF_SSE_SO if sse else REF_SO
+    def __init__(self, sse: bool = False, path: str | None = None):
+        path = path or (REF_SSE_SO if sse else REF_SO)
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.lib = C.CDLL(path)
@@ -261,6 +262,8 @@ class Reference:
         L.mref_render.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] +
                                   [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 5)
         L.mref_node_size.restype = C.c_int
+        if hasattr(L, "mref_scene_use_gpu"):
+            L.mref_scene_use_gpu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_char_p]
         L.mref_render_path.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                         C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_uint,
                                         C.c_void_p, C.c_void_p, C.c_void_p])
@@ -294,6 +297,13 @@ class RefScene:
                                            _ptr(fm), _ptr(mats), mats.shape[0], tri_kind)
         if not self.h:
             raise RuntimeError("reference scene build failed")
+
+    def use_gpu(self, device=0, tri_kind=0, tree_file=None):
+        """Drop-in library only: trace with rfmanta_b200's GpuDynBVH."""
+        rc = self.ref.lib.mref_scene_use_gpu(self.h, device, tri_kind,
+                                             tree_file.encode() if tree_file else None)
+        if rc != 0:
+            raise RuntimeError(f"mref_scene_use_gpu failed ({rc})")
 
     def close(self):
         if self.h:

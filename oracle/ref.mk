@@ -86,6 +86,11 @@ OBJ_SSE   := $(patsubst %.cc,$(OUT)/obj_sse/%.o,$(SRC))
 
 all: $(OUT)/libmanta_ref.so $(OUT)/libmanta_ref_sse.so
 
+# The same checker with this project's C++ drop-in (rfmanta_b200/manta/
+# GpuDynBVH) compiled against the reference headers and linked to the CUDA
+# library: the reference's renderers running on the device path.
+dropin: $(OUT)/libmanta_dropin.so
+
 # ---- generated config headers (one set per SSE variant) -------------------
 define GEN_HEADERS
 $(OUT)/gen_$(1)/include/.stamp: $(wildcard $(REF)/include/*Template)
@@ -143,10 +148,23 @@ $(OUT)/obj_sse/harness.o: $(HERE)ref_harness.cc $(OUT)/gen_sse/include/.stamp
 	@mkdir -p $(dir $@)
 	$(CXX) $(COMMON_FLAGS) -msse4.1 $(INC_SSE) -c $< -o $@
 
+REPO := $(abspath $(HERE)..)
+
+$(OUT)/obj_nosse/harness_dropin.o: $(HERE)ref_harness.cc $(OUT)/gen_nosse/include/.stamp
+	@mkdir -p $(dir $@)
+	$(CXX) $(COMMON_FLAGS) -DMREF_DROPIN $(INC_NOSSE) -I$(REPO) -c $< -o $@
+
+$(OUT)/obj_nosse/GpuDynBVH.o: $(REPO)/rfmanta_b200/manta/GpuDynBVH.cc $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(OUT)/gen_nosse/include/.stamp
+	@mkdir -p $(dir $@)
+	$(CXX) $(COMMON_FLAGS) $(INC_NOSSE) -I$(REPO) -c $< -o $@
+
+$(OUT)/libmanta_dropin.so: $(OBJ_NOSSE) $(OUT)/obj_nosse/harness_dropin.o $(OUT)/obj_nosse/GpuDynBVH.o $(REPO)/rfmanta_b200/librfmanta_b200.so
+	$(CXX) -shared -pthread -o $@ $(OBJ_NOSSE) $(OUT)/obj_nosse/harness_dropin.o $(OUT)/obj_nosse/GpuDynBVH.o -L$(REPO)/rfmanta_b200 -lrfmanta_b200 -Wl,-rpath,'$$ORIGIN/../../rfmanta_b200' -Wl,--no-as-needed -lstdc++ -lm
+
 $(OUT)/libmanta_ref.so: $(OBJ_NOSSE) $(OUT)/obj_nosse/harness.o
 	$(CXX) -shared -pthread -o $@ $^ -Wl,--no-as-needed -lstdc++ -lm
 
 $(OUT)/libmanta_ref_sse.so: $(OBJ_SSE) $(OUT)/obj_sse/harness.o
 	$(CXX) -shared -pthread -o $@ $^ -Wl,--no-as-needed -lstdc++ -lm
 
-.PHONY: all
+.PHONY: all dropin

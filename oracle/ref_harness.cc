@@ -50,6 +50,10 @@
 #include <Model/Primitives/MeshTriangle.h>
 #include <Model/Primitives/WaldTriangle.h>
 
+#ifdef MREF_DROPIN
+#include <rfmanta_b200/manta/GpuDynBVH.h>
+#endif
+
 #include <pthread.h>
 #include <stdio.h>
 #include <string.h>
@@ -123,6 +127,7 @@ public:
 struct RefScene {
   Mesh* mesh;
   ExposedBVH* bvh;
+  Object* object;  // what rays are traced against: bvh, or a drop-in
   std::vector<Material*> materials;
   LightSet* lights;
   Scene* scene;
@@ -173,6 +178,7 @@ void* mref_scene_create(const float* verts, int nverts, const unsigned* idx,
     s->bvh = new ExposedBVH();
     s->bvh->setGroup(m);
     s->bvh->rebuild(0, 1);
+    s->object = s->bvh;
     return s;
   } catch (...) {
     return 0;
@@ -262,7 +268,7 @@ int mref_intersect(void* h, int n, const float* org, const float* dir,
                   Vector(dir[r], dir[n + r], dir[2 * n + r]));
       rays.resetHit(i, tmax[r]);
     }
-    s->bvh->intersect(ctx, rays);
+    s->object->intersect(ctx, rays);
     for (int i = 0; i < cnt; ++i) {
       int r = base + i;
       hit[r] = rays.wasHit(i) ? 1 : 0;
@@ -409,7 +415,7 @@ int mref_render(void* h, int xres, int yres, const float* cam12_args,
   pctx.globalLights = ls;
   for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
   if (!s->scene) s->scene = new Scene();
-  s->scene->setObject(s->bvh);
+  s->scene->setObject(s->object);
   s->scene->setBackground(new ConstantBackground(
       Color(RGB(background[0], background[1], background[2]))));
   s->scene->setLights(ls);
@@ -552,7 +558,7 @@ int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
   pctx.globalLights = ls;
   for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
   if (!s->scene) s->scene = new Scene();
-  s->scene->setObject(s->bvh);
+  s->scene->setObject(s->object);
   s->scene->setBackground(new ConstantBackground(
       Color(RGB(background[0], background[1], background[2]))));
   s->scene->setLights(ls);
@@ -595,5 +601,31 @@ int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
   if (rays) *rays = total;
   return 0;
 }
+
+#ifdef MREF_DROPIN
+// Swaps the scene's DynBVH for the GPU drop-in (rfmanta_b200/manta/
+// GpuDynBVH), so the reference's own Raytracer, Lambertian and HardShadows
+// run unchanged on top of it.  tree_file NULL: the drop-in builds its own
+// tree (GpuDynBVH::rebuild); else the reference tree is written there with
+// DynBVH::saveToFile and read back with GpuDynBVH::buildFromFile.
+int mref_scene_use_gpu(void* h, int device, int tri_kind, const char* tree_file) {
+  RefScene* s = static_cast<RefScene*>(h);
+  try {
+    GpuDynBVH* g = new GpuDynBVH(device, tri_kind);
+    g->setGroup(s->mesh);
+    if (tree_file) {
+      if (!s->bvh->saveToFile(std::string(tree_file))) return 2;
+      if (!g->buildFromFile(std::string(tree_file))) return 3;
+    } else {
+      g->rebuild(0, 1);
+    }
+    s->object = g;
+  } catch (Exception& e) {
+    fprintf(stderr, "mref_scene_use_gpu: %s\n", e.message());
+    return 1;
+  }
+  return 0;
+}
+#endif
 
 }  // extern "C"

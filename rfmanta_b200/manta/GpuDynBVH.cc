@@ -1,0 +1,156 @@
+// GpuDynBVH: see GpuDynBVH.h.
+#include "GpuDynBVH.h"
+
+#include <Core/Color/Color.h>
+#include <Core/Exceptions/InternalError.h>
+#include <Core/Geometry/BBox.h>
+#include <Interface/Context.h>
+#include <Interface/Material.h>
+#include <Interface/TexCoordMapper.h>
+#include <Model/Groups/Mesh.h>
+#include <Model/Primitives/MeshTriangle.h>
+#include <Model/Primitives/WaldTriangle.h>
+
+#include <fstream>
+#include <vector>
+
+using namespace Manta;
+
+GpuDynBVH::GpuDynBVH(int device_, int tri_kind_)
+    : group(0), mesh(0), scene(0), device(device_), tri_kind(tri_kind_), dirty(false) {}
+
+GpuDynBVH::~GpuDynBVH() {
+  if (scene) rq_scene_destroy(scene);
+}
+
+void GpuDynBVH::check(int rc, const char* what) const {
+  if (rc != RQ_OK)
+    throw InternalError(std::string("rfmanta_b200 ") + what + ": " + rq_last_error());
+}
+
+void GpuDynBVH::setGroup(Group* g) {
+  if (g != group) dirty = true;
+  group = g;
+  mesh = dynamic_cast<Mesh*>(g);
+}
+
+void GpuDynBVH::groupDirty() { dirty = true; }
+
+Group* GpuDynBVH::getGroup() const { return group; }
+
+void GpuDynBVH::addToUpdateGraph(ObjectUpdateGraph* graph, ObjectUpdateGraphNode* parent) {
+  (void)graph;
+  (void)parent;
+}
+
+Interpolable::InterpErr GpuDynBVH::parallelInterpolate(const std::vector<keyframe_t>& keyframes, int proc,
+                                         int numProc) {
+  return group->parallelInterpolate(keyframes, proc, numProc);
+}
+
+// Mesh::vertices / vertex_indices / face_material (Model/Groups/Mesh.h:27-50).
+void GpuDynBVH::upload() {
+  if (!mesh) throw InternalError("GpuDynBVH needs a Mesh group");
+  if (scene) {
+    rq_scene_destroy(scene);
+    scene = 0;
+  }
+  const size_t nv = mesh->vertices.size();
+  std::vector<float> v(3 * nv);
+  for (size_t i = 0; i < nv; ++i)
+    for (int c = 0; c < 3; ++c) v[3 * i + c] = mesh->vertices[i][c];
+  const int nt = (int)(mesh->vertex_indices.size() / 3);
+  check(rq_scene_create(&v[0], (int)nv, &mesh->vertex_indices[0], nt,
+                        mesh->face_material.empty() ? 0 : &mesh->face_material[0], tri_kind,
+                        device, &scene),
+        "scene upload");
+  dirty = false;
+}
+
+void GpuDynBVH::preprocess(const PreprocessContext& context) {
+  if (group) group->preprocess(context);
+  if (context.proc == 0 && (dirty || !scene)) rebuild(0, 1);
+  context.done();
+}
+
+void GpuDynBVH::rebuild(int proc, int numProcs) {
+  (void)numProcs;
+  if (proc != 0) return;
+  upload();
+  check(rq_scene_build(scene, 0), "build");
+}
+
+bool GpuDynBVH::buildFromFile(const std::string& file) {
+  std::ifstream in(file.c_str(), std::ios::binary);
+  if (!in) return false;
+  std::vector<char> blob((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  upload();
+  check(rq_scene_import_dynbvh(scene, blob.empty() ? 0 : &blob[0], blob.size()), "import");
+  return true;
+}
+
+bool GpuDynBVH::saveToFile(const std::string& file) {
+  if (!scene) return false;
+  size_t n = 0;
+  check(rq_scene_export_dynbvh(scene, 0, &n), "export");
+  std::vector<char> blob(n);
+  check(rq_scene_export_dynbvh(scene, &blob[0], &n), "export");
+  std::ofstream out(file.c_str(), std::ios::binary);
+  if (!out) return false;
+  out.write(&blob[0], (std::streamsize)n);
+  return true;
+}
+
+void GpuDynBVH::computeBounds(const PreprocessContext& context, BBox& bbox) const {
+  group->computeBounds(context, bbox);
+}
+
+// DynBVH::intersect (Model/Groups/DynBVH.cc:101-404) for one packet: the
+// unmasked (and, for AnyHit, not yet hit) rays go to the device; hits come
+// back through RayPacket::hit with the real MeshTriangle, its material and
+// the scratchpad pair; occluded AnyHit rays are then treated as the
+// reference's opaque shadower path does (hit kept, minT = T_EPSILON).
+void GpuDynBVH::intersect(const RenderContext& context, RayPacket& rays) const {
+  const bool any = rays.getFlag(RayPacket::AnyHit);
+  const int MS = RayPacket::MaxSize;
+  int map[MS];
+  float org[3 * MS], dir[3 * MS], tmax[MS], t[MS], u[MS], v[MS];
+  int prim[MS];
+  int n = 0;
+  for (int i = rays.begin(); i < rays.end(); ++i) {
+    if (rays.rayIsMasked(i)) continue;
+    if (any && rays.wasHit(i)) continue;
+    map[n++] = i;
+  }
+  if (n == 0) return;
+  for (int k = 0; k < n; ++k) {
+    const int i = map[k];
+    for (int c = 0; c < 3; ++c) {
+      org[c * n + k] = rays.getOrigin(i, c);
+      dir[c * n + k] = rays.getDirection(i, c);
+    }
+    tmax[k] = rays.getMinT(i);
+  }
+  check(rq_trace(scene, n, org, dir, tmax, any ? RQ_ANYHIT : RQ_CLOSEST, t, prim, u, v),
+        "trace");
+  for (int k = 0; k < n; ++k) {
+    if (prim[k] < 0) continue;
+    const int i = map[k];
+    const MeshTriangle* tri = mesh->get(prim[k]);
+    const Material* matl = mesh->materials[mesh->face_material[prim[k]]];
+    const TexCoordMapper* tex = dynamic_cast<const TexCoordMapper*>(tri);
+    const Real oldT = rays.getMinT(i);
+    if (rays.hit(i, t[k], matl, tri, tex)) {
+      rays.getScratchpad<Real>(WaldTriangle::SCRATCH_U)[i] = u[k];
+      rays.getScratchpad<Real>(WaldTriangle::SCRATCH_V)[i] = v[k];
+      if (any) {
+        RayPacket one(rays, i, i + 1);
+        matl->attenuateShadows(context, one);
+        if (one.getColor(i) != Color::black())
+          rays.resetHit(i, oldT);
+        else
+          rays.overrideMinT(i, T_EPSILON);
+      }
+    }
+  }
+}

@@ -197,6 +197,26 @@ RQ_API int rq_render_whitted_device(rq_scene* scene, const rq_whitted_params* pa
                                     uint64_t* d_shadow_rays, void* stream);
 
 /*
+ * rq_render_whitted_device without any device allocation.  This entry point
+ * has no counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: a process whose device memory is already handed out to another
+ * allocator, or a render thread that must not make calls which can
+ * synchronise the whole device.  The frame's scratch (hit record per pixel,
+ * compaction queue, counters, material table) lives in a fixed array inside
+ * the library, so the call allocates nothing; the caller still passes the
+ * outputs.  Limits: xres * yres <= 1,048,576 pixels and n_materials <= 1024;
+ * larger frames return RQ_ERR_CAPACITY.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress, with that device
+ * current) and caches it; make that first call before any stream capture.
+ * All calls on a device share the array: calls whose work overlaps on the
+ * GPU race and must be ordered by the caller (one stream, or events).
+ */
+RQ_API int rq_render_whitted_device_noalloc(rq_scene* scene,
+                                            const rq_whitted_params* params,
+                                            float* d_rgb, float* d_t, int32_t* d_prim,
+                                            uint64_t* d_shadow_rays, void* stream);
+
+/*
  * Path-traced frame: KajiyaPathtracer::traceEyeRays
  * (Engine/Renderers/KajiyaPathtracer.cc:113-302) with Lambertian materials,
  * one parallelogram AreaLight sampled with HardShadows shadow rays, cosine

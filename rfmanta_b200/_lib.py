@@ -93,6 +93,8 @@ def _load():
         "rq_render_whitted": ([vp, C.POINTER(WhittedParams), vp, vp, vp,
                                C.POINTER(C.c_uint64)], i),
         "rq_render_whitted_device": ([vp, C.POINTER(WhittedParams), vp, vp, vp, vp, vp], i),
+        "rq_render_whitted_device_noalloc": ([vp, C.POINTER(WhittedParams), vp, vp, vp, vp,
+                                              vp], i),
         "rq_set_stage_events": ([vp, vp, i], i),
         "rq_set_stats": ([vp, vp], i),
         "rq_render_path": ([vp, C.POINTER(PathParams), vp, vp], i),

@@ -1,0 +1,139 @@
+// rq_render_whitted_device_noalloc: the Whitted frame of
+// rq_render_whitted_device for callers that must not allocate device memory,
+// e.g. a render worker whose process has handed all of HBM to another
+// allocator, or a host thread that may not call cudaMalloc/cudaFree because
+// those calls can synchronise the device in the middle of its work.
+//
+// The frame's scratch - per-pixel hit record index, the compacted queue of
+// hit pixels, the stage counters, the shadow-ray counter and the material
+// table - lives in one file-scope __device__ array of fixed size instead of
+// buffers the scene allocates on first use.  Limits: at most
+// kNoAllocMaxPixels pixels and kNoAllocMaxMaterials materials per frame.
+//
+// Host code cannot use the array's name as a device address (on the host it
+// names a host-side stand-in).  The device address is looked up with
+// cudaGetSymbolAddress once per device, with that device current, on the
+// first call made for that device, and cached.
+//
+// Every call on a device shares the one array and the array keeps the last
+// call's contents: the counters are cleared at the start of every frame, and
+// two calls whose work overlaps on the GPU (different streams, no ordering)
+// race on the array.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/rfmanta_b200.h"
+#include "rq_render.h"
+#include "rq_scene.h"
+
+namespace rq {
+
+constexpr size_t kNoAllocMaxPixels = size_t(1) << 20;  // 1,048,576 (1280x720 fits)
+constexpr int kNoAllocMaxMaterials = 1024;
+
+// Byte offsets inside the array (each region 256-byte aligned).
+constexpr size_t kOffPos = 0;
+constexpr size_t kOffQueue = kOffPos + 4 * kNoAllocMaxPixels;
+constexpr size_t kOffCounters = kOffQueue + 4 * kNoAllocMaxPixels;
+constexpr size_t kOffShadow = kOffCounters + 256;
+constexpr size_t kOffMaterials = kOffShadow + 256;
+constexpr size_t kNoAllocBytes = kOffMaterials + 12 * (size_t)kNoAllocMaxMaterials;
+
+static __device__ __align__(256) unsigned char g_frame_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static void* g_scratch_addr[kNoAllocMaxDevices] = {};
+static std::mutex g_scratch_mu;
+
+static int na_fail(int code, const std::string& m) {
+  set_error(m);
+  return code;
+}
+
+// Device address of g_frame_scratch on the current device `device`.
+static int scratch_address(int device, unsigned char** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices)
+    return na_fail(RQ_ERR_ARG, "device ordinal beyond the no-alloc table");
+  std::lock_guard<std::mutex> g(g_scratch_mu);
+  if (!g_scratch_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_frame_scratch);
+    if (e != cudaSuccess || !p)
+      return na_fail(RQ_ERR_CUDA, std::string("cudaGetSymbolAddress(frame scratch): ") +
+                                      cudaGetErrorString(e));
+    g_scratch_addr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_scratch_addr[device]);
+  return RQ_OK;
+}
+
+}  // namespace rq
+
+extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
+                                                const rq_whitted_params* p, float* d_rgb,
+                                                float* d_t, int32_t* d_prim,
+                                                uint64_t* d_shadow_rays, void* stream) {
+  using namespace rq;
+  Scene* s = reinterpret_cast<Scene*>(scene);
+  if (!s || !p || !d_rgb || !d_t || !d_prim) return na_fail(RQ_ERR_ARG, "NULL argument");
+  if (p->xres <= 0 || p->yres <= 0) return na_fail(RQ_ERR_ARG, "bad resolution");
+  const size_t npix = (size_t)p->xres * (size_t)p->yres;
+  if (npix > kNoAllocMaxPixels)
+    return na_fail(RQ_ERR_CAPACITY,
+                   "rq_render_whitted_device_noalloc: " + std::to_string(npix) +
+                       " pixels exceed its fixed scratch of " +
+                       std::to_string(kNoAllocMaxPixels) + " pixels");
+  if (p->n_materials <= 0 || !p->material_rgb) return na_fail(RQ_ERR_ARG, "no materials");
+  if (p->n_materials > kNoAllocMaxMaterials)
+    return na_fail(RQ_ERR_CAPACITY,
+                   "rq_render_whitted_device_noalloc: more than " +
+                       std::to_string(kNoAllocMaxMaterials) + " materials");
+  if (p->n_lights < 0 || p->n_lights > kMaxLights || (p->n_lights > 0 && !p->lights))
+    return na_fail(RQ_ERR_ARG, "0..16 point lights");
+  for (uint32_t m : s->face_mat)
+    if ((int)m >= p->n_materials) return na_fail(RQ_ERR_ARG, "face_material past n_materials");
+  if (!s->has_tree) return na_fail(RQ_ERR_STATE, "scene has no tree");
+  if (cudaSetDevice(s->device) != cudaSuccess) return na_fail(RQ_ERR_CUDA, "cudaSetDevice");
+  unsigned char* base = nullptr;
+  int rc = scratch_address(s->device, &base);
+  if (rc != RQ_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  FrameParams P;
+  std::memset(&P, 0, sizeof(P));
+  camera_basis(p->eye, p->lookat, p->up, p->hfov, p->vfov, P.cam);
+  P.xres = p->xres;
+  P.yres = p->yres;
+  P.n_lights = p->n_lights;
+  std::memcpy(P.lights, p->lights, sizeof(float) * 6 * p->n_lights);
+  std::memcpy(P.ambient, p->ambient, sizeof(P.ambient));
+  std::memcpy(P.background, p->background, sizeof(P.background));
+  float* mats = reinterpret_cast<float*>(base + kOffMaterials);
+  cudaError_t e = cudaMemcpyAsync(mats, p->material_rgb, sizeof(float) * 3 * p->n_materials,
+                                  cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return na_fail(RQ_ERR_CUDA, std::string("materials: ") + cudaGetErrorString(e));
+  P.materials = mats;
+
+  FrameBuffers B;
+  B.rgb = d_rgb;
+  B.t = d_t;
+  B.prim = d_prim;
+  B.pos = reinterpret_cast<int32_t*>(base + kOffPos);
+  B.queue = reinterpret_cast<int32_t*>(base + kOffQueue);
+  B.counters = reinterpret_cast<int32_t*>(base + kOffCounters);
+  B.shadow_rays_ptr = d_shadow_rays ? reinterpret_cast<unsigned long long*>(d_shadow_rays)
+                                    : reinterpret_cast<unsigned long long*>(base + kOffShadow);
+  B.stats = s->stats;
+  const DevScene S = s->dev();
+  const size_t smem = (size_t)S.depth * 128 * sizeof(int2);
+  const int grid = std::max(1, whitted_blocks_per_sm(s->tri_kind, smem) * s->num_sms);
+  const int grid1 = std::min(grid, (int)((npix + 127) / 128));
+  // launch_whitted clears the stage counters and the shadow counter first
+  e = launch_whitted(S, P, B, grid1, grid, st, nullptr, 0);
+  if (e != cudaSuccess) return na_fail(RQ_ERR_CUDA, std::string("whitted launch: ") + cudaGetErrorString(e));
+  return RQ_OK;
+}

@@ -1,0 +1,76 @@
+"""rq_render_whitted_device_noalloc, the Whitted frame for callers that
+cannot allocate device memory (a process whose device memory belongs to
+another allocator, a render thread that must not make device-synchronising
+calls such as cudaMalloc).  Its scratch is a fixed array inside the library,
+so it is checked here against the allocating entry point
+rq_render_whitted_device: two calls in a row, each equal to the allocating
+call bit for bit (the tolerance all frame tests use: none), and no change in
+free device memory between the first and the second call.  The file name
+makes pytest collect it last."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def test_noalloc_frame_matches_allocating_entry_point():
+    import torch
+    from rfmanta_b200 import _lib, scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    sc = scenes.small_frame_scene()
+    bvh = GpuDynBVH()
+    bvh.setGroup(sc.mesh)
+    bvh.rebuild()
+    p = bvh.whitted_params(sc)
+    npx = sc.xres * sc.yres
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def buffers():
+        return (torch.zeros(npx * 3, device="cuda"), torch.zeros(npx, device="cuda"),
+                torch.zeros(npx, dtype=torch.int32, device="cuda"),
+                torch.zeros(1, dtype=torch.int64, device="cuda"))
+
+    want = buffers()
+    _lib.check(_lib.lib.rq_render_whitted_device(
+        bvh.handle, C.byref(p), C.c_void_p(want[0].data_ptr()), C.c_void_p(want[1].data_ptr()),
+        C.c_void_p(want[2].data_ptr()), C.c_void_p(want[3].data_ptr()), C.c_void_p(stream)))
+    torch.cuda.synchronize()
+    outs = [buffers(), buffers()]
+    free = []
+    for got in outs:
+        _lib.check(_lib.lib.rq_render_whitted_device_noalloc(
+            bvh.handle, C.byref(p), C.c_void_p(got[0].data_ptr()),
+            C.c_void_p(got[1].data_ptr()), C.c_void_p(got[2].data_ptr()),
+            C.c_void_p(got[3].data_ptr()), C.c_void_p(stream)))
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+    for got in outs:
+        assert int(got[3].item()) == int(want[3].item())
+        assert np.array_equal(got[2].cpu().numpy(), want[2].cpu().numpy())
+        assert np.array_equal(_bits(got[1].cpu().numpy()), _bits(want[1].cpu().numpy()))
+        assert np.array_equal(_bits(got[0].cpu().numpy()), _bits(want[0].cpu().numpy()))
+    assert free[1] == free[0]
+
+
+def test_noalloc_rejects_frames_beyond_its_scratch():
+    from rfmanta_b200 import _lib, scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    sc = scenes.small_frame_scene(level=2, grid=4, xres=2048, yres=1024)
+    bvh = GpuDynBVH()
+    bvh.setGroup(sc.mesh)
+    bvh.rebuild()
+    import torch
+    p = bvh.whitted_params(sc)
+    tiny = torch.zeros(4, device="cuda")
+    rc = _lib.lib.rq_render_whitted_device_noalloc(bvh.handle, C.byref(p),
+                                                   C.c_void_p(tiny.data_ptr()),
+                                                   C.c_void_p(tiny.data_ptr()),
+                                                   C.c_void_p(tiny.data_ptr()), None, None)
+    assert rc == _lib.RQ_ERR_CAPACITY
+    assert b"exceed" in _lib.lib.rq_last_error()

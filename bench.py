@@ -300,7 +300,171 @@ class SmallFrame:
         return rays / secs / 1e6, threads, text, secs
 
 
-WORKLOADS = {"path_frame": PathFrame, "small_frame": SmallFrame}
+class BatchedQueriesWL:
+    """64 ray batches (log-uniform 1k-4M rays, 50% any hit with tmax uniform
+    in [0.1, diag], 50% closest hit) over 8 resident scenes of 10,240 to
+    5,120,000 triangles, one persistent launch replayed from a CUDA graph
+    with the autotuned configuration."""
+
+    name = "batched_queries"
+
+    def __init__(self):
+        from rfmanta_b200 import scenes
+        self.specs = scenes.query_batches()
+        self.meshes = [scenes.query_scene(i) for i in range(8)]
+        self.sc = None
+
+    def config(self):
+        return {"workload": self.name, "scenes": [int(m.n_tris) for m in self.meshes],
+                "batches": len(self.specs), "rays": int(sum(n for _, n, _ in self.specs)),
+                "anyhit_batches": int(sum(a for _, _, a in self.specs)),
+                "triangle_kind": "wald", "tree": "gpu binned SAH",
+                "l2": "flushed before every timed step (256 MiB write); inputs exceed L2"}
+
+    def build(self, dev):
+        from rfmanta_b200.dynbvh import GpuDynBVH
+        self.bvhs = []
+        self.build_s = 0.0
+        for m in self.meshes:
+            b = GpuDynBVH(tri_kind=0, device=dev.index or 0)
+            b.setGroup(m)
+            b.rebuild()
+            self.build_s += b.build_seconds()
+            self.bvhs.append(b)
+        return self.bvhs[0]
+
+    def setup(self, bvh, dev):
+        from rfmanta_b200 import scenes
+        from rfmanta_b200.batch import BatchedQueries, QueryBatch
+        self.batches = []
+        for k, (si, n, anyhit) in enumerate(self.specs):
+            lo, hi = self.meshes[si].bounds()
+            o, d, tm = scenes.query_rays_torch(n, lo, hi, anyhit, seed=1000 + k, device=dev)
+            self.batches.append(QueryBatch(si, o, d, tm, anyhit))
+        self.bq = BatchedQueries(self.bvhs, self.batches)
+        self.tuned = self.bq.autotune(reps=1)
+        self.n_events = 0
+        self.launches = 1
+        self.total = self.bq.total_rays
+
+    def frame(self, stream_ptr):
+        self.bq.launch(stream_ptr)
+
+    def rays(self):
+        return (self.total,)
+
+    def set_stats(self, ptr):
+        # stats are collected by a plan created while scene 0 counts
+        from rfmanta_b200.batch import BatchedQueries
+        self.bvhs[0].set_stats(ptr)
+        if ptr:
+            self._stats_bq = BatchedQueries(self.bvhs, self.batches, self.tuned)
+        else:
+            self._stats_bq.close()
+
+    def stats_frame(self, stream_ptr):
+        self._stats_bq.launch(stream_ptr)
+
+    def host_frame(self):
+        """Host arrays in pinned memory: rays copied in, the plan replayed,
+        t and triangle ids copied back."""
+        import torch
+        if not hasattr(self, "_pinned"):
+            self._pinned = [(b.org.cpu().pin_memory(), b.dir.cpu().pin_memory(),
+                             b.tmax.cpu().pin_memory(),
+                             torch.empty(b.tmax.shape[0], pin_memory=True),
+                             torch.empty(b.tmax.shape[0], dtype=torch.int32, pin_memory=True))
+                            for b in self.batches]
+        for b, (o, d, tm, _, _) in zip(self.batches, self._pinned):
+            b.org.copy_(o, non_blocking=True)
+            b.dir.copy_(d, non_blocking=True)
+            b.tmax.copy_(tm, non_blocking=True)
+        self.bq.launch(torch.cuda.current_stream().cuda_stream)
+        for i, (_, _, _, t, p) in enumerate(self._pinned):
+            t.copy_(self.bq.t[i], non_blocking=True)
+            p.copy_(self.bq.prim[i], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return 28 * self.total, 8 * self.total
+
+    def roofline_bytes(self, stats, rays):
+        n = rays[0]
+        b, t = stats[0] / max(n, 1), stats[1] / max(n, 1)
+        # 32 B ray in; 8 B (t, id) out for closest, 4 for any hit: 6 on average
+        return (n * (32 + 6 + 32 * b + 48 * t),), {"box_tests": round(b, 3),
+                                                    "tri_tests": round(t, 3)}
+
+    def group_stages(self, frame_ms):
+        return ["batch_kernel"], [frame_ms]
+
+    def extra(self, dev):
+        """The plain per-call GPU form (one rq_trace_device launch per batch)
+        and Manta's per-packet form (rq_trace on 64-ray host packets)."""
+        import torch
+        from rfmanta_b200.dynbvh import RayBatch
+        st = torch.cuda.current_stream(dev).cuda_stream
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            e0.record()
+            for i, b in enumerate(self.batches):
+                n = int(b.tmax.shape[0])
+                self.bvhs[b.scene].intersect_device(n, b.org.data_ptr(), b.dir.data_ptr(),
+                                                    b.tmax.data_ptr(), b.anyhit,
+                                                    self.bq.t[i].data_ptr(),
+                                                    self.bq.prim[i].data_ptr(), stream=st)
+            e1.record()
+            torch.cuda.synchronize(dev)
+        plain = self.total / (e0.elapsed_time(e1) * 1e-3) / 1e6
+        b = self.batches[0]
+        o = b.org[:, :64 * 500].cpu().numpy()
+        d = b.dir[:, :64 * 500].cpu().numpy()
+        tm = b.tmax[:64 * 500].cpu().numpy()
+        npk = o.shape[1] // 64
+        t0 = time.perf_counter()
+        for k in range(npk):
+            r = RayBatch(o[:, 64 * k:64 * k + 64], d[:, 64 * k:64 * k + 64],
+                         tm[64 * k:64 * k + 64], flags=RayBatch.AnyHit if b.anyhit else 0)
+            self.bvhs[b.scene].intersect(r)
+        per_packet = npk * 64 / (time.perf_counter() - t0) / 1e6
+        return {"plain_gpu_per_batch_mrays": round(plain, 1),
+                "manta_per_packet_dropin_mrays": round(per_packet, 3),
+                "autotuned": self.tuned, "build_ms_total": round(self.build_s * 1e3, 1)}
+
+    def cpu_reference(self, seconds_budget, threads):
+        """Reference DynBVH::intersect (64-ray packets, all host threads) on
+        the batches of the five scenes up to 1M triangles, 300k rays of each
+        batch at most."""
+        import numpy as np
+        from oracle.pyoracle import Reference
+        from rfmanta_b200 import scenes
+        sse = Reference.available(sse=True)
+        ref = Reference(sse=sse)
+        cache, secs, rays, used = {}, 0.0, 0, 0
+        for k, (si, n, anyhit) in enumerate(self.specs):
+            if si > 4:
+                continue
+            if si not in cache:
+                cache[si] = ref.scene(self.meshes[si], 0)
+            lo, hi = self.meshes[si].bounds()
+            m = min(n, 300000)
+            o, d, tm, _ = scenes.random_rays(m, lo, hi, seed=k, anyhit_fraction=1.0 if anyhit else 0.0)
+            if not anyhit:
+                tm = np.full(m, 1e19, np.float32)
+            out = cache[si].intersect_mt(o, d, tm, anyhit=anyhit, nthreads=threads)
+            secs += out["seconds"]
+            rays += m
+            used += 1
+            if secs > seconds_budget > 0:
+                break
+        for r in cache.values():
+            r.close()
+        text = (f"{used} batches ({rays} rays, at most 300k per batch) on the scenes of up to "
+                f"983,040 triangles, reference DynBVH::intersect on 64-ray packets "
+                f"({'MANTA_SSE' if sse else 'scalar'} build)")
+        return rays / secs / 1e6, threads, text, secs
+
+
+WORKLOADS = {"path_frame": PathFrame, "small_frame": SmallFrame,
+             "batched_queries": BatchedQueriesWL}
 
 
 # ----------------------------------------------------------------- runs ----
@@ -316,10 +480,14 @@ def run_ours(args):
     from rfmanta_b200.dynbvh import GpuDynBVH
     wl = WORKLOADS[args.workload]()
     dev = torch.device("cuda", local)
-    bvh = GpuDynBVH(tri_kind=0, device=local)
-    bvh.setGroup(wl.sc.mesh)
-    bvh.rebuild()
-    build_s = bvh.build_seconds()
+    if hasattr(wl, "build"):
+        bvh = wl.build(dev)
+        build_s = wl.build_s
+    else:
+        bvh = GpuDynBVH(tri_kind=0, device=local)
+        bvh.setGroup(wl.sc.mesh)
+        bvh.rebuild()
+        build_s = bvh.build_seconds()
     wl.setup(bvh, dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -327,10 +495,16 @@ def run_ours(args):
 
     # statistics frame (untimed): box / triangle tests per ray
     stats = torch.zeros(4, dtype=torch.int64, device=dev)
-    bvh.set_stats(stats.data_ptr())
-    wl.frame(sptr)
-    torch.cuda.synchronize(dev)
-    bvh.set_stats(0)
+    if hasattr(wl, "stats_frame"):
+        wl.set_stats(stats.data_ptr())
+        wl.stats_frame(sptr)
+        torch.cuda.synchronize(dev)
+        wl.set_stats(0)
+    else:
+        bvh.set_stats(stats.data_ptr())
+        wl.frame(sptr)
+        torch.cuda.synchronize(dev)
+        bvh.set_stats(0)
     st = stats.cpu().numpy().astype(np.float64)
     rays = wl.rays()
     rays_per_step = sum(rays)
@@ -344,12 +518,13 @@ def run_ours(args):
         e.record(stream)
     pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
              for _ in range(args.steps)]
-    stage = np.zeros((args.steps, wl.n_events - 1))
+    stage = np.zeros((args.steps, max(wl.n_events - 1, 1)))
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
-        bvh.set_stage_events(ev)
+        if wl.n_events:
+            bvh.set_stage_events(ev)
         for k in range(args.steps):
             flush.fill_(k & 0xff)
             pairs[k][0].record(stream)
@@ -358,7 +533,10 @@ def run_ours(args):
             torch.cuda.synchronize(dev)
             for j in range(wl.n_events - 1):
                 stage[k, j] = ev[j].elapsed_time(ev[j + 1])
-        bvh.set_stage_events([])
+            if not wl.n_events:
+                stage[k, 0] = pairs[k][0].elapsed_time(pairs[k][1])
+        if wl.n_events:
+            bvh.set_stage_events([])
         torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -388,7 +566,7 @@ def run_ours(args):
     # roofline of the dominant kernel
     hbm, peak_kind = _peaks()
     mean_stage = stage.mean(axis=0)
-    names, kms = wl.group_stages(mean_stage)
+    names, kms = wl.group_stages(mean_stage if wl.n_events else float(mean_stage[0]))
     alg, per_ray = wl.roofline_bytes(st, rays)
     dom = int(np.argmax(kms))
     achieved = alg[dom] / (kms[dom] * 1e-3) / 1e9
@@ -402,7 +580,8 @@ def run_ours(args):
             "data": "synthetic (seeded scene generators)",
             "config": dict(wl.config(), parallelism=f"replicas x{world}",
                            rays_per_step=rays_per_step, rays_split=list(rays),
-                           build_ms=round(build_s * 1e3, 2)),
+                           build_ms=round(build_s * 1e3, 2),
+                           **(wl.extra(dev) if hasattr(wl, "extra") else {})),
             "clocks": clk.summary(),
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(bin_), "d2h_bytes_per_step": int(bout)},

@@ -197,6 +197,56 @@ RQ_API int rq_render_whitted_device(rq_scene* scene, const rq_whitted_params* pa
                                     uint64_t* d_shadow_rays, void* stream);
 
 /*
+ * Batched ray queries: many batches of uneven size (closest hit or any hit)
+ * over several resident scenes in one persistent launch, captured in a CUDA
+ * graph.  The batched form of DynBVH::intersect that Manta's render workers
+ * call per 64-ray packet (RTRT.cc:984-990).  All scenes must live on one
+ * device and use one triangle kind.  Ray and output arrays are device SoA
+ * as for rq_trace_device; a plan keeps the pointers, so new rays are traced
+ * by writing them into the same arrays and launching the plan again.
+ */
+typedef struct {
+  int scene;            /* index into the plan's scene array */
+  int n;                /* rays in this batch */
+  int flags;            /* RQ_CLOSEST or RQ_ANYHIT */
+  const float* d_org;   /* device, 3 * n */
+  const float* d_dir;   /* device, 3 * n */
+  const float* d_tmax;  /* device, n */
+  float* d_t;           /* outputs (device, n each; any may be NULL) */
+  int32_t* d_prim;
+  float* d_u;
+  float* d_v;
+} rq_batch;
+
+typedef struct {
+  int block_threads;    /* 32..256, multiple of 32 */
+  int blocks_per_sm;    /* 0 = occupancy maximum */
+  int chunk_rays;       /* rays a warp claims per fetch (multiple of 32) */
+  int refill_threshold; /* idle lanes before a warp refills, 1..32 */
+  int reg_stack;        /* traversal-stack entries kept in registers: 0 or 2 */
+} rq_batch_config;
+
+typedef struct rq_batch_plan rq_batch_plan;
+
+/* cfg NULL = defaults (128 threads, 128-ray chunks, refill 8, 2 registers). */
+RQ_API int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes,
+                                const rq_batch* batches, int n_batches,
+                                const rq_batch_config* cfg, rq_batch_plan** out);
+/* Replays the plan's graph on `stream` (a cudaStream_t; NULL = legacy). */
+RQ_API int rq_batch_plan_launch(rq_batch_plan* plan, void* stream);
+RQ_API int rq_batch_plan_info(const rq_batch_plan* plan, rq_batch_config* cfg,
+                              int* grid, long long* total_rays);
+RQ_API int rq_batch_plan_destroy(rq_batch_plan* plan);
+
+/* Times each candidate configuration (NULL = a built-in sweep over block
+ * size, rays per warp chunk, refill threshold and register stack entries)
+ * on these batches, `reps` graph replays each, and returns the fastest. */
+RQ_API int rq_batch_autotune(rq_scene* const* scenes, int n_scenes,
+                             const rq_batch* batches, int n_batches,
+                             const rq_batch_config* candidates, int n_candidates,
+                             int reps, rq_batch_config* best, float* best_ms);
+
+/*
  * rq_render_whitted_device without any device allocation.  This entry point
  * has no counterpart in the reference.  It is for callers that cannot call
  * cudaMalloc: a process whose device memory is already handed out to another
@@ -275,7 +325,9 @@ RQ_API int rq_set_stage_events(rq_scene* scene, void* events, int n);
  * Traversal statistics (DynBVH COLLECT_STATS: node traversals and
  * intersections per ray).  d_counters is a device array of 4 uint64 the
  * frame paths add to: box tests and triangle tests of primary (or bounce)
- * rays, then of shadow rays.  The caller zeroes it.  NULL turns counting off
+ * rays, then of shadow rays.  Batch plans created while the first scene of
+ * the plan has counters set add box and triangle tests of all their rays to
+ * counters[0] and [1].  The caller zeroes it.  NULL turns counting off
  * (the default; counting builds use separate kernels).
  */
 RQ_API int rq_set_stats(rq_scene* scene, uint64_t* d_counters);

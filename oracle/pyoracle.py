@@ -262,6 +262,8 @@ class Reference:
         L.mref_render.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 2 + [C.c_int] +
                                   [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 5)
         L.mref_node_size.restype = C.c_int
+        L.mref_intersect_mt.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
+                                        [C.c_int, C.c_int] + [C.c_void_p] * 4)
         if hasattr(L, "mref_scene_use_gpu"):
             L.mref_scene_use_gpu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_char_p]
         L.mref_render_path.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
@@ -344,6 +346,21 @@ class RefScene:
         self.ref.lib.mref_intersect(self.h, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
                                     packet, _ptr(hit), _ptr(t), _ptr(prim), _ptr(u), _ptr(v))
         return dict(hit=hit, t=t, prim=prim, u=u, v=v)
+
+    def intersect_mt(self, org, dir, tmax, anyhit=False, nthreads=1):
+        """DynBVH::intersect on 64-ray packets over N threads; returns the
+        outputs and the wall seconds."""
+        n = int(tmax.shape[0])
+        org = np.ascontiguousarray(org, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        hit = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        secs = C.c_double()
+        self.ref.lib.mref_intersect_mt(self.h, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
+                                       nthreads, _ptr(hit), _ptr(t), _ptr(prim), C.byref(secs))
+        return dict(hit=hit, t=t, prim=prim, seconds=secs.value)
 
     def render(self, scene, nthreads=1, want_ids=True):
         cam = scene.camera

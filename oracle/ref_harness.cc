@@ -287,6 +287,94 @@ int mref_intersect(void* h, int n, const float* org, const float* dir,
   return 0;
 }
 
+struct QueryJob {
+  RefScene* s;
+  int n, anyhit;
+  const float *org, *dir, *tmax;
+  int* hit;
+  float* t;
+  int* prim;
+  volatile int next;
+  pthread_mutex_t lock;
+  int nthreads;
+};
+
+struct QueryArg {
+  QueryJob* job;
+  int proc;
+};
+
+static void* query_worker(void* p) {
+  QueryArg* a = static_cast<QueryArg*>(p);
+  QueryJob* j = a->job;
+  RenderContext ctx(0, 0, a->proc, j->nthreads, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+  const int P = RayPacket::MaxSize;
+  for (;;) {
+    pthread_mutex_lock(&j->lock);
+    const int base = j->next;
+    j->next += 16 * P;
+    pthread_mutex_unlock(&j->lock);
+    if (base >= j->n) break;
+    const int stop = base + 16 * P < j->n ? base + 16 * P : j->n;
+    for (int b = base; b < stop; b += P) {
+      const int cnt = stop - b < P ? stop - b : P;
+      RayPacketData data;
+      RayPacket rays(data, RayPacket::UnknownShape, 0, cnt, 0,
+                     j->anyhit ? RayPacket::AnyHit : 0);
+      const int n = j->n;
+      for (int i = 0; i < cnt; ++i) {
+        const int r = b + i;
+        rays.setRay(i, Vector(j->org[r], j->org[n + r], j->org[2 * n + r]),
+                    Vector(j->dir[r], j->dir[n + r], j->dir[2 * n + r]));
+        rays.resetHit(i, j->tmax[r]);
+      }
+      j->s->object->intersect(ctx, rays);
+      for (int i = 0; i < cnt; ++i) {
+        const int r = b + i;
+        j->hit[r] = rays.wasHit(i) ? 1 : 0;
+        j->t[r] = rays.getMinT(i);
+        j->prim[r] = j->hit[r] ? (int)TriId::of(rays.getHitPrimitive(i)) : -1;
+      }
+    }
+  }
+  return 0;
+}
+
+// DynBVH::intersect over 64-ray packets on N pthreads (packets taken 16 at a
+// time from a shared counter).  Returns wall seconds in *seconds.
+int mref_intersect_mt(void* h, int n, const float* org, const float* dir, const float* tmax,
+                      int anyhit, int nthreads, int* hit, float* t, int* prim,
+                      double* seconds) {
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  QueryJob job;
+  job.s = static_cast<RefScene*>(h);
+  job.n = n;
+  job.anyhit = anyhit;
+  job.org = org;
+  job.dir = dir;
+  job.tmax = tmax;
+  job.hit = hit;
+  job.t = t;
+  job.prim = prim;
+  job.next = 0;
+  job.nthreads = nthreads;
+  pthread_mutex_init(&job.lock, 0);
+  std::vector<pthread_t> th(nthreads);
+  std::vector<QueryArg> ar(nthreads);
+  const double t0 = now_s();
+  for (int p = 0; p < nthreads; ++p) {
+    ar[p].job = &job;
+    ar[p].proc = p;
+    pthread_create(&th[p], 0, query_worker, &ar[p]);
+  }
+  for (int p = 0; p < nthreads; ++p) pthread_join(th[p], 0);
+  const double t1 = now_s();
+  pthread_mutex_destroy(&job.lock);
+  if (seconds) *seconds = t1 - t0;
+  return 0;
+}
+
 // Camera basis (eye, lookat-eye, u, v) of PinholeCamera with the given
 // eye/lookat/up/hfov/vfov and -normalizeRays.
 int mref_camera_basis(const float* eye, const float* lookat, const float* up,

@@ -62,6 +62,21 @@ class PathParams(C.Structure):
                 ("chunk_paths", C.c_int)]
 
 
+class Batch(C.Structure):
+    _fields_ = [("scene", C.c_int), ("n", C.c_int), ("flags", C.c_int),
+                ("d_org", C.c_void_p), ("d_dir", C.c_void_p), ("d_tmax", C.c_void_p),
+                ("d_t", C.c_void_p), ("d_prim", C.c_void_p), ("d_u", C.c_void_p),
+                ("d_v", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
+                ("chunk_rays", C.c_int), ("refill_threshold", C.c_int), ("reg_stack", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
                 ("refill_threshold", C.c_int), ("persistent", C.c_int)]
@@ -100,6 +115,11 @@ def _load():
         "rq_render_path": ([vp, C.POINTER(PathParams), vp, vp], i),
         "rq_render_path_device": ([vp, C.POINTER(PathParams), vp, vp, vp], i),
         "rq_set_path_debug": ([vp, vp, vp, vp, C.c_int64], i),
+        "rq_batch_plan_create": ([vp, i, vp, i, vp, C.POINTER(vp)], i),
+        "rq_batch_plan_launch": ([vp, vp], i),
+        "rq_batch_plan_info": ([vp, vp, C.POINTER(i), C.POINTER(C.c_longlong)], i),
+        "rq_batch_plan_destroy": ([vp], i),
+        "rq_batch_autotune": ([vp, i, vp, i, vp, i, i, vp, C.POINTER(C.c_float)], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
     }
     for name, (args, res) in sig.items():

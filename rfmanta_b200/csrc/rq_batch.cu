@@ -1,0 +1,424 @@
+// Batched ray queries: many batches of uneven size, closest hit or any hit,
+// over several resident scenes, in ONE persistent launch.
+//
+// Work is cut into chunks of `chunk_rays` consecutive rays of one batch.
+// Each warp claims a chunk with one atomicAdd and hands its rays to idle
+// lanes; after every while-while step the warp counts idle lanes with a
+// ballot and refills them (from the current chunk, claiming the next chunk
+// when it runs dry) once `refill` or more are idle or none is busy.  A warp
+// can therefore hold rays of different batches, scenes and query kinds at
+// the same time; each lane keeps its own batch, scene and any-hit flag.
+// Scene descriptors are staged in shared memory; the traversal stack keeps
+// `R` entries in registers and spills to the thread's shared-memory column
+// (sized to the deepest scene).
+//
+// A plan uploads the scene and batch tables once and captures the launch
+// (counter reset + kernel) in a CUDA graph; rq_batch_plan_launch replays it.
+// rq_batch_autotune times candidate configurations on the real batches and
+// returns the fastest.  Results do not depend on the configuration: every
+// ray is traced by the same per-ray procedure (tested).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rfmanta_b200.h"
+#include "rq_scene.h"
+#include "rq_traverse.cuh"
+
+namespace rq {
+
+constexpr int kMaxBatchScenes = 32;
+
+struct BatchDesc {
+  int scene;
+  int n;
+  int any;
+  int chunk0;  // first chunk index of this batch
+  const float* org;
+  const float* dir;
+  const float* tmax;
+  float* t;
+  int32_t* prim;
+  float* u;
+  float* v;
+};
+
+struct BatchArgs {
+  const DevScene* scenes;
+  int n_scenes;
+  const BatchDesc* batches;
+  int n_batches;
+  int total_chunks;
+  int chunk_rays;
+  int refill;
+  int stack_depth;  // shared-memory entries per thread
+  int* counter;
+  unsigned long long* stats;  // STATS kernels: box tests, triangle tests
+};
+
+template <int KIND, int R, bool STATS>
+__global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
+  extern __shared__ int2 smem[];
+  __shared__ DevScene sm_scenes[kMaxBatchScenes];
+  for (int i = threadIdx.x; i < A.n_scenes; i += blockDim.x) sm_scenes[i] = A.scenes[i];
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  RegStack<R> st;
+  st.init(smem + threadIdx.x, blockDim.x);
+  // warp-uniform chunk state
+  int w_batch = 0, w_next = 0, w_end = 0;
+  bool exhausted = false;
+  // lane state
+  int my_ray = -1, my_batch = 0, my_scene = 0;
+  bool my_any = false;
+  Ray r;
+  Hit h;
+  int ref = kDone;
+  Counts cnt;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, my_ray < 0);
+    const unsigned busy = ~idle;
+    if (!exhausted && idle && (__popc(idle) >= A.refill || busy == 0u)) {
+      unsigned need = idle;
+      while (need) {
+        if (w_next >= w_end) {
+          int c = 0;
+          if (lane == 0) c = atomicAdd(A.counter, 1);
+          c = __shfl_sync(0xffffffffu, c, 0);
+          if (c >= A.total_chunks) {
+            exhausted = true;
+            break;
+          }
+          int lo = 0, hi = A.n_batches - 1;  // last batch with chunk0 <= c
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&A.batches[mid].chunk0) <= c) lo = mid;
+            else hi = mid - 1;
+          }
+          w_batch = lo;
+          w_next = (c - __ldg(&A.batches[lo].chunk0)) * A.chunk_rays;
+          w_end = min(w_next + A.chunk_rays, __ldg(&A.batches[lo].n));
+        }
+        const int k = min(__popc(need), w_end - w_next);
+        const bool take = ((need >> lane) & 1u) && (int)__popc(need & lt) < k;
+        if (take) {
+          const BatchDesc& B = A.batches[w_batch];
+          my_batch = w_batch;
+          my_ray = w_next + (int)__popc(need & lt);
+          my_scene = B.scene;
+          my_any = B.any != 0;
+          const int n = B.n;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            r.o[c] = __ldg(B.org + (size_t)c * n + my_ray);
+            r.d[c] = __ldg(B.dir + (size_t)c * n + my_ray);
+            r.inv[c] = fdiv(1.f, r.d[c]);
+          }
+          r.minT = __ldg(B.tmax + my_ray);
+          int sp0;
+          start_ray(sm_scenes[my_scene], r, h, ref, sp0);
+          st.init(smem + threadIdx.x, blockDim.x);
+          if (STATS) cnt.boxes += 1;
+        }
+        const unsigned taken = __ballot_sync(0xffffffffu, take);
+        need &= ~taken;
+        w_next += k;
+      }
+    }
+    if (exhausted && __all_sync(0xffffffffu, my_ray < 0)) break;
+    if (my_ray >= 0) {
+      if (ref != kDone)
+        step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, my_any, &cnt);
+      if (ref == kDone) {
+        const BatchDesc& B = A.batches[my_batch];
+        if (B.t) B.t[my_ray] = h.t;
+        if (B.prim) B.prim[my_ray] = h.id;
+        if (B.u) B.u[my_ray] = h.u;
+        if (B.v) B.v[my_ray] = h.v;
+        my_ray = -1;
+      }
+    }
+  }
+  if (STATS) {
+    atomicAdd(&A.stats[0], (unsigned long long)cnt.boxes);
+    atomicAdd(&A.stats[1], (unsigned long long)cnt.tris);
+  }
+}
+
+template <int KIND, int R, bool STATS>
+static cudaError_t batch_go(bool launch, int grid, int block, size_t smem, const BatchArgs& A,
+                            cudaStream_t st, const void** fn) {
+  if (fn) *fn = (const void*)batch_kernel<KIND, R, STATS>;
+  if (launch) batch_kernel<KIND, R, STATS><<<grid, block, smem, st>>>(A);
+  return launch ? cudaGetLastError() : cudaSuccess;
+}
+
+// Resolves (triangle kind, register stack, statistics) to one kernel and
+// either returns its address or launches it.
+static cudaError_t batch_dispatch(int kind, int reg, bool stats, bool launch, int grid,
+                                  int block, size_t smem, const BatchArgs& A, cudaStream_t st,
+                                  const void** fn) {
+  if (kind == kWald) {
+    if (reg) return stats ? batch_go<kWald, 2, true>(launch, grid, block, smem, A, st, fn)
+                          : batch_go<kWald, 2, false>(launch, grid, block, smem, A, st, fn);
+    return stats ? batch_go<kWald, 0, true>(launch, grid, block, smem, A, st, fn)
+                 : batch_go<kWald, 0, false>(launch, grid, block, smem, A, st, fn);
+  }
+  if (reg) return stats ? batch_go<kKS, 2, true>(launch, grid, block, smem, A, st, fn)
+                        : batch_go<kKS, 2, false>(launch, grid, block, smem, A, st, fn);
+  return stats ? batch_go<kKS, 0, true>(launch, grid, block, smem, A, st, fn)
+               : batch_go<kKS, 0, false>(launch, grid, block, smem, A, st, fn);
+}
+
+}  // namespace rq
+
+struct rq_batch_plan {
+  int device = 0;
+  int tri_kind = 0;
+  rq_batch_config cfg{};
+  rq::BatchArgs args{};
+  rq::DevScene* d_scenes = nullptr;
+  rq::BatchDesc* d_batches = nullptr;
+  int* d_counter = nullptr;
+  int grid = 1;
+  size_t smem = 0;
+  long long total_rays = 0;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~rq_batch_plan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    cudaFree(d_scenes);
+    cudaFree(d_batches);
+    cudaFree(d_counter);
+  }
+};
+
+namespace {
+
+int bfail(int code, const std::string& m) {
+  rq::set_error(m);
+  return code;
+}
+
+rq_batch_config default_batch_config() {
+  rq_batch_config c;
+  c.block_threads = 128;
+  c.blocks_per_sm = 0;
+  c.chunk_rays = 128;
+  c.refill_threshold = 8;
+  c.reg_stack = 2;
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* batches,
+                         int n_batches, const rq_batch_config* cfg_in, rq_batch_plan** out) {
+  using namespace rq;
+  if (!out) return bfail(RQ_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!scenes || n_scenes <= 0 || n_scenes > kMaxBatchScenes)
+    return bfail(RQ_ERR_ARG, "1..32 scenes");
+  if (!batches || n_batches <= 0) return bfail(RQ_ERR_ARG, "no batches");
+  rq_batch_config cfg = cfg_in ? *cfg_in : default_batch_config();
+  if (cfg.block_threads < 32 || cfg.block_threads > 256 || cfg.block_threads % 32)
+    return bfail(RQ_ERR_ARG, "block_threads must be a multiple of 32 in [32, 256]");
+  if (cfg.chunk_rays < 32 || cfg.chunk_rays % 32 || cfg.chunk_rays > (1 << 20))
+    return bfail(RQ_ERR_ARG, "chunk_rays must be a multiple of 32");
+  if (cfg.refill_threshold < 1 || cfg.refill_threshold > 32)
+    return bfail(RQ_ERR_ARG, "refill_threshold must be in [1, 32]");
+  if (cfg.reg_stack != 0 && cfg.reg_stack != 2) return bfail(RQ_ERR_ARG, "reg_stack is 0 or 2");
+  const Scene* s0 = reinterpret_cast<const Scene*>(scenes[0]);
+  if (!s0) return bfail(RQ_ERR_ARG, "NULL scene");
+  std::vector<DevScene> ds(n_scenes);
+  int depth = 1;
+  for (int i = 0; i < n_scenes; ++i) {
+    const Scene* s = reinterpret_cast<const Scene*>(scenes[i]);
+    if (!s) return bfail(RQ_ERR_ARG, "NULL scene");
+    if (!s->has_tree) return bfail(RQ_ERR_STATE, "scene " + std::to_string(i) + " has no tree");
+    if (s->device != s0->device) return bfail(RQ_ERR_ARG, "all scenes must be on one device");
+    if (s->tri_kind != s0->tri_kind) return bfail(RQ_ERR_ARG, "all scenes must use one triangle kind");
+    ds[i] = s->dev();
+    depth = std::max(depth, ds[i].depth);
+  }
+  std::vector<BatchDesc> bd(n_batches);
+  int chunks = 0;
+  long long rays = 0;
+  for (int b = 0; b < n_batches; ++b) {
+    const rq_batch& q = batches[b];
+    if (q.scene < 0 || q.scene >= n_scenes) return bfail(RQ_ERR_ARG, "batch scene index out of range");
+    if (q.n < 0 || (q.n > 0 && (!q.d_org || !q.d_dir || !q.d_tmax)))
+      return bfail(RQ_ERR_ARG, "bad batch ray arrays");
+    if (q.flags != RQ_CLOSEST && q.flags != RQ_ANYHIT) return bfail(RQ_ERR_ARG, "bad batch flags");
+    BatchDesc& d = bd[b];
+    d.scene = q.scene;
+    d.n = q.n;
+    d.any = q.flags == RQ_ANYHIT;
+    d.chunk0 = chunks;
+    d.org = q.d_org;
+    d.dir = q.d_dir;
+    d.tmax = q.d_tmax;
+    d.t = q.d_t;
+    d.prim = q.d_prim;
+    d.u = q.d_u;
+    d.v = q.d_v;
+    const long long c = ((long long)q.n + cfg.chunk_rays - 1) / cfg.chunk_rays;
+    if (chunks + c > (1LL << 30)) return bfail(RQ_ERR_CAPACITY, "too many chunks");
+    chunks += (int)c;
+    rays += q.n;
+  }
+  if (cudaSetDevice(s0->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
+  std::unique_ptr<rq_batch_plan> p(new rq_batch_plan());
+  p->device = s0->device;
+  p->tri_kind = s0->tri_kind;
+  p->cfg = cfg;
+  p->total_rays = rays;
+  if (cudaMalloc(&p->d_scenes, sizeof(DevScene) * n_scenes) != cudaSuccess ||
+      cudaMalloc(&p->d_batches, sizeof(BatchDesc) * n_batches) != cudaSuccess ||
+      cudaMalloc(&p->d_counter, sizeof(int)) != cudaSuccess)
+    return bfail(RQ_ERR_OOM, "plan tables");
+  if (cudaMemcpy(p->d_scenes, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(p->d_batches, bd.data(), sizeof(BatchDesc) * n_batches,
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return bfail(RQ_ERR_CUDA, "plan table upload");
+  p->smem = (size_t)depth * cfg.block_threads * sizeof(int2);
+  const bool stats = s0->stats != nullptr;
+  const void* f = nullptr;
+  batch_dispatch(p->tri_kind, cfg.reg_stack, stats, false, 0, 0, 0, p->args, nullptr, &f);
+  if (p->smem > 48 * 1024)
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+  int bps = cfg.blocks_per_sm;
+  if (bps <= 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, f, cfg.block_threads, p->smem) !=
+            cudaSuccess ||
+        bps <= 0)
+      bps = 1;
+  }
+  const int warps_needed = chunks;  // at most one chunk per warp to start
+  const int max_blocks = std::max(1, (warps_needed * 32 + cfg.block_threads - 1) / cfg.block_threads);
+  p->grid = std::max(1, std::min(bps * s0->num_sms, max_blocks));
+  BatchArgs& A = p->args;
+  A.scenes = p->d_scenes;
+  A.n_scenes = n_scenes;
+  A.batches = p->d_batches;
+  A.n_batches = n_batches;
+  A.total_chunks = chunks;
+  A.chunk_rays = cfg.chunk_rays;
+  A.refill = cfg.refill_threshold;
+  A.stack_depth = depth;
+  A.counter = p->d_counter;
+  A.stats = s0->stats;
+  // capture counter reset + launch in a graph
+  if (cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bfail(RQ_ERR_CUDA, "stream");
+  cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(p->d_counter, 0, sizeof(int), p->cap_stream);
+    batch_dispatch(p->tri_kind, cfg.reg_stack, stats, true, p->grid, cfg.block_threads, p->smem,
+                   A, p->cap_stream, nullptr);
+    e = cudaStreamEndCapture(p->cap_stream, &p->graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+  if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+  *out = p.release();
+  return RQ_OK;
+}
+
+int rq_batch_plan_launch(rq_batch_plan* plan, void* stream) {
+  if (!plan) return bfail(RQ_ERR_ARG, "NULL plan");
+  if (cudaSetDevice(plan->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
+  const cudaError_t e = cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+  return RQ_OK;
+}
+
+int rq_batch_plan_info(const rq_batch_plan* plan, rq_batch_config* cfg, int* grid,
+                       long long* total_rays) {
+  if (!plan) return bfail(RQ_ERR_ARG, "NULL plan");
+  if (cfg) *cfg = plan->cfg;
+  if (grid) *grid = plan->grid;
+  if (total_rays) *total_rays = plan->total_rays;
+  return RQ_OK;
+}
+
+int rq_batch_plan_destroy(rq_batch_plan* plan) {
+  if (plan) {
+    cudaSetDevice(plan->device);
+    delete plan;
+  }
+  return RQ_OK;
+}
+
+int rq_batch_autotune(rq_scene* const* scenes, int n_scenes, const rq_batch* batches,
+                      int n_batches, const rq_batch_config* candidates, int n_candidates,
+                      int reps, rq_batch_config* best, float* best_ms) {
+  if (!best) return bfail(RQ_ERR_ARG, "best is NULL");
+  std::vector<rq_batch_config> cand;
+  if (candidates && n_candidates > 0) {
+    cand.assign(candidates, candidates + n_candidates);
+  } else {
+    for (int bt : {64, 128, 256})
+      for (int cr : {32, 128, 512})
+        for (int rf : {1, 8, 24})
+          for (int rs : {0, 2}) {
+            rq_batch_config c;
+            c.block_threads = bt;
+            c.blocks_per_sm = 0;
+            c.chunk_rays = cr;
+            c.refill_threshold = rf;
+            c.reg_stack = rs;
+            cand.push_back(c);
+          }
+  }
+  if (reps < 1) reps = 1;
+  const rq::Scene* s0 = reinterpret_cast<const rq::Scene*>(scenes ? scenes[0] : nullptr);
+  if (!s0) return bfail(RQ_ERR_ARG, "NULL scene");
+  if (cudaSetDevice(s0->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
+  cudaStream_t st;
+  cudaEvent_t e0, e1;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+    return bfail(RQ_ERR_CUDA, "stream");
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float bms = 1e30f;
+  int rc = RQ_OK;
+  for (const rq_batch_config& c : cand) {
+    rq_batch_plan* p = nullptr;
+    rc = rq_batch_plan_create(scenes, n_scenes, batches, n_batches, &c, &p);
+    if (rc != RQ_OK) break;
+    rq_batch_plan_launch(p, st);  // warm-up
+    cudaEventRecord(e0, st);
+    for (int k = 0; k < reps; ++k) rq_batch_plan_launch(p, st);
+    cudaEventRecord(e1, st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    rq_batch_plan_destroy(p);
+    if (e != cudaSuccess) {
+      rc = bfail(RQ_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+      break;
+    }
+    ms /= reps;
+    if (ms < bms) {
+      bms = ms;
+      *best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  if (rc == RQ_OK && best_ms) *best_ms = bms;
+  return rc;
+}
+
+}  // extern "C"

@@ -139,3 +139,118 @@ __device__ __forceinline__ void store_hit(const RayArgs& a, int i,
 }
 
 }  // namespace rq
+
+namespace rq {
+
+// Traversal stack whose top R entries (0 or 2) stay in registers and whose
+// older entries spill to this thread's shared-memory column.  LIFO order is
+// kept: registers hold the newest entries, the shared column the older ones.
+template <int R>
+struct RegStack {
+  int2 r0, r1;
+  int nreg;
+  int sp;
+  int2* col;
+  int stride;
+  __device__ __forceinline__ void init(int2* c, int s) {
+    nreg = 0;
+    sp = 0;
+    col = c;
+    stride = s;
+  }
+  __device__ __forceinline__ void push(int2 e) {
+    if (R == 0) {
+      col[sp * stride] = e;
+      ++sp;
+    } else if (nreg == 2) {
+      col[sp * stride] = r0;
+      ++sp;
+      r0 = r1;
+      r1 = e;
+    } else if (nreg == 1) {
+      r1 = e;
+      nreg = 2;
+    } else {
+      r0 = e;
+      nreg = 1;
+    }
+  }
+  __device__ __forceinline__ bool pop(int2& e) {
+    if (R != 0 && nreg == 2) {
+      e = r1;
+      nreg = 1;
+      return true;
+    }
+    if (R != 0 && nreg == 1) {
+      e = r0;
+      nreg = 0;
+      return true;
+    }
+    if (sp > 0) {
+      --sp;
+      e = col[sp * stride];
+      return true;
+    }
+    return false;
+  }
+};
+
+// The while-while step with the any-hit flag decided per ray at run time
+// (a warp of the batched kernel may hold closest-hit and any-hit rays of
+// different batches and scenes at once) and a RegStack.
+template <int KIND, int R, bool STATS = false>
+__device__ __forceinline__ void step_dyn(const DevScene& S, Ray& r, Hit& h, int& ref,
+                                         RegStack<R>& st, bool any, Counts* cnt = nullptr) {
+  while (ref >= 0 && ref != kDone) {
+    if (STATS) cnt->boxes += 2;
+    const float4* p = S.nodes + 4 * (size_t)ref;
+    const float4 q0 = __ldg(p);
+    const float4 q1 = __ldg(p + 1);
+    const float4 q2 = __ldg(p + 2);
+    const int4 q3 = __ldg(reinterpret_cast<const int4*>(p + 3));
+    float tl, tr;
+    const bool hl = box_test(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, tl);
+    const bool hr = box_test(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, tr);
+    if (hl && hr) {
+      const bool left_first =
+          any ? (((q3.z >> 2) & 1) != 0) : (pick3(r.d, q3.z & 3) > 0.f);
+      st.push(make_int2(left_first ? q3.y : q3.x, __float_as_int(left_first ? tr : tl)));
+      ref = left_first ? q3.x : q3.y;
+    } else if (hl) {
+      ref = q3.x;
+    } else if (hr) {
+      ref = q3.y;
+    } else {
+      ref = kDone;
+      int2 e;
+      while (st.pop(e))
+        if (__int_as_float(e.y) <= r.minT) {
+          ref = e.x;
+          break;
+        }
+    }
+  }
+  if (ref == kDone) return;
+  const float4* p = S.tris + 3 * (size_t)(~ref);
+  for (;;) {
+    bool last;
+    if (STATS) cnt->tris += 1;
+    const bool hit = tri_test<KIND>(r, p, h, last);
+    if (hit) h.pos = (int)((p - S.tris) / 3);
+    if (any && hit) {
+      ref = kDone;
+      return;
+    }
+    if (last) break;
+    p += 3;
+  }
+  ref = kDone;
+  int2 e;
+  while (st.pop(e))
+    if (__int_as_float(e.y) <= r.minT) {
+      ref = e.x;
+      break;
+    }
+}
+
+}  // namespace rq

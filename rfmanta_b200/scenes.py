@@ -326,3 +326,65 @@ def tiny_path_scene(xres: int = 40, yres: int = 30, spp: int = 4) -> PathScene:
     """The path-tracing layout scaled down for committed checks."""
     return path_scene(hf_nx=16, hf_nz=16, n_spheres=3, sphere_level=2, xres=xres,
                       yres=yres, spp=spp, max_depth=4, rr_depth=2, seed=5)
+
+
+def sphere_set(n: int, level: int, seed: int, extent: float = 6.0) -> Mesh:
+    """n displaced icospheres of the given level at seeded positions."""
+    rng = np.random.default_rng(seed)
+    v, f = icosphere(level)
+    parts = []
+    for k in range(n):
+        noise = ValueNoise(seed * 1000 + k).noise3(v * 4.0 + 17.0)
+        r = float(rng.uniform(0.2, 0.6)) * (1.0 + 0.05 * (2.0 * noise - 1.0))
+        c = rng.uniform(-extent / 2, extent / 2, 3)
+        parts.append(Mesh((v * r[:, None] + c).astype(np.float32), f.astype(np.uint32),
+                          np.zeros(f.shape[0], np.uint32)))
+    return merge(parts, np.array([[0.7, 0.7, 0.7]], np.float32))
+
+
+# (kind, size) of the eight resident scenes of the batched-query workload,
+# 10,240 to 5,120,000 triangles
+QUERY_SCENE_SPECS = [("spheres", (2, 4)), ("heightfield", 128), ("spheres", (20, 4)),
+                     ("heightfield", 384), ("spheres", (12, 6)), ("heightfield", 1024),
+                     ("spheres", (40, 6)), ("heightfield", 1600)]
+
+
+def query_scene(i: int, seed: int = 100) -> Mesh:
+    kind, size = QUERY_SCENE_SPECS[i]
+    if kind == "spheres":
+        return sphere_set(size[0], size[1], seed + i)
+    m = heightfield(size, size, seed + i, extent=6.0, y=0.0)
+    m.materials = np.array([[0.7, 0.7, 0.7]], np.float32)
+    return m
+
+
+def query_batches(n_batches: int = 64, n_scenes: int = 8, lo: int = 1000,
+                  hi: int = 4_000_000, seed: int = 7, scale: float = 1.0):
+    """(scene, rays, anyhit) per batch: sizes log-uniform in [lo, hi]
+    (times `scale`), scenes uniform, half any-hit."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), n_batches))
+    sizes = np.maximum((sizes * scale).astype(np.int64), 1)
+    scene = rng.integers(0, n_scenes, n_batches)
+    anyhit = rng.random(n_batches) < 0.5
+    return [(int(s), int(n), bool(a)) for s, n, a in zip(scene, sizes, anyhit)]
+
+
+def query_rays_torch(n: int, lo, hi, anyhit: bool, seed: int, device="cuda"):
+    """Origins uniform in [lo, hi], directions uniform on the sphere; tmax
+    uniform in [0.1, |hi-lo|] for any-hit rays, 1e19 otherwise (torch, on
+    the device, from a seeded generator)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    lo_t = torch.tensor(np.asarray(lo, np.float32), device=device).view(3, 1)
+    hi_t = torch.tensor(np.asarray(hi, np.float32), device=device).view(3, 1)
+    org = lo_t + (hi_t - lo_t) * torch.rand(3, n, generator=g, device=device)
+    d = torch.randn(3, n, generator=g, device=device)
+    d = d / d.norm(dim=0, keepdim=True)
+    diag = float(np.linalg.norm(np.asarray(hi) - np.asarray(lo)))
+    if anyhit:
+        tmax = 0.1 + (max(diag, 0.1) - 0.1) * torch.rand(n, generator=g, device=device)
+    else:
+        tmax = torch.full((n,), 1e19, device=device)
+    return org.contiguous(), d.contiguous(), tmax.contiguous()

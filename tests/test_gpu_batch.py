@@ -1,0 +1,116 @@
+"""Batched multi-scene queries in one persistent, graph-captured launch:
+every configuration (block size, rays per warp chunk, refill threshold,
+register stack entries) and the autotuned one give, for every batch, the
+same bits as tracing that batch alone (rq_trace), which the other tests tie
+to the reference."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def setup():
+    import torch
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.batch import QueryBatch
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    meshes = [scenes.sphere_set(3, 3, seed=1), scenes.heightfield(40, 30, seed=2, extent=4.0),
+              scenes.small_frame_scene(level=3, grid=10).mesh]
+    bvhs = []
+    for m in meshes:
+        b = GpuDynBVH()
+        b.setGroup(m)
+        b.rebuild()
+        bvhs.append(b)
+    rng = np.random.default_rng(5)
+    sizes = [1, 31, 32, 33, 1000, 4097, 17, 20000, 0, 250, 3000, 64]
+    batches, host = [], []
+    for k, n in enumerate(sizes):
+        si = int(rng.integers(0, 3))
+        lo, hi = meshes[si].bounds()
+        o, d, tm, _ = scenes.random_rays(n, lo - 0.3, hi + 0.3, seed=100 + k,
+                                         anyhit_fraction=1.0 if k % 2 else 0.0)
+        anyhit = bool(k % 2)
+        if not anyhit:
+            tm = np.full(n, 1e19, np.float32)
+        host.append((si, o, d, tm, anyhit))
+        batches.append(QueryBatch(si, torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda(),
+                                  torch.from_numpy(tm).cuda(), anyhit, want_uv=True))
+    return bvhs, batches, host
+
+
+def _expected(bvhs, host):
+    from rfmanta_b200.dynbvh import RayBatch
+    out = []
+    for si, o, d, tm, anyhit in host:
+        r = RayBatch(o, d, tm, flags=RayBatch.AnyHit if anyhit else 0)
+        if len(r):
+            bvhs[si].intersect(r)
+        out.append(r)
+    return out
+
+
+def _check(bq, exp):
+    import torch
+    torch.cuda.synchronize()
+    for i, r in enumerate(exp):
+        assert np.array_equal(bq.prim[i].cpu().numpy(), r.hitPrim), i
+        assert np.array_equal(_bits(bq.t[i].cpu().numpy()), _bits(r.minT)), i
+
+
+@pytest.mark.parametrize("cfg", [None,
+                                 dict(block_threads=64, chunk_rays=32, refill_threshold=1, reg_stack=0),
+                                 dict(block_threads=256, chunk_rays=512, refill_threshold=32, reg_stack=2),
+                                 dict(block_threads=128, chunk_rays=96, refill_threshold=5, reg_stack=2,
+                                      blocks_per_sm=1)])
+def test_batches_match_single_queries(setup, cfg):
+    from rfmanta_b200.batch import BatchedQueries
+    bvhs, batches, host = setup
+    bq = BatchedQueries(bvhs, batches, cfg)
+    bq.launch()
+    _check(bq, _expected(bvhs, host))
+    bq.launch()  # graph replay
+    _check(bq, _expected(bvhs, host))
+    bq.close()
+
+
+def test_autotune_and_new_rays(setup):
+    import torch
+    from rfmanta_b200.batch import BatchedQueries
+    bvhs, batches, host = setup
+    bq = BatchedQueries(bvhs, batches)
+    cfg = bq.autotune(reps=1, candidates=[dict(chunk_rays=32), dict(chunk_rays=256, reg_stack=0)])
+    assert cfg["chunk_rays"] in (32, 256)
+    # write new rays into the same device arrays and replay the plan
+    rng = np.random.default_rng(9)
+    for b, h in zip(batches, host):
+        n = b.tmax.shape[0]
+        if n:
+            flip = torch.from_numpy(np.where(rng.random(n) < 0.5, -1, 1).astype(np.float32)).cuda()
+            b.dir.mul_(flip)
+    new_host = [(si, None, None, tm, a) for (si, o, d, tm, a) in host]
+    new_host = [(si, b.org.cpu().numpy(), b.dir.cpu().numpy(), tm, a)
+                for (si, _, _, tm, a), b in zip(new_host, batches)]
+    bq.launch()
+    _check(bq, _expected(bvhs, new_host))
+    bq.close()
+
+
+def test_plan_errors(setup):
+    import ctypes as C
+    from rfmanta_b200 import _lib
+    bvhs, batches, host = setup
+    arr = (_lib.Batch * 1)()
+    arr[0].scene = 5
+    arr[0].n = 1
+    arr[0].flags = 0
+    scenes = (C.c_void_p * 1)(bvhs[0].handle.value)
+    plan = C.c_void_p()
+    assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, None, C.byref(plan)) == _lib.RQ_ERR_ARG
+    arr[0].scene = 0
+    assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, None, C.byref(plan)) == _lib.RQ_ERR_ARG

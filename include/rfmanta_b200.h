@@ -247,6 +247,52 @@ RQ_API int rq_batch_autotune(rq_scene* const* scenes, int n_scenes,
                              int reps, rq_batch_config* best, float* best_ms);
 
 /*
+ * Served path tracing with continuous batching.  A server keeps its scenes'
+ * trees resident, queues submitted render requests, admits them in arrival
+ * order while their output images fit `hbm_budget_bytes`, and each step
+ * packs fixed pixel chunks (chunk_pixels whole pixels, all samples) of many
+ * admitted requests - different scenes, resolutions, spp and depths - into
+ * one wavefront of up to path_capacity paths.  At most two steps are in
+ * flight.  A request's image is identical, bit for bit, whether it ran
+ * alone or with others, and identical to rq_render_path with the same
+ * parameters.  All scenes share one device and triangle kind.
+ */
+typedef struct {
+  int scene;                       /* index into the server's scenes */
+  float eye[3], lookat[3], up[3];  /* PinholeCamera */
+  float hfov, vfov;
+  int xres, yres, spp, max_depth, rr_depth;
+  uint64_t seed;
+  float light_anchor[3], light_v1[3], light_v2[3], light_color[3];
+  float background[3];
+  int n_materials;
+  const float* material_rgb;       /* host, copied on submit */
+} rq_serve_request;
+
+typedef struct rq_server rq_server;
+
+RQ_API int rq_server_create(rq_scene* const* scenes, int n_scenes,
+                            long long path_capacity, int chunk_pixels,
+                            size_t hbm_budget_bytes, rq_server** out);
+/* Queues a request (admitted by a later rq_server_step). */
+RQ_API int rq_server_submit(rq_server* server, const rq_serve_request* request,
+                            int* request_id);
+/* Admits what fits, enqueues one step; *scheduled_paths = its path count
+ * (0 when nothing was waiting).  Blocks only to keep two steps in flight. */
+RQ_API int rq_server_step(rq_server* server, int* scheduled_paths);
+/* Ids of requests finished on the device since the last poll. */
+RQ_API int rq_server_poll(rq_server* server, int* done_ids, int max_ids, int* n_done);
+/* Copies a finished request's image (rgb may be NULL) and reports its
+ * latency (submit to observed completion) and its admission wait. */
+RQ_API int rq_server_result(rq_server* server, int request_id, float* rgb,
+                            double* latency_s, double* queue_s);
+/* Frees a request's image and returns its bytes to the budget. */
+RQ_API int rq_server_release(rq_server* server, int request_id);
+RQ_API int rq_server_stats(rq_server* server, uint64_t* ray_counts, long long* steps,
+                           int* pending, int* active, size_t* bytes_in_use);
+RQ_API int rq_server_destroy(rq_server* server);
+
+/*
  * rq_render_whitted_device without any device allocation.  This entry point
  * has no counterpart in the reference.  It is for callers that cannot call
  * cudaMalloc: a process whose device memory is already handed out to another

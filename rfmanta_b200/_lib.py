@@ -77,6 +77,16 @@ class BatchConfig(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServeRequest(C.Structure):
+    _fields_ = [("scene", C.c_int), ("eye", C.c_float * 3), ("lookat", C.c_float * 3),
+                ("up", C.c_float * 3), ("hfov", C.c_float), ("vfov", C.c_float),
+                ("xres", C.c_int), ("yres", C.c_int), ("spp", C.c_int), ("max_depth", C.c_int),
+                ("rr_depth", C.c_int), ("seed", C.c_uint64), ("light_anchor", C.c_float * 3),
+                ("light_v1", C.c_float * 3), ("light_v2", C.c_float * 3),
+                ("light_color", C.c_float * 3), ("background", C.c_float * 3),
+                ("n_materials", C.c_int), ("material_rgb", C.c_void_p)]
+
+
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
                 ("refill_threshold", C.c_int), ("persistent", C.c_int)]
@@ -120,6 +130,15 @@ def _load():
         "rq_batch_plan_info": ([vp, vp, C.POINTER(i), C.POINTER(C.c_longlong)], i),
         "rq_batch_plan_destroy": ([vp], i),
         "rq_batch_autotune": ([vp, i, vp, i, vp, i, i, vp, C.POINTER(C.c_float)], i),
+        "rq_server_create": ([vp, i, C.c_longlong, i, sz, C.POINTER(vp)], i),
+        "rq_server_submit": ([vp, C.POINTER(ServeRequest), C.POINTER(i)], i),
+        "rq_server_step": ([vp, C.POINTER(i)], i),
+        "rq_server_poll": ([vp, vp, i, C.POINTER(i)], i),
+        "rq_server_result": ([vp, i, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)], i),
+        "rq_server_release": ([vp, i], i),
+        "rq_server_stats": ([vp, vp, C.POINTER(C.c_longlong), C.POINTER(i), C.POINTER(i),
+                             C.POINTER(sz)], i),
+        "rq_server_destroy": ([vp], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
     }
     for name, (args, res) in sig.items():

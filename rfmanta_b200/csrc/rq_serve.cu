@@ -1,0 +1,633 @@
+// Served path tracing with continuous batching (rq_server_*).
+//
+// Device side: one wavefront step serves chunks of many requests at once.
+// A chunk is a fixed range of whole pixels of one request (all of their
+// samples); each path slot of the step's pool records its request and its
+// global path id inside that request, and every kernel reads the slot's own
+// request parameters and scene.  A path's computation depends only on
+// (request, path id) - its PCG32 stream, camera sample, scene and depth -
+// and every pixel is resolved inside the chunk that holds all its samples,
+// so a request's image is the same bits whether it ran alone or mixed with
+// any other requests.
+//
+// Host side (the engine): requests are queued on submit, admitted in
+// arrival order while their output image fits the HBM budget, and each
+// step takes chunks round-robin from the admitted requests until the path
+// pool is full; at most two steps are in flight, and a request completes
+// when the step holding its last chunk has finished on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/rfmanta_b200.h"
+#include "rq_pathcore.cuh"
+#include "rq_render.h"
+#include "rq_scene.h"
+
+namespace rq {
+
+constexpr int kMaxServeScenes = 32;
+
+struct ServeReq {
+  PathParams P;
+  int scene;
+  float* out;  // device rgb image
+};
+
+struct ServeChunk {
+  int req;    // index into the step's request table
+  int pix0;   // first pixel of the chunk in the request's image
+  int npix;
+  int slot0;  // first path slot of the chunk in the pool
+  int px0;    // prefix of pixels over the step's chunks
+};
+
+struct ServeArgs {
+  const DevScene* scenes;
+  int n_scenes;
+  const ServeReq* reqs;
+  const ServeChunk* chunks;
+  int n_chunks;
+  int n_slots;  // paths in this step
+  int n_pix;    // pixels in this step
+  int* slot_req;
+  long long* slot_g;
+};
+
+__device__ __forceinline__ int find_chunk_by_slot(const ServeArgs& A, int s) {
+  int lo = 0, hi = A.n_chunks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (A.chunks[mid].slot0 <= s) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void serve_generate_kernel(ServeArgs A, PathBuffers B) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n_slots;
+       s += gridDim.x * blockDim.x) {
+    const ServeChunk c = A.chunks[find_chunk_by_slot(A, s)];
+    const ServeReq& R = A.reqs[c.req];
+    const long long g = (long long)c.pix0 * R.P.spp + (s - c.slot0);
+    generate_path(R.P, B, g, s);
+    A.slot_req[s] = c.req;
+    A.slot_g[s] = g;
+  }
+}
+
+__device__ __forceinline__ void stage_scenes(const ServeArgs& A, DevScene* sm) {
+  for (int i = threadIdx.x; i < A.n_scenes; i += blockDim.x) sm[i] = A.scenes[i];
+  __syncthreads();
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128) serve_extend_kernel(ServeArgs A, PathBuffers B, int depth) {
+  extern __shared__ int2 smem_stack[];
+  __shared__ DevScene sm_scenes[kMaxServeScenes];
+  stage_scenes(A, sm_scenes);
+  int2* stk = smem_stack + threadIdx.x;
+  const int nq = depth == 0 ? A.n_slots : *(volatile const int*)&B.counters[depth];
+  const int* qin = B.queue[depth & 1];
+  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
+    const int qi = base + threadIdx.x;
+    if (qi < nq) {
+      const int p = depth == 0 ? qi : qin[qi];
+      const ServeReq& R = A.reqs[A.slot_req[p]];
+      Counts cnt;
+      extend_path<KIND, false>(sm_scenes[R.scene], R.P, B, depth, p, stk, blockDim.x, cnt);
+    }
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128) serve_shade_kernel(ServeArgs A, PathBuffers B, int depth) {
+  extern __shared__ int2 smem_stack[];
+  __shared__ DevScene sm_scenes[kMaxServeScenes];
+  stage_scenes(A, sm_scenes);
+  int2* stk = smem_stack + threadIdx.x;
+  const int nq = depth == 0 ? A.n_slots : *(volatile const int*)&B.counters[depth];
+  const int* qin = B.queue[depth & 1];
+  int* qout = B.queue[(depth + 1) & 1];
+  const unsigned lane = threadIdx.x & 31u;
+  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
+    const int qi = base + threadIdx.x;
+    bool alive = false;
+    int p = 0, nshadow = 0;
+    if (qi < nq) {
+      p = depth == 0 ? qi : qin[qi];
+      const ServeReq& R = A.reqs[A.slot_req[p]];
+      Counts cnt;
+      // a request whose depth is already reached keeps no live paths here
+      alive = shade_path<KIND, false>(sm_scenes[R.scene], R.P, B, depth, p, A.slot_g[p], stk,
+                                      blockDim.x, cnt, nshadow);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, alive);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      int q = 0;
+      if ((int)lane == leader) q = atomicAdd(&B.counters[depth + 1], __popc(m));
+      q = __shfl_sync(0xffffffffu, q, leader);
+      if (alive) qout[q + __popc(m & ((1u << lane) - 1u))] = p;
+    }
+    int tot = nshadow;
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0 && tot) atomicAdd(&B.ray_counts[1], (unsigned long long)tot);
+  }
+}
+
+__global__ void serve_count_kernel(ServeArgs A, PathBuffers B, int depth) {
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    atomicAdd(&B.ray_counts[0],
+              (unsigned long long)(depth == 0 ? A.n_slots : B.counters[depth]));
+}
+
+// Per pixel of the step: the mean of its samples in sample order, written
+// into the request's image.
+__global__ void serve_resolve_kernel(ServeArgs A, PathBuffers B) {
+  const size_t C = B.capacity;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < A.n_pix; k += gridDim.x * blockDim.x) {
+    int lo = 0, hi = A.n_chunks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (A.chunks[mid].px0 <= k) lo = mid;
+      else hi = mid - 1;
+    }
+    const ServeChunk c = A.chunks[lo];
+    const ServeReq& R = A.reqs[c.req];
+    const int j = k - c.px0;
+    const int spp = R.P.spp;
+    const float inv = fdiv(1.f, (float)spp);
+    float acc[3] = {0.f, 0.f, 0.f};
+    for (int s = 0; s < spp; ++s) {
+      const int p = c.slot0 + j * spp + s;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) acc[q] = fadd(acc[q], B.rad[q * C + p]);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) R.out[3 * (size_t)(c.pix0 + j) + q] = fmul(acc[q], inv);
+  }
+}
+
+template <int KIND>
+static cudaError_t serve_launch_step(const ServeArgs& A, PathBuffers B, int max_depth,
+                                     int grid, size_t smem, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(B.counters, 0, kPathCounters * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int gg = std::max(1, std::min(grid, (A.n_slots + 255) / 256));
+  serve_generate_kernel<<<gg, 256, 0, st>>>(A, B);
+  for (int depth = 0; depth < max_depth; ++depth) {
+    serve_count_kernel<<<1, 32, 0, st>>>(A, B, depth);
+    serve_extend_kernel<KIND><<<grid, 128, smem, st>>>(A, B, depth);
+    serve_shade_kernel<KIND><<<grid, 128, smem, st>>>(A, B, depth);
+  }
+  const int rg = std::max(1, std::min(grid, (A.n_pix + 255) / 256));
+  serve_resolve_kernel<<<rg, 256, 0, st>>>(A, B);
+  return cudaGetLastError();
+}
+
+static int serve_blocks_per_sm(int kind, size_t smem) {
+  const void* fs[2] = {kind == kWald ? (const void*)serve_extend_kernel<kWald>
+                                     : (const void*)serve_extend_kernel<kKS>,
+                       kind == kWald ? (const void*)serve_shade_kernel<kWald>
+                                     : (const void*)serve_shade_kernel<kKS>};
+  int a = 1, b = 1;
+  for (const void* f : fs)
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, fs[0], 128, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fs[1], 128, smem);
+  return std::max(1, std::min(a, b));
+}
+
+}  // namespace rq
+
+namespace {
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+int sfail(int code, const std::string& m) {
+  rq::set_error(m);
+  return code;
+}
+
+struct HostReq {
+  int id = 0;
+  rq_serve_request spec{};
+  std::vector<float> materials;
+  rq::ServeReq dev{};  // parameters as the kernels see them (out, materials set on admission)
+  float* d_mat = nullptr;
+  float* d_out = nullptr;
+  size_t bytes = 0;
+  int npix = 0;
+  int next_pix = 0;
+  bool admitted = false;
+  bool scheduled_all = false;
+  bool done = false;
+  bool reported = false;
+  cudaEvent_t done_ev = nullptr;
+  double t_submit = 0, t_admit = 0, t_done = 0;
+};
+
+}  // namespace
+
+struct rq_server {
+  int device = 0;
+  int tri_kind = 0;
+  int num_sms = 148;
+  std::vector<rq::Scene*> scenes;
+  rq::DevScene* d_scenes = nullptr;
+  int n_scenes = 0;
+  int depth = 1;
+  long long capacity = 0;
+  int chunk_pixels = 0;
+  size_t budget = 0;
+  size_t used = 0;
+  int max_active = 256;
+  int max_chunks = 8192;
+  rq::PathBuffers B{};
+  int* slot_req = nullptr;
+  long long* slot_g = nullptr;
+  unsigned long long* counts = nullptr;
+  rq::ServeReq* d_reqs = nullptr;
+  rq::ServeChunk* d_chunks = nullptr;
+  // pinned staging ring for the per-step tables
+  static const int kRing = 3;
+  rq::ServeReq* h_reqs[kRing] = {};
+  rq::ServeChunk* h_chunks[kRing] = {};
+  cudaEvent_t ring_ev[kRing] = {};   // after a step's table upload
+  cudaEvent_t end_ev[kRing] = {};    // after a step's last kernel
+  bool ring_used[kRing] = {};
+  cudaStream_t stream = nullptr;
+  std::map<int, std::unique_ptr<HostReq>> reqs;
+  std::deque<int> pending;   // submitted, not admitted
+  std::vector<int> active;   // admitted, not finished (admission order)
+  std::vector<int> table;    // request id per device-table slot
+  int rr = 0;                // round-robin cursor
+  int next_id = 1;
+  long long steps = 0;
+  int grid = 1;
+  size_t smem = 0;
+
+  ~rq_server() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& kv : reqs) {
+      HostReq& r = *kv.second;
+      cudaFree(r.d_out);
+      cudaFree(r.d_mat);
+      if (r.done_ev) cudaEventDestroy(r.done_ev);
+    }
+    cudaFree(B.o); cudaFree(B.d); cudaFree(B.imp); cudaFree(B.rad); cudaFree(B.rng);
+    cudaFree(B.t); cudaFree(B.pos); cudaFree(B.prim); cudaFree(B.queue[0]); cudaFree(B.queue[1]);
+    cudaFree(B.counters); cudaFree(slot_req); cudaFree(slot_g); cudaFree(counts);
+    cudaFree(d_reqs); cudaFree(d_chunks); cudaFree(d_scenes);
+    for (int i = 0; i < kRing; ++i) {
+      cudaFreeHost(h_reqs[i]);
+      cudaFreeHost(h_chunks[i]);
+      if (ring_ev[i]) cudaEventDestroy(ring_ev[i]);
+      if (end_ev[i]) cudaEventDestroy(end_ev[i]);
+    }
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  bool admit(HostReq& r) {
+    const size_t need = r.bytes + r.materials.size() * sizeof(float);
+    if ((int)active.size() >= max_active || used + need > budget) return false;
+    if (cudaMalloc(&r.d_out, r.bytes) != cudaSuccess) return false;
+    if (cudaMalloc(&r.d_mat, r.materials.size() * sizeof(float)) != cudaSuccess) {
+      cudaFree(r.d_out);
+      r.d_out = nullptr;
+      return false;
+    }
+    cudaMemcpyAsync(r.d_mat, r.materials.data(), r.materials.size() * sizeof(float),
+                    cudaMemcpyHostToDevice, stream);
+    cudaEventCreateWithFlags(&r.done_ev, cudaEventDisableTiming);
+    r.dev.P.materials = r.d_mat;
+    r.dev.out = r.d_out;
+    used += need;
+    r.admitted = true;
+    r.t_admit = now_s();
+    active.push_back(r.id);
+    return true;
+  }
+};
+
+namespace {
+
+// PathParams of a request (camera basis and Parallelogram as in the frame path).
+void request_params(const rq_serve_request& q, rq::PathParams& P) {
+  std::memset(&P, 0, sizeof(P));
+  rq::camera_basis(q.eye, q.lookat, q.up, q.hfov, q.vfov, P.cam);
+  P.xres = q.xres;
+  P.yres = q.yres;
+  P.spp = q.spp;
+  P.strata = (int)std::lround(std::sqrt((double)q.spp));
+  P.max_depth = q.max_depth;
+  P.rr_depth = q.rr_depth;
+  P.seed = q.seed;
+  for (int c = 0; c < 3; ++c) {
+    P.light_anchor[c] = q.light_anchor[c];
+    P.light_v1[c] = q.light_v1[c];
+    P.light_v2[c] = q.light_v2[c];
+    P.light_color[c] = q.light_color[c];
+    P.background[c] = q.background[c];
+  }
+  const float* v1 = q.light_v1;
+  const float* v2 = q.light_v2;
+  float n[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2],
+                v1[0] * v2[1] - v1[1] * v2[0]};
+  const float l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  const float sc = 1 / l;
+  for (int c = 0; c < 3; ++c) P.light_normal[c] = n[c] * sc;
+  P.light_inv_area = (float)1 / l;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capacity,
+                     int chunk_pixels, size_t hbm_budget_bytes, rq_server** out) {
+  using namespace rq;
+  if (!out) return sfail(RQ_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!scenes || n_scenes <= 0 || n_scenes > kMaxServeScenes) return sfail(RQ_ERR_ARG, "1..32 scenes");
+  if (path_capacity < 1024 || path_capacity > (1LL << 30)) return sfail(RQ_ERR_ARG, "bad path capacity");
+  if (chunk_pixels <= 0 || (long long)chunk_pixels * 4096 > (1LL << 40))
+    return sfail(RQ_ERR_ARG, "bad chunk_pixels");
+  std::unique_ptr<rq_server> s(new rq_server());
+  const Scene* s0 = reinterpret_cast<const Scene*>(scenes[0]);
+  if (!s0) return sfail(RQ_ERR_ARG, "NULL scene");
+  std::vector<DevScene> ds(n_scenes);
+  for (int i = 0; i < n_scenes; ++i) {
+    Scene* sc = reinterpret_cast<Scene*>(scenes[i]);
+    if (!sc || !sc->has_tree) return sfail(RQ_ERR_STATE, "scene without a tree");
+    if (sc->device != s0->device || sc->tri_kind != s0->tri_kind)
+      return sfail(RQ_ERR_ARG, "scenes must share device and triangle kind");
+    ds[i] = sc->dev();
+    s->depth = std::max(s->depth, ds[i].depth);
+    s->scenes.push_back(sc);
+  }
+  s->device = s0->device;
+  s->tri_kind = s0->tri_kind;
+  s->num_sms = s0->num_sms;
+  s->n_scenes = n_scenes;
+  s->capacity = path_capacity;
+  s->chunk_pixels = chunk_pixels;
+  s->budget = hbm_budget_bytes;
+  if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  const size_t C = (size_t)path_capacity;
+  PathBuffers& B = s->B;
+  B.capacity = C;
+  bool ok = cudaMalloc(&B.o, 12 * C) == cudaSuccess && cudaMalloc(&B.d, 12 * C) == cudaSuccess &&
+            cudaMalloc(&B.imp, 12 * C) == cudaSuccess && cudaMalloc(&B.rad, 12 * C) == cudaSuccess &&
+            cudaMalloc(&B.rng, 8 * C) == cudaSuccess && cudaMalloc(&B.t, 4 * C) == cudaSuccess &&
+            cudaMalloc(&B.pos, 4 * C) == cudaSuccess && cudaMalloc(&B.prim, 4 * C) == cudaSuccess &&
+            cudaMalloc(&B.queue[0], 4 * C) == cudaSuccess &&
+            cudaMalloc(&B.queue[1], 4 * C) == cudaSuccess &&
+            cudaMalloc(&B.counters, kPathCounters * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&s->slot_req, 4 * C) == cudaSuccess &&
+            cudaMalloc(&s->slot_g, 8 * C) == cudaSuccess &&
+            cudaMalloc(&s->counts, 16) == cudaSuccess &&
+            cudaMalloc(&s->d_reqs, sizeof(ServeReq) * s->max_active) == cudaSuccess &&
+            cudaMalloc(&s->d_chunks, sizeof(ServeChunk) * s->max_chunks) == cudaSuccess &&
+            cudaMalloc(&s->d_scenes, sizeof(DevScene) * n_scenes) == cudaSuccess;
+  for (int i = 0; ok && i < rq_server::kRing; ++i)
+    ok = cudaMallocHost(&s->h_reqs[i], sizeof(ServeReq) * s->max_active) == cudaSuccess &&
+         cudaMallocHost(&s->h_chunks[i], sizeof(ServeChunk) * s->max_chunks) == cudaSuccess &&
+         cudaEventCreateWithFlags(&s->ring_ev[i], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&s->end_ev[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) return sfail(RQ_ERR_OOM, "server pool allocation failed");
+  B.ray_counts = s->counts;
+  if (cudaMemset(s->counts, 0, 16) != cudaSuccess ||
+      cudaMemcpy(s->d_scenes, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return sfail(RQ_ERR_CUDA, "server setup");
+  s->smem = (size_t)s->depth * 128 * sizeof(int2);
+  s->grid = std::max(1, serve_blocks_per_sm(s->tri_kind, s->smem) * s->num_sms);
+  s->table.assign(s->max_active, 0);
+  *out = s.release();
+  return RQ_OK;
+}
+
+int rq_server_submit(rq_server* s, const rq_serve_request* q, int* request_id) {
+  if (!s || !q || !request_id) return sfail(RQ_ERR_ARG, "NULL argument");
+  const int strata = (int)std::lround(std::sqrt((double)q->spp));
+  if (q->scene < 0 || q->scene >= s->n_scenes) return sfail(RQ_ERR_ARG, "scene index out of range");
+  if (q->xres <= 0 || q->yres <= 0) return sfail(RQ_ERR_ARG, "bad resolution");
+  if (q->spp <= 0 || strata * strata != q->spp) return sfail(RQ_ERR_ARG, "spp must be a perfect square");
+  if ((long long)s->chunk_pixels * q->spp > s->capacity)
+    return sfail(RQ_ERR_CAPACITY, "a chunk of this request does not fit the path pool");
+  if (q->max_depth < 1 || q->max_depth > rq::kMaxPathDepth) return sfail(RQ_ERR_ARG, "max_depth in [1, 16]");
+  if (q->n_materials <= 0 || !q->material_rgb) return sfail(RQ_ERR_ARG, "no materials");
+  for (uint32_t m : s->scenes[q->scene]->face_mat)
+    if ((int)m >= q->n_materials) return sfail(RQ_ERR_ARG, "face_material past n_materials");
+  const size_t bytes = (size_t)q->xres * q->yres * 12;
+  if (bytes + (size_t)q->n_materials * 12 > s->budget)
+    return sfail(RQ_ERR_CAPACITY, "request larger than the server's HBM budget");
+  std::unique_ptr<HostReq> r(new HostReq());
+  r->id = s->next_id++;
+  r->spec = *q;
+  r->materials.assign(q->material_rgb, q->material_rgb + 3 * q->n_materials);
+  r->spec.material_rgb = nullptr;
+  request_params(*q, r->dev.P);
+  r->dev.scene = q->scene;
+  r->bytes = bytes;
+  r->npix = q->xres * q->yres;
+  r->t_submit = now_s();
+  *request_id = r->id;
+  s->pending.push_back(r->id);
+  s->reqs[r->id] = std::move(r);
+  return RQ_OK;
+}
+
+int rq_server_step(rq_server* s, int* scheduled_paths) {
+  using namespace rq;
+  if (!s) return sfail(RQ_ERR_ARG, "NULL server");
+  if (scheduled_paths) *scheduled_paths = 0;
+  if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  // admission in arrival order while the budget allows
+  while (!s->pending.empty()) {
+    HostReq& r = *s->reqs[s->pending.front()];
+    if (!s->admit(r)) break;
+    s->pending.pop_front();
+  }
+  // requests with pixels left, round-robin from the cursor
+  std::vector<int> cand;
+  for (int id : s->active)
+    if (!s->reqs[id]->scheduled_all) cand.push_back(id);
+  if (cand.empty()) return RQ_OK;
+  const int slot = (int)(s->steps % rq_server::kRing);
+  if (s->ring_used[slot] && cudaEventSynchronize(s->ring_ev[slot]) != cudaSuccess)
+    return sfail(RQ_ERR_CUDA, "staging ring wait failed");
+  ServeReq* hreq = s->h_reqs[slot];
+  ServeChunk* hch = s->h_chunks[slot];
+  std::map<int, int> tidx;  // request id -> table index this step
+  int n_chunks = 0, n_req = 0, max_depth = 1;
+  long long slots = 0, pix = 0;
+  bool progress = true;
+  size_t start = (size_t)(s->rr % (int)cand.size());
+  while (progress && n_chunks < s->max_chunks) {
+    progress = false;
+    for (size_t k = 0; k < cand.size() && n_chunks < s->max_chunks; ++k) {
+      HostReq& r = *s->reqs[cand[(start + k) % cand.size()]];
+      if (r.scheduled_all) continue;
+      const int npx = std::min(s->chunk_pixels, r.npix - r.next_pix);
+      const long long need = (long long)npx * r.spec.spp;
+      if (slots + need > s->capacity) continue;
+      int ti;
+      auto it = tidx.find(r.id);
+      if (it == tidx.end()) {
+        ti = n_req++;
+        tidx[r.id] = ti;
+        hreq[ti] = r.dev;
+      } else {
+        ti = it->second;
+      }
+      ServeChunk& c = hch[n_chunks++];
+      c.req = ti;
+      c.pix0 = r.next_pix;
+      c.npix = npx;
+      c.slot0 = (int)slots;
+      c.px0 = (int)pix;
+      slots += need;
+      pix += npx;
+      max_depth = std::max(max_depth, r.spec.max_depth);
+      r.next_pix += npx;
+      if (r.next_pix >= r.npix) r.scheduled_all = true;
+      progress = true;
+    }
+  }
+  s->rr = (int)((start + 1) % cand.size());
+  if (n_chunks == 0) return RQ_OK;
+  cudaStream_t st = s->stream;
+  cudaError_t e = cudaMemcpyAsync(s->d_reqs, hreq, sizeof(ServeReq) * n_req, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_chunks, hch, sizeof(ServeChunk) * n_chunks, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaEventRecord(s->ring_ev[slot], st);
+  s->ring_used[slot] = true;
+  ServeArgs A;
+  A.scenes = s->d_scenes;
+  A.n_scenes = s->n_scenes;
+  A.reqs = s->d_reqs;
+  A.chunks = s->d_chunks;
+  A.n_chunks = n_chunks;
+  A.n_slots = (int)slots;
+  A.n_pix = (int)pix;
+  A.slot_req = s->slot_req;
+  A.slot_g = s->slot_g;
+  if (e == cudaSuccess)
+    e = s->tri_kind == kWald ? serve_launch_step<kWald>(A, s->B, max_depth, s->grid, s->smem, st)
+                             : serve_launch_step<kKS>(A, s->B, max_depth, s->grid, s->smem, st);
+  if (e != cudaSuccess) return sfail(RQ_ERR_CUDA, std::string("serve step: ") + cudaGetErrorString(e));
+  for (auto& kv : tidx) {
+    HostReq& r = *s->reqs[kv.first];
+    if (r.scheduled_all) cudaEventRecord(r.done_ev, st);
+  }
+  cudaEventRecord(s->end_ev[slot], st);
+  ++s->steps;
+  if (scheduled_paths) *scheduled_paths = (int)slots;
+  // keep at most two steps in flight: wait for the end of the step before
+  // the one just enqueued
+  if (s->steps >= 2) {
+    const int prev = (int)((s->steps - 2) % rq_server::kRing);
+    if (cudaEventSynchronize(s->end_ev[prev]) != cudaSuccess)
+      return sfail(RQ_ERR_CUDA, "serve step failed on the device");
+  }
+  return RQ_OK;
+}
+
+int rq_server_poll(rq_server* s, int* done_ids, int max_ids, int* n_done) {
+  if (!s || !n_done) return sfail(RQ_ERR_ARG, "NULL argument");
+  *n_done = 0;
+  const double t = now_s();
+  std::vector<int> still;
+  for (int id : s->active) {
+    HostReq& r = *s->reqs[id];
+    if (r.scheduled_all && !r.done && cudaEventQuery(r.done_ev) == cudaSuccess) {
+      r.done = true;
+      r.t_done = t;
+    }
+    if (r.done) {
+      if (*n_done < max_ids && done_ids) done_ids[(*n_done)++] = id;
+      else if (!done_ids) ++*n_done;
+    } else {
+      still.push_back(id);
+    }
+  }
+  s->active.swap(still);
+  return RQ_OK;
+}
+
+int rq_server_result(rq_server* s, int request_id, float* rgb, double* latency_s,
+                     double* queue_s) {
+  if (!s) return sfail(RQ_ERR_ARG, "NULL server");
+  auto it = s->reqs.find(request_id);
+  if (it == s->reqs.end()) return sfail(RQ_ERR_ARG, "unknown request");
+  HostReq& r = *it->second;
+  if (!r.done) return sfail(RQ_ERR_STATE, "request not finished");
+  if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  if (rgb && cudaMemcpy(rgb, r.d_out, r.bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return sfail(RQ_ERR_CUDA, "result copy failed");
+  if (latency_s) *latency_s = r.t_done - r.t_submit;
+  if (queue_s) *queue_s = r.t_admit - r.t_submit;
+  return RQ_OK;
+}
+
+int rq_server_release(rq_server* s, int request_id) {
+  if (!s) return sfail(RQ_ERR_ARG, "NULL server");
+  auto it = s->reqs.find(request_id);
+  if (it == s->reqs.end()) return sfail(RQ_ERR_ARG, "unknown request");
+  HostReq& r = *it->second;
+  if (r.admitted && !r.done) return sfail(RQ_ERR_STATE, "request still running");
+  cudaSetDevice(s->device);
+  if (r.admitted) s->used -= r.bytes + r.materials.size() * sizeof(float);
+  cudaFree(r.d_out);
+  cudaFree(r.d_mat);
+  if (r.done_ev) cudaEventDestroy(r.done_ev);
+  if (!r.admitted) {
+    for (auto p = s->pending.begin(); p != s->pending.end(); ++p)
+      if (*p == request_id) {
+        s->pending.erase(p);
+        break;
+      }
+  }
+  s->reqs.erase(it);
+  return RQ_OK;
+}
+
+int rq_server_stats(rq_server* s, uint64_t* ray_counts, long long* steps, int* pending,
+                     int* active, size_t* bytes_in_use) {
+  if (!s) return sfail(RQ_ERR_ARG, "NULL server");
+  cudaSetDevice(s->device);
+  if (ray_counts) {
+    cudaStreamSynchronize(s->stream);
+    if (cudaMemcpy(ray_counts, s->counts, 16, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return sfail(RQ_ERR_CUDA, "counter copy failed");
+  }
+  if (steps) *steps = s->steps;
+  if (pending) *pending = (int)s->pending.size();
+  if (active) *active = (int)s->active.size();
+  if (bytes_in_use) *bytes_in_use = s->used;
+  return RQ_OK;
+}
+
+int rq_server_destroy(rq_server* s) {
+  delete s;
+  return RQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,184 @@
+"""Continuous-batching render server (rq_server_* in the C ABI).
+
+``RenderServer`` wraps the native engine; ``run_stream`` drives it with a
+timed arrival stream: requests are submitted when their arrival time comes,
+the engine is stepped whenever it has work, finished requests are collected
+and their latency (submit to completion observed on the host) recorded."""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+
+@dataclass
+class RenderRequest:
+    scene: int
+    eye: tuple
+    lookat: tuple
+    up: tuple
+    hfov: float
+    vfov: float
+    xres: int
+    yres: int
+    spp: int
+    max_depth: int
+    rr_depth: int
+    seed: int
+    light_anchor: tuple
+    light_v1: tuple
+    light_v2: tuple
+    light_color: tuple
+    background: tuple
+    materials: np.ndarray = field(default_factory=lambda: np.full((1, 3), 0.7, np.float32))
+
+    def to_c(self) -> _lib.ServeRequest:
+        q = _lib.ServeRequest()
+        q.scene = self.scene
+        q.eye[:], q.lookat[:], q.up[:] = self.eye, self.lookat, self.up
+        q.hfov, q.vfov = self.hfov, self.vfov
+        q.xres, q.yres, q.spp = self.xres, self.yres, self.spp
+        q.max_depth, q.rr_depth, q.seed = self.max_depth, self.rr_depth, self.seed
+        q.light_anchor[:], q.light_v1[:], q.light_v2[:] = (self.light_anchor, self.light_v1,
+                                                           self.light_v2)
+        q.light_color[:], q.background[:] = self.light_color, self.background
+        m = np.ascontiguousarray(self.materials, np.float32)
+        q.n_materials = m.shape[0]
+        q.material_rgb = m.ctypes.data
+        q._keep = m
+        return q
+
+    @property
+    def rays_upper(self) -> int:
+        return self.xres * self.yres * self.spp * self.max_depth * 2
+
+
+class RenderServer:
+    def __init__(self, scenes, path_capacity: int = 1 << 22, chunk_pixels: int = 16384,
+                 hbm_budget_bytes: int = 8 << 30):
+        self.scenes = scenes
+        arr = (C.c_void_p * len(scenes))(*[s.handle.value for s in scenes])
+        self._h = C.c_void_p()
+        check(lib.rq_server_create(arr, len(scenes), path_capacity, chunk_pixels,
+                                   hbm_budget_bytes, C.byref(self._h)))
+
+    def submit(self, req: RenderRequest) -> int:
+        rid = C.c_int()
+        q = req.to_c()
+        check(lib.rq_server_submit(self._h, C.byref(q), C.byref(rid)))
+        return rid.value
+
+    def step(self) -> int:
+        n = C.c_int()
+        check(lib.rq_server_step(self._h, C.byref(n)))
+        return n.value
+
+    def poll(self) -> list[int]:
+        ids = (C.c_int * 1024)()
+        n = C.c_int()
+        check(lib.rq_server_poll(self._h, ids, 1024, C.byref(n)))
+        return list(ids[: n.value])
+
+    def result(self, rid: int, xres: int, yres: int, copy: bool = True):
+        rgb = np.empty((xres * yres, 3), np.float32) if copy else None
+        lat, qs = C.c_double(), C.c_double()
+        check(lib.rq_server_result(self._h, rid, rgb.ctypes.data if copy else None,
+                                   C.byref(lat), C.byref(qs)))
+        return rgb, lat.value, qs.value
+
+    def release(self, rid: int) -> None:
+        check(lib.rq_server_release(self._h, rid))
+
+    def stats(self) -> dict:
+        counts = (C.c_uint64 * 2)()
+        steps, pend, act = C.c_longlong(), C.c_int(), C.c_int()
+        used = C.c_size_t()
+        check(lib.rq_server_stats(self._h, counts, C.byref(steps), C.byref(pend), C.byref(act),
+                                  C.byref(used)))
+        return dict(rays=int(counts[0]), shadow_rays=int(counts[1]), steps=steps.value,
+                    pending=pend.value, active=act.value, bytes_in_use=used.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib.rq_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_stream(self, stream: list[tuple[float, RenderRequest]], keep_images: bool = False,
+                   timeout_s: float = 600.0) -> dict:
+        """Submits each request at its arrival time (seconds from start),
+        steps until all are done.  Returns per-request latencies (s) and,
+        optionally, the images."""
+        order = sorted(range(len(stream)), key=lambda i: stream[i][0])
+        t0 = time.perf_counter()
+        ids, info = {}, {}
+        k = 0
+        done = 0
+        while done < len(stream):
+            now = time.perf_counter() - t0
+            if now > timeout_s:
+                raise TimeoutError("serving stream did not finish")
+            while k < len(order) and stream[order[k]][0] <= now:
+                i = order[k]
+                ids[self.submit(stream[i][1])] = i
+                k += 1
+            n = self.step()
+            for rid in self.poll():
+                i = ids[rid]
+                req = stream[i][1]
+                img, lat, qs = self.result(rid, req.xres, req.yres, copy=keep_images)
+                info[i] = dict(latency=lat, queue=qs, image=img)
+                self.release(rid)
+                done += 1
+            if n == 0 and k < len(order):
+                wait = stream[order[k]][0] - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.0005))
+            elif n == 0:
+                time.sleep(0.0002)
+        return dict(info=info, wall_s=time.perf_counter() - t0)
+
+
+def request_for_scene(scene_index: int, mesh, xres: int, yres: int, spp: int,
+                      max_depth: int, seed: int) -> RenderRequest:
+    """A camera looking at the scene from above and in front, a parallelogram
+    light above it."""
+    lo, hi = mesh.bounds()
+    c = (lo + hi) / 2
+    ext = float(np.max(hi - lo))
+    eye = (float(c[0]), float(hi[1] + 0.6 * ext), float(c[2] + 1.2 * ext))
+    vfov = float(2 * np.degrees(np.arctan(np.tan(np.radians(30.0)) * yres / xres)))
+    return RenderRequest(scene_index, eye, tuple(float(x) for x in c), (0.0, 1.0, 0.0), 60.0,
+                         vfov, xres, yres, spp, max_depth, 2, seed,
+                         (float(c[0] - 0.2 * ext), float(hi[1] + ext), float(c[2] - 0.2 * ext)),
+                         (0.4 * ext, 0.0, 0.0), (0.0, 0.0, 0.4 * ext), (20.0, 19.0, 17.0),
+                         (0.15, 0.2, 0.3), np.asarray(mesh.materials, np.float32))
+
+
+def poisson_stream(meshes, n: int, rate: float = 200.0, seed: int = 11):
+    """Seeded Poisson arrivals (mean `rate` per second) of render requests:
+    scene uniform over `meshes`, resolution from {256^2, 512^2, 1280x720,
+    1920x1080}, spp from {1, 4, 16}, bounce depth from {0, 2, 4}."""
+    rng = np.random.default_rng(seed)
+    res = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        si = int(rng.integers(0, len(meshes)))
+        xr, yr = res[int(rng.integers(0, 4))]
+        spp = int(rng.choice([1, 4, 16]))
+        bounces = int(rng.choice([0, 2, 4]))
+        out.append((t, request_for_scene(si, meshes[si], xr, yr, spp, bounces + 1,
+                                         seed=1000 + i)))
+    return out

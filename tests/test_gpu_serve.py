@@ -1,0 +1,107 @@
+"""Continuous-batching server: each request's image is the same bits alone
+and in a mix of requests of other scenes, sizes, spp and depths; equal to
+the single-frame path tracer for the same parameters; admission respects
+the HBM budget."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def scenes3():
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    meshes = [scenes.tiny_path_scene().mesh, scenes.sphere_set(4, 3, seed=2),
+              scenes.heightfield(30, 30, seed=3, extent=4.0, y=0.0)]
+    meshes[2].materials = np.array([[0.6, 0.5, 0.4]], np.float32)
+    bvhs = []
+    for m in meshes:
+        b = GpuDynBVH()
+        b.setGroup(m)
+        b.rebuild()
+        bvhs.append(b)
+    return meshes, bvhs
+
+
+def _requests(meshes):
+    from rfmanta_b200.serve import request_for_scene
+    spec = [(0, 40, 30, 4, 4), (1, 64, 48, 1, 1), (2, 33, 17, 16, 3), (0, 90, 60, 1, 5),
+            (1, 20, 20, 4, 2), (2, 128, 72, 4, 4), (0, 7, 5, 16, 4), (1, 50, 40, 9, 3)]
+    return [request_for_scene(s, meshes[s], x, y, spp, d, seed=50 + i)
+            for i, (s, x, y, spp, d) in enumerate(spec)]
+
+
+def _run(server, reqs):
+    ids = [server.submit(r) for r in reqs]
+    out = {}
+    for _ in range(100000):
+        server.step()
+        for rid in server.poll():
+            i = ids.index(rid)
+            img, lat, _ = server.result(rid, reqs[i].xres, reqs[i].yres)
+            out[i] = img
+            server.release(rid)
+        if len(out) == len(reqs):
+            return [out[i] for i in range(len(reqs))]
+    raise AssertionError("server did not finish")
+
+
+def test_alone_equals_mixed(scenes3):
+    from rfmanta_b200.serve import RenderServer
+    meshes, bvhs = scenes3
+    reqs = _requests(meshes)
+    alone = []
+    for r in reqs:
+        srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000)
+        alone.append(_run(srv, [r])[0])
+        srv.close()
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000)
+    mixed = _run(srv, reqs)
+    st = srv.stats()
+    assert st["steps"] > 1 and st["rays"] > 0
+    srv.close()
+    for a, m in zip(alone, mixed):
+        assert np.array_equal(_bits(a), _bits(m))
+
+
+def test_server_equals_frame_path_tracer(scenes3):
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.serve import RenderServer
+    meshes, bvhs = scenes3
+    r = _requests(meshes)[0]
+    srv = RenderServer(bvhs, path_capacity=1 << 15, chunk_pixels=333)
+    img = _run(srv, [r])[0]
+    srv.close()
+    ps = scenes.PathScene(meshes[0], scenes.Camera(r.eye, r.lookat, r.up, r.hfov, r.vfov),
+                          scenes.AreaLightSpec(r.light_anchor, r.light_v1, r.light_v2,
+                                               r.light_color),
+                          r.background, r.xres, r.yres, r.spp, r.max_depth, r.rr_depth, r.seed)
+    ref = bvhs[0].render_path(ps)
+    assert np.array_equal(_bits(img), _bits(ref["rgb"]))
+
+
+def test_admission_waits_for_budget(scenes3):
+    from rfmanta_b200 import _lib
+    from rfmanta_b200.serve import RenderServer
+    meshes, bvhs = scenes3
+    reqs = _requests(meshes)[:4]
+    big = max(r.xres * r.yres * 12 for r in reqs)
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000,
+                       hbm_budget_bytes=big + 64)
+    for r in reqs:
+        srv.submit(r)
+    srv.step()
+    st = srv.stats()
+    assert st["active"] + st["pending"] == 4 and st["pending"] >= 1
+    assert st["bytes_in_use"] <= big + 64
+    srv.close()
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000, hbm_budget_bytes=1000)
+    with pytest.raises(_lib.RQError) as e:
+        srv.submit(reqs[3])
+    assert e.value.code == _lib.RQ_ERR_CAPACITY
+    srv.close()

@@ -463,8 +463,111 @@ class BatchedQueriesWL:
         return rays / secs / 1e6, threads, text, secs
 
 
+class ServingWL(BatchedQueriesWL):
+    """Poisson stream (mean 200 requests/s, seeded) of render requests over
+    the 8 resident scenes: resolution from {256^2, 512^2, 1280x720,
+    1920x1080}, spp from {1, 4, 16}, bounce depth from {0, 2, 4}; served by
+    the continuous-batching engine (4Mi-path wavefront steps, 64Ki-pixel
+    chunks, images admitted against an HBM budget).  A step is one stream of
+    `requests` requests; value = rays traced / wall time from the first
+    arrival to the last completion."""
+
+    name = "serving"
+    requests = 64
+
+    def config(self):
+        return {"workload": self.name, "scenes": [int(m.n_tris) for m in self.meshes],
+                "requests_per_step": self.requests, "arrival_rate_per_s": 200,
+                "resolutions": ["256x256", "512x512", "1280x720", "1920x1080"],
+                "spp": [1, 4, 16], "bounces": [0, 2, 4], "path_capacity": 1 << 22,
+                "chunk_pixels": 65536, "triangle_kind": "wald", "tree": "gpu binned SAH"}
+
+    def run_custom(self, args, dev):
+        import torch
+        from rfmanta_b200 import scenes
+        from rfmanta_b200.serve import RenderServer, poisson_stream
+        self.build(dev)
+        srv = RenderServer(self.bvhs, path_capacity=1 << 22, chunk_pixels=65536,
+                           hbm_budget_bytes=24 << 30)
+        warm = poisson_stream(self.meshes, 8, 200.0, seed=3)
+        srv.run_stream(warm)
+        lat, rays, wall, queue = [], 0, 0.0, []
+        for k in range(args.steps):
+            base = srv.stats()
+            stream = poisson_stream(self.meshes, self.requests, 200.0, seed=100 + k)
+            out = srv.run_stream(stream)
+            st = srv.stats()
+            rays += (st["rays"] - base["rays"]) + (st["shadow_rays"] - base["shadow_rays"])
+            wall += out["wall_s"]
+            lat += [v["latency"] for v in out["info"].values()]
+            queue += [v["queue"] for v in out["info"].values()]
+        # e2e: the same stream with every image copied back to host memory
+        e2e_rays0 = srv.stats()
+        stream = poisson_stream(self.meshes, self.requests, 200.0, seed=100)
+        out_e2e = srv.run_stream(stream, keep_images=True)
+        st = srv.stats()
+        e2e_rays = (st["rays"] - e2e_rays0["rays"]) + (st["shadow_rays"] - e2e_rays0["shadow_rays"])
+        d2h = sum(r.xres * r.yres * 12 for _, r in stream)
+        srv.close()
+        # serial plain per-request GPU calls (rq_render_path, one at a time)
+        stream = poisson_stream(self.meshes, self.requests, 200.0, seed=100)
+        t0 = time.perf_counter()
+        serial_rays = 0
+        for _, r in stream:
+            ps = scenes.PathScene(self.meshes[r.scene],
+                                  scenes.Camera(r.eye, r.lookat, r.up, r.hfov, r.vfov),
+                                  scenes.AreaLightSpec(r.light_anchor, r.light_v1, r.light_v2,
+                                                       r.light_color),
+                                  r.background, r.xres, r.yres, r.spp, r.max_depth,
+                                  r.rr_depth, r.seed)
+            o = self.bvhs[r.scene].render_path(ps)
+            serial_rays += o["rays"] + o["shadow_rays"]
+        serial = serial_rays / (time.perf_counter() - t0) / 1e6
+        lat_ms = np.array(lat) * 1e3
+        return {
+            "value": rays / wall / 1e6, "ms_per_step": wall / args.steps * 1e3,
+            "e2e": rays_or(e2e_rays) / out_e2e["wall_s"] / 1e6, "h2d": 200 * self.requests,
+            "d2h": d2h, "rays_per_step": rays // max(args.steps, 1),
+            "extra": {"p50_ms": round(float(np.percentile(lat_ms, 50)), 2),
+                      "p99_ms": round(float(np.percentile(lat_ms, 99)), 2),
+                      "mean_admission_wait_ms": round(float(np.mean(queue) * 1e3), 2),
+                      "serial_plain_gpu_mrays": round(serial, 1),
+                      "served_over_serial": round(rays / wall / 1e6 / serial, 3)},
+        }
+
+    def cpu_reference(self, seconds_budget, threads):
+        """Reference KajiyaPathtracer on 256x256 requests of the scenes up to
+        983,040 triangles (1 spp, depth 3)."""
+        from oracle.pyoracle import Reference
+        from rfmanta_b200 import scenes
+        from rfmanta_b200.serve import request_for_scene
+        sse = Reference.available(sse=True)
+        ref = Reference(sse=sse)
+        secs, rays, used = 0.0, 0, 0
+        for si in range(5):
+            r = request_for_scene(si, self.meshes[si], 256, 256, 1, 3, seed=si)
+            ps = scenes.PathScene(self.meshes[si], scenes.Camera(r.eye, r.lookat, r.up, r.hfov,
+                                                                 r.vfov),
+                                  scenes.AreaLightSpec(r.light_anchor, r.light_v1, r.light_v2,
+                                                       r.light_color),
+                                  r.background, 256, 256, 1, 3, 2, r.seed)
+            rs = ref.scene(self.meshes[si], 0)
+            o = rs.render_path(ps, nthreads=threads)
+            rs.close()
+            secs += o["seconds"]
+            rays += o["rays"]
+            used += 1
+        text = (f"{used} requests of 256x256, 1 spp, depth 3 on the scenes of up to 983,040 "
+                f"triangles, reference KajiyaPathtracer ({'MANTA_SSE' if sse else 'scalar'} build)")
+        return rays / secs / 1e6, threads, text, secs
+
+
+def rays_or(x):
+    return max(int(x), 1)
+
+
 WORKLOADS = {"path_frame": PathFrame, "small_frame": SmallFrame,
-             "batched_queries": BatchedQueriesWL}
+             "batched_queries": BatchedQueriesWL, "serving": ServingWL}
 
 
 # ----------------------------------------------------------------- runs ----
@@ -480,6 +583,8 @@ def run_ours(args):
     from rfmanta_b200.dynbvh import GpuDynBVH
     wl = WORKLOADS[args.workload]()
     dev = torch.device("cuda", local)
+    if hasattr(wl, "run_custom"):
+        return run_custom(args, wl, dev, world, rank)
     if hasattr(wl, "build"):
         bvh = wl.build(dev)
         build_s = wl.build_s
@@ -591,6 +696,41 @@ def run_ours(args):
                          "frac": round(achieved / hbm, 4), "traffic": None,
                          "kernel_ms_per_step": {n: round(v, 4) for n, v in zip(names, kms)},
                          "per_ray": per_ray},
+        }
+        if not args.no_cpu_baseline:
+            v, threads, text, _ = wl.cpu_reference(args.cpu_seconds, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mrays/s", "cores": threads,
+                                    "kind": "reference", "sample": text}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_custom(args, wl, dev, world, rank):
+    """Workloads that drive their own loop (serving): wall-clock rates."""
+    import torch
+    import torch.distributed as dist
+    with ClockSampler(dev.index or 0) as clk:
+        r = wl.run_custom(args, dev)
+    value = torch.tensor([r["value"]], dtype=torch.float64, device=dev)
+    e2e = torch.tensor([r["e2e"]], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(value, op=dist.ReduceOp.SUM)
+        dist.all_reduce(e2e, op=dist.ReduceOp.SUM)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(float(value.item()), 2), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(r["ms_per_step"], 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generators and request stream)",
+            "config": dict(wl.config(), parallelism=f"replicas x{world}",
+                           rays_per_step=r["rays_per_step"], **r["extra"]),
+            "clocks": clk.summary(),
+            "e2e": {"value": round(float(e2e.item()), 2), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(r["h2d"]), "d2h_bytes_per_step": int(r["d2h"])},
+            "gpu_launches": None,
+            "roofline": None,
         }
         if not args.no_cpu_baseline:
             v, threads, text, _ = wl.cpu_reference(args.cpu_seconds, os.cpu_count() or 1)

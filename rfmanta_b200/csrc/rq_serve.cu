@@ -285,8 +285,8 @@ struct rq_server {
     if (stream) cudaStreamSynchronize(stream);
     for (auto& kv : reqs) {
       HostReq& r = *kv.second;
-      cudaFree(r.d_out);
-      cudaFree(r.d_mat);
+      if (r.d_out) cudaFreeAsync(r.d_out, stream);
+      if (r.d_mat) cudaFreeAsync(r.d_mat, stream);
       if (r.done_ev) cudaEventDestroy(r.done_ev);
     }
     cudaFree(B.o); cudaFree(B.d); cudaFree(B.imp); cudaFree(B.rad); cudaFree(B.rng);
@@ -305,9 +305,11 @@ struct rq_server {
   bool admit(HostReq& r) {
     const size_t need = r.bytes + r.materials.size() * sizeof(float);
     if ((int)active.size() >= max_active || used + need > budget) return false;
-    if (cudaMalloc(&r.d_out, r.bytes) != cudaSuccess) return false;
-    if (cudaMalloc(&r.d_mat, r.materials.size() * sizeof(float)) != cudaSuccess) {
-      cudaFree(r.d_out);
+    // stream-ordered allocation: no device-wide synchronisation while
+    // other steps are in flight
+    if (cudaMallocAsync(&r.d_out, r.bytes, stream) != cudaSuccess) return false;
+    if (cudaMallocAsync(&r.d_mat, r.materials.size() * sizeof(float), stream) != cudaSuccess) {
+      cudaFreeAsync(r.d_out, stream);
       r.d_out = nullptr;
       return false;
     }
@@ -580,7 +582,10 @@ int rq_server_result(rq_server* s, int request_id, float* rgb, double* latency_s
   HostReq& r = *it->second;
   if (!r.done) return sfail(RQ_ERR_STATE, "request not finished");
   if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
-  if (rgb && cudaMemcpy(rgb, r.d_out, r.bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (rgb && (cudaMemcpyAsync(rgb, r.d_out, r.bytes, cudaMemcpyDeviceToHost, s->stream) !=
+                  cudaSuccess ||
+              cudaEventSynchronize(r.done_ev) != cudaSuccess ||
+              cudaStreamSynchronize(s->stream) != cudaSuccess))
     return sfail(RQ_ERR_CUDA, "result copy failed");
   if (latency_s) *latency_s = r.t_done - r.t_submit;
   if (queue_s) *queue_s = r.t_admit - r.t_submit;
@@ -595,8 +600,8 @@ int rq_server_release(rq_server* s, int request_id) {
   if (r.admitted && !r.done) return sfail(RQ_ERR_STATE, "request still running");
   cudaSetDevice(s->device);
   if (r.admitted) s->used -= r.bytes + r.materials.size() * sizeof(float);
-  cudaFree(r.d_out);
-  cudaFree(r.d_mat);
+  if (r.d_out) cudaFreeAsync(r.d_out, s->stream);
+  if (r.d_mat) cudaFreeAsync(r.d_mat, s->stream);
   if (r.done_ev) cudaEventDestroy(r.done_ev);
   if (!r.admitted) {
     for (auto p = s->pending.begin(); p != s->pending.end(); ++p)

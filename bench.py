@@ -16,6 +16,11 @@ Prints ONE JSON line (rank 0).  A step is one frame of the named workload:
   small_frame  512x512, 1 spp primary + hard-shadow rays from one point
                light over a displaced level-6 icosphere (81,920 triangles)
                and a 2x2 ground grid of 20,000 triangles.
+  coherent_frame
+               1920x1080, 4 spp jittered primary + hard-shadow rays from two
+               point lights over a two-level scene: a 1024x1024 fBm
+               heightfield (2,097,152 triangles) plus 64 InstanceT copies of
+               a displaced level-6 icosphere (81,920 triangles each).
 
 value     Mrays/s with the scene and frame buffers resident in HBM, device
           time from CUDA events around each frame, L2 flushed (a 256 MiB
@@ -297,6 +302,117 @@ class SmallFrame:
         text = (f"{frames} full {self.sc.xres}x{self.sc.yres} frame(s), reference Raytracer/"
                 f"DynBVH/WaldTriangle/Lambertian/HardShadows "
                 f"({'MANTA_SSE' if sse else 'scalar'} build)")
+        return rays / secs / 1e6, threads, text, secs
+
+
+class CoherentFrame:
+    """1920x1080, 4 spp jittered primary + hard-shadow rays from two point
+    lights over a two-level scene: a 1024x1024 fBm heightfield (2,097,152
+    triangles, nested DynBVH) plus 64 InstanceT copies of a displaced level-6
+    icosphere (81,920 triangles each)."""
+
+    name = "coherent_frame"
+
+    def __init__(self):
+        from rfmanta_b200 import scenes
+        self.sc = scenes.coherent_scene()
+
+    def config(self):
+        sc = self.sc
+        return {"workload": self.name, "resolution": [sc.xres, sc.yres], "spp": sc.spp,
+                "triangles_instanced": sc.n_tris,
+                "triangles_stored": int(sum(m.n_tris for m in sc.inner)),
+                "instances": int(np.count_nonzero(sc.kind == 0)),
+                "lights": len(sc.lights), "triangle_kind": "wald",
+                "tree": "gpu binned SAH (inner and top level)",
+                "l2": "flushed before every timed frame (256 MiB write)"}
+
+    def build(self, dev):
+        from rfmanta_b200.dynbvh import GpuDynBVH, InstancedBVH
+        self.inner = []
+        self.build_s = 0.0
+        for m in self.sc.inner:
+            b = GpuDynBVH(tri_kind=0, device=dev.index or 0)
+            b.setGroup(m)
+            b.rebuild()
+            self.build_s += b.build_seconds()
+            self.inner.append(b)
+        top = InstancedBVH(self.inner, self.sc.inst_scene, self.sc.translation, self.sc.kind)
+        top.rebuild()
+        self.build_s += top.build_seconds()
+        return top
+
+    def setup(self, bvh, dev):
+        import torch
+        self.bvh = bvh
+        self.params = bvh.frame_params(self.sc, self.sc.materials)
+        npx = self.sc.xres * self.sc.yres
+        self.rgb = torch.empty(npx * 3, device=dev)
+        self.nshadow = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.n_events = 4
+        self.stage_names = ["frame_primary_kernel", "frame_shade_kernel", "frame_resolve_kernel"]
+        self.launches = 3
+
+    def frame(self, stream_ptr):
+        self.bvh.render_frame_device(self.params, self.rgb.data_ptr(), self.nshadow.data_ptr(),
+                                     stream_ptr)
+
+    def rays(self):
+        return self.sc.xres * self.sc.yres * self.sc.spp, int(self.nshadow.item())
+
+    def host_frame(self):
+        from rfmanta_b200 import _lib
+        npx = self.sc.xres * self.sc.yres
+        if not hasattr(self, "_h"):
+            self._h = (np.empty((npx, 3), np.float32), C.c_uint64())
+        rgb, ns = self._h
+        _lib.check(_lib.lib.rq_render_frame(self.bvh.handle, C.byref(self.params),
+                                            rgb.ctypes.data, C.byref(ns)))
+        return C.sizeof(self.params) + 24 * len(self.sc.lights), rgb.nbytes + 8
+
+    def roofline_bytes(self, stats, rays):
+        prim, shadow = rays
+        b_p, t_p = stats[0] / max(prim, 1), stats[1] / max(prim, 1)
+        b_s, t_s = stats[2] / max(shadow, 1), stats[3] / max(shadow, 1)
+        per_ray = {"primary_box_tests": round(b_p, 3), "primary_tri_tests": round(t_p, 3),
+                   "shadow_box_tests": round(b_s, 3), "shadow_tri_tests": round(t_s, 3)}
+        return (prim * (32 + 16 + 32 * b_p + 48 * t_p),
+                shadow * (32 + 4 + 32 * b_s + 48 * t_s),
+                12 * prim + 12 * (prim // self.sc.spp)), per_ray
+
+    def group_stages(self, stage_ms):
+        return self.stage_names, [stage_ms[0], stage_ms[1], stage_ms[2]]
+
+    def cpu_reference(self, seconds_budget, threads):
+        """Reference Raytracer over the reference's own two-level DynBVH
+        (InstanceT objects + the nested heightfield DynBVH) on every 16th
+        image row of the frame's samples."""
+        from oracle.pyoracle import Reference, Restatement
+        sse = Reference.available(sse=True)
+        ref = Reference(sse=sse)
+        sc = self.sc
+        inner = [ref.scene(m, 0) for m in sc.inner]
+        top = ref.instanced(inner, sc.inst_scene, sc.translation, sc.kind)
+        rs = Restatement()
+        per_row = sc.xres * sc.spp
+        rows = list(range(0, sc.yres, 16))
+        cs = [rs.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed,
+                               items=(y * per_row, (y + 1) * per_row)) for y in rows]
+        px = np.concatenate([c[0] for c in cs])
+        py = np.concatenate([c[1] for c in cs])
+        passes, secs, rays = 0, 0.0, 0
+        while passes < 1 or secs < seconds_budget:
+            t0 = time.perf_counter()
+            out = top.render_coords(sc, px, py, nthreads=threads)
+            secs += time.perf_counter() - t0
+            rays += px.size + out["shadow_rays"]
+            passes += 1
+        for r in inner:
+            r.close()
+        text = (f"{passes} pass(es) over every 16th row of the {sc.xres}x{sc.yres}x{sc.spp} "
+                f"frame ({len(rows)} rows, {px.size} samples), reference Raytracer over a "
+                f"top-level DynBVH of InstanceT + nested DynBVH objects, WaldTriangle/"
+                f"Lambertian/HardShadows ({'MANTA_SSE' if sse else 'scalar'} build)")
         return rays / secs / 1e6, threads, text, secs
 
 
@@ -587,6 +703,7 @@ def rays_or(x):
 
 
 WORKLOADS = {"path_frame": PathFrame, "small_frame": SmallFrame,
+             "coherent_frame": CoherentFrame,
              "batched_queries": BatchedQueriesWL, "serving": ServingWL}
 
 

@@ -313,6 +313,58 @@ RQ_API int rq_render_whitted_device_noalloc(rq_scene* scene,
                                             uint64_t* d_shadow_rays, void* stream);
 
 /*
+ * Two-level scene: instances of inner triangle scenes under a top-level
+ * DynBVH.  inst_scene[k] indexes `inner`, inst_translation holds 3 floats
+ * per instance, inst_kind[k] (NULL = all RQ_INST_TRANSLATE) is
+ *   RQ_INST_TRANSLATE  an InstanceT (Model/Instances/InstanceT.cc:31-90):
+ *                      rays enter with o - translation and the current minT,
+ *                      a closer inner hit is taken through RayPacket::hit;
+ *                      like the reference, an any-hit (shadow) query does not
+ *                      report occlusion found inside it (the inner
+ *                      OpaqueShadower pins minT to T_EPSILON, DynBVH.cc:
+ *                      331-349, which RayPacket::hit rejects);
+ *   RQ_INST_NESTED     the inner DynBVH placed in the top-level group as an
+ *                      object itself (translation must be 0): hits and
+ *                      occlusion as for its own triangles.
+ * The top-level tree is built on the GPU over the instance boxes (inner mesh
+ * bounds + translation, InstanceT::computeBounds) and can be replaced with
+ * rq_scene_import_tree / rq_scene_import_dynbvh (object ids = instance
+ * indices).  Inner scenes are referenced and must outlive this one; all share
+ * one device and triangle kind.  Queries and frames accept the result like
+ * any scene; a hit reports the inner triangle id (and, through
+ * rq_trace_device_ex, the instance).
+ */
+#define RQ_INST_TRANSLATE 0
+#define RQ_INST_NESTED 1
+RQ_API int rq_scene_create_instanced(rq_scene* const* inner, int n_inner,
+                                     const int32_t* inst_scene,
+                                     const float* inst_translation,
+                                     const int32_t* inst_kind, int n_instances,
+                                     rq_scene** out);
+
+/* rq_trace_device plus the hit instance per ray (d_inst, -1 for none or a
+ * flat scene). */
+RQ_API int rq_trace_device_ex(rq_scene* scene, int n, const float* d_org,
+                              const float* d_dir, const float* d_tmax, int flags,
+                              float* d_t, int32_t* d_prim, float* d_u, float* d_v,
+                              int32_t* d_inst, void* stream);
+
+/* Supersampled Whitted frame over a flat or instanced scene: `spp`
+ * stratified jittered samples per pixel (PCG32 keyed by seed and sample),
+ * averaged in sample order; spp = 1 samples pixel centres and equals
+ * rq_render_whitted. */
+typedef struct {
+  rq_whitted_params whitted;
+  int spp;        /* 1, 4, 16, ... */
+  uint64_t seed;
+} rq_frame_params;
+
+RQ_API int rq_render_frame(rq_scene* scene, const rq_frame_params* params, float* rgb,
+                           uint64_t* shadow_rays);
+RQ_API int rq_render_frame_device(rq_scene* scene, const rq_frame_params* params,
+                                  float* d_rgb, uint64_t* d_shadow_rays, void* stream);
+
+/*
  * Path-traced frame: KajiyaPathtracer::traceEyeRays
  * (Engine/Renderers/KajiyaPathtracer.cc:113-302) with Lambertian materials,
  * one parallelogram AreaLight sampled with HardShadows shadow rays, cosine

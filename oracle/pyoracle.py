@@ -65,6 +65,65 @@ class Tree:
                     z["left_cheaper"], z["ids"])
 
 
+class _OrqTree(C.Structure):
+    _fields_ = [("bounds", C.c_void_p), ("child", C.c_void_p), ("children", C.c_void_p),
+                ("axis", C.c_void_p), ("left_cheaper", C.c_void_p), ("ids", C.c_void_p),
+                ("tri_kind", C.c_int), ("verts", C.c_void_p), ("idx", C.c_void_p),
+                ("wald", C.c_void_p), ("face_mat", C.c_void_p)]
+
+
+class _OrqWorld(C.Structure):
+    _fields_ = [("top", C.c_void_p), ("inner", C.c_void_p), ("inst_scene", C.c_void_p),
+                ("inst_T", C.c_void_p), ("inst_kind", C.c_void_p)]
+
+
+class World:
+    """A flat triangle scene or a two-level scene for the restatement: the
+    top-level tree over instances of inner (tree, mesh) pairs.  Keeps every
+    array it hands to C alive."""
+
+    def __init__(self, rs: "Restatement", top_tree: Tree, top_mesh=None, inner=None,
+                 inst_scene=None, translation=None, kind=None, tri_kind=0):
+        self._keep = []
+        self.inner_meshes = [m for _, m in inner] if inner else None
+        if inner is None:
+            self._top = self._tree(rs, top_tree, top_mesh, tri_kind)
+            self.world = _OrqWorld(C.addressof(self._top), None, None, None, None)
+        else:
+            self._top = self._tree(rs, top_tree, None, tri_kind)
+            arr = (_OrqTree * len(inner))()
+            for i, (t, m) in enumerate(inner):
+                arr[i] = self._tree(rs, t, m, tri_kind)
+            self._inner = arr
+            sc = np.ascontiguousarray(inst_scene, np.int32)
+            tr = np.ascontiguousarray(translation, np.float32).reshape(-1, 3)
+            kd = np.ascontiguousarray(kind if kind is not None else np.zeros(sc.shape[0]),
+                                      np.int32)
+            self._keep += [sc, tr, kd]
+            self.world = _OrqWorld(C.addressof(self._top), C.addressof(arr), _ptr(sc).value,
+                                   _ptr(tr).value, _ptr(kd).value)
+
+    def _tree(self, rs, tree, mesh, tri_kind):
+        b, c, ch, ax, lc, ids = tree.arrays()
+        keep = [b, c, ch, ax, lc, ids]
+        t = _OrqTree(_ptr(b).value, _ptr(c).value, _ptr(ch).value, _ptr(ax).value,
+                     _ptr(lc).value, _ptr(ids).value, tri_kind, None, None, None, None)
+        if mesh is not None:
+            v = np.ascontiguousarray(mesh.vertices, np.float32)
+            ix = np.ascontiguousarray(mesh.indices, np.uint32)
+            fm = np.ascontiguousarray(mesh.face_material, np.uint32)
+            w = rs.wald_setup(mesh) if tri_kind == 0 else None
+            keep += [v, ix, fm, w]
+            t.verts, t.idx, t.face_mat = _ptr(v).value, _ptr(ix).value, _ptr(fm).value
+            t.wald = _ptr(w).value if w is not None else None
+        self._keep += keep
+        return t
+
+    @property
+    def ptr(self):
+        return C.byref(self.world)
+
+
 def build_restatement() -> str:
     if not os.path.exists(ORACLE_SO) or (
             os.path.getmtime(ORACLE_SO) < os.path.getmtime(os.path.join(HERE, "rq_oracle.c"))):
@@ -97,6 +156,65 @@ class Restatement:
         L.orq_render_path.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 7 +
                                       [C.c_uint64, C.c_longlong, C.c_longlong] +
                                       [C.c_void_p] * 3)
+        L.orq_trace_world.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 + [C.c_int] +
+                                      [C.c_void_p] * 6)
+        L.orq_sample_coords.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_longlong,
+                                        C.c_longlong, C.c_void_p, C.c_void_p]
+        L.orq_render_frame.argtypes = ([C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_uint64] +
+                                       [C.c_void_p, C.c_int] + [C.c_void_p] * 2 +
+                                       [C.c_int, C.c_int] + [C.c_void_p] * 4)
+        L.orq_render_frame.restype = C.c_longlong
+
+    def world(self, top_tree, top_mesh=None, inner=None, inst_scene=None, translation=None,
+              kind=None, tri_kind=0) -> World:
+        return World(self, top_tree, top_mesh, inner, inst_scene, translation, kind, tri_kind)
+
+    def trace_world(self, world: World, org, dir, tmax, anyhit=False):
+        n = int(tmax.shape[0])
+        org = np.ascontiguousarray(org, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        hit = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        inst = np.zeros(n, np.int32)
+        self.lib.orq_trace_world(world.ptr, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
+                                 _ptr(hit), _ptr(t), _ptr(prim), _ptr(u), _ptr(v), _ptr(inst))
+        return dict(hit=hit, t=t, prim=prim, u=u, v=v, inst=inst)
+
+    def sample_coords(self, xres, yres, spp, seed, items=None):
+        i0, i1 = items if items else (0, xres * yres * spp)
+        px = np.zeros(i1 - i0, np.float32)
+        py = np.zeros(i1 - i0, np.float32)
+        self.lib.orq_sample_coords(xres, yres, spp, int(seed), i0, i1, _ptr(px), _ptr(py))
+        return px, py
+
+    def render_frame(self, world: World, scene, materials, rows=None, per_sample=False):
+        """Supersampled Whitted frame (scenes.FrameScene-like: camera, lights,
+        ambient, background, xres, yres, spp, seed) over a world."""
+        basis = self.camera_basis(scene.camera)
+        xres, yres, spp = scene.xres, scene.yres, scene.spp
+        y0, y1 = rows if rows else (0, yres)
+        lights = np.array([list(l.position) + list(l.color) for l in scene.lights],
+                          np.float32).reshape(-1, 6)
+        amb = np.asarray(scene.ambient, np.float32)
+        bg = np.asarray(scene.background, np.float32)
+        mats = np.ascontiguousarray(materials, np.float32)
+        npx = (y1 - y0) * xres
+        rgb = np.zeros((npx, 3), np.float32)
+        srgb = np.zeros((npx * spp, 3), np.float32) if per_sample else None
+        st = np.zeros(npx * spp, np.float32) if per_sample else None
+        sp = np.zeros(npx * spp, np.int32) if per_sample else None
+        ns = self.lib.orq_render_frame(world.ptr, _ptr(mats), _ptr(basis), xres, yres, spp,
+                                       int(scene.seed), _ptr(lights), lights.shape[0],
+                                       _ptr(amb), _ptr(bg), y0, y1, _ptr(rgb), _ptr(srgb),
+                                       _ptr(st), _ptr(sp))
+        out = dict(rgb=rgb, shadow_rays=int(ns))
+        if per_sample:
+            out.update(sample_rgb=srgb, sample_t=st, sample_prim=sp)
+        return out
 
     def sincos_2pi(self, u):
         u = np.ascontiguousarray(u, np.float32)
@@ -269,6 +387,13 @@ class Reference:
         L.mref_render_path.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                         C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_uint,
                                         C.c_void_p, C.c_void_p, C.c_void_p])
+        L.mref_intersect2.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
+                                      [C.c_int, C.c_int] + [C.c_void_p] * 6)
+        L.mref_scene_create_instanced.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
+                                                  [C.c_int])
+        L.mref_scene_create_instanced.restype = C.c_void_p
+        L.mref_render_coords.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 4 + [C.c_int] +
+                                         [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 4)
 
     @staticmethod
     def available(sse: bool = False) -> bool:
@@ -276,6 +401,11 @@ class Reference:
 
     def scene(self, mesh, tri_kind=0) -> "RefScene":
         return RefScene(self, mesh, tri_kind)
+
+    def instanced(self, inner: list, inst_scene, translation, kind=None) -> "RefScene":
+        """Top-level DynBVH over InstanceT (kind 0) / nested DynBVH (kind 1)
+        objects of the inner RefScenes."""
+        return RefScene(self, None, 0, inner=(inner, inst_scene, translation, kind))
 
     def camera_basis(self, cam) -> np.ndarray:
         e = np.asarray(cam.eye, np.float32)
@@ -287,9 +417,22 @@ class Reference:
 
 
 class RefScene:
-    def __init__(self, ref: Reference, mesh, tri_kind=0):
+    def __init__(self, ref: Reference, mesh, tri_kind=0, inner=None):
         self.ref = ref
         self.mesh = mesh
+        if inner is not None:
+            scenes, inst_scene, translation, kind = inner
+            hs = (C.c_void_p * len(scenes))(*[x.h for x in scenes])
+            sc = np.ascontiguousarray(inst_scene, np.int32)
+            tr = np.ascontiguousarray(translation, np.float32).reshape(-1, 3)
+            kd = np.ascontiguousarray(kind if kind is not None else np.zeros(sc.shape[0]),
+                                      np.int32)
+            self._keep = (scenes, hs, sc, tr, kd)
+            self.h = ref.lib.mref_scene_create_instanced(hs, len(scenes), _ptr(sc), _ptr(tr),
+                                                         _ptr(kd), sc.shape[0])
+            if not self.h:
+                raise RuntimeError("reference instanced scene build failed")
+            return
         v = np.ascontiguousarray(mesh.vertices, np.float32)
         ix = np.ascontiguousarray(mesh.indices, np.uint32)
         fm = np.ascontiguousarray(mesh.face_material, np.uint32)
@@ -346,6 +489,43 @@ class RefScene:
         self.ref.lib.mref_intersect(self.h, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
                                     packet, _ptr(hit), _ptr(t), _ptr(prim), _ptr(u), _ptr(v))
         return dict(hit=hit, t=t, prim=prim, u=u, v=v)
+
+    def intersect2(self, org, dir, tmax, anyhit=False, packet=64):
+        """intersect plus the hit instance (-1: none or not an InstanceT);
+        u/v are 0 for InstanceT hits (the reference keeps them in the
+        instance's own packet)."""
+        n = int(tmax.shape[0])
+        org = np.ascontiguousarray(org, np.float32)
+        dir = np.ascontiguousarray(dir, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        out = {k: np.zeros(n, np.int32 if k in ("hit", "prim", "inst") else np.float32)
+               for k in ("hit", "t", "prim", "u", "v", "inst")}
+        self.ref.lib.mref_intersect2(self.h, n, _ptr(org), _ptr(dir), _ptr(tmax), int(anyhit),
+                                     packet, *[_ptr(out[k]) for k in
+                                               ("hit", "t", "prim", "u", "v", "inst")])
+        return out
+
+    def render_coords(self, scene, px, py, nthreads=1):
+        """Raytracer::traceEyeRays at the given image coordinates (one eye
+        ray each); per-ray colour, primary t and triangle id."""
+        cam = scene.camera
+        args = np.array(list(cam.eye) + list(cam.lookat) + list(cam.up) +
+                        [cam.hfov, cam.vfov, 0.0], np.float32)
+        lights = np.array([list(l.position) + list(l.color) for l in scene.lights],
+                          np.float32).reshape(-1, 6)
+        amb = np.asarray(scene.ambient, np.float32)
+        bg = np.asarray(scene.background, np.float32)
+        px = np.ascontiguousarray(px, np.float32)
+        py = np.ascontiguousarray(py, np.float32)
+        n = px.shape[0]
+        rgb = np.zeros((n, 3), np.float32)
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        nsr = C.c_longlong()
+        self.ref.lib.mref_render_coords(self.h, n, _ptr(px), _ptr(py), _ptr(args), _ptr(lights),
+                                        lights.shape[0], _ptr(amb), _ptr(bg), nthreads,
+                                        _ptr(rgb), _ptr(t), _ptr(prim), C.byref(nsr))
+        return dict(rgb=rgb, t=t, prim=prim, shadow_rays=nsr.value)
 
     def intersect_mt(self, org, dir, tmax, anyhit=False, nthreads=1):
         """DynBVH::intersect on 64-ray packets over N threads; returns the

@@ -69,7 +69,8 @@ MODEL_SRC := \
   Model/Backgrounds/ConstantBackground.cc \
   Model/Cameras/PinholeCamera.cc \
   Model/Lights/AreaLight.cc Model/Primitives/Parallelogram.cc \
-  Model/Primitives/PrimitiveCommon.cc Model/TexCoordMappers/UniformMapper.cc
+  Model/Primitives/PrimitiveCommon.cc Model/TexCoordMappers/UniformMapper.cc \
+  Model/Instances/InstanceT.cc Model/Instances/InstanceMaterial.cc
 
 ENGINE_SRC := \
   Engine/Shadows/HardShadows.cc Engine/Renderers/Raytracer.cc \

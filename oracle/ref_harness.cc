@@ -43,7 +43,10 @@
 #include <Model/Backgrounds/ConstantBackground.h>
 #include <Model/Cameras/PinholeCamera.h>
 #include <Model/Groups/DynBVH.h>
+#include <Model/Groups/Group.h>
 #include <Model/Groups/Mesh.h>
+#include <Model/Instances/InstanceT.h>
+#include <Model/Instances/MPT.h>
 #include <Model/Lights/PointLight.h>
 #include <Model/Materials/Lambertian.h>
 #include <Model/Primitives/KenslerShirleyTriangle.h>
@@ -58,6 +61,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <sys/time.h>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -124,14 +128,55 @@ public:
   }
 };
 
+// Hands a packet to an InstanceT with the derived-data flags cleared.
+// InstanceT::intersect (Model/Instances/InstanceT.cc:60-66) builds its local
+// packet from rays.getAllFlags(); HaveInverseDirections / HaveSigns set by
+// the enclosing DynBVH would then make the inner DynBVH::intersect skip
+// computing inverse directions and signs for a packet whose data
+// InstanceT never filled (it would read uninitialised memory).  Cleared,
+// the inner DynBVH computes both itself (DynBVH.cc:116-120).  The flags are
+// restored afterwards; the outer packet's data is untouched.
+class InstanceGuard : public Object {
+public:
+  explicit InstanceGuard(InstanceT* it) : it(it) {}
+  void computeBounds(const PreprocessContext& c, BBox& b) const { it->computeBounds(c, b); }
+  void intersect(const RenderContext& c, RayPacket& rays) const {
+    const int mask = RayPacket::HaveInverseDirections | RayPacket::HaveSigns |
+                     RayPacket::ConstantSigns;
+    const int saved = rays.getAllFlags() & mask;
+    rays.resetFlag(mask);
+    it->intersect(c, rays);
+    rays.setFlag(saved);
+  }
+  InstanceT* it;
+};
+
 struct RefScene {
-  Mesh* mesh;
+  Mesh* mesh;      // NULL for a two-level scene
   ExposedBVH* bvh;
   Object* object;  // what rays are traced against: bvh, or a drop-in
   std::vector<Material*> materials;
   LightSet* lights;
   Scene* scene;
+  // two-level scenes: instance index of each top-level InstanceT object
+  std::map<const Primitive*, int> instance_of;
 };
+
+// Triangle id (and instance index, -1 for none) of a hit: a hit on an
+// InstanceT carries the inner primitive in its MPT scratchpad
+// (Model/Instances/InstanceT.cc:80-87).
+int hit_prim(const RefScene* s, RayPacket& rays, int i, int* inst) {
+  const Primitive* p = rays.getHitPrimitive(i);
+  if (!s->instance_of.empty()) {
+    std::map<const Primitive*, int>::const_iterator it = s->instance_of.find(p);
+    if (it != s->instance_of.end()) {
+      if (inst) *inst = it->second;
+      return (int)TriId::of(rays.scratchpad<MPT>(i).primitive);
+    }
+  }
+  if (inst) *inst = -1;
+  return (int)TriId::of(p);
+}
 
 double now_s() {
   struct timeval tv;
@@ -251,9 +296,9 @@ double mref_tree_cost(void* h) {
 // SoA ([x0..xn-1, y0.., z0..]).  Per ray: hit flag, t, triangle id, scratch
 // u/v (WaldTriangle lambda/mue, KS uoverd/voverd).  anyhit sets
 // RayPacket::AnyHit (HardShadows.cc:79).
-int mref_intersect(void* h, int n, const float* org, const float* dir,
-                   const float* tmax, int anyhit, int packet, int* hit,
-                   float* t, int* prim, float* u, float* v) {
+int mref_intersect2(void* h, int n, const float* org, const float* dir,
+                    const float* tmax, int anyhit, int packet, int* hit,
+                    float* t, int* prim, float* u, float* v, int* inst) {
   RefScene* s = static_cast<RefScene*>(h);
   if (packet < 1 || packet > RayPacket::MaxSize) packet = RayPacket::MaxSize;
   RenderContext ctx(0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
@@ -273,18 +318,27 @@ int mref_intersect(void* h, int n, const float* org, const float* dir,
       int r = base + i;
       hit[r] = rays.wasHit(i) ? 1 : 0;
       t[r] = rays.getMinT(i);
+      int k = -1;
       if (hit[r]) {
-        prim[r] = (int)TriId::of(rays.getHitPrimitive(i));
-        u[r] = rays.getScratchpad<Real>(WaldTriangle::SCRATCH_U)[i];
-        v[r] = rays.getScratchpad<Real>(WaldTriangle::SCRATCH_V)[i];
+        prim[r] = hit_prim(s, rays, i, &k);
+        // an InstanceT hit keeps the inner u/v in the instance's own packet
+        u[r] = k < 0 ? rays.getScratchpad<Real>(WaldTriangle::SCRATCH_U)[i] : 0.f;
+        v[r] = k < 0 ? rays.getScratchpad<Real>(WaldTriangle::SCRATCH_V)[i] : 0.f;
       } else {
         prim[r] = -1;
         u[r] = 0.f;
         v[r] = 0.f;
       }
+      if (inst) inst[r] = k;
     }
   }
   return 0;
+}
+
+int mref_intersect(void* h, int n, const float* org, const float* dir,
+                   const float* tmax, int anyhit, int packet, int* hit,
+                   float* t, int* prim, float* u, float* v) {
+  return mref_intersect2(h, n, org, dir, tmax, anyhit, packet, hit, t, prim, u, v, 0);
 }
 
 struct QueryJob {
@@ -333,7 +387,7 @@ static void* query_worker(void* p) {
         const int r = b + i;
         j->hit[r] = rays.wasHit(i) ? 1 : 0;
         j->t[r] = rays.getMinT(i);
-        j->prim[r] = j->hit[r] ? (int)TriId::of(rays.getHitPrimitive(i)) : -1;
+        j->prim[r] = j->hit[r] ? hit_prim(j->s, rays, i, 0) : -1;
       }
     }
   }
@@ -457,7 +511,7 @@ static void* render_worker(void* p) {
         j->rgb[3 * pix + 2] = c[2];
         if (j->prim) {
           bool h = rays.wasHit(i);
-          j->prim[pix] = h ? (int)TriId::of(rays.getHitPrimitive(i)) : -1;
+          j->prim[pix] = h ? hit_prim(j->s, rays, i, 0) : -1;
           j->tprim[pix] = rays.getMinT(i);
         }
       }
@@ -542,6 +596,171 @@ int mref_render(void* h, int xres, int yres, const float* cam12_args,
   long long total = 0;
   for (int p = 0; p < nthreads; ++p) total += job.shadow_rays[p];
   if (seconds) *seconds = t1 - t0;
+  if (shadow_rays) *shadow_rays = total;
+  return 0;
+}
+
+// Two-level scene: per instance the inner scene's DynBVH wrapped in an
+// InstanceT (kind 0, Model/Instances/InstanceT.cc; called through
+// InstanceGuard) or placed in the top-level Group itself (kind 1); a
+// top-level DynBVH is built over the Group.  Inner scenes come from
+// mref_scene_create and must outlive it.
+void* mref_scene_create_instanced(void* const* inner, int n_inner, const int* inst_scene,
+                                  const float* inst_T, const int* inst_kind, int n_inst) {
+  try {
+    RefScene* s = new RefScene();
+    s->mesh = 0;
+    s->scene = 0;
+    Group* g = new Group();
+    for (int k = 0; k < n_inst; ++k) {
+      if (inst_scene[k] < 0 || inst_scene[k] >= n_inner) return 0;
+      RefScene* b = static_cast<RefScene*>(inner[inst_scene[k]]);
+      const int kind = inst_kind ? inst_kind[k] : 0;
+      if (kind == 0) {
+        InstanceT* it = new InstanceT(
+            b->bvh, Vector(inst_T[3 * k], inst_T[3 * k + 1], inst_T[3 * k + 2]));
+        s->instance_of[it] = k;
+        g->add(new InstanceGuard(it));
+      } else {
+        g->add(b->bvh);
+      }
+    }
+    for (int i = 0; i < n_inner; ++i) {
+      RefScene* b = static_cast<RefScene*>(inner[i]);
+      s->materials.insert(s->materials.end(), b->materials.begin(), b->materials.end());
+    }
+    s->lights = new LightSet();
+    s->lights->setAmbientLight(new ConstantAmbient(Color(RGB(0, 0, 0))));
+    s->bvh = new ExposedBVH();
+    s->bvh->setGroup(g);
+    s->bvh->rebuild(0, 1);
+    s->object = s->bvh;
+    return s;
+  } catch (...) {
+    return 0;
+  }
+}
+
+struct CoordJob {
+  RefScene* s;
+  Raytracer* renderer;
+  ExposedCamera* camera;
+  ConstantSampleGenerator* sampler;
+  int n;
+  const float* px;
+  const float* py;
+  float* rgb;
+  float* tprim;
+  int* prim;
+  volatile int next;
+  pthread_mutex_t lock;
+  long long shadow_rays[256];
+  int nthreads;
+};
+
+struct CoordArg {
+  CoordJob* job;
+  int proc;
+};
+
+static void* coord_worker(void* p) {
+  CoordArg* a = static_cast<CoordArg*>(p);
+  CoordJob* j = a->job;
+  CountingShadows shadows;
+  shadows.counter = &j->shadow_rays[a->proc];
+  RenderContext ctx(0, 0, a->proc, j->nthreads, 0, 0, 0, j->renderer, &shadows,
+                    j->camera, j->s->scene, 0, 0, j->sampler);
+  const int P = RayPacket::MaxSize;
+  for (;;) {
+    pthread_mutex_lock(&j->lock);
+    const int base = j->next;
+    j->next += P;
+    pthread_mutex_unlock(&j->lock);
+    if (base >= j->n) break;
+    const int cnt = j->n - base < P ? j->n - base : P;
+    RayPacketData data;
+    RayPacket rays(data, RayPacket::UnknownShape, 0, cnt, 0,
+                   RayPacket::HaveImageCoordinates | RayPacket::ConstantEye);
+    for (int i = 0; i < cnt; ++i) rays.setPixel(i, 0, j->px[base + i], j->py[base + i]);
+    j->renderer->traceEyeRays(ctx, rays);
+    for (int i = 0; i < cnt; ++i) {
+      const size_t r = (size_t)base + i;
+      Color c = rays.getColor(i);
+      for (int k = 0; k < 3; ++k) j->rgb[3 * r + k] = c[k];
+      if (j->prim) {
+        j->prim[r] = rays.wasHit(i) ? hit_prim(j->s, rays, i, 0) : -1;
+        j->tprim[r] = rays.getMinT(i);
+      }
+    }
+  }
+  return 0;
+}
+
+// Raytracer::traceEyeRays (as mref_render) for n eye rays at the given image
+// coordinates, in packets of 64 consecutive rays on N pthreads.
+int mref_render_coords(void* h, int n, const float* px, const float* py,
+                       const float* cam12_args, const float* lights, int nlights,
+                       const float* ambient, const float* background, int nthreads,
+                       float* rgb, float* tprim, int* prim, long long* shadow_rays) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  char buf[16][32];
+  std::vector<std::string> args;
+  const char* names[3] = {"-eye", "-lookat", "-up"};
+  for (int k = 0; k < 3; ++k) {
+    args.push_back(names[k]);
+    for (int i = 0; i < 3; ++i) {
+      snprintf(buf[3 * k + i], 32, "%.9g", cam12_args[3 * k + i]);
+      args.push_back(buf[3 * k + i]);
+    }
+  }
+  args.push_back("-hfov"); snprintf(buf[9], 32, "%.9g", cam12_args[9]); args.push_back(buf[9]);
+  args.push_back("-vfov"); snprintf(buf[10], 32, "%.9g", cam12_args[10]); args.push_back(buf[10]);
+  args.push_back("-normalizeRays");
+  ExposedCamera camera(args);
+  LightSet* ls = new LightSet();
+  ls->setAmbientLight(new ConstantAmbient(Color(RGB(ambient[0], ambient[1], ambient[2]))));
+  for (int k = 0; k < nlights; ++k) {
+    const float* L = lights + 6 * k;
+    ls->add(new PointLight(Vector(L[0], L[1], L[2]), Color(RGB(L[3], L[4], L[5]))));
+  }
+  PreprocessContext pctx;
+  pctx.globalLights = ls;
+  for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
+  if (!s->scene) s->scene = new Scene();
+  s->scene->setObject(s->object);
+  s->scene->setBackground(new ConstantBackground(
+      Color(RGB(background[0], background[1], background[2]))));
+  s->scene->setLights(ls);
+  Raytracer renderer;
+  ConstantSampleGenerator sampler(0.f);
+  CoordJob job;
+  job.s = s;
+  job.renderer = &renderer;
+  job.camera = &camera;
+  job.sampler = &sampler;
+  job.n = n;
+  job.px = px;
+  job.py = py;
+  job.rgb = rgb;
+  job.tprim = tprim;
+  job.prim = prim;
+  job.next = 0;
+  job.nthreads = nthreads;
+  memset(job.shadow_rays, 0, sizeof(job.shadow_rays));
+  pthread_mutex_init(&job.lock, 0);
+  std::vector<pthread_t> th(nthreads);
+  std::vector<CoordArg> ar(nthreads);
+  for (int p = 0; p < nthreads; ++p) {
+    ar[p].job = &job;
+    ar[p].proc = p;
+    pthread_create(&th[p], 0, coord_worker, &ar[p]);
+  }
+  for (int p = 0; p < nthreads; ++p) pthread_join(th[p], 0);
+  pthread_mutex_destroy(&job.lock);
+  long long total = 0;
+  for (int p = 0; p < nthreads; ++p) total += job.shadow_rays[p];
   if (shadow_rays) *shadow_rays = total;
   return 0;
 }

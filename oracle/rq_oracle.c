@@ -817,3 +817,258 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
     for (int c = 0; c < 3; ++c) rad_out[3 * (g - p0) + c] = rad[c];
   }
 }
+
+/* ------------------------------------------------- two-level scenes --- */
+/* Scenes given as a "world": a flat triangle tree, or a top-level tree whose
+ * objects are instances of inner triangle trees.  Instance kinds:
+ *   0  InstanceT (Model/Instances/InstanceT.cc:60-90): the ray enters with
+ *      o - translation, the same direction and the current minT; a closer
+ *      inner hit is accepted through RayPacket::hit.  In an AnyHit query the
+ *      inner DynBVH pins an occluded ray's minT to T_EPSILON (DynBVH.cc:
+ *      331-349) and RayPacket::hit(T_EPSILON) fails, so the top level never
+ *      sees that occlusion: any-hit queries skip these instances.
+ *   1  the inner DynBVH as an object of the top-level group itself
+ *      (translation 0): hits and occlusion as for its own triangles. */
+
+typedef struct {
+  const float* bounds;
+  const int* child;
+  const int* children;
+  const unsigned char* axis;
+  const unsigned char* left_cheaper;
+  const int* ids;
+  int tri_kind;
+  const float* verts;
+  const unsigned* idx;
+  const float* wald;
+  const unsigned* face_mat;
+} orq_tree;
+
+typedef struct {
+  const orq_tree* top;   /* flat world: the triangle tree */
+  const orq_tree* inner; /* NULL for a flat world */
+  const int* inst_scene;
+  const float* inst_T;
+  const int* inst_kind;
+} orq_world;
+
+static Tree as_tree(const orq_tree* t) {
+  Tree T = {t->bounds, t->child, t->children, t->axis, t->left_cheaper,
+            t->ids, t->tri_kind, t->verts, t->idx, t->wald};
+  return T;
+}
+
+/* DynBVH::intersectNode of the top-level tree; leaves hand the ray to the
+ * instances. */
+static void visit_top(const orq_world* W, int node, Ray* r, int* inst) {
+  const orq_tree* T = W->top;
+  if (r->anyhit && r->hit) return;
+  r->node_tests++;
+  if (!box_test(T->bounds + 6 * (size_t)node, r)) return;
+  const int nch = T->children[node];
+  const int first = T->child[node];
+  if (nch != 0) {
+    for (int i = 0; i < nch; ++i) {
+      const int k = T->ids[first + i];
+      const int kind = W->inst_kind ? W->inst_kind[k] : 0;
+      if (r->anyhit && kind == 0) continue;
+      const Tree IT = as_tree(&W->inner[W->inst_scene[k]]);
+      Ray lr = *r;
+      for (int c = 0; c < 3; ++c) lr.o[c] = r->o[c] - W->inst_T[3 * k + c];
+      lr.hit = 0;
+      lr.prim = -1;
+      lr.u = lr.v = 0.f;
+      visit(&IT, 0, &lr);
+      r->node_tests = lr.node_tests;
+      r->tri_tests = lr.tri_tests;
+      if (lr.hit) {
+        r->minT = lr.minT;
+        r->hit = 1;
+        r->prim = lr.prim;
+        r->u = lr.u;
+        r->v = lr.v;
+        *inst = k;
+        if (r->anyhit) return;
+      }
+    }
+    return;
+  }
+  int front;
+  if (r->anyhit)
+    front = T->left_cheaper[node] ? 0 : 1;
+  else
+    front = r->d[T->axis[node]] > 0 ? 0 : 1;
+  visit_top(W, first + front, r, inst);
+  visit_top(W, first + 1 - front, r, inst);
+}
+
+static void world_trace(const orq_world* W, Ray* r, int* inst) {
+  *inst = -1;
+  if (!W->inner) {
+    const Tree T = as_tree(W->top);
+    visit(&T, 0, r);
+  } else {
+    visit_top(W, 0, r, inst);
+  }
+}
+
+/* orq_trace over a world; inst = hit instance (-1: none / flat world). */
+int orq_trace_world(const orq_world* W, int n, const float* org, const float* dir,
+                    const float* tmax, int anyhit, int* hit, float* t, int* prim,
+                    float* u, float* v, int* inst) {
+  for (int i = 0; i < n; ++i) {
+    Ray r;
+    ray_init(&r, org, dir, n, i, tmax[i], anyhit);
+    int k;
+    world_trace(W, &r, &k);
+    hit[i] = r.hit;
+    t[i] = r.minT;
+    prim[i] = r.hit ? r.prim : -1;
+    u[i] = r.u;
+    v[i] = r.v;
+    if (inst) inst[i] = r.hit ? k : -1;
+  }
+  return 0;
+}
+
+/* Image coordinates of frame samples [i0, i1) (item = pixel * spp + s):
+ * spp == 1 the SingleSampler pixel centres, otherwise stratified jitter
+ * (strata x strata cells, PCG32 keyed by seed and item) - the sampling of
+ * rfmanta_b200/csrc/rq_instance.cu sample_ray. */
+static void sample_coords(int xres, int yres, int spp, uint64_t seed, long long item,
+                          float* px, float* py) {
+  const long long pix = item / spp;
+  const int s = (int)(item - pix * spp);
+  const int x = (int)(pix % xres), y = (int)(pix / xres);
+  const float xscale = (float)2 / xres;
+  const float yscale = (float)2 / yres;
+  if (spp == 1) {
+    const float xoffset = (-xres / (float)2 + (float)0.5) * xscale;
+    const float yoffset = (-yres / (float)2 + (float)0.5) * yscale;
+    *px = (float)x * xscale + xoffset;
+    *py = (float)y * yscale + yoffset;
+    return;
+  }
+  int strata = 1;
+  while (strata * strata < spp) ++strata;
+  Pcg32 g;
+  pcg_seed(&g, seed ^ ((uint64_t)item * 0x9E3779B97F4A7C15ULL), (uint64_t)item);
+  const float jx = ((float)(s % strata) + pcg_float(&g)) / (float)strata;
+  const float jy = ((float)(s / strata) + pcg_float(&g)) / (float)strata;
+  *px = ((float)x + jx) * xscale + ((float)(-xres) / 2.f) * xscale;
+  *py = ((float)y + jy) * yscale + ((float)(-yres) / 2.f) * yscale;
+}
+
+void orq_sample_coords(int xres, int yres, int spp, unsigned long long seed, long long i0,
+                       long long i1, float* px, float* py) {
+  for (long long i = i0; i < i1; ++i)
+    sample_coords(xres, yres, spp, seed, i, &px[i - i0], &py[i - i0]);
+}
+
+/* One Whitted sample (the body of orq_render_whitted) at image coordinates
+ * (px, py) over a world; returns the shadow rays sent. */
+static long long whitted_sample(const orq_world* W, const float* mat_rgb, const float* cam,
+                                float px, float py, const float* lights, int nl,
+                                const float* ambient, const float* background,
+                                float* rgb, float* tprim, int* prim) {
+  Ray r;
+  const float* dir = cam + 3;
+  const float* cu = cam + 6;
+  const float* cv = cam + 9;
+  for (int c = 0; c < 3; ++c) {
+    r.o[c] = cam[c];
+    r.d[c] = cv[c] * px + cu[c] * py + dir[c];
+  }
+  v_normalize(r.d);
+  for (int c = 0; c < 3; ++c) r.inv[c] = (float)1 / r.d[c];
+  r.minT = MAXT;
+  r.hit = 0;
+  r.prim = -1;
+  r.u = r.v = 0.f;
+  r.anyhit = 0;
+  r.node_tests = r.tri_tests = 0;
+  int k;
+  world_trace(W, &r, &k);
+  *tprim = r.minT;
+  *prim = r.hit ? r.prim : -1;
+  if (!r.hit) {
+    for (int c = 0; c < 3; ++c) rgb[c] = background[c];
+    return 0;
+  }
+  const orq_tree* HT = W->inner ? &W->inner[W->inst_scene[k]] : W->top;
+  const Tree T = as_tree(HT);
+  const float* kd = mat_rgb + 3 * HT->face_mat[r.prim];
+  float nrm[3];
+  tri_normal(&T, r.prim, nrm);
+  float ffn[3];
+  const float dn = nrm[0] * r.d[0] + nrm[1] * r.d[1] + nrm[2] * r.d[2];
+  for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0) ? nrm[c] : -nrm[c];
+  float total[3] = {ambient[0], ambient[1], ambient[2]};
+  float hp[3];
+  for (int c = 0; c < 3; ++c) hp[c] = r.o[c] + r.d[c] * r.minT;
+  long long shadow_rays = 0;
+  for (int j = 0; j < nl; ++j) {
+    const float* L = lights + 6 * j;
+    float sd[3] = {L[0] - hp[0], L[1] - hp[1], L[2] - hp[2]};
+    if (!(sd[0] * ffn[0] + sd[1] * ffn[1] + sd[2] * ffn[2] > 0)) continue;
+    Ray s;
+    for (int c = 0; c < 3; ++c) {
+      s.o[c] = hp[c];
+      s.d[c] = sd[c];
+      s.inv[c] = (float)1 / sd[c];
+    }
+    s.minT = 1 - T_EPSILON;
+    s.hit = 0;
+    s.prim = -1;
+    s.u = s.v = 0.f;
+    s.anyhit = 1;
+    s.node_tests = s.tri_tests = 0;
+    shadow_rays++;
+    int sk;
+    world_trace(W, &s, &sk);
+    if (s.hit) continue;
+    float sum = 0;
+    for (int c = 0; c < 3; ++c) sum += sd[c] * sd[c];
+    float scale = 1 / sqrtf(sum);
+    for (int c = 0; c < 3; ++c) sd[c] *= scale;
+    const float cos_theta = sd[0] * ffn[0] + sd[1] * ffn[1] + sd[2] * ffn[2];
+    for (int c = 0; c < 3; ++c) total[c] += L[3 + c] * cos_theta;
+  }
+  for (int c = 0; c < 3; ++c) rgb[c] = total[c] * kd[c];
+  return shadow_rays;
+}
+
+/* Supersampled Whitted frame over a world, pixel rows [y0, y1): per pixel
+ * the spp samples' colours summed in sample order and scaled by 1/spp.
+ * Optional per-sample outputs (indexed by item - y0 * xres * spp): colour,
+ * primary t and triangle id.  Returns the shadow rays sent. */
+long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float* cam,
+                           int xres, int yres, int spp, unsigned long long seed,
+                           const float* lights, int nl, const float* ambient,
+                           const float* background, int y0, int y1, float* rgb,
+                           float* sample_rgb, float* sample_t, int* sample_prim) {
+  long long shadow = 0;
+  const float inv = (float)1 / (float)spp;
+  for (int y = y0; y < y1; ++y)
+    for (int x = 0; x < xres; ++x) {
+      const long long pix = (long long)y * xres + x;
+      float acc[3] = {0.f, 0.f, 0.f};
+      for (int s = 0; s < spp; ++s) {
+        const long long item = pix * spp + s;
+        const long long o = item - (long long)y0 * xres * spp;
+        float px, py, c[3], t;
+        int p;
+        sample_coords(xres, yres, spp, seed, item, &px, &py);
+        shadow += whitted_sample(W, mat_rgb, cam, px, py, lights, nl, ambient, background,
+                                 c, &t, &p);
+        for (int j = 0; j < 3; ++j) acc[j] += c[j];
+        if (sample_rgb)
+          for (int j = 0; j < 3; ++j) sample_rgb[3 * o + j] = c[j];
+        if (sample_t) sample_t[o] = t;
+        if (sample_prim) sample_prim[o] = p;
+      }
+      const long long po = pix - (long long)y0 * xres;
+      for (int j = 0; j < 3; ++j) rgb[3 * po + j] = acc[j] * inv;
+    }
+  return shadow;
+}

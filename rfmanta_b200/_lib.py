@@ -23,6 +23,8 @@ RQ_ERR_NODEV = 8
 
 RQ_TRI_WALD = 0
 RQ_TRI_KS = 1
+RQ_INST_TRANSLATE = 0
+RQ_INST_NESTED = 1
 RQ_CLOSEST = 0
 RQ_ANYHIT = 1
 
@@ -49,6 +51,10 @@ class WhittedParams(C.Structure):
                 ("n_lights", C.c_int), ("lights", C.c_void_p), ("ambient", C.c_float * 3),
                 ("background", C.c_float * 3), ("n_materials", C.c_int),
                 ("material_rgb", C.c_void_p)]
+
+
+class FrameParams(C.Structure):
+    _fields_ = [("whitted", WhittedParams), ("spp", C.c_int), ("seed", C.c_uint64)]
 
 
 class PathParams(C.Structure):
@@ -140,6 +146,10 @@ def _load():
                              C.POINTER(sz)], i),
         "rq_server_destroy": ([vp], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
+        "rq_scene_create_instanced": ([vp, i, vp, vp, vp, i, C.POINTER(vp)], i),
+        "rq_trace_device_ex": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp, vp, vp], i),
+        "rq_render_frame": ([vp, C.POINTER(FrameParams), vp, C.POINTER(C.c_uint64)], i),
+        "rq_render_frame_device": ([vp, C.POINTER(FrameParams), vp, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

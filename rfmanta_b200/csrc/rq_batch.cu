@@ -245,6 +245,7 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
     const Scene* s = reinterpret_cast<const Scene*>(scenes[i]);
     if (!s) return bfail(RQ_ERR_ARG, "NULL scene");
     if (!s->has_tree) return bfail(RQ_ERR_STATE, "scene " + std::to_string(i) + " has no tree");
+    if (s->instanced) return bfail(RQ_ERR_ARG, "batched queries take triangle scenes");
     if (s->device != s0->device) return bfail(RQ_ERR_ARG, "all scenes must be on one device");
     if (s->tri_kind != s0->tri_kind) return bfail(RQ_ERR_ARG, "all scenes must use one triangle kind");
     ds[i] = s->dev();

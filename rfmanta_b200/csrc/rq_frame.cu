@@ -102,6 +102,7 @@ static int prepare(Scene* s, const rq_whitted_params* p, FrameParams& P) {
     if ((int)m >= p->n_materials)
       return set_fail(RQ_ERR_ARG, "face_material refers past n_materials");
   if (!s->has_tree) return set_fail(RQ_ERR_STATE, "scene has no tree");
+  if (s->instanced) return set_fail(RQ_ERR_ARG, "instanced scene: render it with rq_render_frame");
   std::memset(&P, 0, sizeof(P));
   camera_basis(p->eye, p->lookat, p->up, p->hfov, p->vfov, P.cam);
   P.xres = p->xres;

@@ -97,6 +97,7 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
   for (uint32_t m : s->face_mat)
     if ((int)m >= p->n_materials) return na_fail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return na_fail(RQ_ERR_STATE, "scene has no tree");
+  if (s->instanced) return na_fail(RQ_ERR_ARG, "instanced scene: render it with rq_render_frame");
   if (cudaSetDevice(s->device) != cudaSuccess) return na_fail(RQ_ERR_CUDA, "cudaSetDevice");
   unsigned char* base = nullptr;
   int rc = scratch_address(s->device, &base);

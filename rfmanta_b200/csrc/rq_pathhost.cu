@@ -66,6 +66,7 @@ static int path_prepare(Scene* s, const rq_path_params* p, PathParams& P, long l
   for (uint32_t m : s->face_mat)
     if ((int)m >= p->n_materials) return pfail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return pfail(RQ_ERR_STATE, "scene has no tree");
+  if (s->instanced) return pfail(RQ_ERR_ARG, "path tracing takes triangle scenes");
   std::memset(&P, 0, sizeof(P));
   camera_basis(p->eye, p->lookat, p->up, p->hfov, p->vfov, P.cam);
   P.xres = p->xres;

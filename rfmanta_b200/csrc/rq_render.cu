@@ -24,32 +24,6 @@
 
 namespace rq {
 
-__device__ __forceinline__ void primary_ray(const FrameParams& P, int x, int y,
-                                            Ray& r) {
-  const float xscale = fdiv(2.f, (float)P.xres);
-  const float yscale = fdiv(2.f, (float)P.yres);
-  const float xoffset = fmul(fadd(fdiv((float)(-P.xres), 2.f), 0.5f), xscale);
-  const float yoffset = fmul(fadd(fdiv((float)(-P.yres), 2.f), 0.5f), yscale);
-  const float px = fadd(fmul((float)x, xscale), xoffset);
-  const float py = fadd(fmul((float)y, yscale), yoffset);
-  float d[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    r.o[c] = P.cam[c];
-    d[c] = fadd(fadd(fmul(P.cam[9 + c], px), fmul(P.cam[6 + c], py)), P.cam[3 + c]);
-  }
-  // Vector::normalize (Core/Geometry/Vector.h:322-331)
-  const float l = __fsqrt_rn(fadd(fadd(fmul(d[0], d[0]), fmul(d[1], d[1])),
-                                  fmul(d[2], d[2])));
-  const float s = fdiv(1.f, l);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    r.d[c] = fmul(d[c], s);
-    r.inv[c] = fdiv(1.f, r.d[c]);
-  }
-  r.minT = kMaxT;
-}
-
 // Adds a warp's counters into the frame statistics (one atomic per warp).
 __device__ __forceinline__ void flush_counts(unsigned long long* dst, int a, int b) {
   for (int o = 16; o > 0; o >>= 1) {

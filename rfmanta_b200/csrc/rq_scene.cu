@@ -61,6 +61,8 @@ Scene::~Scene() {
   if (d_idx) cudaFree(d_idx);
   if (d_face_mat) cudaFree(d_face_mat);
   if (d_counter) cudaFree(d_counter);
+  if (d_blas) cudaFree(d_blas);
+  if (samples) destroy_sample_scratch(samples);
   if (frame) destroy_frame(frame);
   if (paths) destroy_path_scratch(paths);
   staging.clear();
@@ -96,14 +98,15 @@ DevScene Scene::dev() const {
 // leaf-ordered triangle permutation.  Records are numbered in depth-first
 // pre-order of the internal nodes (root = record 0), leaves' triangles are
 // placed in the same pre-order, each leaf's object_ids in stored order.
-int Scene::set_tree(const HostTree& t) {
+int layout_tree(const HostTree& t, int n_objects, TreeLayout& L) {
   const int nn = (int)t.children.size();
   if (nn < 1) return fail(RQ_ERR_FORMAT, "tree has no nodes");
   const int nids = (int)t.ids.size();
   std::vector<int> rec_of(nn, -1);
   std::vector<int> leaf_start(nn, -1);
   std::vector<uint8_t> seen(nn, 0);
-  std::vector<int32_t> perm;
+  std::vector<int32_t>& perm = L.perm;
+  perm.clear();
   perm.reserve(nids);
   std::vector<int> order;  // internal nodes in record order
   // iterative pre-order DFS; stack holds (node, depth)
@@ -125,7 +128,7 @@ int Scene::set_tree(const HostTree& t) {
       leaf_start[node] = (int)perm.size();
       for (int i = 0; i < ch; ++i) {
         const int obj = t.ids[c + i];
-        if (obj < 0 || obj >= n_tris)
+        if (obj < 0 || obj >= n_objects)
           return fail(RQ_ERR_FORMAT, "object id out of range");
         perm.push_back(obj);
       }
@@ -141,7 +144,8 @@ int Scene::set_tree(const HostTree& t) {
       st.push_back({c, d + 1});
     }
   }
-  std::vector<float4> recs(order.size() * 4);
+  std::vector<float4>& recs = L.recs;
+  recs.assign(order.size() * 4, make_float4(0.f, 0.f, 0.f, 0.f));
   auto ref_of = [&](int node) -> int {
     return t.children[node] != 0 ? ~leaf_start[node] : rec_of[node];
   };
@@ -157,6 +161,29 @@ int Scene::set_tree(const HostTree& t) {
     int4 q3 = make_int4(ref_of(L), ref_of(R), meta, 0);
     std::memcpy(&recs[4 * r + 3], &q3, sizeof(q3));
   }
+  L.n_records = (int)order.size();
+  L.n_leaves = 0;
+  for (int i = 0; i < nn; ++i)
+    if (seen[i] && t.children[i] != 0) ++L.n_leaves;
+  L.root_ref = ref_of(0);
+  for (int c = 0; c < 3; ++c) {
+    L.root_lo[c] = t.bounds[c];
+    L.root_hi[c] = t.bounds[3 + c];
+  }
+  L.depth = max_depth;
+  if (L.depth > kMaxDepth)
+    return fail(RQ_ERR_CAPACITY, "tree depth " + std::to_string(L.depth) +
+                                     " exceeds the traversal stack limit");
+  return RQ_OK;
+}
+
+int Scene::set_tree(const HostTree& t) {
+  if (instanced) return set_instance_tree(this, t);
+  TreeLayout L;
+  const int rc = layout_tree(t, n_tris, L);
+  if (rc != RQ_OK) return rc;
+  const std::vector<float4>& recs = L.recs;
+  const std::vector<int32_t>& perm = L.perm;
   // device upload
   free_tree();
   const size_t rec_bytes = std::max<size_t>(recs.size(), 4) * sizeof(float4);
@@ -177,20 +204,15 @@ int Scene::set_tree(const HostTree& t) {
   cudaFree(d_perm);
   if (e != cudaSuccess) return cuda_fail(e, "triangle setup");
   tree = t;
-  n_records = (int)order.size();
+  n_records = L.n_records;
   n_leaf_tris = (int)perm.size();
-  n_leaves = 0;
-  for (int i = 0; i < nn; ++i)
-    if (seen[i] && t.children[i] != 0) ++n_leaves;
-  root_ref = ref_of(0);
+  n_leaves = L.n_leaves;
+  root_ref = L.root_ref;
   for (int c = 0; c < 3; ++c) {
-    root_lo[c] = t.bounds[c];
-    root_hi[c] = t.bounds[3 + c];
+    root_lo[c] = L.root_lo[c];
+    root_hi[c] = L.root_hi[c];
   }
-  depth = max_depth;
-  if (depth > kMaxDepth)
-    return fail(RQ_ERR_CAPACITY, "tree depth " + std::to_string(depth) +
-                                     " exceeds the traversal stack limit");
+  depth = L.depth;
   has_tree = true;
   return RQ_OK;
 }
@@ -310,7 +332,8 @@ int Scene::trace_device(int n, const float* org, const float* dir,
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
   }
-  cudaError_t e = launch_trace(dev(), a, anyhit, p, st);
+  cudaError_t e = instanced ? launch_trace2(*this, a, anyhit, nullptr, st)
+                            : launch_trace(dev(), a, anyhit, p, st);
   if (e != cudaSuccess) return cuda_fail(e, "trace launch");
   return RQ_OK;
 }
@@ -323,8 +346,6 @@ using rq::fail;
 using rq::cuda_fail;
 
 extern "C" {
-
-struct rq_scene : public rq::Scene {};
 
 const char* rq_last_error(void) { return rq::g_error.c_str(); }
 

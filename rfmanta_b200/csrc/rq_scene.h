@@ -18,6 +18,13 @@ struct FrameScratch;
 void destroy_frame(FrameScratch* f);
 struct PathScratch;
 void destroy_path_scratch(PathScratch* p);
+struct SampleScratch;
+void destroy_sample_scratch(SampleScratch* p);
+struct Scene;
+struct HostTree;
+cudaError_t launch_trace2(const Scene& s, const RayArgs& a, bool anyhit, int32_t* inst,
+                          cudaStream_t st);
+int set_instance_tree(Scene* s, const HostTree& t);
 
 // The reference DynBVH tree, field by field (Model/Groups/DynBVH.h:37-79).
 struct HostTree {
@@ -30,6 +37,22 @@ struct HostTree {
 };
 
 double tree_sah_cost(const HostTree& t);
+
+// A validated tree laid out for the kernels: node records (4 float4 each,
+// depth-first pre-order) and the leaf-ordered object permutation (bit 31 on
+// the last object of each leaf).
+struct TreeLayout {
+  std::vector<float4> recs;
+  std::vector<int32_t> perm;
+  int n_records = 0;
+  int n_leaves = 0;
+  int root_ref = 0;
+  float root_lo[3] = {0, 0, 0};
+  float root_hi[3] = {0, 0, 0};
+  int depth = 0;
+};
+
+int layout_tree(const HostTree& t, int n_objects, TreeLayout& out);
 
 // Per-call resources for the host-array entry point.
 struct Staging {
@@ -67,6 +90,18 @@ struct Scene {
   float root_lo[3] = {0, 0, 0};
   float root_hi[3] = {0, 0, 0};
 
+  // two-level scenes (InstanceT): the tree above is the top-level tree over
+  // instances and d_tris holds 2 float4 per instance in leaf order
+  // (translation xyz, inner scene index | instance id with the last-in-leaf
+  // bit, kind); the inner scenes are referenced, not owned.
+  bool instanced = false;
+  std::vector<Scene*> blas;
+  std::vector<int32_t> inst_blas;
+  std::vector<float> inst_translation;
+  std::vector<int32_t> inst_kind;
+  DevScene* d_blas = nullptr;
+  int max_blas_depth = 0;
+
   rq_launch_config cfg[2];
   int* d_counter = nullptr;  // persistent-launch counters for rq_trace_device
 
@@ -75,6 +110,7 @@ struct Scene {
 
   FrameScratch* frame = nullptr;  // frame-path scratch (rq_frame.cu)
   PathScratch* paths = nullptr;   // path-tracing scratch (rq_pathhost.cu)
+  SampleScratch* samples = nullptr;  // supersampled-frame scratch (rq_instance.cu)
   int32_t* path_dbg_prim = nullptr;
   float* path_dbg_org = nullptr;
   float* path_dbg_dir = nullptr;
@@ -98,3 +134,6 @@ struct Scene {
 };
 
 }  // namespace rq
+
+// The opaque handle of the C ABI is the scene itself.
+struct rq_scene : public rq::Scene {};

@@ -376,6 +376,7 @@ int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capac
   for (int i = 0; i < n_scenes; ++i) {
     Scene* sc = reinterpret_cast<Scene*>(scenes[i]);
     if (!sc || !sc->has_tree) return sfail(RQ_ERR_STATE, "scene without a tree");
+    if (sc->instanced) return sfail(RQ_ERR_ARG, "the server takes triangle scenes");
     if (sc->device != s0->device || sc->tri_kind != s0->tri_kind)
       return sfail(RQ_ERR_ARG, "scenes must share device and triangle kind");
     ds[i] = sc->dev();

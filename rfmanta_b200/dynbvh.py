@@ -245,6 +245,44 @@ class GpuDynBVH:
                                            C.c_void_p(shadow_ptr or None),
                                            C.c_void_p(stream or None)))
 
+    @staticmethod
+    def frame_params(scene, materials=None) -> "_lib.FrameParams":
+        """rq_frame_params for a supersampled frame (any scene object with
+        camera, lights, ambient, background, xres, yres, spp, seed)."""
+        p = _lib.FrameParams()
+        mats = getattr(scene, "materials", None) if materials is None else materials
+        w = GpuDynBVH.whitted_params(scene, mats)
+        p.whitted = w
+        p.spp = int(scene.spp)
+        p.seed = int(scene.seed)
+        p._keep = w._keep
+        return p
+
+    def render_frame(self, scene, materials=None):
+        """Supersampled Whitted frame (spp jittered samples per pixel,
+        averaged) over this scene; host outputs."""
+        p = self.frame_params(scene, materials)
+        rgb = np.zeros((scene.xres * scene.yres, 3), np.float32)
+        ns = C.c_uint64()
+        check(lib.rq_render_frame(self._h, C.byref(p), _p(rgb), C.byref(ns)))
+        return dict(rgb=rgb, shadow_rays=int(ns.value))
+
+    def render_frame_device(self, params, rgb_ptr: int, shadow_ptr: int = 0,
+                            stream: int = 0) -> None:
+        check(lib.rq_render_frame_device(self._h, C.byref(params), C.c_void_p(rgb_ptr),
+                                         C.c_void_p(shadow_ptr or None),
+                                         C.c_void_p(stream or None)))
+
+    def intersect_device_ex(self, n: int, org_ptr: int, dir_ptr: int, tmax_ptr: int,
+                            anyhit: bool, t_ptr: int, prim_ptr: int, u_ptr: int = 0,
+                            v_ptr: int = 0, inst_ptr: int = 0, stream: int = 0) -> None:
+        """intersect_device plus the hit instance per ray (-1: none)."""
+        check(lib.rq_trace_device_ex(self._h, n, C.c_void_p(org_ptr), C.c_void_p(dir_ptr),
+                                     C.c_void_p(tmax_ptr), RQ_ANYHIT if anyhit else RQ_CLOSEST,
+                                     C.c_void_p(t_ptr), C.c_void_p(prim_ptr),
+                                     C.c_void_p(u_ptr or None), C.c_void_p(v_ptr or None),
+                                     C.c_void_p(inst_ptr or None), C.c_void_p(stream or None)))
+
     def set_stage_events(self, events) -> None:
         """events: list of torch.cuda.Event (created with timing enabled and
         recorded at least once, which is when torch creates the CUDA event),
@@ -324,6 +362,49 @@ class GpuDynBVH:
             pass
 
 
+class InstancedBVH(GpuDynBVH):
+    """A top-level DynBVH over a Group of InstanceT objects
+    (Model/Instances/InstanceT.cc) and nested DynBVHs: instance k places
+    inner scene inst_scene[k] (a built GpuDynBVH) at translation[k], as an
+    InstanceT (kind RQ_INST_TRANSLATE) or as the nested acceleration
+    structure itself (RQ_INST_NESTED, zero translation).  The inner
+    GpuDynBVHs must stay alive and keep their trees while this one is used.
+    rebuild() builds the top-level tree on the GPU; importTree / importBlob
+    take a reference top-level tree (object ids = instance indices)."""
+
+    def __init__(self, inner: list, inst_scene, translation, kind=None):
+        super().__init__(inner[0].tri_kind, inner[0].device)
+        self._inner = list(inner)
+        self._sc = np.ascontiguousarray(inst_scene, np.int32)
+        self._tr = np.ascontiguousarray(translation, np.float32).reshape(-1, 3)
+        self._kd = np.ascontiguousarray(
+            np.zeros(self._sc.shape[0]) if kind is None else kind, np.int32)
+        self._group = self._inner  # setGroup is not used: the instances are the group
+
+    def setGroup(self, group) -> None:
+        raise _lib.RQError(_lib.RQ_ERR_ARG, "an InstancedBVH takes its instances at construction")
+
+    def _upload(self) -> None:
+        self.close()
+        hs = (C.c_void_p * len(self._inner))(*[b.handle.value for b in self._inner])
+        self._hs = hs
+        check(lib.rq_scene_create_instanced(hs, len(self._inner), _p(self._sc), _p(self._tr),
+                                            _p(self._kd), self._sc.shape[0],
+                                            C.byref(self._h)))
+        self._dirty = False
+
+    def rebuild(self, bins: int = 0) -> None:
+        if not self._h:
+            self._upload()  # builds the top-level tree
+            if bins == 0:
+                return
+        check(lib.rq_scene_build(self._h, bins))
+
+    @property
+    def n_instances(self) -> int:
+        return int(self._sc.shape[0])
+
+
 def camera_basis(cam) -> np.ndarray:
     """PinholeCamera::setup basis (host-only C-ABI call)."""
     e = np.asarray(cam.eye, np.float32)
@@ -334,4 +415,4 @@ def camera_basis(cam) -> np.ndarray:
     return out
 
 
-__all__ = ["GpuDynBVH", "RayBatch", "RQ_TRI_WALD", "RQ_TRI_KS", "T_EPSILON", "MAXT"]
+__all__ = ["GpuDynBVH", "InstancedBVH", "RayBatch", "RQ_TRI_WALD", "RQ_TRI_KS", "T_EPSILON", "MAXT"]

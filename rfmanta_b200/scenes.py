@@ -388,3 +388,66 @@ def query_rays_torch(n: int, lo, hi, anyhit: bool, seed: int, device="cuda"):
     else:
         tmax = torch.full((n,), 1e19, device=device)
     return org.contiguous(), d.contiguous(), tmax.contiguous()
+
+
+# ------------------------------------------------- two-level frame scene ---
+
+@dataclass
+class InstancedFrameScene:
+    """A supersampled Whitted frame over a two-level scene: inner meshes
+    sharing one material table, instances (inner index, translation, kind:
+    0 InstanceT, 1 nested DynBVH)."""
+    inner: list
+    inst_scene: np.ndarray
+    translation: np.ndarray
+    kind: np.ndarray
+    materials: np.ndarray
+    camera: Camera
+    lights: list
+    ambient: tuple
+    background: tuple
+    xres: int
+    yres: int
+    spp: int
+    seed: int
+
+    @property
+    def n_tris(self) -> int:
+        return int(sum(self.inner[i].n_tris for i in self.inst_scene))
+
+
+def coherent_scene(hf_n: int = 1024, n_instances: int = 64, sphere_level: int = 6,
+                   xres: int = 1920, yres: int = 1080, spp: int = 4,
+                   seed: int = 23) -> InstancedFrameScene:
+    """Large coherent frame: an hf_n x hf_n fBm heightfield (2*hf_n^2
+    triangles, 5 octaves, amplitude 0.2) placed in the top-level group as a
+    nested DynBVH, plus n_instances InstanceT copies of one displaced
+    icosphere (level 6: 81,920 triangles, amplitude 0.05, frequency 4) at
+    seeded uniform positions above it; two point lights, Lambertian, spp
+    stratified jittered samples per pixel.  Defaults: 1920x1080x4,
+    2,097,152 + 64 x 81,920 triangles."""
+    rng = np.random.default_rng(seed)
+    ext = 8.0
+    hf = heightfield(hf_n, hf_n, seed=seed + 1, extent=ext, y=0.0, material=0)
+    sphere = displaced_icosphere(sphere_level, seed=seed + 2, radius=0.35, material=1)
+    pos = np.stack([rng.uniform(-3.5, 3.5, n_instances), rng.uniform(0.45, 0.9, n_instances),
+                    rng.uniform(-3.5, 3.5, n_instances)], 1).astype(np.float32)
+    inst_scene = np.concatenate([[0], np.ones(n_instances)]).astype(np.int32)
+    translation = np.concatenate([np.zeros((1, 3), np.float32), pos]).astype(np.float32)
+    kind = np.concatenate([[1], np.zeros(n_instances)]).astype(np.int32)
+    mats = np.array([[0.7, 0.7, 0.65], [0.8, 0.3, 0.2]], np.float32)
+    hf.materials = mats
+    sphere.materials = mats
+    cam = Camera((0.0, 4.0, 8.5), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 60.0,
+                 float(2.0 * np.degrees(np.arctan(np.tan(np.radians(30.0)) * yres / xres))))
+    lights = [PointLightSpec((3.0, 6.0, 4.0), (0.8, 0.8, 0.75)),
+              PointLightSpec((-4.0, 5.0, -2.0), (0.35, 0.4, 0.5))]
+    return InstancedFrameScene([hf, sphere], inst_scene, translation, kind, mats, cam, lights,
+                               (0.08, 0.08, 0.1), (0.2, 0.3, 0.5), xres, yres, spp, seed)
+
+
+def tiny_coherent_scene(xres: int = 48, yres: int = 40, spp: int = 4,
+                        n_instances: int = 6) -> InstancedFrameScene:
+    """The coherent-frame layout scaled down for committed checks."""
+    return coherent_scene(hf_n=12, n_instances=n_instances, sphere_level=2, xres=xres,
+                          yres=yres, spp=spp, seed=9)

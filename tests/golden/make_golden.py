@@ -16,7 +16,12 @@ DynBVH::rebuild, and records what the reference computes:
   * the Raytracer::traceEyeRays frame (RGB, primary t and triangle id) and
     the number of shadow rays HardShadows sent.
 It also records DynBVH::computeCost of the reference's own tree for a few
-larger seeded scenes (sah_costs.json), the bound for the GPU builder.
+larger seeded scenes (sah_costs.json), the bound for the GPU builder, and a
+two-level scene (tiny_instanced.npz): a 12x12 heightfield placed in the
+top-level group as a nested DynBVH plus six InstanceT copies of a level-2
+displaced icosphere, with the reference's inner and top-level trees, its
+DynBVH::intersect results (closest and AnyHit) for seeded rays and its
+Raytracer colours for the 4-spp jittered samples of a 48x40 frame.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -87,6 +92,42 @@ def main() -> None:
         print(path, os.path.getsize(path), "bytes")
 
 
+def write_instanced() -> None:
+    ref = Reference()
+    restated = Restatement()
+    sc = scenes.tiny_coherent_scene()
+    inner = [ref.scene(m, 0) for m in sc.inner]
+    top = ref.instanced(inner, sc.inst_scene, sc.translation, sc.kind)
+    lo = np.array([-4.5, -0.5, -4.5], np.float32)
+    hi = np.array([4.5, 2.0, 4.5], np.float32)
+    o_r, d_r, _, _ = scenes.random_rays(4096, lo, hi, seed=31)
+    o_a, d_a, tm_a, _ = scenes.random_rays(4096, lo, hi, seed=32, anyhit_fraction=1.0)
+    rnd_q = top.intersect2(o_r, d_r, np.full(o_r.shape[1], 1e19, np.float32))
+    any_q = top.intersect2(o_a, d_a, tm_a, anyhit=True)
+    px, py = restated.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed)
+    img = top.render_coords(sc, px, py)
+    out = dict(n_inner=np.int32(len(sc.inner)), inst_scene=sc.inst_scene,
+               translation=sc.translation, kind=sc.kind, materials=sc.materials,
+               xres=np.int32(sc.xres), yres=np.int32(sc.yres), spp=np.int32(sc.spp),
+               seed=np.int64(sc.seed), sample_px=px, sample_py=py,
+               rand_org=o_r, rand_dir=d_r, **{f"rand_{k}": v for k, v in rnd_q.items()},
+               any_org=o_a, any_dir=d_a, any_tmax=tm_a,
+               **{f"any_{k}": v for k, v in any_q.items()},
+               sample_rgb=img["rgb"], sample_t=img["t"], sample_prim=img["prim"],
+               shadow_rays=np.int64(img["shadow_rays"]))
+    trees = [(f"inner{i}", r.tree()) for i, r in enumerate(inner)] + [("top", top.tree())]
+    for name, t in trees:
+        for f in ("bounds", "child", "children", "axis", "left_cheaper", "ids"):
+            out[f"{name}_{f}"] = getattr(t, f)
+    for i, m in enumerate(sc.inner):
+        out[f"inner{i}_vertices"] = m.vertices
+        out[f"inner{i}_indices"] = m.indices
+        out[f"inner{i}_face_material"] = m.face_material
+    path = os.path.join(OUT, "tiny_instanced.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 def sah_scenes():
     """Scenes whose reference SAH cost pins the GPU builder (2% bound)."""
     out = {"small_frame": scenes.small_frame_scene().mesh,
@@ -118,5 +159,9 @@ def write_sah_costs() -> None:
 
 
 if __name__ == "__main__":
-    main()
-    write_sah_costs()
+    if "--instanced" in sys.argv:
+        write_instanced()
+    else:
+        main()
+        write_sah_costs()
+        write_instanced()

@@ -167,7 +167,7 @@ class PathFrame:
         self.n_events = 2 + 2 * self.sc.max_depth
         self.stage_names = []
         for d in range(self.sc.max_depth):
-            self.stage_names += [f"path_extend_kernel[{d}]", f"path_shade_kernel[{d}]"]
+            self.stage_names += [f"path_extend_persistent_kernel[{d}]", f"path_shade_persistent_kernel[{d}]"]
         self.stage_names.append("path_resolve_kernel")
         self.launches = 1 + 3 * self.sc.max_depth + 1
 
@@ -205,7 +205,7 @@ class PathFrame:
         D = self.sc.max_depth
         ext = sum(stage_ms[2 * d] for d in range(D))
         shade = sum(stage_ms[2 * d + 1] for d in range(D))
-        return ["path_extend_kernel", "path_shade_kernel"], [ext, shade]
+        return ["path_extend_persistent_kernel", "path_shade_persistent_kernel"], [ext, shade]
 
     def cpu_reference(self, seconds_budget, threads):
         """Reference KajiyaPathtracer on a 1 spp sample of the same frame."""
@@ -389,10 +389,13 @@ class CoherentFrame:
         image row of the frame's samples."""
         from oracle.pyoracle import Reference, Restatement
         sse = Reference.available(sse=True)
-        ref = Reference(sse=sse)
         sc = self.sc
-        inner = [ref.scene(m, 0) for m in sc.inner]
-        top = ref.instanced(inner, sc.inst_scene, sc.translation, sc.kind)
+        if not hasattr(self, "_ref"):  # the reference's trees, built once
+            ref = Reference(sse=sse)
+            inner = [ref.scene(m, 0) for m in sc.inner]
+            self._ref = (ref, inner, ref.instanced(inner, sc.inst_scene, sc.translation,
+                                                   sc.kind))
+        top = self._ref[2]
         rs = Restatement()
         per_row = sc.xres * sc.spp
         rows = list(range(0, sc.yres, 16))
@@ -407,8 +410,6 @@ class CoherentFrame:
             secs += time.perf_counter() - t0
             rays += px.size + out["shadow_rays"]
             passes += 1
-        for r in inner:
-            r.close()
         text = (f"{passes} pass(es) over every 16th row of the {sc.xres}x{sc.yres}x{sc.spp} "
                 f"frame ({len(rows)} rows, {px.size} samples), reference Raytracer over a "
                 f"top-level DynBVH of InstanceT + nested DynBVH objects, WaldTriangle/"
@@ -698,6 +699,19 @@ class ServingWL(BatchedQueriesWL):
         return rays / secs / 1e6, threads, text, secs
 
 
+def make_workload(args):
+    wl = WORKLOADS[args.workload]()
+    sc = getattr(wl, "sc", None)
+    if (args.res or args.spp) and sc is None:
+        raise SystemExit(f"--res/--spp apply to frame workloads, not {args.workload}")
+    if args.res:
+        w, h = (int(x) for x in args.res.lower().split("x"))
+        sc.xres, sc.yres = w, h
+    if args.spp:
+        sc.spp = args.spp
+    return wl
+
+
 def rays_or(x):
     return max(int(x), 1)
 
@@ -718,7 +732,7 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://",
                                 timeout=datetime.timedelta(seconds=120))
     from rfmanta_b200.dynbvh import GpuDynBVH
-    wl = WORKLOADS[args.workload]()
+    wl = make_workload(args)
     dev = torch.device("cuda", local)
     if hasattr(wl, "run_custom"):
         return run_custom(args, wl, dev, world, rank)
@@ -887,7 +901,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libmanta_ref.so was not built (needs the reference sources)"}))
         return
-    wl = WORKLOADS[args.workload]()
+    wl = make_workload(args)
     threads = os.cpu_count() or 1
     per_step = []
     text = ""
@@ -919,6 +933,10 @@ def main():
     ap.add_argument("--workload", default="path_frame", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--res", default=None,
+                    help="WxH override of a frame workload's resolution (small ncu cases)")
+    ap.add_argument("--spp", type=int, default=None,
+                    help="samples per pixel override of a frame workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -4,7 +4,7 @@
 //
 //   generate   camera ray per path (pixel, sample): stratified jitter inside
 //              the pixel, PinholeCamera basis (PinholeCamera.cc:356-366)
-//   per bounce
+//   per bounce (both stages persistent, warps refilling idle lanes)
 //     extend   closest-hit traversal of the live paths (compacted queue)
 //     shade    fused stage per live path: background on a miss
 //              (KajiyaPathtracer.cc:283-291), Lambertian::sampleBSDF cosine
@@ -41,78 +41,158 @@ __device__ __forceinline__ int queue_count(const PathBuffers& B, int depth, int 
   return depth == 0 ? n0 : *(volatile const int*)&B.counters[depth];
 }
 
+// Persistent form of the extension stage: each lane keeps one path's ray in
+// flight; after every while-while step the warp counts its idle lanes with a
+// ballot and, once `refill` or more are idle (or none is busy), one lane
+// claims that many queue entries with a single atomicAdd on the bounce's
+// work counter and the idle lanes start them.  Lanes stay busy while a
+// warp's rays finish at different times; results do not depend on the
+// schedule.
 template <int KIND, bool STATS>
 __global__ void __launch_bounds__(128)
-    path_extend_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0) {
+    path_extend_persistent_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0,
+                                  int refill) {
   extern __shared__ int2 smem_stack[];
   int2* stk = smem_stack + threadIdx.x;
   const int stride = blockDim.x;
   const int nq = queue_count(B, depth, n0);
   const int* qin = B.queue[depth & 1];
-  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
-    const int qi = base + threadIdx.x;
-    Counts cnt;
-    if (qi < nq) {
-      const int p = depth == 0 ? qi : qin[qi];
-      extend_path<KIND, STATS>(S, P, B, depth, p, stk, stride, cnt);
+  int* counter = &B.counters[kFetchBase + depth];
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int p = -1;  // path slot in flight, -1 = idle
+  bool exhausted = false;
+  Counts cnt;
+  Ray r;
+  Hit h;
+  int ref = kDone, sp = 0;
+  for (;;) {
+    const bool idle = (p < 0) && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, idle);
+    const unsigned busy = __ballot_sync(0xffffffffu, p >= 0);
+    if (m != 0u && (__popc(m) >= refill || busy == 0u)) {
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (idle) {
+        const int qi = base + __popc(m & lt_mask);
+        if (qi < nq) {
+          p = depth == 0 ? qi : qin[qi];
+          load_extension_ray(B, p, r);
+          start_ray(S, r, h, ref, sp);
+          if (STATS) cnt.boxes += 1;
+        } else {
+          exhausted = true;
+        }
+      }
     }
-    if (STATS) {
-      int a = cnt.boxes, b = cnt.tris;
-      for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        b += __shfl_xor_sync(0xffffffffu, b, o);
+    if (__all_sync(0xffffffffu, exhausted)) break;
+    if (p >= 0) {
+      if (ref != kDone) step<KIND, false, STATS>(S, r, h, ref, sp, stk, stride, &cnt);
+      if (ref == kDone) {
+        store_extension(P, B, depth, p, r, h);
+        p = -1;
       }
-      if ((threadIdx.x & 31u) == 0) {
-        atomicAdd(&B.stats[0], (unsigned long long)a);
-        atomicAdd(&B.stats[1], (unsigned long long)b);
-      }
+    }
+  }
+  if (STATS) {
+    int a = cnt.boxes, b = cnt.tris;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&B.stats[0], (unsigned long long)a);
+      atomicAdd(&B.stats[1], (unsigned long long)b);
     }
   }
 }
 
+// Persistent form of the shade stage, with the same warp-ballot refill as
+// the extension kernel: a lane takes a live path, runs shade_begin, then
+// steps its shadow ray's any-hit traversal; when the ray is done (or none was
+// needed) it applies shade_finish and the survivors are compacted into the
+// next queue at the warp's common point, one atomic per warp.
 template <int KIND, bool STATS>
 __global__ void __launch_bounds__(128)
-    path_shade_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0) {
+    path_shade_persistent_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0,
+                                 int refill) {
   extern __shared__ int2 smem_stack[];
   int2* stk = smem_stack + threadIdx.x;
   const int stride = blockDim.x;
   const int nq = queue_count(B, depth, n0);
   const int* qin = B.queue[depth & 1];
   int* qout = B.queue[(depth + 1) & 1];
+  int* counter = &B.counters[kShadeFetchBase + depth];
   const unsigned lane = threadIdx.x & 31u;
-  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
-    const int qi = base + threadIdx.x;
-    bool alive = false;
-    int p = 0;
-    int nshadow = 0;
-    Counts cnt;
-    if (qi < nq) {
-      p = depth == 0 ? qi : qin[qi];
-      alive = shade_path<KIND, STATS>(S, P, B, depth, p, B.g0 + p, stk, stride, cnt, nshadow);
-    }
-    // compaction of the survivors, one atomic per warp
-    const unsigned m = __ballot_sync(0xffffffffu, alive);
-    if (m) {
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int p = -1;  // path slot in flight, -1 = idle
+  bool exhausted = false, alive = false, traced = false;
+  int nshadow = 0;
+  Counts cnt;
+  float contrib[3];
+  Ray sr;
+  Hit sh;
+  int ref = kDone, sp = 0;
+  for (;;) {
+    const bool idle = (p < 0) && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, idle);
+    const unsigned busy = __ballot_sync(0xffffffffu, p >= 0);
+    if (m != 0u && (__popc(m) >= refill || busy == 0u)) {
       const int leader = __ffs(m) - 1;
-      int q = 0;
-      if ((int)lane == leader) q = atomicAdd(&B.counters[depth + 1], __popc(m));
-      q = __shfl_sync(0xffffffffu, q, leader);
-      if (alive) qout[q + __popc(m & ((1u << lane) - 1u))] = p;
+      int base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (idle) {
+        const int qi = base + __popc(m & lt_mask);
+        if (qi < nq) {
+          p = depth == 0 ? qi : qin[qi];
+          traced = shade_begin<KIND>(S, P, B, depth, p, B.g0 + p, sr, contrib, alive);
+          ref = kDone;
+          if (traced) {
+            ++nshadow;
+            start_ray(S, sr, sh, ref, sp);
+            if (STATS) cnt.boxes += 1;
+          }
+        } else {
+          exhausted = true;
+        }
+      }
     }
-    int tot = nshadow;
+    if (__all_sync(0xffffffffu, exhausted)) break;
+    bool fin = false;
+    if (p >= 0) {
+      if (ref != kDone) step<KIND, true, STATS>(S, sr, sh, ref, sp, stk, stride, &cnt);
+      if (ref == kDone) {
+        if (traced && sh.id < 0) shade_finish(B, p, contrib);
+        fin = true;
+      }
+    }
+    const bool push = fin && alive;
+    const unsigned pm = __ballot_sync(0xffffffffu, push);
+    if (pm) {
+      const int leader = __ffs(pm) - 1;
+      int q = 0;
+      if ((int)lane == leader) q = atomicAdd(&B.counters[depth + 1], __popc(pm));
+      q = __shfl_sync(0xffffffffu, q, leader);
+      if (push) qout[q + __popc(pm & lt_mask)] = p;
+    }
+    if (fin) p = -1;
+  }
+  int tot = nshadow;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    if (lane == 0 && tot) atomicAdd(&B.ray_counts[1], (unsigned long long)tot);
-    if (STATS) {
-      int a = cnt.boxes, b = cnt.tris;
-      for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        b += __shfl_xor_sync(0xffffffffu, b, o);
-      }
-      if (lane == 0) {
-        atomicAdd(&B.stats[2], (unsigned long long)a);
-        atomicAdd(&B.stats[3], (unsigned long long)b);
-      }
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  if (lane == 0 && tot) atomicAdd(&B.ray_counts[1], (unsigned long long)tot);
+  if (STATS) {
+    int a = cnt.boxes, b = cnt.tris;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&B.stats[2], (unsigned long long)a);
+      atomicAdd(&B.stats[3], (unsigned long long)b);
     }
   }
 }
@@ -143,16 +223,38 @@ __global__ void path_resolve_kernel(PathParams P, PathBuffers B, long long g0, i
   }
 }
 
+// Lanes that must be idle before a warp of the persistent extension / shade
+// kernels fetches new paths.
+constexpr int kExtendRefill = 8;
+constexpr int kShadeRefill = 8;
+
 template <int KIND, bool STATS>
 static void launch_bounces(const DevScene& S, const PathParams& P, const PathBuffers& B,
-                           int n, int grid, size_t smem, cudaStream_t st,
+                           int n, size_t smem, cudaStream_t st,
                            const cudaEvent_t* ev, int nev) {
   const int bs = 128;
+  // the persistent extension kernel fills every SM once at its own occupancy
+  const void* ef = (const void*)path_extend_persistent_kernel<KIND, STATS>;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(ef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int eb = 0, dev = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&eb, ef, bs, smem);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int egrid = std::max(1, eb * sms);
+  const void* sf = (const void*)path_shade_persistent_kernel<KIND, STATS>;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(sf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int sb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sb, sf, bs, smem);
+  const int sgrid = std::max(1, sb * sms);
   for (int depth = 0; depth < P.max_depth; ++depth) {
     path_count_kernel<<<1, 32, 0, st>>>(B, depth, n);
-    path_extend_kernel<KIND, STATS><<<grid, bs, smem, st>>>(S, P, B, depth, n);
+    path_extend_persistent_kernel<KIND, STATS><<<egrid, bs, smem, st>>>(S, P, B, depth, n,
+                                                                        kExtendRefill);
     if (nev > 1 + 2 * depth) cudaEventRecord(ev[1 + 2 * depth], st);
-    path_shade_kernel<KIND, STATS><<<grid, bs, smem, st>>>(S, P, B, depth, n);
+    path_shade_persistent_kernel<KIND, STATS><<<sgrid, bs, smem, st>>>(S, P, B, depth, n,
+                                                                       kShadeRefill);
     if (nev > 2 + 2 * depth) cudaEventRecord(ev[2 + 2 * depth], st);
   }
 }
@@ -170,11 +272,11 @@ cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffer
   if (nev > 0) cudaEventRecord(ev[0], st);
   const bool stats = B.stats != nullptr;
   if (S.tri_kind == kWald) {
-    if (stats) launch_bounces<kWald, true>(S, P, B, n, grid, smem, st, ev, nev);
-    else launch_bounces<kWald, false>(S, P, B, n, grid, smem, st, ev, nev);
+    if (stats) launch_bounces<kWald, true>(S, P, B, n, smem, st, ev, nev);
+    else launch_bounces<kWald, false>(S, P, B, n, smem, st, ev, nev);
   } else {
-    if (stats) launch_bounces<kKS, true>(S, P, B, n, grid, smem, st, ev, nev);
-    else launch_bounces<kKS, false>(S, P, B, n, grid, smem, st, ev, nev);
+    if (stats) launch_bounces<kKS, true>(S, P, B, n, smem, st, ev, nev);
+    else launch_bounces<kKS, false>(S, P, B, n, smem, st, ev, nev);
   }
   path_resolve_kernel<<<std::max(1, std::min(grid, (n / P.spp + 255) / 256)), 256, 0, st>>>(
       P, B, g0, n, rgb);
@@ -183,21 +285,16 @@ cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffer
 }
 
 int path_blocks_per_sm(int tri_kind, size_t smem) {
-  const void* fs[8] = {(const void*)path_extend_kernel<kWald, false>,
-                       (const void*)path_extend_kernel<kWald, true>,
-                       (const void*)path_extend_kernel<kKS, false>,
-                       (const void*)path_extend_kernel<kKS, true>,
-                       (const void*)path_shade_kernel<kWald, false>,
-                       (const void*)path_shade_kernel<kWald, true>,
-                       (const void*)path_shade_kernel<kKS, false>,
-                       (const void*)path_shade_kernel<kKS, true>};
+  const void* fs[4] = {(const void*)path_shade_persistent_kernel<kWald, false>,
+                       (const void*)path_shade_persistent_kernel<kWald, true>,
+                       (const void*)path_shade_persistent_kernel<kKS, false>,
+                       (const void*)path_shade_persistent_kernel<kKS, true>};
   if (smem > 48 * 1024)
     for (const void* f : fs)
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int a = 0, b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, fs[tri_kind == kWald ? 0 : 2], 128, smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fs[tri_kind == kWald ? 4 : 6], 128, smem);
-  return std::max(1, std::min(a, b));
+  int b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fs[tri_kind == kWald ? 0 : 2], 128, smem);
+  return std::max(1, b);
 }
 
 }  // namespace rq

@@ -10,7 +10,12 @@
 namespace rq {
 
 constexpr int kMaxPathDepth = 16;
-constexpr int kPathCounters = kMaxPathDepth + 2;
+// counters[0..kMaxPathDepth]: live paths per depth; counters[kFetchBase + d]
+// and counters[kShadeFetchBase + d]: the work counters of bounce d's
+// persistent extension and shade launches
+constexpr int kFetchBase = kMaxPathDepth + 1;
+constexpr int kShadeFetchBase = kFetchBase + kMaxPathDepth;
+constexpr int kPathCounters = kShadeFetchBase + kMaxPathDepth;
 
 struct PathParams {
   float cam[12];  // eye, lookat-eye, u, v
@@ -39,7 +44,7 @@ struct PathBuffers {
   int32_t* pos;
   int32_t* prim;
   int32_t* queue[2];
-  int32_t* counters;            // kPathCounters: live paths per depth
+  int32_t* counters;            // kPathCounters (see above)
   unsigned long long* ray_counts;  // [0] extension rays, [1] shadow rays
   unsigned long long* stats;       // optional box/tri test counters (4)
   // optional per-bounce dump for parity checks: [depth][path]

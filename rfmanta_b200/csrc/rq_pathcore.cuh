@@ -91,13 +91,9 @@ __device__ __forceinline__ void record_normal(const DevScene& S, int pos, float*
   }
 }
 
-// Closest hit of one live path's current ray.
-template <int KIND, bool STATS>
-__device__ __forceinline__ void extend_path(const DevScene& S, const PathParams& P,
-                                            const PathBuffers& B, int depth, int p,
-                                            int2* stk, int stride, Counts& cnt) {
+// Extension ray of path slot p (o, d of the current bounce, minT = MAXT).
+__device__ __forceinline__ void load_extension_ray(const PathBuffers& B, int p, Ray& r) {
   const size_t C = B.capacity;
-  Ray r;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     r.o[c] = B.o[c * C + p];
@@ -105,11 +101,13 @@ __device__ __forceinline__ void extend_path(const DevScene& S, const PathParams&
     r.inv[c] = fdiv(1.f, r.d[c]);
   }
   r.minT = kMaxT;
-  Hit h;
-  int ref, sp;
-  start_ray(S, r, h, ref, sp);
-  if (STATS) cnt.boxes = 1;
-  while (ref != kDone) step<KIND, false, STATS>(S, r, h, ref, sp, stk, stride, &cnt);
+}
+
+// Closest hit of path slot p at this bounce (and the optional dump).
+__device__ __forceinline__ void store_extension(const PathParams& P, const PathBuffers& B,
+                                                int depth, int p, const Ray& r,
+                                                const Hit& h) {
+  const size_t C = B.capacity;
   B.t[p] = h.t;
   B.pos[p] = h.pos;
   B.prim[p] = h.id;
@@ -122,157 +120,195 @@ __device__ __forceinline__ void extend_path(const DevScene& S, const PathParams&
       B.dbg_dir[(size_t)c * P.max_depth * C + k] = r.d[c];
     }
   }
-    }
+}
 
-// One live path at one bounce: background on a miss, else BSDF sample,
-// light sample with its any-hit shadow ray, Russian roulette and the state
-// update for the next bounce.  Returns true when the path continues.
+// Closest hit of one live path's current ray.
 template <int KIND, bool STATS>
-__device__ __forceinline__ bool shade_path(const DevScene& S, const PathParams& P,
-                                           const PathBuffers& B, int depth, int p,
-                                           long long g, int2* stk, int stride, Counts& cnt,
-                                           int& nshadow) {
+__device__ __forceinline__ void extend_path(const DevScene& S, const PathParams& P,
+                                            const PathBuffers& B, int depth, int p,
+                                            int2* stk, int stride, Counts& cnt) {
+  Ray r;
+  load_extension_ray(B, p, r);
+  Hit h;
+  int ref, sp;
+  start_ray(S, r, h, ref, sp);
+  if (STATS) cnt.boxes = 1;
+  while (ref != kDone) step<KIND, false, STATS>(S, r, h, ref, sp, stk, stride, &cnt);
+  store_extension(P, B, depth, p, r, h);
+}
+
+// First half of one live path's bounce: background on a miss, else BSDF
+// sample, the light sample and Russian roulette, with the path's next state
+// (o, d, importance, RNG) written when it survives.  When the light sample
+// needs a shadow ray, returns true with the ray in `sr` and the radiance it
+// adds when unoccluded in `contrib`; shade_finish then applies it.  `alive`
+// tells whether the path continues.
+template <int KIND>
+__device__ __forceinline__ bool shade_begin(const DevScene& S, const PathParams& P,
+                                            const PathBuffers& B, int depth, int p,
+                                            long long g, Ray& sr, float* contrib,
+                                            bool& alive) {
   const size_t C = B.capacity;
   const bool last_depth = depth + 1 >= P.max_depth;
   const bool do_rr = depth >= P.rr_depth && depth != P.max_depth - 1;
-  bool alive = false;
-  float imp[3], rad[3], o[3], d[3];
+  alive = false;
+  bool traced = false;
+  float imp[3], o[3], d[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     imp[c] = B.imp[c * C + p];
-    rad[c] = B.rad[c * C + p];
     o[c] = B.o[c * C + p];
     d[c] = B.d[c * C + p];
   }
   const int prim = B.prim[p];
   if (prim < 0) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rad[c] = fadd(rad[c], fmul(P.background[c], imp[c]));
-  } else {
-    Pcg32 rng;
-    rng.state = B.rng[p];
-    rng.inc = ((unsigned long long)g << 1u) | 1u;
-    const float t = B.t[p];
-    float hp[3], ng[3], ffn[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) hp[c] = fadd(o[c], fmul(d[c], t));
-    record_normal<KIND>(S, B.pos[p], ng);
-    const float dn = dot3(ng, d);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0.f) ? ng[c] : -ng[c];
-    // Lambertian::sampleBSDF
-    const float r1 = pcg32_float(rng);
-    const float r2 = pcg32_float(rng);
-    const float sintheta = __fsqrt_rn(r1);
-    const float costheta = __fsqrt_rn(fsub(1.f, r1));
-    float cph, sph;
-    sincos_2pi(r2, cph, sph);
-    const float cosphi = fmul(cph, sintheta);
-    const float sinphi = fmul(sph, sintheta);
-    float v1[3];
-    {  // Vector::findPerpendicular (Core/Geometry/Vector.h:450-462)
-      const float d2 = fmul(ffn[2], ffn[2]);
-      const float d1 = fmul(ffn[1], ffn[1]);
-      if (fadd(d2, d1) < 1e-4f) {
-        v1[0] = -ffn[2];
-        v1[1] = 0.f;
-        v1[2] = ffn[0];
-      } else {
-        v1[0] = 0.f;
-        v1[1] = ffn[2];
-        v1[2] = -ffn[1];
-      }
-      const float l = __fsqrt_rn(fadd(fadd(fmul(v1[0], v1[0]), fmul(v1[1], v1[1])),
-                                      fmul(v1[2], v1[2])));
-      const float s = fdiv(1.f, l);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) v1[c] = fmul(v1[c], s);
-    }
-    float v2[3];
-    cross3(v1, ffn, v2);
-    float nd[3];
-#pragma unroll
     for (int c = 0; c < 3; ++c)
-      nd[c] = fadd(fadd(fmul(ffn[c], costheta), fmul(v1[c], cosphi)), fmul(v2[c], sinphi));
-    const float* kd = P.materials + 3 * (size_t)__ldg(S.face_material + prim);
-    float refl[3];
+      B.rad[c * C + p] = fadd(B.rad[c * C + p], fmul(P.background[c], imp[c]));
+    return false;
+  }
+  Pcg32 rng;
+  rng.state = B.rng[p];
+  rng.inc = ((unsigned long long)g << 1u) | 1u;
+  const float t = B.t[p];
+  float hp[3], ng[3], ffn[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) hp[c] = fadd(o[c], fmul(d[c], t));
+  record_normal<KIND>(S, B.pos[p], ng);
+  const float dn = dot3(ng, d);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0.f) ? ng[c] : -ng[c];
+  // Lambertian::sampleBSDF
+  const float r1 = pcg32_float(rng);
+  const float r2 = pcg32_float(rng);
+  const float sintheta = __fsqrt_rn(r1);
+  const float costheta = __fsqrt_rn(fsub(1.f, r1));
+  float cph, sph;
+  sincos_2pi(r2, cph, sph);
+  const float cosphi = fmul(cph, sintheta);
+  const float sinphi = fmul(sph, sintheta);
+  float v1[3];
+  {  // Vector::findPerpendicular (Core/Geometry/Vector.h:450-462)
+    const float d2 = fmul(ffn[2], ffn[2]);
+    const float d1 = fmul(ffn[1], ffn[1]);
+    if (fadd(d2, d1) < 1e-4f) {
+      v1[0] = -ffn[2];
+      v1[1] = 0.f;
+      v1[2] = ffn[0];
+    } else {
+      v1[0] = 0.f;
+      v1[1] = ffn[2];
+      v1[2] = -ffn[1];
+    }
+    const float l = __fsqrt_rn(fadd(fadd(fmul(v1[0], v1[0]), fmul(v1[1], v1[1])),
+                                    fmul(v1[2], v1[2])));
+    const float s = fdiv(1.f, l);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v1[c] = fmul(v1[c], s);
+  }
+  float v2[3];
+  cross3(v1, ffn, v2);
+  float nd[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    nd[c] = fadd(fadd(fmul(ffn[c], costheta), fmul(v1[c], cosphi)), fmul(v2[c], sinphi));
+  const float* kd = P.materials + 3 * (size_t)__ldg(S.face_material + prim);
+  float refl[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    refl[c] = __ldg(kd + c);
+    imp[c] = fmul(imp[c], refl[c]);
+  }
+  // one area-light sample
+  const float lr1 = pcg32_float(rng);
+  const float lr2 = pcg32_float(rng);
+  float ld[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    ld[c] = fsub(fadd(fadd(P.light_anchor[c], fmul(lr1, P.light_v1[c])),
+                      fmul(lr2, P.light_v2[c])),
+                 hp[c]);
+  const float len = __fsqrt_rn(fadd(fadd(fmul(ld[0], ld[0]), fmul(ld[1], ld[1])),
+                                    fmul(ld[2], ld[2])));
+  {
+    const float s = fdiv(1.f, len);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ld[c] = fmul(ld[c], s);
+  }
+  const float cosine = -dot3(ld, P.light_normal);
+  if (cosine > 0.f && dot3(ld, ffn) > 0.f) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      refl[c] = __ldg(kd + c);
-      imp[c] = fmul(imp[c], refl[c]);
+      sr.o[c] = hp[c];
+      sr.d[c] = ld[c];
+      sr.inv[c] = fdiv(1.f, ld[c]);
     }
-    // one area-light sample
-    const float lr1 = pcg32_float(rng);
-    const float lr2 = pcg32_float(rng);
-    float ld[3];
+    sr.minT = fsub(len, kTEpsilon);
+    traced = true;
+    // what the light adds when the shadow ray is unoccluded
+    const float solid_pdf = fmul(P.light_inv_area, fmul(len, len));
+    const float f = fdiv(cosine, solid_pdf);
+    // RayPacket::normalizeDirections on the shadow ray
+    const float sum = fadd(fadd(fmul(ld[0], ld[0]), fmul(ld[1], ld[1])), fmul(ld[2], ld[2]));
+    const float s = fdiv(1.f, __fsqrt_rn(sum));
+    float ldn[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-      ld[c] = fsub(fadd(fadd(P.light_anchor[c], fmul(lr1, P.light_v1[c])),
-                        fmul(lr2, P.light_v2[c])),
-                   hp[c]);
-    const float len = __fsqrt_rn(fadd(fadd(fmul(ld[0], ld[0]), fmul(ld[1], ld[1])),
-                                      fmul(ld[2], ld[2])));
-    {
-      const float s = fdiv(1.f, len);
+    for (int c = 0; c < 3; ++c) ldn[c] = fmul(ld[c], s);
+    const float w = dot3(ffn, ldn);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) ld[c] = fmul(ld[c], s);
-    }
-    const float cosine = -dot3(ld, P.light_normal);
-    if (cosine > 0.f && dot3(ld, ffn) > 0.f) {
-      Ray sr;
+    for (int c = 0; c < 3; ++c) contrib[c] = fmul(fmul(imp[c], fmul(f, P.light_color[c])), w);
+  }
+  alive = !last_depth;
+  if (alive && do_rr) {
+    const float rr = pcg32_float(rng);
+    const float mx = fmaxf(fmaxf(refl[0], refl[1]), refl[2]);
+    if (rr > mx) {
+      alive = false;
+    } else {
+      const float sc = fdiv(1.f, mx);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        sr.o[c] = hp[c];
-        sr.d[c] = ld[c];
-        sr.inv[c] = fdiv(1.f, ld[c]);
-      }
-      sr.minT = fsub(len, kTEpsilon);
-      ++nshadow;
-      Hit sh;
-      int ref, sp;
-      start_ray(S, sr, sh, ref, sp);
-      if (STATS) cnt.boxes += 1;
-      while (ref != kDone) step<KIND, true, STATS>(S, sr, sh, ref, sp, stk, stride, &cnt);
-      if (sh.id < 0) {
-        const float solid_pdf = fmul(P.light_inv_area, fmul(len, len));
-        const float f = fdiv(cosine, solid_pdf);
-        // RayPacket::normalizeDirections on the shadow ray
-        const float sum = fadd(fadd(fmul(ld[0], ld[0]), fmul(ld[1], ld[1])),
-                               fmul(ld[2], ld[2]));
-        const float s = fdiv(1.f, __fsqrt_rn(sum));
-        float ldn[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) ldn[c] = fmul(ld[c], s);
-        const float w = dot3(ffn, ldn);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          rad[c] = fadd(rad[c], fmul(fmul(imp[c], fmul(f, P.light_color[c])), w));
-      }
-    }
-    alive = !last_depth;
-    if (alive && do_rr) {
-      const float rr = pcg32_float(rng);
-      const float mx = fmaxf(fmaxf(refl[0], refl[1]), refl[2]);
-      if (rr > mx) {
-        alive = false;
-      } else {
-        const float sc = fdiv(1.f, mx);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) imp[c] = fmul(imp[c], sc);
-      }
-    }
-    if (alive) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        B.o[c * C + p] = hp[c];
-        B.d[c * C + p] = nd[c];
-        B.imp[c * C + p] = imp[c];
-      }
-      B.rng[p] = rng.state;
+      for (int c = 0; c < 3; ++c) imp[c] = fmul(imp[c], sc);
     }
   }
+  if (alive) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) B.rad[c * C + p] = rad[c];
+    for (int c = 0; c < 3; ++c) {
+      B.o[c * C + p] = hp[c];
+      B.d[c * C + p] = nd[c];
+      B.imp[c * C + p] = imp[c];
+    }
+    B.rng[p] = rng.state;
+  }
+  return traced;
+}
+
+// Second half: the unoccluded light sample's radiance.
+__device__ __forceinline__ void shade_finish(const PathBuffers& B, int p,
+                                             const float* contrib) {
+  const size_t C = B.capacity;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) B.rad[c * C + p] = fadd(B.rad[c * C + p], contrib[c]);
+}
+
+// One live path at one bounce in one thread: shade_begin, the any-hit
+// shadow ray, shade_finish.  Returns true when the path continues.
+template <int KIND, bool STATS>
+__device__ __forceinline__ bool shade_path(const DevScene& S, const PathParams& P,
+                                           const PathBuffers& B, int depth, int p,
+                                           long long g, int2* stk, int stride, Counts& cnt,
+                                           int& nshadow) {
+  Ray sr;
+  float contrib[3];
+  bool alive;
+  if (shade_begin<KIND>(S, P, B, depth, p, g, sr, contrib, alive)) {
+    ++nshadow;
+    Hit sh;
+    int ref, sp;
+    start_ray(S, sr, sh, ref, sp);
+    if (STATS) cnt.boxes += 1;
+    while (ref != kDone) step<KIND, true, STATS>(S, sr, sh, ref, sp, stk, stride, &cnt);
+    if (sh.id < 0) shade_finish(B, p, contrib);
+  }
   return alive;
 }
 

@@ -56,9 +56,15 @@ struct Ray {
 
 // DynBVH::firstIntersects scalar box test (Model/Groups/DynBVH.cc:666-681):
 // returns the entry distance when the slab interval is non-empty.
-__device__ __forceinline__ bool box_test(const Ray& r, float lx, float ly,
-                                         float lz, float hx, float hy,
-                                         float hz, float& tentry) {
+// FAST = true evaluates the reference's ternary min/max with fminf/fmaxf,
+// which is exact whenever no slab distance is NaN; that holds for every ray
+// whose inverse direction is finite on all three axes (inv_finite), since
+// box bounds and origins are finite.  (With t0 == t1 the two forms may pick
+// zeros of different sign, which changes neither tmin >= T_EPSILON nor the
+// comparison.)
+template <bool FAST>
+__device__ __forceinline__ bool box_test_t(const Ray& r, float lx, float ly, float lz,
+                                           float hx, float hy, float hz, float& tentry) {
   float tmin = kTEpsilon;
   float tmax = r.minT;
   const float lo[3] = {lx, ly, lz};
@@ -67,13 +73,43 @@ __device__ __forceinline__ bool box_test(const Ray& r, float lx, float ly,
   for (int c = 0; c < 3; ++c) {
     const float t0 = fmul(fsub(lo[c], r.o[c]), r.inv[c]);
     const float t1 = fmul(fsub(hi[c], r.o[c]), r.inv[c]);
-    const float nr = (t0 < t1) ? t0 : t1;
-    const float fr = (t0 < t1) ? t1 : t0;
-    tmin = (tmin < nr) ? nr : tmin;
-    tmax = (fr < tmax) ? fr : tmax;
+    if (FAST) {
+      tmin = fmaxf(tmin, fminf(t0, t1));
+      tmax = fminf(tmax, fmaxf(t0, t1));
+    } else {
+      const float nr = (t0 < t1) ? t0 : t1;
+      const float fr = (t0 < t1) ? t1 : t0;
+      tmin = (tmin < nr) ? nr : tmin;
+      tmax = (fr < tmax) ? fr : tmax;
+    }
   }
   tentry = tmin;
   return tmin <= tmax;
+}
+
+__device__ __forceinline__ bool box_test(const Ray& r, float lx, float ly, float lz,
+                                         float hx, float hy, float hz, float& tentry) {
+  return box_test_t<false>(r, lx, ly, lz, hx, hy, hz, tentry);
+}
+
+// Whether box_test_t<true> is exact for this ray (see above).  minT may be
+// +inf, which fminf/fmaxf and the ternaries treat alike.
+__device__ __forceinline__ bool inv_finite(const Ray& r) {
+  return fabsf(r.inv[0]) < INFINITY && fabsf(r.inv[1]) < INFINITY &&
+         fabsf(r.inv[2]) < INFINITY && !(r.minT != r.minT);
+}
+
+// Both child boxes of a node record (q0..q2) for one ray.
+__device__ __forceinline__ void box_pair(const Ray& r, bool fast, const float4& q0,
+                                         const float4& q1, const float4& q2, bool& hl,
+                                         bool& hr, float& tl, float& tr) {
+  if (fast) {
+    hl = box_test_t<true>(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, tl);
+    hr = box_test_t<true>(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, tr);
+  } else {
+    hl = box_test_t<false>(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, tl);
+    hr = box_test_t<false>(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, tr);
+  }
 }
 
 struct Hit {

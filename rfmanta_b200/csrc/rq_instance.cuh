@@ -32,6 +32,7 @@ __device__ __forceinline__ void trace_two_level(const DevScene& T, const DevScen
     return;
   int ref = T.root_ref;
   int sp = 0;
+  const bool fast = inv_finite(r);
   for (;;) {
     while (ref >= 0 && ref != kDone) {
       if (STATS) cnt->boxes += 2;
@@ -41,8 +42,8 @@ __device__ __forceinline__ void trace_two_level(const DevScene& T, const DevScen
       const float4 q2 = __ldg(p + 2);
       const int4 q3 = __ldg(reinterpret_cast<const int4*>(p + 3));
       float tl, tr;
-      const bool hl = box_test(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, tl);
-      const bool hr = box_test(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, tr);
+      bool hl, hr;
+      box_pair(r, fast, q0, q1, q2, hl, hr, tl, tr);
       if (hl && hr) {
         const bool left_first =
             ANY ? (((q3.z >> 2) & 1) != 0) : (pick3(r.d, q3.z & 3) > 0.f);

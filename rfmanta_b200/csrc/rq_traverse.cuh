@@ -74,6 +74,7 @@ template <int KIND, bool ANY, bool STATS = false>
 __device__ __forceinline__ void step(const DevScene& S, Ray& r, Hit& h,
                                      int& ref, int& sp, int2* stk,
                                      int stride, Counts* cnt = nullptr) {
+  const bool fast = inv_finite(r);
   while (ref >= 0 && ref != kDone) {
     if (STATS) cnt->boxes += 2;
     const float4* p = S.nodes + 4 * (size_t)ref;
@@ -82,8 +83,8 @@ __device__ __forceinline__ void step(const DevScene& S, Ray& r, Hit& h,
     const float4 q2 = __ldg(p + 2);
     const int4 q3 = __ldg(reinterpret_cast<const int4*>(p + 3));
     float tl, tr;
-    const bool hl = box_test(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, tl);
-    const bool hr = box_test(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, tr);
+    bool hl, hr;
+    box_pair(r, fast, q0, q1, q2, hl, hr, tl, tr);
     if (hl && hr) {
       const bool left_first =
           ANY ? (((q3.z >> 2) & 1) != 0) : (pick3(r.d, q3.z & 3) > 0.f);
@@ -201,6 +202,7 @@ struct RegStack {
 template <int KIND, int R, bool STATS = false>
 __device__ __forceinline__ void step_dyn(const DevScene& S, Ray& r, Hit& h, int& ref,
                                          RegStack<R>& st, bool any, Counts* cnt = nullptr) {
+  const bool fast = inv_finite(r);
   while (ref >= 0 && ref != kDone) {
     if (STATS) cnt->boxes += 2;
     const float4* p = S.nodes + 4 * (size_t)ref;
@@ -209,8 +211,8 @@ __device__ __forceinline__ void step_dyn(const DevScene& S, Ray& r, Hit& h, int&
     const float4 q2 = __ldg(p + 2);
     const int4 q3 = __ldg(reinterpret_cast<const int4*>(p + 3));
     float tl, tr;
-    const bool hl = box_test(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, tl);
-    const bool hr = box_test(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, tr);
+    bool hl, hr;
+    box_pair(r, fast, q0, q1, q2, hl, hr, tl, tr);
     if (hl && hr) {
       const bool left_first =
           any ? (((q3.z >> 2) & 1) != 0) : (pick3(r.d, q3.z & 3) > 0.f);

@@ -201,6 +201,17 @@ class PathFrame:
         return (ext * (32 + 16 + 32 * b_e + 48 * t_e),
                 shadow * (32 + 4 + 32 * b_s + 48 * t_s)), per_ray
 
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per extension
+    # ray of path_extend_persistent_kernel, from one ncu capture of bounce 0
+    # of this workload at 640x360 x 4 spp (921,600 rays, same scene).
+    DRAM_BYTES_PER_RAY = 79.9
+
+    def traffic(self, rays):
+        ext, _ = rays
+        per_launch = self.DRAM_BYTES_PER_RAY * ext / self.sc.max_depth
+        return per_launch, ("ncu DRAM bytes per extension ray at 640x360x4 spp (79.9 B) x "
+                            "extension rays per launch (all bounces / depth)")
+
     def group_stages(self, stage_ms):
         D = self.sc.max_depth
         ext = sum(stage_ms[2 * d] for d in range(D))
@@ -283,6 +294,15 @@ class SmallFrame:
                    "shadow_box_tests": round(b_s, 3), "shadow_tri_tests": round(t_s, 3)}
         return (prim * (32 + 16 + 32 * b_p + 48 * t_p),
                 shadow * (32 + 4 + 32 * b_s + 48 * t_s)), per_ray
+
+    # DRAM bytes per primary ray of whitted_primary_kernel, from one ncu
+    # capture of this workload at full size (262,144 rays, 3.97 MB).
+    DRAM_BYTES_PER_RAY = 15.1
+
+    def traffic(self, rays):
+        prim, _ = rays
+        return self.DRAM_BYTES_PER_RAY * prim, ("ncu DRAM bytes of one whitted_primary_kernel "
+                                                "launch at full size (15.1 B per ray)")
 
     def group_stages(self, stage_ms):
         return self.stage_names, [stage_ms[0], stage_ms[1]]
@@ -379,6 +399,15 @@ class CoherentFrame:
         return (prim * (32 + 16 + 32 * b_p + 48 * t_p),
                 shadow * (32 + 4 + 32 * b_s + 48 * t_s),
                 12 * prim + 12 * (prim // self.sc.spp)), per_ray
+
+    # DRAM bytes per primary ray of frame_primary_kernel, from one ncu
+    # capture of this workload at 960x540 x 1 spp (518,400 rays, same scene).
+    DRAM_BYTES_PER_RAY = 127.7
+
+    def traffic(self, rays):
+        prim, _ = rays
+        return self.DRAM_BYTES_PER_RAY * prim, ("ncu DRAM bytes per primary ray at 960x540x1 "
+                                                "(127.7 B) x primary rays of the launch")
 
     def group_stages(self, stage_ms):
         return self.stage_names, [stage_ms[0], stage_ms[1], stage_ms[2]]
@@ -826,6 +855,8 @@ def run_ours(args):
     alg, per_ray = wl.roofline_bytes(st, rays)
     dom = int(np.argmax(kms))
     achieved = alg[dom] / (kms[dom] * 1e-3) / 1e9
+    traffic, traffic_basis = (wl.traffic(rays) if hasattr(wl, "traffic") and dom == 0
+                              else (None, None))
 
     if rank == 0:
         line = {
@@ -844,7 +875,9 @@ def run_ours(args):
             "gpu_launches": wl.launches * args.steps,
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1),
                          "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": None,
+                         "frac": round(achieved / hbm, 4),
+                         "traffic": None if traffic is None else int(traffic),
+                         "traffic_basis": traffic_basis,
                          "kernel_ms_per_step": {n: round(v, 4) for n, v in zip(names, kms)},
                          "per_ray": per_ray},
         }

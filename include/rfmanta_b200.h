@@ -111,6 +111,14 @@ RQ_API int rq_scene_import_tree(rq_scene* scene, int n_nodes, const float* bound
 RQ_API int rq_scene_build(rq_scene* scene, int bins);
 
 /* SAH cost of the scene's tree, DynBVH::computeCost<>(0) with C_isec=C_trav=1. */
+/* DynBVH::update (Model/Groups/DynBVH.cc:1574-1581, 2012-2123): new
+ * positions for the scene's vertices (same count and triangles); the
+ * triangles' precomputation is redone and every node box refitted bottom up
+ * on the GPU, keeping the tree's topology, as the reference's refit does.
+ * Not for two-level scenes (refit the inner scenes, then create the
+ * two-level scene again). */
+RQ_API int rq_scene_update_vertices(rq_scene* scene, const float* vertices, int n_vertices);
+
 RQ_API int rq_scene_sah_cost(const rq_scene* scene, double* cost);
 
 /* Counts: internal records, leaves, maximum traversal depth. */
@@ -154,6 +162,12 @@ typedef struct {
   int refill_threshold; /* idle lanes in a warp before it fetches new rays */
   int persistent;       /* 0 = one thread per ray, 1 = persistent */
 } rq_launch_config;
+
+/* rq_set_launch_config / rq_get_launch_config also take these flags for the
+ * path tracer's two persistent stages (rq_render_path*): block_threads,
+ * blocks_per_sm and refill_threshold apply, `persistent` is ignored. */
+#define RQ_PATH_EXTEND 2
+#define RQ_PATH_SHADE 3
 
 RQ_API int rq_set_launch_config(rq_scene* scene, int flags,
                          const rq_launch_config* cfg);
@@ -352,11 +366,17 @@ RQ_API int rq_trace_device_ex(rq_scene* scene, int n, const float* d_org,
 /* Supersampled Whitted frame over a flat or instanced scene: `spp`
  * stratified jittered samples per pixel (PCG32 keyed by seed and sample),
  * averaged in sample order; spp = 1 samples pixel centres and equals
- * rq_render_whitted. */
+ * rq_render_whitted.  Materials are Lambertian (Model/Materials/
+ * Lambertian.cc) unless material_specpow[m] >= 0: then material m is a Phong
+ * without reflection (Model/Materials/Phong.cc:130-410, refl = 0) with
+ * diffuse material_rgb[m], specular material_specular[m] and that
+ * exponent.  Both Phong arrays NULL = all Lambertian. */
 typedef struct {
   rq_whitted_params whitted;
   int spp;        /* 1, 4, 16, ... */
   uint64_t seed;
+  const float* material_specular;   /* 3 per material, or NULL */
+  const int32_t* material_specpow;  /* 1 per material, or NULL */
 } rq_frame_params;
 
 RQ_API int rq_render_frame(rq_scene* scene, const rq_frame_params* params, float* rgb,

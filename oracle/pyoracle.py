@@ -160,7 +160,7 @@ class Restatement:
                                       [C.c_void_p] * 6)
         L.orq_sample_coords.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_longlong,
                                         C.c_longlong, C.c_void_p, C.c_void_p]
-        L.orq_render_frame.argtypes = ([C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_uint64] +
+        L.orq_render_frame.argtypes = ([C.c_void_p] * 5 + [C.c_int] * 3 + [C.c_uint64] +
                                        [C.c_void_p, C.c_int] + [C.c_void_p] * 2 +
                                        [C.c_int, C.c_int] + [C.c_void_p] * 4)
         L.orq_render_frame.restype = C.c_longlong
@@ -191,9 +191,11 @@ class Restatement:
         self.lib.orq_sample_coords(xres, yres, spp, int(seed), i0, i1, _ptr(px), _ptr(py))
         return px, py
 
-    def render_frame(self, world: World, scene, materials, rows=None, per_sample=False):
-        """Supersampled Whitted frame (scenes.FrameScene-like: camera, lights,
-        ambient, background, xres, yres, spp, seed) over a world."""
+    def render_frame(self, world: World, scene, materials, rows=None, per_sample=False,
+                     specular=None, specpow=None):
+        """Supersampled Whitted frame (any scene with camera, lights,
+        ambient, background, xres, yres, spp, seed) over a world; materials
+        with specpow >= 0 are Phong with the given specular colour."""
         basis = self.camera_basis(scene.camera)
         xres, yres, spp = scene.xres, scene.yres, scene.spp
         y0, y1 = rows if rows else (0, yres)
@@ -202,12 +204,15 @@ class Restatement:
         amb = np.asarray(scene.ambient, np.float32)
         bg = np.asarray(scene.background, np.float32)
         mats = np.ascontiguousarray(materials, np.float32)
+        spec = None if specpow is None else np.ascontiguousarray(specular, np.float32)
+        spow = None if specpow is None else np.ascontiguousarray(specpow, np.int32)
         npx = (y1 - y0) * xres
         rgb = np.zeros((npx, 3), np.float32)
         srgb = np.zeros((npx * spp, 3), np.float32) if per_sample else None
         st = np.zeros(npx * spp, np.float32) if per_sample else None
         sp = np.zeros(npx * spp, np.int32) if per_sample else None
-        ns = self.lib.orq_render_frame(world.ptr, _ptr(mats), _ptr(basis), xres, yres, spp,
+        ns = self.lib.orq_render_frame(world.ptr, _ptr(mats), _ptr(spec), _ptr(spow),
+                                       _ptr(basis), xres, yres, spp,
                                        int(scene.seed), _ptr(lights), lights.shape[0],
                                        _ptr(amb), _ptr(bg), y0, y1, _ptr(rgb), _ptr(srgb),
                                        _ptr(st), _ptr(sp))
@@ -392,6 +397,8 @@ class Reference:
         L.mref_scene_create_instanced.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
                                                   [C.c_int])
         L.mref_scene_create_instanced.restype = C.c_void_p
+        L.mref_scene_set_phong.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.mref_scene_update_vertices.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.mref_render_coords.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 4 + [C.c_int] +
                                          [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 4)
 
@@ -442,6 +449,20 @@ class RefScene:
                                            _ptr(fm), _ptr(mats), mats.shape[0], tri_kind)
         if not self.h:
             raise RuntimeError("reference scene build failed")
+
+    def set_phong(self, material: int, specular, specpow: int) -> None:
+        """Material `material` becomes a Phong (no reflection) with its
+        diffuse colour and the given specular colour and exponent."""
+        sp = np.ascontiguousarray(specular, np.float32)
+        if self.ref.lib.mref_scene_set_phong(self.h, material, _ptr(sp), int(specpow)) != 0:
+            raise RuntimeError("mref_scene_set_phong failed")
+
+    def update_vertices(self, vertices) -> None:
+        """Animated mesh: new vertex positions, WaldTriangle::update and
+        DynBVH::update (the reference's refit)."""
+        v = np.ascontiguousarray(vertices, np.float32)
+        if self.ref.lib.mref_scene_update_vertices(self.h, _ptr(v), v.shape[0]) != 0:
+            raise RuntimeError("mref_scene_update_vertices failed")
 
     def use_gpu(self, device=0, tri_kind=0, tree_file=None):
         """Drop-in library only: trace with rfmanta_b200's GpuDynBVH."""

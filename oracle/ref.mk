@@ -62,7 +62,7 @@ MODEL_SRC := \
   Model/Primitives/WaldTriangle.cc Model/Primitives/KenslerShirleyTriangle.cc \
   Model/Primitives/MeshTriangle.cc \
   Model/Materials/Lambertian.cc Model/Materials/LitMaterial.cc \
-  Model/Materials/OpaqueShadower.cc \
+  Model/Materials/OpaqueShadower.cc Model/Materials/Phong.cc \
   Model/Textures/Constant.cc \
   Model/Lights/PointLight.cc \
   Model/AmbientLights/ConstantAmbient.cc \

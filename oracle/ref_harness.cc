@@ -49,6 +49,7 @@
 #include <Model/Instances/MPT.h>
 #include <Model/Lights/PointLight.h>
 #include <Model/Materials/Lambertian.h>
+#include <Model/Materials/Phong.h>
 #include <Model/Primitives/KenslerShirleyTriangle.h>
 #include <Model/Primitives/MeshTriangle.h>
 #include <Model/Primitives/WaldTriangle.h>
@@ -156,6 +157,7 @@ struct RefScene {
   ExposedBVH* bvh;
   Object* object;  // what rays are traced against: bvh, or a drop-in
   std::vector<Material*> materials;
+  std::vector<float> diffuse;  // rgb per mesh material
   LightSet* lights;
   Scene* scene;
   // two-level scenes: instance index of each top-level InstanceT object
@@ -202,6 +204,7 @@ void* mref_scene_create(const float* verts, int nverts, const unsigned* idx,
       m->vertices[i] = Vector(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
     m->vertex_indices.assign(idx, idx + 3 * (size_t)ntris);
     m->face_material.assign(face_mat, face_mat + ntris);
+    s->diffuse.assign(mat_rgb, mat_rgb + 3 * nmat);
     for (int k = 0; k < nmat; ++k) {
       Material* mat = new Lambertian(
           Color(RGB(mat_rgb[3 * k], mat_rgb[3 * k + 1], mat_rgb[3 * k + 2])));
@@ -228,6 +231,41 @@ void* mref_scene_create(const float* verts, int nverts, const unsigned* idx,
   } catch (...) {
     return 0;
   }
+}
+
+// Makes material k of a scene a Phong (Model/Materials/Phong.cc) with the
+// material's diffuse colour, the given specular colour and exponent and no
+// reflection, in place of its Lambertian.
+int mref_scene_set_phong(void* h, int k, const float* specular, int specpow) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (!s->mesh || k < 0 || k >= (int)s->mesh->materials.size()) return 1;
+  Material* old = s->mesh->materials[k];
+  Lambertian* lam = dynamic_cast<Lambertian*>(old);
+  if (!lam) return 2;
+  const float* kd = s->diffuse.data() + 3 * k;
+  Material* ph = new Phong(Color(RGB(kd[0], kd[1], kd[2])),
+                           Color(RGB(specular[0], specular[1], specular[2])), specpow, 0);
+  s->mesh->materials[k] = ph;
+  for (size_t i = 0; i < s->materials.size(); ++i)
+    if (s->materials[i] == old) s->materials[i] = ph;
+  return 0;
+}
+
+// Moves the mesh's vertices and refits the way the reference does for an
+// animated mesh: WaldTriangle::update on every triangle (WaldTriangle.cc:
+// 17-25; Kensler-Shirley triangles read the mesh directly), then
+// DynBVH::update (DynBVH.cc:1574-1581).
+int mref_scene_update_vertices(void* h, const float* verts, int nverts) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (!s->mesh || nverts != (int)s->mesh->vertices.size()) return 1;
+  for (int i = 0; i < nverts; ++i)
+    s->mesh->vertices[i] = Vector(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+  for (size_t t = 0; t < s->mesh->size(); ++t) {
+    WaldTriangle* w = dynamic_cast<WaldTriangle*>(s->mesh->get(t));
+    if (w) w->update();
+  }
+  s->bvh->update(0, 1);
+  return 0;
 }
 
 void mref_scene_destroy(void* h) {

@@ -967,7 +967,22 @@ void orq_sample_coords(int xres, int yres, int spp, unsigned long long seed, lon
 
 /* One Whitted sample (the body of orq_render_whitted) at image coordinates
  * (px, py) over a world; returns the shadow rays sent. */
-static long long whitted_sample(const orq_world* W, const float* mat_rgb, const float* cam,
+/* ipow (Core/Math/ipow.h:21-31). */
+static float ipow_f(float x, int p) {
+  float result = 1;
+  while (p) {
+    if (p & 1) result *= x;
+    x *= x;
+    p >>= 1;
+  }
+  return result;
+}
+
+/* Material m is a Phong (Model/Materials/Phong.cc:130-410, scalar branch,
+ * no reflection) when mat_pow is given and mat_pow[m] >= 0, else a
+ * Lambertian. */
+static long long whitted_sample(const orq_world* W, const float* mat_rgb,
+                                const float* mat_spec, const int* mat_pow, const float* cam,
                                 float px, float py, const float* lights, int nl,
                                 const float* ambient, const float* background,
                                 float* rgb, float* tprim, int* prim) {
@@ -997,7 +1012,10 @@ static long long whitted_sample(const orq_world* W, const float* mat_rgb, const 
   }
   const orq_tree* HT = W->inner ? &W->inner[W->inst_scene[k]] : W->top;
   const Tree T = as_tree(HT);
-  const float* kd = mat_rgb + 3 * HT->face_mat[r.prim];
+  const unsigned m = HT->face_mat[r.prim];
+  const float* kd = mat_rgb + 3 * m;
+  const int phong = mat_pow && mat_pow[m] >= 0;
+  float spec[3] = {0.f, 0.f, 0.f};
   float nrm[3];
   tri_normal(&T, r.prim, nrm);
   float ffn[3];
@@ -1033,16 +1051,32 @@ static long long whitted_sample(const orq_world* W, const float* mat_rgb, const 
     for (int c = 0; c < 3; ++c) sd[c] *= scale;
     const float cos_theta = sd[0] * ffn[0] + sd[1] * ffn[1] + sd[2] * ffn[2];
     for (int c = 0; c < 3; ++c) total[c] += L[3 + c] * cos_theta;
+    if (phong) {
+      const float H[3] = {sd[0] - r.d[0], sd[1] - r.d[1], sd[2] - r.d[2]};
+      const float cos_alpha = H[0] * ffn[0] + H[1] * ffn[1] + H[2] * ffn[2];
+      if (cos_alpha > 0) {
+        const float length = sqrtf(H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
+        const float scale = ipow_f(cos_alpha / length, mat_pow[m]);
+        for (int c = 0; c < 3; ++c) spec[c] += L[3 + c] * scale;
+      }
+    }
   }
-  for (int c = 0; c < 3; ++c) rgb[c] = total[c] * kd[c];
+  if (phong) {
+    const float* ks = mat_spec + 3 * m;
+    for (int c = 0; c < 3; ++c) rgb[c] = spec[c] * ks[c] + total[c] * kd[c];
+  } else {
+    for (int c = 0; c < 3; ++c) rgb[c] = total[c] * kd[c];
+  }
   return shadow_rays;
 }
 
-/* Supersampled Whitted frame over a world, pixel rows [y0, y1): per pixel
+/* Supersampled Whitted frame over a world (Lambertian or non-reflective
+ * Phong materials, see whitted_sample), pixel rows [y0, y1): per pixel
  * the spp samples' colours summed in sample order and scaled by 1/spp.
  * Optional per-sample outputs (indexed by item - y0 * xres * spp): colour,
  * primary t and triangle id.  Returns the shadow rays sent. */
-long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float* cam,
+long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float* mat_spec,
+                           const int* mat_pow, const float* cam,
                            int xres, int yres, int spp, unsigned long long seed,
                            const float* lights, int nl, const float* ambient,
                            const float* background, int y0, int y1, float* rgb,
@@ -1059,8 +1093,8 @@ long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float
         float px, py, c[3], t;
         int p;
         sample_coords(xres, yres, spp, seed, item, &px, &py);
-        shadow += whitted_sample(W, mat_rgb, cam, px, py, lights, nl, ambient, background,
-                                 c, &t, &p);
+        shadow += whitted_sample(W, mat_rgb, mat_spec, mat_pow, cam, px, py, lights, nl,
+                                 ambient, background, c, &t, &p);
         for (int j = 0; j < 3; ++j) acc[j] += c[j];
         if (sample_rgb)
           for (int j = 0; j < 3; ++j) sample_rgb[3 * o + j] = c[j];

@@ -24,6 +24,8 @@ RQ_ERR_NODEV = 8
 RQ_TRI_WALD = 0
 RQ_TRI_KS = 1
 RQ_INST_TRANSLATE = 0
+RQ_PATH_EXTEND = 2
+RQ_PATH_SHADE = 3
 RQ_INST_NESTED = 1
 RQ_CLOSEST = 0
 RQ_ANYHIT = 1
@@ -54,7 +56,8 @@ class WhittedParams(C.Structure):
 
 
 class FrameParams(C.Structure):
-    _fields_ = [("whitted", WhittedParams), ("spp", C.c_int), ("seed", C.c_uint64)]
+    _fields_ = [("whitted", WhittedParams), ("spp", C.c_int), ("seed", C.c_uint64),
+                ("material_specular", C.c_void_p), ("material_specpow", C.c_void_p)]
 
 
 class PathParams(C.Structure):
@@ -146,6 +149,7 @@ def _load():
                              C.POINTER(sz)], i),
         "rq_server_destroy": ([vp], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
+        "rq_scene_update_vertices": ([vp, vp, i], i),
         "rq_scene_create_instanced": ([vp, i, vp, vp, vp, i, C.POINTER(vp)], i),
         "rq_trace_device_ex": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp, vp, vp], i),
         "rq_render_frame": ([vp, C.POINTER(FrameParams), vp, C.POINTER(C.c_uint64)], i),

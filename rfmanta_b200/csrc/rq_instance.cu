@@ -211,7 +211,7 @@ int rq_scene_create_instanced(rq_scene* const* inner, int n_inner, const int32_t
   s->inst_kind.assign(n_instances, RQ_INST_TRANSLATE);
   if (inst_kind) s->inst_kind.assign(inst_kind, inst_kind + n_instances);
   s->max_blas_depth = maxd;
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 4; ++k) {
     s->cfg[k].block_threads = 128;
     s->cfg[k].blocks_per_sm = 0;
     s->cfg[k].refill_threshold = 8;
@@ -261,9 +261,9 @@ int rq_trace_device_ex(rq_scene* scene, int n, const float* d_org, const float* 
 // ------------------------------------------------ supersampled frame ----
 //
 // Raytracer::traceEyeRays per sample (PinholeCamera -normalizeRays,
-// Lambertian, HardShadows, PointLight; the Whitted wavefront of
-// rq_render.cu) with `spp` stratified jittered samples per pixel averaged
-// in sample order, over a flat or an instanced scene.  With spp = 1 the
+// Lambertian or non-reflective Phong, HardShadows, PointLight; the Whitted
+// wavefront of rq_render.cu) with `spp` stratified jittered samples per
+// pixel averaged in sample order, over a flat or an instanced scene.  With spp = 1 the
 // samples sit at the pixel centres of the SingleSampler mapping and the
 // frame equals rq_render_whitted bit for bit.
 
@@ -403,6 +403,17 @@ __global__ void __launch_bounds__(128)
       const float t = B.t[it];
       const int bh = B.blas[it];
       const DevScene& HS = TWO ? blas[bh] : S;
+      const int mat = (int)__ldg(HS.face_material + B.prim[it]);
+      float ks[3] = {0.f, 0.f, 0.f};
+      int specpow = -1;
+      if (P.phong) {
+        const float4 ph = __ldg(reinterpret_cast<const float4*>(P.phong) + mat);
+        ks[0] = ph.x;
+        ks[1] = ph.y;
+        ks[2] = ph.z;
+        specpow = __float_as_int(ph.w);
+      }
+      float spec[3] = {0.f, 0.f, 0.f};
       float nrm[3];
       record_normal<KIND>(HS, B.pos[it], nrm);
       const float dn = dot3(nrm, r.d);
@@ -438,10 +449,32 @@ __global__ void __launch_bounds__(128)
         const float cos_theta = dot3(sd, ffn);
 #pragma unroll
         for (int c = 0; c < 3; ++c) total[c] = fadd(total[c], fmul(L[3 + c], cos_theta));
-      }
-      const float* kd = P.materials + 3 * (size_t)__ldg(HS.face_material + B.prim[it]);
+        if (specpow >= 0) {
+          // Phong::shade scalar branch (Phong.cc:367-383): H = L - d,
+          // ipow(Dot(H, N) / |H|, exponent) (Core/Math/ipow.h:21-31)
+          const float H[3] = {fsub(sd[0], r.d[0]), fsub(sd[1], r.d[1]), fsub(sd[2], r.d[2])};
+          const float cos_alpha = dot3(H, ffn);
+          if (cos_alpha > 0.f) {
+            const float len = __fsqrt_rn(dot3(H, H));
+            float x = fdiv(cos_alpha, len), sc = 1.f;
+            for (int pw = specpow; pw; pw >>= 1) {
+              if (pw & 1) sc = fmul(sc, x);
+              x = fmul(x, x);
+            }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = fmul(total[c], __ldg(kd + c));
+            for (int c = 0; c < 3; ++c) spec[c] = fadd(spec[c], fmul(L[3 + c], sc));
+          }
+        }
+      }
+      const float* kd = P.materials + 3 * (size_t)mat;
+      if (specpow >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          B.col[3 * (size_t)it + c] = fadd(fmul(spec[c], ks[c]), fmul(total[c], __ldg(kd + c)));
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = fmul(total[c], __ldg(kd + c));
+      }
     }
     int tot = nshadow;
     for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
@@ -508,6 +541,8 @@ struct SampleScratch {
   SampleBufs B{};
   float* materials = nullptr;
   std::vector<float> host_materials;
+  float4* phong = nullptr;
+  std::vector<float4> host_phong;
   float* d_rgb = nullptr;
   size_t rgb_pix = 0;
   cudaStream_t stream = nullptr;
@@ -523,6 +558,7 @@ struct SampleScratch {
     cudaFree(B.counters);
     cudaFree(B.shadow);
     cudaFree(materials);
+    cudaFree(phong);
     cudaFree(d_rgb);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -591,6 +627,28 @@ int frame_prepare(rq::Scene* s, const rq_frame_params* fp, rq::FrameParams& P,
     x->host_materials.assign(mrgb, mrgb + 3 * p->n_materials);
   }
   P.materials = x->materials;
+  P.phong = nullptr;
+  if (fp->material_specpow) {
+    if (!fp->material_specular) return ifail(RQ_ERR_ARG, "material_specpow without material_specular");
+    std::vector<float4> ph(p->n_materials);
+    for (int m = 0; m < p->n_materials; ++m) {
+      const int sp = fp->material_specpow[m];
+      if (sp > 4096) return ifail(RQ_ERR_ARG, "Phong exponent above 4096");
+      ph[m] = make_float4(fp->material_specular[3 * m], fp->material_specular[3 * m + 1],
+                          fp->material_specular[3 * m + 2], bits_as_float(sp));
+    }
+    if (x->host_phong.size() != ph.size() ||
+        std::memcmp(x->host_phong.data(), ph.data(), ph.size() * sizeof(float4)) != 0) {
+      cudaFree(x->phong);
+      x->phong = nullptr;
+      if (cudaMalloc(&x->phong, ph.size() * sizeof(float4)) != cudaSuccess ||
+          cudaMemcpy(x->phong, ph.data(), ph.size() * sizeof(float4), cudaMemcpyHostToDevice) !=
+              cudaSuccess)
+        return ifail(RQ_ERR_OOM, "Phong table");
+      x->host_phong = ph;
+    }
+    P.phong = reinterpret_cast<const float*>(x->phong);
+  }
   return RQ_OK;
 }
 

@@ -49,7 +49,7 @@ __device__ __forceinline__ int queue_count(const PathBuffers& B, int depth, int 
 // warp's rays finish at different times; results do not depend on the
 // schedule.
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
     path_extend_persistent_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0,
                                   int refill) {
   extern __shared__ int2 smem_stack[];
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128)
 // needed) it applies shade_finish and the survivors are compacted into the
 // next queue at the warp's common point, one atomic per warp.
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
     path_shade_persistent_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0,
                                  int refill) {
   extern __shared__ int2 smem_stack[];
@@ -223,47 +223,45 @@ __global__ void path_resolve_kernel(PathParams P, PathBuffers B, long long g0, i
   }
 }
 
-// Lanes that must be idle before a warp of the persistent extension / shade
-// kernels fetches new paths.
-constexpr int kExtendRefill = 8;
-constexpr int kShadeRefill = 8;
+// Grid of a persistent stage: every SM filled once at the kernel's own
+// occupancy for this block size and stack (or blocks_per_sm if smaller).
+static int stage_grid(const void* f, int block, int blocks_per_sm, size_t smem) {
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int b = 0, dev = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, block, smem);
+  if (blocks_per_sm > 0) b = std::min(b, blocks_per_sm);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, b * sms);
+}
 
 template <int KIND, bool STATS>
 static void launch_bounces(const DevScene& S, const PathParams& P, const PathBuffers& B,
-                           int n, size_t smem, cudaStream_t st,
+                           int n, const PathLaunch& L, cudaStream_t st,
                            const cudaEvent_t* ev, int nev) {
-  const int bs = 128;
-  // the persistent extension kernel fills every SM once at its own occupancy
-  const void* ef = (const void*)path_extend_persistent_kernel<KIND, STATS>;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(ef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int eb = 0, dev = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&eb, ef, bs, smem);
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int egrid = std::max(1, eb * sms);
-  const void* sf = (const void*)path_shade_persistent_kernel<KIND, STATS>;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(sf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int sb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sb, sf, bs, smem);
-  const int sgrid = std::max(1, sb * sms);
+  const int eb = L.block_threads[0], sb = L.block_threads[1];
+  const size_t esm = (size_t)S.depth * eb * sizeof(int2);
+  const size_t ssm = (size_t)S.depth * sb * sizeof(int2);
+  const int egrid = stage_grid((const void*)path_extend_persistent_kernel<KIND, STATS>, eb,
+                               L.blocks_per_sm[0], esm);
+  const int sgrid = stage_grid((const void*)path_shade_persistent_kernel<KIND, STATS>, sb,
+                               L.blocks_per_sm[1], ssm);
   for (int depth = 0; depth < P.max_depth; ++depth) {
     path_count_kernel<<<1, 32, 0, st>>>(B, depth, n);
-    path_extend_persistent_kernel<KIND, STATS><<<egrid, bs, smem, st>>>(S, P, B, depth, n,
-                                                                        kExtendRefill);
+    path_extend_persistent_kernel<KIND, STATS><<<egrid, eb, esm, st>>>(S, P, B, depth, n,
+                                                                       L.refill[0]);
     if (nev > 1 + 2 * depth) cudaEventRecord(ev[1 + 2 * depth], st);
-    path_shade_persistent_kernel<KIND, STATS><<<sgrid, bs, smem, st>>>(S, P, B, depth, n,
-                                                                       kShadeRefill);
+    path_shade_persistent_kernel<KIND, STATS><<<sgrid, sb, ssm, st>>>(S, P, B, depth, n,
+                                                                      L.refill[1]);
     if (nev > 2 + 2 * depth) cudaEventRecord(ev[2 + 2 * depth], st);
   }
 }
 
 cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffers B,
-                              long long g0, int n, float* rgb, int grid, cudaStream_t st,
-                              const cudaEvent_t* ev, int nev) {
-  const int bs = 128;
-  const size_t smem = (size_t)S.depth * bs * sizeof(int2);
+                              long long g0, int n, float* rgb, int grid,
+                              const PathLaunch& L, cudaStream_t st, const cudaEvent_t* ev,
+                              int nev) {
   B.g0 = g0;
   cudaError_t e = cudaMemsetAsync(B.counters, 0, kPathCounters * sizeof(int), st);
   if (e != cudaSuccess) return e;
@@ -272,11 +270,11 @@ cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffer
   if (nev > 0) cudaEventRecord(ev[0], st);
   const bool stats = B.stats != nullptr;
   if (S.tri_kind == kWald) {
-    if (stats) launch_bounces<kWald, true>(S, P, B, n, smem, st, ev, nev);
-    else launch_bounces<kWald, false>(S, P, B, n, smem, st, ev, nev);
+    if (stats) launch_bounces<kWald, true>(S, P, B, n, L, st, ev, nev);
+    else launch_bounces<kWald, false>(S, P, B, n, L, st, ev, nev);
   } else {
-    if (stats) launch_bounces<kKS, true>(S, P, B, n, smem, st, ev, nev);
-    else launch_bounces<kKS, false>(S, P, B, n, smem, st, ev, nev);
+    if (stats) launch_bounces<kKS, true>(S, P, B, n, L, st, ev, nev);
+    else launch_bounces<kKS, false>(S, P, B, n, L, st, ev, nev);
   }
   path_resolve_kernel<<<std::max(1, std::min(grid, (n / P.spp + 255) / 256)), 256, 0, st>>>(
       P, B, g0, n, rgb);

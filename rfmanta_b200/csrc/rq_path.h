@@ -53,9 +53,17 @@ struct PathBuffers {
   float* dbg_dir;
 };
 
+// Launch shape of the two persistent bounce stages ([0] extend, [1] shade).
+struct PathLaunch {
+  int block_threads[2];
+  int blocks_per_sm[2];  // 0 = occupancy maximum
+  int refill[2];
+};
+
 cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffers B,
-                              long long g0, int n, float* rgb, int grid, cudaStream_t st,
-                              const cudaEvent_t* ev, int nev);
+                              long long g0, int n, float* rgb, int grid,
+                              const PathLaunch& L, cudaStream_t st, const cudaEvent_t* ev,
+                              int nev);
 int path_blocks_per_sm(int tri_kind, size_t smem);
 
 }  // namespace rq

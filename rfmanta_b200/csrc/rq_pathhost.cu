@@ -142,11 +142,19 @@ static int path_run(Scene* s, const PathParams& P, long long total, int chunk, f
   const DevScene S = s->dev();
   const size_t smem = (size_t)S.depth * 128 * sizeof(int2);
   const int grid = std::max(1, path_blocks_per_sm(s->tri_kind, smem) * s->num_sms);
+  PathLaunch L;
+  for (int k = 0; k < 2; ++k) {
+    const rq_launch_config& c = s->cfg[RQ_PATH_EXTEND + k];
+    L.block_threads[k] = c.block_threads;
+    L.blocks_per_sm[k] = c.blocks_per_sm;
+    L.refill[k] = c.refill_threshold;
+  }
   cudaError_t e = cudaMemsetAsync(B.ray_counts, 0, 2 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return pfail(RQ_ERR_CUDA, cudaGetErrorString(e));
   for (long long g0 = 0; g0 < total; g0 += chunk) {
     const int n = (int)std::min<long long>(chunk, total - g0);
-    e = launch_path_chunk(S, P, B, g0, n, d_rgb, grid, st, s->stage_events, s->n_stage_events);
+    e = launch_path_chunk(S, P, B, g0, n, d_rgb, grid, L, st, s->stage_events,
+                          s->n_stage_events);
     if (e != cudaSuccess) return pfail(RQ_ERR_CUDA, std::string("path launch: ") + cudaGetErrorString(e));
   }
   return RQ_OK;

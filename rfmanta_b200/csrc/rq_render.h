@@ -22,6 +22,10 @@ struct FrameParams {
   float ambient[3];
   float background[3];
   const float* materials;  // device, 3 floats per material id
+  // optional (rq_render_frame): Phong materials, 4 per material id =
+  // specular rgb + exponent bits; exponent < 0 = Lambertian.  NULL = all
+  // Lambertian.
+  const float* phong;
 };
 
 // Device buffers of one frame.  rgb/t/prim are outputs; pos, queue and the

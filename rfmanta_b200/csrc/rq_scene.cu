@@ -72,8 +72,15 @@ Scene::~Scene() {
 void Scene::free_tree() {
   if (d_nodes) cudaFree(d_nodes);
   if (d_tris) cudaFree(d_tris);
+  if (d_perm) cudaFree(d_perm);
+  if (d_level_recs) cudaFree(d_level_recs);
   d_nodes = nullptr;
   d_tris = nullptr;
+  d_perm = nullptr;
+  d_level_recs = nullptr;
+  level_offsets.clear();
+  rec_node.clear();
+  tree_stale = false;
   has_tree = false;
 }
 
@@ -108,6 +115,7 @@ int layout_tree(const HostTree& t, int n_objects, TreeLayout& L) {
   std::vector<int32_t>& perm = L.perm;
   perm.clear();
   perm.reserve(nids);
+  L.rec_depth.clear();
   std::vector<int> order;  // internal nodes in record order
   // iterative pre-order DFS; stack holds (node, depth)
   std::vector<std::pair<int, int>> st;
@@ -139,6 +147,7 @@ int layout_tree(const HostTree& t, int n_objects, TreeLayout& L) {
       if (t.axis[node] > 2) return fail(RQ_ERR_FORMAT, "split axis out of range");
       rec_of[node] = (int)order.size();
       order.push_back(node);
+      L.rec_depth.push_back(d);
       // push right first so the left subtree is laid out first
       st.push_back({c + 1, d + 1});
       st.push_back({c, d + 1});
@@ -161,6 +170,7 @@ int layout_tree(const HostTree& t, int n_objects, TreeLayout& L) {
     int4 q3 = make_int4(ref_of(L), ref_of(R), meta, 0);
     std::memcpy(&recs[4 * r + 3], &q3, sizeof(q3));
   }
+  L.rec_node = order;
   L.n_records = (int)order.size();
   L.n_leaves = 0;
   for (int i = 0; i < nn; ++i)
@@ -193,16 +203,33 @@ int Scene::set_tree(const HostTree& t) {
   if (!recs.empty())
     RQ_CUDA(cudaMemcpy(d_nodes, recs.data(), recs.size() * sizeof(float4),
                        cudaMemcpyHostToDevice));
-  int32_t* d_perm = nullptr;
   RQ_CUDA(cudaMalloc(&d_perm, std::max<size_t>(perm.size(), 1) * sizeof(int32_t)));
   cudaError_t e = cudaMemcpy(d_perm, perm.data(), perm.size() * sizeof(int32_t),
                              cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = launch_tri_setup(tri_kind, d_verts, d_idx, d_perm, (int)perm.size(),
                          d_tris, 0);
+  // records grouped by depth, deepest first (the refit's bottom-up order)
+  const int nrec = L.n_records;
+  std::vector<int32_t> by_level(nrec);
+  level_offsets.assign(1, 0);
+  if (nrec > 0) {
+    int maxd = 0;
+    for (int d : L.rec_depth) maxd = std::max(maxd, d);
+    std::vector<int> count(maxd + 1, 0);
+    for (int d : L.rec_depth) ++count[d];
+    std::vector<int> start(maxd + 2, 0);
+    for (int d = maxd; d >= 0; --d) start[maxd - d + 1] = start[maxd - d] + count[d];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int r = 0; r < nrec; ++r) by_level[fill[maxd - L.rec_depth[r]]++] = r;
+    level_offsets.assign(start.begin(), start.end());
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&d_level_recs, std::max(nrec, 1) * sizeof(int32_t));
+  if (e == cudaSuccess && nrec > 0)
+    e = cudaMemcpy(d_level_recs, by_level.data(), nrec * sizeof(int32_t), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  cudaFree(d_perm);
   if (e != cudaSuccess) return cuda_fail(e, "triangle setup");
+  rec_node = L.rec_node;
   tree = t;
   n_records = L.n_records;
   n_leaf_tris = (int)perm.size();
@@ -393,7 +420,7 @@ int rq_scene_create(const float* vertices, int n_vertices,
                      cudaMemcpyHostToDevice));
   RQ_CUDA(cudaMemcpy(s->d_face_mat, s->face_mat.data(),
                      s->face_mat.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 4; ++k) {
     s->cfg[k].block_threads = 128;
     s->cfg[k].blocks_per_sm = 0;
     s->cfg[k].refill_threshold = 8;
@@ -473,6 +500,8 @@ int rq_scene_import_dynbvh(rq_scene* s, const void* blob, size_t bytes) {
 int rq_scene_export_dynbvh(const rq_scene* s, void* blob, size_t* bytes) {
   if (!s || !bytes) return fail(RQ_ERR_ARG, "NULL argument");
   if (!s->has_tree) return fail(RQ_ERR_STATE, "scene has no tree");
+  const int rc = s->refresh_tree();
+  if (rc != RQ_OK) return rc;
   const rq::HostTree& t = s->tree;
   const uint32_t nids = (uint32_t)t.ids.size();
   const uint32_t nn = (uint32_t)t.children.size();
@@ -505,6 +534,8 @@ int rq_scene_export_dynbvh(const rq_scene* s, void* blob, size_t* bytes) {
 int rq_scene_sah_cost(const rq_scene* s, double* cost) {
   if (!s || !cost) return fail(RQ_ERR_ARG, "NULL argument");
   if (!s->has_tree) return fail(RQ_ERR_STATE, "scene has no tree");
+  const int rc = s->refresh_tree();
+  if (rc != RQ_OK) return rc;
   *cost = rq::tree_sah_cost(s->tree);
   return RQ_OK;
 }
@@ -600,7 +631,7 @@ int rq_set_stage_events(rq_scene* s, void* events, int n) {
 
 int rq_set_launch_config(rq_scene* s, int flags, const rq_launch_config* cfg) {
   if (!s || !cfg) return fail(RQ_ERR_ARG, "NULL argument");
-  if (flags != RQ_CLOSEST && flags != RQ_ANYHIT) return fail(RQ_ERR_ARG, "bad flags");
+  if (flags < RQ_CLOSEST || flags > RQ_PATH_SHADE) return fail(RQ_ERR_ARG, "bad flags");
   if (cfg->block_threads < 32 || cfg->block_threads > 256 || cfg->block_threads % 32)
     return fail(RQ_ERR_ARG, "block_threads must be a multiple of 32 in [32, 256]");
   if (cfg->blocks_per_sm < 0 || cfg->blocks_per_sm > 64)
@@ -613,7 +644,7 @@ int rq_set_launch_config(rq_scene* s, int flags, const rq_launch_config* cfg) {
 
 int rq_get_launch_config(const rq_scene* s, int flags, rq_launch_config* cfg) {
   if (!s || !cfg) return fail(RQ_ERR_ARG, "NULL argument");
-  if (flags != RQ_CLOSEST && flags != RQ_ANYHIT) return fail(RQ_ERR_ARG, "bad flags");
+  if (flags < RQ_CLOSEST || flags > RQ_PATH_SHADE) return fail(RQ_ERR_ARG, "bad flags");
   *cfg = s->cfg[flags];
   return RQ_OK;
 }

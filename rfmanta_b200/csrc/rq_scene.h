@@ -44,6 +44,8 @@ double tree_sah_cost(const HostTree& t);
 struct TreeLayout {
   std::vector<float4> recs;
   std::vector<int32_t> perm;
+  std::vector<int32_t> rec_node;   // DynBVH node id of each record
+  std::vector<int32_t> rec_depth;  // depth of each record (root = 0)
   int n_records = 0;
   int n_leaves = 0;
   int root_ref = 0;
@@ -79,7 +81,15 @@ struct Scene {
 
   // tree
   bool has_tree = false;
-  HostTree tree;
+  mutable HostTree tree;      // bounds stale after a refit until refresh_tree()
+  mutable bool tree_stale = false;
+  // refit support: leaf-order object ids (bit 31 = last of leaf), records
+  // grouped by depth (deepest level first) with level offsets, and each
+  // record's DynBVH node id
+  int32_t* d_perm = nullptr;
+  int32_t* d_level_recs = nullptr;
+  std::vector<int> level_offsets;
+  std::vector<int32_t> rec_node;
   float4* d_nodes = nullptr;
   float4* d_tris = nullptr;
   int n_records = 0;
@@ -102,7 +112,7 @@ struct Scene {
   DevScene* d_blas = nullptr;
   int max_blas_depth = 0;
 
-  rq_launch_config cfg[2];
+  rq_launch_config cfg[4];  // RQ_CLOSEST, RQ_ANYHIT, RQ_PATH_EXTEND, RQ_PATH_SHADE
   int* d_counter = nullptr;  // persistent-launch counters for rq_trace_device
 
   std::mutex mu;
@@ -124,6 +134,7 @@ struct Scene {
   ~Scene();
   void free_tree();
   int set_tree(const HostTree& t);
+  int refresh_tree() const;  // host tree bounds from the device records
   DevScene dev() const;
   Staging* acquire(size_t bytes_in, size_t bytes_out);
   void release(Staging* s);

@@ -114,6 +114,15 @@ class GpuDynBVH:
             self._upload()
         check(lib.rq_scene_build(self._h, bins))
 
+    def update(self) -> None:
+        """DynBVH::update: the group's vertices moved (same triangles); the
+        tree keeps its topology and is refitted on the GPU."""
+        if self._dirty or not self._h:
+            self.rebuild()
+            return
+        v = np.ascontiguousarray(self._group.vertices, np.float32)
+        check(lib.rq_scene_update_vertices(self._h, _p(v), v.shape[0]))
+
     def importTree(self, tree) -> None:
         """Reference tree given field by field (oracle Tree or compatible)."""
         if self._dirty or not self._h:
@@ -190,15 +199,17 @@ class GpuDynBVH:
                                   C.c_void_p(stream or None)))
 
     def set_launch_config(self, anyhit: bool, block_threads=128, blocks_per_sm=0,
-                          refill_threshold=8, persistent=True) -> None:
+                          refill_threshold=8, persistent=True, stage=None) -> None:
+        """Launch shape of ray queries (closest / any hit), or with
+        stage=RQ_PATH_EXTEND / RQ_PATH_SHADE of a path-tracer stage."""
         cfg = _lib.LaunchConfig(block_threads, blocks_per_sm, refill_threshold, int(persistent))
-        check(lib.rq_set_launch_config(self._h, RQ_ANYHIT if anyhit else RQ_CLOSEST,
-                                       C.byref(cfg)))
+        flags = stage if stage is not None else (RQ_ANYHIT if anyhit else RQ_CLOSEST)
+        check(lib.rq_set_launch_config(self._h, flags, C.byref(cfg)))
 
-    def get_launch_config(self, anyhit: bool) -> dict:
+    def get_launch_config(self, anyhit: bool, stage=None) -> dict:
         cfg = _lib.LaunchConfig()
-        check(lib.rq_get_launch_config(self._h, RQ_ANYHIT if anyhit else RQ_CLOSEST,
-                                       C.byref(cfg)))
+        flags = stage if stage is not None else (RQ_ANYHIT if anyhit else RQ_CLOSEST)
+        check(lib.rq_get_launch_config(self._h, flags, C.byref(cfg)))
         return dict(block_threads=cfg.block_threads, blocks_per_sm=cfg.blocks_per_sm,
                     refill_threshold=cfg.refill_threshold, persistent=bool(cfg.persistent))
 
@@ -248,14 +259,23 @@ class GpuDynBVH:
     @staticmethod
     def frame_params(scene, materials=None) -> "_lib.FrameParams":
         """rq_frame_params for a supersampled frame (any scene object with
-        camera, lights, ambient, background, xres, yres, spp, seed)."""
+        camera, lights, ambient, background, xres, yres, spp, seed, and
+        optionally Phong `specular` / `specpow` per material)."""
         p = _lib.FrameParams()
         mats = getattr(scene, "materials", None) if materials is None else materials
         w = GpuDynBVH.whitted_params(scene, mats)
         p.whitted = w
         p.spp = int(scene.spp)
         p.seed = int(scene.seed)
-        p._keep = w._keep
+        keep = list(w._keep)
+        specpow = getattr(scene, "specpow", None)
+        if specpow is not None:
+            sp = np.ascontiguousarray(specpow, np.int32)
+            ks = np.ascontiguousarray(scene.specular, np.float32)
+            p.material_specular = ks.ctypes.data
+            p.material_specpow = sp.ctypes.data
+            keep += [sp, ks]
+        p._keep = keep
         return p
 
     def render_frame(self, scene, materials=None):

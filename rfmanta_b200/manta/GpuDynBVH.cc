@@ -80,6 +80,22 @@ void GpuDynBVH::rebuild(int proc, int numProcs) {
   check(rq_scene_build(scene, 0), "build");
 }
 
+// DynBVH::update (DynBVH.cc:1574-1581): the mesh moved, the topology
+// stays; the device refits the tree to the new vertex positions.
+void GpuDynBVH::update(int proc, int numProcs) {
+  (void)numProcs;
+  if (proc != 0) return;
+  if (dirty || !scene) {
+    rebuild(0, 1);
+    return;
+  }
+  const size_t nv = mesh->vertices.size();
+  std::vector<float> v(3 * nv);
+  for (size_t i = 0; i < nv; ++i)
+    for (int c = 0; c < 3; ++c) v[3 * i + c] = mesh->vertices[i][c];
+  check(rq_scene_update_vertices(scene, v.empty() ? 0 : &v[0], (int)nv), "refit");
+}
+
 bool GpuDynBVH::buildFromFile(const std::string& file) {
   std::ifstream in(file.c_str(), std::ios::binary);
   if (!in) return false;

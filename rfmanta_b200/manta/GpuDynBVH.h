@@ -27,6 +27,7 @@ class GpuDynBVH : public AccelerationStructure {
   virtual void groupDirty();
   virtual Group* getGroup() const;
   virtual void rebuild(int proc = 0, int numProcs = 1);
+  virtual void update(int proc = 0, int numProcs = 1);
   virtual void addToUpdateGraph(ObjectUpdateGraph* graph, ObjectUpdateGraphNode* parent);
   virtual bool buildFromFile(const std::string& file);
   virtual bool saveToFile(const std::string& file);

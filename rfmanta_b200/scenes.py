@@ -410,6 +410,10 @@ class InstancedFrameScene:
     yres: int
     spp: int
     seed: int
+    # Phong materials (Model/Materials/Phong.cc without reflection): specular
+    # colour per material and exponent, specpow < 0 = Lambertian
+    specular: np.ndarray | None = None
+    specpow: np.ndarray | None = None
 
     @property
     def n_tris(self) -> int:
@@ -420,11 +424,12 @@ def coherent_scene(hf_n: int = 1024, n_instances: int = 64, sphere_level: int = 
                    xres: int = 1920, yres: int = 1080, spp: int = 4,
                    seed: int = 23) -> InstancedFrameScene:
     """Large coherent frame: an hf_n x hf_n fBm heightfield (2*hf_n^2
-    triangles, 5 octaves, amplitude 0.2) placed in the top-level group as a
-    nested DynBVH, plus n_instances InstanceT copies of one displaced
-    icosphere (level 6: 81,920 triangles, amplitude 0.05, frequency 4) at
-    seeded uniform positions above it; two point lights, Lambertian, spp
-    stratified jittered samples per pixel.  Defaults: 1920x1080x4,
+    triangles, 5 octaves, amplitude 0.2, Lambertian) placed in the top-level
+    group as a nested DynBVH, plus n_instances InstanceT copies of one
+    displaced icosphere (level 6: 81,920 triangles, amplitude 0.05,
+    frequency 4; Phong, specular 0.6, exponent 32) at seeded uniform
+    positions above it; two point lights, spp stratified jittered samples
+    per pixel.  Defaults: 1920x1080x4,
     2,097,152 + 64 x 81,920 triangles."""
     rng = np.random.default_rng(seed)
     ext = 8.0
@@ -442,8 +447,11 @@ def coherent_scene(hf_n: int = 1024, n_instances: int = 64, sphere_level: int = 
                  float(2.0 * np.degrees(np.arctan(np.tan(np.radians(30.0)) * yres / xres))))
     lights = [PointLightSpec((3.0, 6.0, 4.0), (0.8, 0.8, 0.75)),
               PointLightSpec((-4.0, 5.0, -2.0), (0.35, 0.4, 0.5))]
+    specular = np.array([[0.0, 0.0, 0.0], [0.6, 0.6, 0.6]], np.float32)
+    specpow = np.array([-1, 32], np.int32)
     return InstancedFrameScene([hf, sphere], inst_scene, translation, kind, mats, cam, lights,
-                               (0.08, 0.08, 0.1), (0.2, 0.3, 0.5), xres, yres, spp, seed)
+                               (0.08, 0.08, 0.1), (0.2, 0.3, 0.5), xres, yres, spp, seed,
+                               specular, specpow)
 
 
 def tiny_coherent_scene(xres: int = 48, yres: int = 40, spp: int = 4,

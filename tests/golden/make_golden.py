@@ -19,7 +19,7 @@ It also records DynBVH::computeCost of the reference's own tree for a few
 larger seeded scenes (sah_costs.json), the bound for the GPU builder, and a
 two-level scene (tiny_instanced.npz): a 12x12 heightfield placed in the
 top-level group as a nested DynBVH plus six InstanceT copies of a level-2
-displaced icosphere, with the reference's inner and top-level trees, its
+displaced icosphere (Phong), with the reference's inner and top-level trees, its
 DynBVH::intersect results (closest and AnyHit) for seeded rays and its
 Raytracer colours for the 4-spp jittered samples of a 48x40 frame.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
@@ -97,6 +97,10 @@ def write_instanced() -> None:
     restated = Restatement()
     sc = scenes.tiny_coherent_scene()
     inner = [ref.scene(m, 0) for m in sc.inner]
+    for r in inner:
+        for m, sp in enumerate(sc.specpow):
+            if sp >= 0:
+                r.set_phong(m, sc.specular[m], int(sp))
     top = ref.instanced(inner, sc.inst_scene, sc.translation, sc.kind)
     lo = np.array([-4.5, -0.5, -4.5], np.float32)
     hi = np.array([4.5, 2.0, 4.5], np.float32)
@@ -108,6 +112,7 @@ def write_instanced() -> None:
     img = top.render_coords(sc, px, py)
     out = dict(n_inner=np.int32(len(sc.inner)), inst_scene=sc.inst_scene,
                translation=sc.translation, kind=sc.kind, materials=sc.materials,
+               specular=sc.specular, specpow=sc.specpow,
                xres=np.int32(sc.xres), yres=np.int32(sc.yres), spp=np.int32(sc.spp),
                seed=np.int64(sc.seed), sample_px=px, sample_py=py,
                rand_org=o_r, rand_dir=d_r, **{f"rand_{k}": v for k, v in rnd_q.items()},

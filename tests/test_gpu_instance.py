@@ -137,7 +137,8 @@ def test_gpu_built_trees_match_restatement(restatement):
                 assert np.array_equal(_bits(got[k]), _bits(exp[k])), k
     sc = tiny_scene_from_golden(g)
     out = top.render_frame(sc, g["materials"])
-    exp = restatement.render_frame(W, sc, g["materials"])
+    exp = restatement.render_frame(W, sc, g["materials"], specular=sc.specular,
+                                   specpow=sc.specpow)
     assert out["shadow_rays"] == exp["shadow_rays"]
     assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))
 
@@ -170,11 +171,17 @@ def test_flat_frame_spp16_matches_restatement(restatement):
         bvh = GpuDynBVH(tri_kind=kind)
         bvh.setGroup(golden_mesh(g))
         bvh.importTree(golden_tree(g))
-        out = bvh.render_frame(sc, sc.mesh.materials)
         W = restatement.world(golden_tree(g), golden_mesh(g), tri_kind=kind)
-        exp = restatement.render_frame(W, sc, sc.mesh.materials)
-        assert out["shadow_rays"] == exp["shadow_rays"]
-        assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))
+        # all Lambertian, then material 0 a Phong (specular 0.5, exponent 20)
+        for specpow in (None, np.array([20] + [-1] * (len(sc.mesh.materials) - 1), np.int32)):
+            sc.specpow = specpow
+            sc.specular = None if specpow is None else np.full(
+                (len(sc.mesh.materials), 3), 0.5, np.float32)
+            out = bvh.render_frame(sc, sc.mesh.materials)
+            exp = restatement.render_frame(W, sc, sc.mesh.materials, specular=sc.specular,
+                                           specpow=sc.specpow)
+            assert out["shadow_rays"] == exp["shadow_rays"]
+            assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))
 
 
 def test_flat_scene_reports_no_instance():

@@ -10,6 +10,8 @@ here:
   * InstanceT::intersect (Model/Instances/InstanceT.cc:60-90) reports the
     inner triangle through its MPT scratchpad and keeps the inner u/v in its
     own packet, so u/v are compared only for hits outside an InstanceT;
+  * the spheres are Phong (Model/Materials/Phong.cc, scalar branch, no
+    reflection), the heightfield Lambertian;
   * an AnyHit query never reports occlusion inside an InstanceT: the inner
     DynBVH pins minT to T_EPSILON (DynBVH.cc:331-349) and RayPacket::hit
     rejects t = T_EPSILON (RayPacket.h:531-543); a nested DynBVH object
@@ -55,6 +57,7 @@ def tiny_scene_from_golden(g):
     sc = scenes.tiny_coherent_scene()
     assert (sc.xres, sc.yres, sc.spp, sc.seed) == (int(g["xres"]), int(g["yres"]),
                                                    int(g["spp"]), int(g["seed"]))
+    assert np.array_equal(sc.specpow, g["specpow"]) and np.array_equal(sc.specular, g["specular"])
     return sc
 
 
@@ -95,7 +98,9 @@ def test_fixture_frame_samples(restatement):
     px, py = restatement.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed)
     assert np.array_equal(_bits(px), _bits(g["sample_px"]))
     assert np.array_equal(_bits(py), _bits(g["sample_py"]))
-    out = restatement.render_frame(W, sc, g["materials"], per_sample=True)
+    assert np.any(g["specpow"] >= 0), "the fixture has a Phong material"
+    out = restatement.render_frame(W, sc, g["materials"], per_sample=True,
+                                   specular=g["specular"], specpow=g["specpow"])
     assert out["shadow_rays"] == int(g["shadow_rays"])
     assert np.array_equal(out["sample_prim"], g["sample_prim"])
     assert np.array_equal(_bits(out["sample_t"]), _bits(g["sample_t"]))
@@ -145,6 +150,10 @@ def test_live_reference(restatement, tri_kind):
     sc = scenes.coherent_scene(hf_n=10, n_instances=9, sphere_level=1, xres=32, yres=24,
                                spp=4, seed=41)
     inner = [ref.scene(m, tri_kind) for m in sc.inner]
+    for r in inner:
+        for m, sp in enumerate(sc.specpow):
+            if sp >= 0:
+                r.set_phong(m, sc.specular[m], int(sp))
     top = ref.instanced(inner, sc.inst_scene, sc.translation, sc.kind)
     W = restatement.world(top.tree(), inner=[(r.tree(), m) for r, m in zip(inner, sc.inner)],
                           inst_scene=sc.inst_scene, translation=sc.translation, kind=sc.kind,
@@ -158,7 +167,8 @@ def test_live_reference(restatement, tri_kind):
         compare_queries(got, exp, sc.kind)
     px, py = restatement.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed)
     img = top.render_coords(sc, px, py)
-    out = restatement.render_frame(W, sc, sc.materials, per_sample=True)
+    out = restatement.render_frame(W, sc, sc.materials, per_sample=True,
+                                   specular=sc.specular, specpow=sc.specpow)
     assert out["shadow_rays"] == img["shadow_rays"]
     assert np.array_equal(out["sample_prim"], img["prim"])
     assert np.array_equal(_bits(out["sample_rgb"]), _bits(img["rgb"]))
@@ -167,6 +177,7 @@ def test_live_reference(restatement, tri_kind):
     px1, py1 = restatement.sample_coords(sc.xres, sc.yres, 1, sc.seed)
     flat = restatement.primary_rays(restatement.camera_basis(sc.camera), sc.xres, sc.yres)
     img1 = top.render_coords(sc, px1, py1)
-    out1 = restatement.render_frame(W, sc, sc.materials)
+    out1 = restatement.render_frame(W, sc, sc.materials, specular=sc.specular,
+                                    specpow=sc.specpow)
     assert np.array_equal(_bits(out1["rgb"]), _bits(img1["rgb"]))
     assert flat[0].shape[1] == sc.xres * sc.yres

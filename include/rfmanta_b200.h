@@ -44,7 +44,8 @@ enum {
   RQ_ERR_STATE = 5,    /* scene has no acceleration structure yet */
   RQ_ERR_CAPACITY = 6, /* tree deeper than the traversal stack supports */
   RQ_ERR_TIMEOUT = 7,  /* a bounded device wait gave up */
-  RQ_ERR_NODEV = 8     /* no usable sm_100 device */
+  RQ_ERR_NODEV = 8,    /* no usable sm_100 device */
+  RQ_ERR_NOTFOUND = 9  /* a file could not be opened */
 };
 
 /* Triangle intersection kernels of the reference. */
@@ -118,6 +119,24 @@ RQ_API int rq_scene_build(rq_scene* scene, int bins);
  * Not for two-level scenes (refit the inner scenes, then create the
  * two-level scene again). */
 RQ_API int rq_scene_update_vertices(rq_scene* scene, const float* vertices, int n_vertices);
+
+/*
+ * Mesh files.  rq_mesh_read_ply reads a PLY file (ascii or binary) the way
+ * Manta::readPlyFile does (Model/Readers/PlyReader.cc:135-269): vertex
+ * x/y/z as floats moved by `transform` (3x4 row-major, NULL = identity,
+ * AffineTransform::multiply_point), `vertex_indices` polygons as triangle
+ * fans with face material `material`, degenerate triangles removed
+ * (Mesh::removeDegenerateTriangles).  The arrays then feed rq_scene_create.
+ */
+typedef struct rq_mesh rq_mesh;
+RQ_API int rq_mesh_read_ply(const char* path, const float* transform, uint32_t material,
+                            rq_mesh** out);
+RQ_API int rq_mesh_info(const rq_mesh* mesh, int* n_vertices, int* n_tris);
+/* Copies 3 floats per vertex, 3 indices and 1 material per triangle; any
+ * output may be NULL. */
+RQ_API int rq_mesh_copy(const rq_mesh* mesh, float* vertices, uint32_t* indices,
+                        uint32_t* face_material);
+RQ_API int rq_mesh_destroy(rq_mesh* mesh);
 
 RQ_API int rq_scene_sah_cost(const rq_scene* scene, double* cost);
 

@@ -370,6 +370,9 @@ class Reference:
             raise FileNotFoundError(path)
         self.lib = C.CDLL(path)
         L = self.lib
+        # keep the process exit status (the reference's thread library would
+        # replace it with 0 at exit)
+        L.mref_keep_exit_status()
         L.mref_scene_create.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.mref_scene_create.restype = C.c_void_p
@@ -398,6 +401,8 @@ class Reference:
                                                   [C.c_int])
         L.mref_scene_create_instanced.restype = C.c_void_p
         L.mref_scene_set_phong.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.mref_read_ply.argtypes = ([C.c_char_p, C.c_void_p, C.c_int] + [C.c_void_p] * 5 +
+                                    [C.c_int, C.c_int])
         L.mref_scene_update_vertices.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.mref_render_coords.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 4 + [C.c_int] +
                                          [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 4)
@@ -413,6 +418,25 @@ class Reference:
         """Top-level DynBVH over InstanceT (kind 0) / nested DynBVH (kind 1)
         objects of the inner RefScenes."""
         return RefScene(self, None, 0, inner=(inner, inst_scene, translation, kind))
+
+    def read_ply(self, path, transform=None, tri_kind=0):
+        """Manta::readPlyFile into a fresh Mesh: (vertices, indices,
+        face_material), or None when the reader fails."""
+        t = None if transform is None else np.ascontiguousarray(transform, np.float32).reshape(12)
+        nv, nt = C.c_int(), C.c_int()
+        rc = self.lib.mref_read_ply(str(path).encode(), _ptr(t), tri_kind, C.byref(nv),
+                                    C.byref(nt), None, None, None, 0, 0)
+        if rc != 0:
+            return None
+        v = np.zeros((nv.value, 3), np.float32)
+        ix = np.zeros((nt.value, 3), np.uint32)
+        fm = np.zeros(nt.value, np.uint32)
+        rc = self.lib.mref_read_ply(str(path).encode(), _ptr(t), tri_kind, C.byref(nv),
+                                    C.byref(nt), _ptr(v), _ptr(ix), _ptr(fm), v.shape[0],
+                                    ix.shape[0])
+        if rc != 0:
+            return None
+        return v, ix, fm
 
     def camera_basis(self, cam) -> np.ndarray:
         e = np.asarray(cam.eye, np.float32)

@@ -70,7 +70,8 @@ MODEL_SRC := \
   Model/Cameras/PinholeCamera.cc \
   Model/Lights/AreaLight.cc Model/Primitives/Parallelogram.cc \
   Model/Primitives/PrimitiveCommon.cc Model/TexCoordMappers/UniformMapper.cc \
-  Model/Instances/InstanceT.cc Model/Instances/InstanceMaterial.cc
+  Model/Instances/InstanceT.cc Model/Instances/InstanceMaterial.cc \
+  Model/Readers/PlyReader.cc
 
 ENGINE_SRC := \
   Engine/Shadows/HardShadows.cc Engine/Renderers/Raytracer.cc \
@@ -82,8 +83,12 @@ SRC := $(CORE_SRC) $(IFACE_SRC) $(MODEL_SRC) $(ENGINE_SRC)
 
 COMMON_FLAGS := -std=gnu++98 -O2 -fPIC -w -pthread -fno-strict-aliasing
 
-OBJ_NOSSE := $(patsubst %.cc,$(OUT)/obj_nosse/%.o,$(SRC))
-OBJ_SSE   := $(patsubst %.cc,$(OUT)/obj_sse/%.o,$(SRC))
+# C sources (the PLY parser the reference vendors, Model/Readers/rply)
+C_SRC := Model/Readers/rply/rply.c
+CC := /usr/bin/gcc
+
+OBJ_NOSSE := $(patsubst %.cc,$(OUT)/obj_nosse/%.o,$(SRC)) $(patsubst %.c,$(OUT)/obj_c/%.o,$(C_SRC))
+OBJ_SSE   := $(patsubst %.cc,$(OUT)/obj_sse/%.o,$(SRC)) $(patsubst %.c,$(OUT)/obj_c/%.o,$(C_SRC))
 
 all: $(OUT)/libmanta_ref.so $(OUT)/libmanta_ref_sse.so
 
@@ -139,6 +144,10 @@ $(OUT)/obj_nosse/%.o: $(REF)/%.cc $(OUT)/gen_nosse/include/.stamp
 $(OUT)/obj_sse/%.o: $(REF)/%.cc $(OUT)/gen_sse/include/.stamp
 	@mkdir -p $(dir $@)
 	$(CXX) $(COMMON_FLAGS) -msse4.1 $(INC_SSE) -c $< -o $@
+
+$(OUT)/obj_c/%.o: $(REF)/%.c
+	@mkdir -p $(dir $@)
+	$(CC) -O2 -fPIC -w -c $< -o $@
 
 # The harness is this project's code: it drives the reference classes above.
 $(OUT)/obj_nosse/harness.o: $(HERE)ref_harness.cc $(OUT)/gen_nosse/include/.stamp

@@ -28,6 +28,8 @@
 #include <Core/Geometry/BBox.h>
 #include <Core/Geometry/Vector.h>
 #include <Core/Math/CheapRNG.h>
+#include <Core/Thread/Barrier.h>
+#include <Core/Thread/Thread.h>
 #include <Engine/Renderers/KajiyaPathtracer.h>
 #include <Engine/Renderers/Raytracer.h>
 #include <Engine/SampleGenerators/UniformRandomGenerator.h>
@@ -50,6 +52,7 @@
 #include <Model/Lights/PointLight.h>
 #include <Model/Materials/Lambertian.h>
 #include <Model/Materials/Phong.h>
+#include <Model/Readers/PlyReader.h>
 #include <Model/Primitives/KenslerShirleyTriangle.h>
 #include <Model/Primitives/MeshTriangle.h>
 #include <Model/Primitives/WaldTriangle.h>
@@ -59,6 +62,7 @@
 #endif
 
 #include <pthread.h>
+#include <unistd.h>
 #include <stdio.h>
 #include <string.h>
 #include <sys/time.h>
@@ -188,7 +192,32 @@ double now_s() {
 
 }  // namespace
 
+// The reference's thread library registers an atexit handler that calls
+// ::exit(0) from inside process exit (Core/Thread/Thread_pthreads.cc:
+// 596-655, 841-846, 874), which replaces the process's exit status with 0:
+// a test run or benchmark that loaded this library would report success
+// whatever failed.  (Thread::setCallExit(false) avoids the call but then
+// process exit blocks in that handler.)  mref_keep_exit_status makes sure the
+// thread library is initialised (a Barrier does that, Barrier_default.cc:
+// 72-76), then registers an on_exit handler - run before every handler
+// registered earlier - that flushes stdio and ends the process with the
+// status exit() was given.
+static void keep_exit_status(int status, void*) {
+  fflush(NULL);
+  _exit(status);
+}
+
 extern "C" {
+
+void mref_keep_exit_status(void) {
+  static bool done = false;
+  if (done) return;
+  done = true;
+  if (!Thread::isInitialized()) {
+    Barrier b("mref exit status");
+  }
+  on_exit(keep_exit_status, 0);
+}
 
 // Builds Mesh + triangles + DynBVH.  tri_kind 0 = WaldTriangle,
 // 1 = KenslerShirleyTriangle.  mat_rgb holds nmat diffuse colours.
@@ -266,6 +295,37 @@ int mref_scene_update_vertices(void* h, const float* verts, int nverts) {
   }
   s->bvh->update(0, 1);
   return 0;
+}
+
+// Manta::readPlyFile (Model/Readers/PlyReader.cc:135-269) into a fresh
+// Mesh with the given 3x4 transform (NULL = identity).  Returns the counts
+// and, when the arrays are given and large enough, the vertices, indices
+// and face materials.  0 = ok, 1 = the reader failed, 2 = arrays too small.
+int mref_read_ply(const char* path, const float* transform, int tri_kind, int* nv, int* nt,
+                  float* verts, unsigned* idx, unsigned* fmat, int cap_v, int cap_t) {
+  try {
+    AffineTransform t;
+    t.initWithIdentity();
+    if (transform)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) t.mat[i][j] = transform[4 * i + j];
+    Mesh* m = new Mesh();
+    if (!readPlyFile(std::string(path), t, m, 0,
+                     tri_kind == 0 ? MeshTriangle::WALD_TRI
+                                   : MeshTriangle::KENSLER_SHIRLEY_TRI))
+      return 1;
+    *nv = (int)m->vertices.size();
+    *nt = (int)(m->vertex_indices.size() / 3);
+    if (!verts) return 0;
+    if (*nv > cap_v || *nt > cap_t) return 2;
+    for (int i = 0; i < *nv; ++i)
+      for (int c = 0; c < 3; ++c) verts[3 * i + c] = m->vertices[i][c];
+    for (int i = 0; i < 3 * *nt; ++i) idx[i] = m->vertex_indices[i];
+    for (int i = 0; i < *nt; ++i) fmat[i] = m->face_material[i];
+    return 0;
+  } catch (...) {
+    return 1;
+  }
 }
 
 void mref_scene_destroy(void* h) {

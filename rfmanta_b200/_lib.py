@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librfmanta_b200.so")
 
 RQ_OK = 0
+RQ_ERR_NOTFOUND = 9
 RQ_ERR_ARG = 1
 RQ_ERR_CUDA = 2
 RQ_ERR_OOM = 3
@@ -150,6 +151,10 @@ def _load():
         "rq_server_destroy": ([vp], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
         "rq_scene_update_vertices": ([vp, vp, i], i),
+        "rq_mesh_read_ply": ([C.c_char_p, vp, C.c_uint32, C.POINTER(vp)], i),
+        "rq_mesh_info": ([vp, C.POINTER(i), C.POINTER(i)], i),
+        "rq_mesh_copy": ([vp, vp, vp, vp], i),
+        "rq_mesh_destroy": ([vp], i),
         "rq_scene_create_instanced": ([vp, i, vp, vp, vp, i, C.POINTER(vp)], i),
         "rq_trace_device_ex": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp, vp, vp], i),
         "rq_render_frame": ([vp, C.POINTER(FrameParams), vp, C.POINTER(C.c_uint64)], i),

@@ -3,7 +3,8 @@
     python -m rfmanta_b200.build [--verbose]
 
 Every .cu file under csrc/ is compiled with
-``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` into _build/ and
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` into _build/, every
+host-only .cc file there with g++ (IEEE float, no contraction), and all are
 linked into one shared library next to this file, so it travels with the
 source tree.  Host objects use the image's g++ through nvcc.
 """
@@ -24,6 +25,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-ccbin", "/usr/bin/g++"]
+CXX = "/usr/bin/g++"
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off",
+            "-fno-fast-math"]
 
 
 def _deps(src: str) -> list[str]:
@@ -51,6 +55,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
             jobs.append(cmd)
+    for s in sorted(glob.glob(os.path.join(CSRC, "*.cc"))):
+        o = os.path.join(BUILD, os.path.basename(s)[:-3] + ".host.o")
+        objs.append(o)
+        if _stale(o, _deps(s)):
+            jobs.append([CXX, *CXXFLAGS, "-c", s, "-o", o])
 
     def run(cmd):
         if verbose:

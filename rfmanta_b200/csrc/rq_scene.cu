@@ -426,6 +426,10 @@ int rq_scene_create(const float* vertices, int n_vertices,
     s->cfg[k].refill_threshold = 8;
     s->cfg[k].persistent = 1;
   }
+  // path stages: refill thresholds from a sweep of the 1280x720x16 path
+  // frame (block 64/128/256 x refill 4..24)
+  s->cfg[RQ_PATH_EXTEND].refill_threshold = 16;
+  s->cfg[RQ_PATH_SHADE].refill_threshold = 24;
   *out = s.release();
   return RQ_OK;
 }

@@ -21,7 +21,9 @@ two-level scene (tiny_instanced.npz): a 12x12 heightfield placed in the
 top-level group as a nested DynBVH plus six InstanceT copies of a level-2
 displaced icosphere (Phong), with the reference's inner and top-level trees, its
 DynBVH::intersect results (closest and AnyHit) for seeded rays and its
-Raytracer colours for the 4-spp jittered samples of a 48x40 frame.
+Raytracer colours for the 4-spp jittered samples of a 48x40 frame, and
+ply_cases.npz: Manta::readPlyFile's vertices, triangles and face materials
+for the PLY files the tests write (tests/test_mesh_io.py).
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -133,6 +135,26 @@ def write_instanced() -> None:
     print(path, os.path.getsize(path), "bytes")
 
 
+def write_ply_cases() -> None:
+    import tempfile
+    sys.path.insert(0, os.path.dirname(OUT))
+    from test_mesh_io import cases, write_ply
+    ref = Reference()
+    out = {"names": np.array([n for n, _, _ in cases()])}
+    with tempfile.TemporaryDirectory() as td:
+        for name, kw, transform in cases():
+            p = os.path.join(td, name + ".ply")
+            write_ply(p, **kw)
+            v, ix, fm = ref.read_ply(p, transform)
+            out[f"{name}_bytes"] = np.frombuffer(open(p, "rb").read(), np.uint8)
+            out[f"{name}_vertices"] = v
+            out[f"{name}_indices"] = ix
+            out[f"{name}_face_material"] = fm
+    path = os.path.join(OUT, "ply_cases.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 def sah_scenes():
     """Scenes whose reference SAH cost pins the GPU builder (2% bound)."""
     out = {"small_frame": scenes.small_frame_scene().mesh,
@@ -166,7 +188,10 @@ def write_sah_costs() -> None:
 if __name__ == "__main__":
     if "--instanced" in sys.argv:
         write_instanced()
+    elif "--ply" in sys.argv:
+        write_ply_cases()
     else:
         main()
         write_sah_costs()
         write_instanced()
+        write_ply_cases()

@@ -12,9 +12,10 @@
 //
 // Host side (the engine): requests are queued on submit, admitted in
 // arrival order while their output image fits the HBM budget, and each
-// step takes chunks round-robin from the admitted requests until the path
-// pool is full; at most two steps are in flight, and a request completes
-// when the step holding its last chunk has finished on the device.
+// step gives every admitted request one chunk, then fills the rest of the
+// path pool oldest request first; at most two steps are in flight, and a
+// request completes when the step holding its last chunk has finished on the
+// device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -89,59 +90,139 @@ __device__ __forceinline__ void stage_scenes(const ServeArgs& A, DevScene* sm) {
   __syncthreads();
 }
 
+// Lanes that must be idle before a warp of the persistent stages fetches
+// new path slots (the path tracer's tuned defaults).
+constexpr int kServeExtendRefill = 16;
+constexpr int kServeShadeRefill = 24;
+
+// Persistent extension stage over the step's live slots: each lane keeps one
+// slot's ray in flight in that slot's request scene; warps refill idle lanes
+// with one atomic on the bounce's work counter (as path_extend_persistent_
+// kernel does for a single frame).
 template <int KIND>
 __global__ void __launch_bounds__(128) serve_extend_kernel(ServeArgs A, PathBuffers B, int depth) {
   extern __shared__ int2 smem_stack[];
   __shared__ DevScene sm_scenes[kMaxServeScenes];
   stage_scenes(A, sm_scenes);
   int2* stk = smem_stack + threadIdx.x;
+  const int stride = blockDim.x;
   const int nq = depth == 0 ? A.n_slots : *(volatile const int*)&B.counters[depth];
   const int* qin = B.queue[depth & 1];
-  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
-    const int qi = base + threadIdx.x;
-    if (qi < nq) {
-      const int p = depth == 0 ? qi : qin[qi];
-      const ServeReq& R = A.reqs[A.slot_req[p]];
-      Counts cnt;
-      extend_path<KIND, false>(sm_scenes[R.scene], R.P, B, depth, p, stk, blockDim.x, cnt);
+  int* counter = &B.counters[kFetchBase + depth];
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int p = -1, scene = 0;
+  const ServeReq* R = nullptr;
+  bool exhausted = false;
+  Ray r;
+  Hit h;
+  int ref = kDone, sp = 0;
+  for (;;) {
+    const bool idle = (p < 0) && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, idle);
+    const unsigned busy = __ballot_sync(0xffffffffu, p >= 0);
+    if (m != 0u && (__popc(m) >= kServeExtendRefill || busy == 0u)) {
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (idle) {
+        const int qi = base + __popc(m & lt_mask);
+        if (qi < nq) {
+          p = depth == 0 ? qi : qin[qi];
+          R = &A.reqs[A.slot_req[p]];
+          scene = R->scene;
+          load_extension_ray(B, p, r);
+          start_ray(sm_scenes[scene], r, h, ref, sp);
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, exhausted)) break;
+    if (p >= 0) {
+      if (ref != kDone) step<KIND, false>(sm_scenes[scene], r, h, ref, sp, stk, stride);
+      if (ref == kDone) {
+        store_extension(R->P, B, depth, p, r, h);
+        p = -1;
+      }
     }
   }
 }
 
+// Persistent shade stage: shade_begin, the shadow ray's any-hit steps and
+// shade_finish per lane, survivors compacted into the next queue at the
+// warp's common point.
 template <int KIND>
 __global__ void __launch_bounds__(128) serve_shade_kernel(ServeArgs A, PathBuffers B, int depth) {
   extern __shared__ int2 smem_stack[];
   __shared__ DevScene sm_scenes[kMaxServeScenes];
   stage_scenes(A, sm_scenes);
   int2* stk = smem_stack + threadIdx.x;
+  const int stride = blockDim.x;
   const int nq = depth == 0 ? A.n_slots : *(volatile const int*)&B.counters[depth];
   const int* qin = B.queue[depth & 1];
   int* qout = B.queue[(depth + 1) & 1];
+  int* counter = &B.counters[kShadeFetchBase + depth];
   const unsigned lane = threadIdx.x & 31u;
-  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
-    const int qi = base + threadIdx.x;
-    bool alive = false;
-    int p = 0, nshadow = 0;
-    if (qi < nq) {
-      p = depth == 0 ? qi : qin[qi];
-      const ServeReq& R = A.reqs[A.slot_req[p]];
-      Counts cnt;
-      // a request whose depth is already reached keeps no live paths here
-      alive = shade_path<KIND, false>(sm_scenes[R.scene], R.P, B, depth, p, A.slot_g[p], stk,
-                                      blockDim.x, cnt, nshadow);
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, alive);
-    if (m) {
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int p = -1, scene = 0, nshadow = 0;
+  bool exhausted = false, alive = false, traced = false;
+  float contrib[3];
+  Ray sr;
+  Hit sh;
+  int ref = kDone, sp = 0;
+  for (;;) {
+    const bool idle = (p < 0) && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, idle);
+    const unsigned busy = __ballot_sync(0xffffffffu, p >= 0);
+    if (m != 0u && (__popc(m) >= kServeShadeRefill || busy == 0u)) {
       const int leader = __ffs(m) - 1;
-      int q = 0;
-      if ((int)lane == leader) q = atomicAdd(&B.counters[depth + 1], __popc(m));
-      q = __shfl_sync(0xffffffffu, q, leader);
-      if (alive) qout[q + __popc(m & ((1u << lane) - 1u))] = p;
+      int base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (idle) {
+        const int qi = base + __popc(m & lt_mask);
+        if (qi < nq) {
+          p = depth == 0 ? qi : qin[qi];
+          const ServeReq& R = A.reqs[A.slot_req[p]];
+          scene = R.scene;
+          // a request whose depth is already reached keeps no live paths here
+          traced = shade_begin<KIND>(sm_scenes[scene], R.P, B, depth, p, A.slot_g[p], sr,
+                                     contrib, alive);
+          ref = kDone;
+          if (traced) {
+            ++nshadow;
+            start_ray(sm_scenes[scene], sr, sh, ref, sp);
+          }
+        } else {
+          exhausted = true;
+        }
+      }
     }
-    int tot = nshadow;
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    if (lane == 0 && tot) atomicAdd(&B.ray_counts[1], (unsigned long long)tot);
+    if (__all_sync(0xffffffffu, exhausted)) break;
+    bool fin = false;
+    if (p >= 0) {
+      if (ref != kDone) step<KIND, true>(sm_scenes[scene], sr, sh, ref, sp, stk, stride);
+      if (ref == kDone) {
+        if (traced && sh.id < 0) shade_finish(B, p, contrib);
+        fin = true;
+      }
+    }
+    const bool push = fin && alive;
+    const unsigned pm = __ballot_sync(0xffffffffu, push);
+    if (pm) {
+      const int leader = __ffs(pm) - 1;
+      int q = 0;
+      if ((int)lane == leader) q = atomicAdd(&B.counters[depth + 1], __popc(pm));
+      q = __shfl_sync(0xffffffffu, q, leader);
+      if (push) qout[q + __popc(pm & lt_mask)] = p;
+    }
+    if (fin) p = -1;
   }
+  int tot = nshadow;
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  if (lane == 0 && tot) atomicAdd(&B.ray_counts[1], (unsigned long long)tot);
 }
 
 __global__ void serve_count_kernel(ServeArgs A, PathBuffers B, int depth) {
@@ -274,7 +355,6 @@ struct rq_server {
   std::deque<int> pending;   // submitted, not admitted
   std::vector<int> active;   // admitted, not finished (admission order)
   std::vector<int> table;    // request id per device-table slot
-  int rr = 0;                // round-robin cursor
   int next_id = 1;
   long long steps = 0;
   int grid = 1;
@@ -481,40 +561,41 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
   std::map<int, int> tidx;  // request id -> table index this step
   int n_chunks = 0, n_req = 0, max_depth = 1;
   long long slots = 0, pix = 0;
-  bool progress = true;
-  size_t start = (size_t)(s->rr % (int)cand.size());
-  while (progress && n_chunks < s->max_chunks) {
-    progress = false;
-    for (size_t k = 0; k < cand.size() && n_chunks < s->max_chunks; ++k) {
-      HostReq& r = *s->reqs[cand[(start + k) % cand.size()]];
-      if (r.scheduled_all) continue;
-      const int npx = std::min(s->chunk_pixels, r.npix - r.next_pix);
-      const long long need = (long long)npx * r.spec.spp;
-      if (slots + need > s->capacity) continue;
-      int ti;
-      auto it = tidx.find(r.id);
-      if (it == tidx.end()) {
-        ti = n_req++;
-        tidx[r.id] = ti;
-        hreq[ti] = r.dev;
-      } else {
-        ti = it->second;
-      }
-      ServeChunk& c = hch[n_chunks++];
-      c.req = ti;
-      c.pix0 = r.next_pix;
-      c.npix = npx;
-      c.slot0 = (int)slots;
-      c.px0 = (int)pix;
-      slots += need;
-      pix += npx;
-      max_depth = std::max(max_depth, r.spec.max_depth);
-      r.next_pix += npx;
-      if (r.next_pix >= r.npix) r.scheduled_all = true;
-      progress = true;
+  // Two passes over the admitted requests in admission order: first one
+  // chunk each (every request advances every step), then the rest of the
+  // pool oldest first, so the oldest requests - the ones whose latency is
+  // the tail - get most of each step.
+  auto take = [&](HostReq& r) -> bool {
+    if (r.scheduled_all || n_chunks >= s->max_chunks) return false;
+    const int npx = std::min(s->chunk_pixels, r.npix - r.next_pix);
+    const long long need = (long long)npx * r.spec.spp;
+    if (slots + need > s->capacity) return false;
+    int ti;
+    auto it = tidx.find(r.id);
+    if (it == tidx.end()) {
+      ti = n_req++;
+      tidx[r.id] = ti;
+      hreq[ti] = r.dev;
+    } else {
+      ti = it->second;
     }
-  }
-  s->rr = (int)((start + 1) % cand.size());
+    ServeChunk& c = hch[n_chunks++];
+    c.req = ti;
+    c.pix0 = r.next_pix;
+    c.npix = npx;
+    c.slot0 = (int)slots;
+    c.px0 = (int)pix;
+    slots += need;
+    pix += npx;
+    max_depth = std::max(max_depth, r.spec.max_depth);
+    r.next_pix += npx;
+    if (r.next_pix >= r.npix) r.scheduled_all = true;
+    return true;
+  };
+  for (int id : cand) take(*s->reqs[id]);
+  for (int id : cand)
+    while (take(*s->reqs[id])) {
+    }
   if (n_chunks == 0) return RQ_OK;
   cudaStream_t st = s->stream;
   cudaError_t e = cudaMemcpyAsync(s->d_reqs, hreq, sizeof(ServeReq) * n_req, cudaMemcpyHostToDevice, st);

@@ -665,26 +665,31 @@ class ServingWL(BatchedQueriesWL):
         sat_rays = (st2["rays"] - b0["rays"]) + (st2["shadow_rays"] - b0["shadow_rays"])
         srv2.close()
         # serial plain per-request GPU calls (rq_render_path), FIFO in arrival
-        # order: service times measured one request at a time, then replayed
-        # against the same arrival times
-        service, serial_rays = [], 0
-        for _, r in stream:
-            ps = scenes.PathScene(self.meshes[r.scene],
-                                  scenes.Camera(r.eye, r.lookat, r.up, r.hfov, r.vfov),
-                                  scenes.AreaLightSpec(r.light_anchor, r.light_v1, r.light_v2,
-                                                       r.light_color),
-                                  r.background, r.xres, r.yres, r.spp, r.max_depth,
-                                  r.rr_depth, r.seed)
-            t0 = time.perf_counter()
-            o = self.bvhs[r.scene].render_path(ps)
-            service.append(time.perf_counter() - t0)
-            serial_rays += o["rays"] + o["shadow_rays"]
-        finish, serial_lat = 0.0, []
-        for (arr, _), sv in zip(stream, service):
-            finish = max(finish, arr) + sv
-            serial_lat.append(finish - arr)
-        serial_stream = serial_rays / (finish - stream[0][0]) / 1e6
-        serial_sat = serial_rays / sum(service) / 1e6
+        # order over the same streams the server ran: service times measured
+        # one request at a time, then replayed against the arrival times
+        serial_rays, serial_lat, serial_wall, serial_service = 0, [], 0.0, 0.0
+        for k in range(args.steps):
+            sk = poisson_stream(self.meshes, self.requests, 200.0, seed=100 + k)
+            service = []
+            for _, r in sk:
+                ps = scenes.PathScene(self.meshes[r.scene],
+                                      scenes.Camera(r.eye, r.lookat, r.up, r.hfov, r.vfov),
+                                      scenes.AreaLightSpec(r.light_anchor, r.light_v1,
+                                                           r.light_v2, r.light_color),
+                                      r.background, r.xres, r.yres, r.spp, r.max_depth,
+                                      r.rr_depth, r.seed)
+                t0 = time.perf_counter()
+                o = self.bvhs[r.scene].render_path(ps)
+                service.append(time.perf_counter() - t0)
+                serial_rays += o["rays"] + o["shadow_rays"]
+            finish = 0.0
+            for (arr, _), sv in zip(sk, service):
+                finish = max(finish, arr) + sv
+                serial_lat.append(finish - arr)
+            serial_wall += finish - sk[0][0]
+            serial_service += sum(service)
+        serial_stream = serial_rays / serial_wall / 1e6
+        serial_sat = serial_rays / serial_service / 1e6
         serial_ms = np.array(serial_lat) * 1e3
         lat_ms = np.array(lat) * 1e3
         return {

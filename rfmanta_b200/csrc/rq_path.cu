@@ -6,7 +6,9 @@
 //              the pixel, PinholeCamera basis (PinholeCamera.cc:356-366)
 //   per bounce (both stages persistent, warps refilling idle lanes)
 //     extend   closest-hit traversal of the live paths (compacted queue)
-//     shade    fused stage per live path: background on a miss
+//     shade    fused stage per live path (the survivors are then compacted
+//              in path order, which keeps neighbouring paths together in
+//              the next bounce's warps): background on a miss
 //              (KajiyaPathtracer.cc:283-291), Lambertian::sampleBSDF cosine
 //              sampling (Lambertian.cc:248-280), importance *= reflectance,
 //              one area-light sample (AreaLight::computeLight,
@@ -169,6 +171,11 @@ __global__ void __launch_bounds__(256)
         fin = true;
       }
     }
+    if (B.alive) {
+      if (fin) B.alive[p] = alive ? 1 : 0;
+      if (fin) p = -1;
+      continue;
+    }
     const bool push = fin && alive;
     const unsigned pm = __ballot_sync(0xffffffffu, push);
     if (pm) {
@@ -223,6 +230,89 @@ __global__ void path_resolve_kernel(PathParams P, PathBuffers B, long long g0, i
   }
 }
 
+// Ordered compaction of the survivor flags into the next queue (path order):
+// per-tile counts, one-block scan of the tile counts (the total becomes the
+// next bounce's live count), then every tile writes its survivors in order.
+constexpr int kCompactThreads = 256, kCompactPer = 16;
+constexpr int kCompactTile = kCompactThreads * kCompactPer;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    int s = lane < nw ? warp_sums[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) warp_sums[lane] = s;
+  }
+  __syncthreads();
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  const int before = warp == 0 ? 0 : warp_sums[warp - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(kCompactThreads)
+    compact_count_kernel(const uint8_t* __restrict__ alive, int n, int* tile_counts) {
+  __shared__ int ws[32];
+  const int base = blockIdx.x * kCompactTile + threadIdx.x * kCompactPer;
+  int c = 0;
+  for (int k = 0; k < kCompactPer; ++k) c += (base + k < n && alive[base + k]) ? 1 : 0;
+  int total;
+  block_exclusive_scan(c, ws, total);
+  if (threadIdx.x == 0) tile_counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024)
+    compact_scan_kernel(int* tile_counts, int ntiles, int* total_out) {
+  __shared__ int ws[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < ntiles; b0 += blockDim.x) {
+    const int i = b0 + threadIdx.x;
+    const int v = i < ntiles ? tile_counts[i] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, ws, total);
+    if (i < ntiles) tile_counts[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(kCompactThreads)
+    compact_scatter_kernel(const uint8_t* __restrict__ alive, int n,
+                           const int* __restrict__ tile_offsets, int* qout) {
+  __shared__ int ws[32];
+  const int base = blockIdx.x * kCompactTile + threadIdx.x * kCompactPer;
+  int c = 0;
+  for (int k = 0; k < kCompactPer; ++k) c += (base + k < n && alive[base + k]) ? 1 : 0;
+  int total;
+  int o = tile_offsets[blockIdx.x] + block_exclusive_scan(c, ws, total);
+  for (int k = 0; k < kCompactPer; ++k)
+    if (base + k < n && alive[base + k]) qout[o++] = base + k;
+}
+
+cudaError_t launch_ordered_compaction(const PathBuffers& B, int n, int depth, cudaStream_t st) {
+  const int tiles = std::max(1, (n + kCompactTile - 1) / kCompactTile);
+  compact_count_kernel<<<tiles, kCompactThreads, 0, st>>>(B.alive, n, B.tile_counts);
+  compact_scan_kernel<<<1, 1024, 0, st>>>(B.tile_counts, tiles, &B.counters[depth + 1]);
+  compact_scatter_kernel<<<tiles, kCompactThreads, 0, st>>>(B.alive, n, B.tile_counts,
+                                                            B.queue[(depth + 1) & 1]);
+  return cudaGetLastError();
+}
+
 // Grid of a persistent stage: every SM filled once at the kernel's own
 // occupancy for this block size and stack (or blocks_per_sm if smaller).
 static int stage_grid(const void* f, int block, int blocks_per_sm, size_t smem) {
@@ -252,8 +342,10 @@ static void launch_bounces(const DevScene& S, const PathParams& P, const PathBuf
     path_extend_persistent_kernel<KIND, STATS><<<egrid, eb, esm, st>>>(S, P, B, depth, n,
                                                                        L.refill[0]);
     if (nev > 1 + 2 * depth) cudaEventRecord(ev[1 + 2 * depth], st);
+    if (B.alive) cudaMemsetAsync(B.alive, 0, (size_t)n, st);
     path_shade_persistent_kernel<KIND, STATS><<<sgrid, sb, ssm, st>>>(S, P, B, depth, n,
                                                                       L.refill[1]);
+    if (B.alive) launch_ordered_compaction(B, n, depth, st);
     if (nev > 2 + 2 * depth) cudaEventRecord(ev[2 + 2 * depth], st);
   }
 }

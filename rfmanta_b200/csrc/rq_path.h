@@ -45,6 +45,11 @@ struct PathBuffers {
   int32_t* prim;
   int32_t* queue[2];
   int32_t* counters;            // kPathCounters (see above)
+  // optional: survivor flag per path slot; when set, the next bounce's queue
+  // is built in path order by an ordered compaction instead of per-warp
+  // appends
+  uint8_t* alive;
+  int* tile_counts;  // scratch of the ordered compaction
   unsigned long long* ray_counts;  // [0] extension rays, [1] shadow rays
   unsigned long long* stats;       // optional box/tri test counters (4)
   // optional per-bounce dump for parity checks: [depth][path]
@@ -65,5 +70,8 @@ cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffer
                               const PathLaunch& L, cudaStream_t st, const cudaEvent_t* ev,
                               int nev);
 int path_blocks_per_sm(int tri_kind, size_t smem);
+// Builds bounce depth+1's queue (and live count) from B.alive over slots
+// [0, n), in slot order.
+cudaError_t launch_ordered_compaction(const PathBuffers& B, int n, int depth, cudaStream_t st);
 
 }  // namespace rq

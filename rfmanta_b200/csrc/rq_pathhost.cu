@@ -26,10 +26,11 @@ struct PathScratch {
   void free_paths() {
     cudaFree(B.o); cudaFree(B.d); cudaFree(B.imp); cudaFree(B.rad); cudaFree(B.rng);
     cudaFree(B.t); cudaFree(B.pos); cudaFree(B.prim); cudaFree(B.queue[0]);
-    cudaFree(B.queue[1]); cudaFree(B.counters);
+    cudaFree(B.queue[1]); cudaFree(B.counters); cudaFree(B.alive); cudaFree(B.tile_counts);
     B.o = B.d = B.imp = B.rad = B.t = nullptr;
     B.rng = nullptr;
-    B.pos = B.prim = B.queue[0] = B.queue[1] = B.counters = nullptr;
+    B.alive = nullptr;
+    B.pos = B.prim = B.queue[0] = B.queue[1] = B.counters = B.tile_counts = nullptr;
     capacity = 0;
   }
   ~PathScratch() {
@@ -104,7 +105,8 @@ static int path_prepare(Scene* s, const rq_path_params* p, PathParams& P, long l
     if (!palloc(&B.o, 3 * C) || !palloc(&B.d, 3 * C) || !palloc(&B.imp, 3 * C) ||
         !palloc(&B.rad, 3 * C) || !palloc(&B.rng, C) || !palloc(&B.t, C) ||
         !palloc(&B.pos, C) || !palloc(&B.prim, C) || !palloc(&B.queue[0], C) ||
-        !palloc(&B.queue[1], C) || !palloc(&B.counters, kPathCounters)) {
+        !palloc(&B.queue[1], C) || !palloc(&B.counters, kPathCounters) ||
+        !palloc(&B.alive, C) || !palloc(&B.tile_counts, C / 4096 + 2)) {
       ps->free_paths();
       return pfail(RQ_ERR_OOM, "path state allocation failed");
     }

@@ -209,6 +209,13 @@ __global__ void __launch_bounds__(128) serve_shade_kernel(ServeArgs A, PathBuffe
         fin = true;
       }
     }
+    if (B.alive) {  // survivors are compacted in slot order after the kernel
+      if (fin) {
+        B.alive[p] = alive ? 1 : 0;
+        p = -1;
+      }
+      continue;
+    }
     const bool push = fin && alive;
     const unsigned pm = __ballot_sync(0xffffffffu, push);
     if (pm) {
@@ -268,7 +275,9 @@ static cudaError_t serve_launch_step(const ServeArgs& A, PathBuffers B, int max_
   for (int depth = 0; depth < max_depth; ++depth) {
     serve_count_kernel<<<1, 32, 0, st>>>(A, B, depth);
     serve_extend_kernel<KIND><<<grid, 128, smem, st>>>(A, B, depth);
+    cudaMemsetAsync(B.alive, 0, (size_t)A.n_slots, st);
     serve_shade_kernel<KIND><<<grid, 128, smem, st>>>(A, B, depth);
+    launch_ordered_compaction(B, A.n_slots, depth, st);
   }
   const int rg = std::max(1, std::min(grid, (A.n_pix + 255) / 256));
   serve_resolve_kernel<<<rg, 256, 0, st>>>(A, B);
@@ -371,7 +380,8 @@ struct rq_server {
     }
     cudaFree(B.o); cudaFree(B.d); cudaFree(B.imp); cudaFree(B.rad); cudaFree(B.rng);
     cudaFree(B.t); cudaFree(B.pos); cudaFree(B.prim); cudaFree(B.queue[0]); cudaFree(B.queue[1]);
-    cudaFree(B.counters); cudaFree(slot_req); cudaFree(slot_g); cudaFree(counts);
+    cudaFree(B.counters); cudaFree(B.alive); cudaFree(B.tile_counts);
+    cudaFree(slot_req); cudaFree(slot_g); cudaFree(counts);
     cudaFree(d_reqs); cudaFree(d_chunks); cudaFree(d_scenes);
     for (int i = 0; i < kRing; ++i) {
       cudaFreeHost(h_reqs[i]);
@@ -481,6 +491,8 @@ int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capac
             cudaMalloc(&B.queue[0], 4 * C) == cudaSuccess &&
             cudaMalloc(&B.queue[1], 4 * C) == cudaSuccess &&
             cudaMalloc(&B.counters, kPathCounters * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&B.alive, C) == cudaSuccess &&
+            cudaMalloc(&B.tile_counts, 4 * (C / 4096 + 2)) == cudaSuccess &&
             cudaMalloc(&s->slot_req, 4 * C) == cudaSuccess &&
             cudaMalloc(&s->slot_g, 8 * C) == cudaSuccess &&
             cudaMalloc(&s->counts, 16) == cudaSuccess &&

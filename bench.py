@@ -140,6 +140,24 @@ def _dist():
     return world, rank, local
 
 
+def reduce_over_ranks(x: float, op: str = "max", device=None) -> float:
+    """x reduced over the process group ("max" for step times, "sum" for
+    rates); the value itself when no group is running."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_rate(rays_per_step: int, steps: int, world: int, seconds: float) -> float:
+    """Whole-job Mrays/s: every rank traces rays_per_step per step (weak
+    scaling), over the slowest rank's time."""
+    return rays_per_step * steps * world / seconds / 1e6
+
+
 # ------------------------------------------------------------- workloads ---
 
 class PathFrame:
@@ -830,12 +848,8 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    total_ms = sum(a.elapsed_time(b) for a, b in pairs)
-    t_max = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    total_ms = float(t_max.item())
-    value = rays_per_step * args.steps * world / (total_ms * 1e-3) / 1e6
+    total_ms = reduce_over_ranks(sum(a.elapsed_time(b) for a, b in pairs), "max", dev)
+    value = job_rate(rays_per_step, args.steps, world, total_ms * 1e-3)
 
     # end to end through the host-buffer public call
     e2e = []
@@ -848,10 +862,8 @@ def run_ours(args):
         t1 = time.perf_counter()
         if k >= args.warmup:
             e2e.append(t1 - t0)
-    e2e_t = torch.tensor([sum(e2e)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = rays_per_step * args.steps * world / float(e2e_t.item()) / 1e6
+    e2e_value = job_rate(rays_per_step, args.steps, world,
+                         reduce_over_ranks(sum(e2e), "max", dev))
 
     # roofline of the dominant kernel
     hbm, peak_kind = _peaks()
@@ -901,14 +913,11 @@ def run_custom(args, wl, dev, world, rank):
     import torch.distributed as dist
     with ClockSampler(dev.index or 0) as clk:
         r = wl.run_custom(args, dev)
-    value = torch.tensor([r["value"]], dtype=torch.float64, device=dev)
-    e2e = torch.tensor([r["e2e"]], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(value, op=dist.ReduceOp.SUM)
-        dist.all_reduce(e2e, op=dist.ReduceOp.SUM)
+    value = reduce_over_ranks(r["value"], "sum", dev)
+    e2e = reduce_over_ranks(r["e2e"], "sum", dev)
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(float(value.item()), 2), "unit": "Mrays/s",
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(r["ms_per_step"], 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -916,7 +925,7 @@ def run_custom(args, wl, dev, world, rank):
             "config": dict(wl.config(), parallelism=f"replicas x{world}",
                            rays_per_step=r["rays_per_step"], **r["extra"]),
             "clocks": clk.summary(),
-            "e2e": {"value": round(float(e2e.item()), 2), "unit": "Mrays/s",
+            "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(r["h2d"]), "d2h_bytes_per_step": int(r["d2h"])},
             "gpu_launches": None,
             "roofline": None,

@@ -65,6 +65,37 @@ class Tree:
                     z["left_cheaper"], z["ids"])
 
 
+class DynTree:
+    """A DynBVH as DynBVH::update sees it: the node array with room for
+    `cap` nodes (the reference allocates 2 per object, DynBVH.cc:1680-1684),
+    the per-node SAH costs, object_ids and nextFree."""
+
+    def __init__(self, tree: Tree, n_objects: int, costs=None, next_free=None, cap=None):
+        n = tree.children.shape[0]
+        self.cap = int(cap if cap is not None else max(2 * n_objects, n))
+        self.bounds = np.zeros((self.cap, 6), np.float32)
+        self.child = np.zeros(self.cap, np.int32)
+        self.children = np.zeros(self.cap, np.int32)
+        self.axis = np.zeros(self.cap, np.uint8)
+        self.left_cheaper = np.zeros(self.cap, np.uint8)
+        self.costs = np.zeros(self.cap, np.float32)
+        self.bounds[:n] = tree.bounds
+        self.child[:n] = tree.child
+        self.children[:n] = tree.children
+        self.axis[:n] = tree.axis
+        self.left_cheaper[:n] = tree.left_cheaper
+        self.ids = np.ascontiguousarray(tree.ids, np.int32).copy()
+        if costs is not None:
+            self.costs[:len(costs)] = costs
+        # nodes are allocated in pairs after the root
+        self.next_free = int(next_free if next_free is not None else n)
+
+    def tree(self, n=None) -> Tree:
+        n = self.next_free if n is None else n
+        return Tree(self.bounds[:n].copy(), self.child[:n].copy(), self.children[:n].copy(),
+                    self.axis[:n].copy(), self.left_cheaper[:n].copy(), self.ids.copy())
+
+
 class _OrqTree(C.Structure):
     _fields_ = [("bounds", C.c_void_p), ("child", C.c_void_p), ("children", C.c_void_p),
                 ("axis", C.c_void_p), ("left_cheaper", C.c_void_p), ("ids", C.c_void_p),
@@ -126,7 +157,8 @@ class World:
 
 def build_restatement() -> str:
     if not os.path.exists(ORACLE_SO) or (
-            os.path.getmtime(ORACLE_SO) < os.path.getmtime(os.path.join(HERE, "rq_oracle.c"))):
+            os.path.getmtime(ORACLE_SO) < max(os.path.getmtime(os.path.join(HERE, f))
+                                          for f in ("rq_oracle.c", "rq_oracle_update.c"))):
         subprocess.check_call(["make", "-s", "-f", os.path.join(HERE, "Makefile")],
                               cwd=os.path.dirname(HERE))
     return ORACLE_SO
@@ -146,6 +178,10 @@ class Restatement:
                                [C.c_int] + [C.c_void_p] * 7)
         L.orq_sah_cost.argtypes = [C.c_void_p] * 3
         L.orq_sah_cost.restype = C.c_double
+        L.orq_tree_costs.argtypes = [C.c_void_p] * 4
+        L.orq_tree_costs.restype = C.c_float
+        L.orq_tree_update.argtypes = ([C.c_void_p] * 7 + [C.c_int, C.c_void_p, C.c_void_p,
+                                                          C.c_void_p, C.c_int, C.c_int])
         L.orq_camera_basis.argtypes = [C.c_void_p] * 3 + [C.c_float, C.c_float, C.c_void_p]
         L.orq_primary_rays.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.orq_render_whitted.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 6 +
@@ -319,6 +355,24 @@ class Restatement:
         b, c, ch, *_ = tree.arrays()
         return float(self.lib.orq_sah_cost(_ptr(b), _ptr(c), _ptr(ch)))
 
+    def tree_costs(self, t: DynTree) -> float:
+        """DynBVH::computeCost<true>(0) into t.costs (a rebuild's state)."""
+        return float(self.lib.orq_tree_costs(_ptr(t.bounds), _ptr(t.child), _ptr(t.children),
+                                             _ptr(t.costs)))
+
+    def tree_update(self, t: DynTree, vertices, indices, rotate=True) -> None:
+        """DynBVH::update(0, 1) of t in place after the vertices moved."""
+        v = np.ascontiguousarray(vertices, np.float32)
+        ix = np.ascontiguousarray(indices, np.uint32)
+        nf = C.c_int(t.next_free)
+        rc = self.lib.orq_tree_update(_ptr(t.bounds), _ptr(t.child), _ptr(t.children),
+                                      _ptr(t.axis), _ptr(t.left_cheaper), _ptr(t.costs),
+                                      _ptr(t.ids), t.cap, C.byref(nf), _ptr(v), _ptr(ix),
+                                      ix.shape[0], int(rotate))
+        if rc != 0:
+            raise RuntimeError(f"orq_tree_update failed ({rc})")
+        t.next_free = nf.value
+
     def camera_basis(self, cam) -> np.ndarray:
         e = np.asarray(cam.eye, np.float32)
         la = np.asarray(cam.lookat, np.float32)
@@ -380,6 +434,7 @@ class Reference:
         L.mref_tree_count.argtypes = [C.c_void_p] * 4
         L.mref_tree_export.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 6
         L.mref_tree_save.argtypes = [C.c_void_p, C.c_char_p]
+        L.mref_tree_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.mref_tree_cost.argtypes = [C.c_void_p]
         L.mref_tree_cost.restype = C.c_double
         L.mref_intersect.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
@@ -513,6 +568,18 @@ class RefScene:
         self.ref.lib.mref_tree_export(self.h, n, _ptr(b), _ptr(c), _ptr(ch), _ptr(ax),
                                       _ptr(lc), _ptr(ids))
         return Tree(b, c, ch, ax, lc, ids)
+
+    def dyn_tree(self) -> DynTree:
+        """The tree with its costs and nextFree (no call may run
+        computeCost in between: it rewrites the costs)."""
+        used, alloc, nids = C.c_int(), C.c_int(), C.c_int()
+        self.ref.lib.mref_tree_count(self.h, C.byref(used), C.byref(alloc), C.byref(nids))
+        costs = np.zeros(used.value, np.float32)
+        nf = C.c_int()
+        if self.ref.lib.mref_tree_state(self.h, _ptr(costs), used.value, C.byref(nf)) != 0:
+            raise RuntimeError("mref_tree_state failed")
+        return DynTree(self.tree(), nids.value, costs=costs, next_free=nf.value,
+                       cap=alloc.value)
 
     def save_blob(self, path: str):
         if self.ref.lib.mref_tree_save(self.h, path.encode()) != 0:

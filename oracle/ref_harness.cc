@@ -94,6 +94,10 @@ public:
   const std::vector<BVHNode>& treeNodes() const { return nodes; }
   const std::vector<int>& treeIds() const { return object_ids; }
   float sahCost() { return computeCost<true>(0); }
+  // DynBVH::costs and DynBVH::nextFree (DynBVH.h:105, 382): the state the
+  // tree rotations of the next update start from.
+  const std::vector<Real>& treeCosts() const { return costs; }
+  int nextFreeNode() const { return nextFree; }
 };
 
 // Reads MeshTriangle::myID (protected, Model/Primitives/MeshTriangle.h:63).
@@ -374,6 +378,16 @@ int mref_tree_export(void* h, int nodes_used, float* bounds, int* child,
   }
   const std::vector<int>& o = s->bvh->treeIds();
   for (size_t i = 0; i < o.size(); ++i) ids[i] = o[i];
+  return 0;
+}
+
+// The first n per-node costs (n <= the node vector's size) and nextFree.
+int mref_tree_state(void* h, float* costs, int n, int* next_free) {
+  RefScene* s = static_cast<RefScene*>(h);
+  const std::vector<Real>& c = s->bvh->treeCosts();
+  if (n > (int)c.size()) return 1;
+  for (int i = 0; i < n; ++i) costs[i] = c[i];
+  *next_free = s->bvh->nextFreeNode();
   return 0;
 }
 

@@ -253,6 +253,17 @@ def tiny_frame_scene(xres: int = 48, yres: int = 40, seed: int = 3) -> WhittedSc
     return s
 
 
+def animated_vertices(v0: np.ndarray, frame: int, amplitude: float = 0.04,
+                      jitter: float = 0.01, seed: int = 100) -> np.ndarray:
+    """Frame `frame` of a seeded non-rigid animation of a mesh's vertices:
+    a travelling sine displacement whose amplitude grows with the frame,
+    plus per-vertex noise (the animated-mesh refit workload)."""
+    rng = np.random.default_rng(seed + frame)
+    w = np.sin(3.0 * v0[:, [1, 2, 0]] + 0.7 * frame).astype(np.float32)
+    return (v0 + np.float32(amplitude * (1 + frame)) * w +
+            rng.normal(scale=jitter, size=v0.shape)).astype(np.float32)
+
+
 def random_rays(n: int, lo: np.ndarray, hi: np.ndarray, seed: int,
                 anyhit_fraction: float = 0.0):
     """Origins uniform in [lo, hi], directions uniform on the sphere, tmax

@@ -23,7 +23,9 @@ displaced icosphere (Phong), with the reference's inner and top-level trees, its
 DynBVH::intersect results (closest and AnyHit) for seeded rays and its
 Raytracer colours for the 4-spp jittered samples of a 48x40 frame, and
 ply_cases.npz: Manta::readPlyFile's vertices, triangles and face materials
-for the PLY files the tests write (tests/test_mesh_io.py).
+for the PLY files the tests write (tests/test_mesh_io.py), and
+tree_update.npz: DynBVH::update with its tree rotations over four frames of a
+seeded animation (the tree, per-node costs and nextFree after every frame).
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -155,6 +157,47 @@ def write_ply_cases() -> None:
     print(path, os.path.getsize(path), "bytes")
 
 
+def update_cases():
+    """Meshes for the animated-mesh update fixture: the tiny frame scene and
+    a small one, four frames each of scenes.animated_vertices."""
+    return {"tiny": scenes.tiny_frame_scene().mesh,
+            "small": scenes.small_frame_scene(level=3, grid=12, xres=8, yres=8).mesh}
+
+
+UPDATE_FRAMES = 4
+DYN_FIELDS = ("bounds", "child", "children", "axis", "left_cheaper", "costs", "ids")
+
+
+def write_tree_update() -> None:
+    """DynBVH::update(0, 1) (tree rotations and leaf re-splits, TREE_ROT 1)
+    of the reference's rebuilt tree over four animation frames: the tree,
+    per-node costs and nextFree before and after every frame."""
+    ref = Reference()
+    out = {"names": np.array(list(update_cases()))}
+    for name, mesh in update_cases().items():
+        rs = ref.scene(mesh, 0)
+        v0 = mesh.vertices.copy()
+        states = [rs.dyn_tree()]
+        for k in range(1, UPDATE_FRAMES + 1):
+            v = scenes.animated_vertices(v0, k)
+            out[f"{name}_vertices{k}"] = v
+            rs.update_vertices(v)
+            states.append(rs.dyn_tree())
+        for k, st in enumerate(states):
+            n = st.next_free
+            for f in DYN_FIELDS:
+                a = getattr(st, f)
+                out[f"{name}_s{k}_{f}"] = a if f == "ids" else a[:n]
+            out[f"{name}_s{k}_next_free"] = np.int64(n)
+            out[f"{name}_s{k}_cap"] = np.int64(st.cap)
+        out[f"{name}_indices"] = mesh.indices
+        out[f"{name}_vertices0"] = v0
+        rs.close()
+    path = os.path.join(OUT, "tree_update.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 def sah_scenes():
     """Scenes whose reference SAH cost pins the GPU builder (2% bound)."""
     out = {"small_frame": scenes.small_frame_scene().mesh,
@@ -190,8 +233,12 @@ if __name__ == "__main__":
         write_instanced()
     elif "--ply" in sys.argv:
         write_ply_cases()
+        write_tree_update()
+    elif "--update" in sys.argv:
+        write_tree_update()
     else:
         main()
         write_sah_costs()
         write_instanced()
         write_ply_cases()
+        write_tree_update()

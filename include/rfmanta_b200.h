@@ -111,14 +111,43 @@ RQ_API int rq_scene_import_tree(rq_scene* scene, int n_nodes, const float* bound
  */
 RQ_API int rq_scene_build(rq_scene* scene, int bins);
 
-/* SAH cost of the scene's tree, DynBVH::computeCost<>(0) with C_isec=C_trav=1. */
-/* DynBVH::update (Model/Groups/DynBVH.cc:1574-1581, 2012-2123): new
- * positions for the scene's vertices (same count and triangles); the
- * triangles' precomputation is redone and every node box refitted bottom up
- * on the GPU, keeping the tree's topology, as the reference's refit does.
- * Not for two-level scenes (refit the inner scenes, then create the
- * two-level scene again). */
+/*
+ * DynBVH::update (Model/Groups/DynBVH.cc:1574-1581, 2012-2123): new
+ * positions for the scene's vertices (same count and triangles), the
+ * triangles' precomputation redone and the tree updated on the GPU.
+ *   RQ_UPDATE_ROTATE  the update as the reference ships it (TREE_ROT 1,
+ *                     DynBVH.h:377): boxes refitted bottom up and, at every
+ *                     internal node, leaf children of more than one object
+ *                     re-split by the approximate binned build and the best
+ *                     of Kopta et al.'s six tree rotations applied
+ *                     (rotateNode, DynBVH.cc:3051-3348).  The tree, its
+ *                     per-node costs and next free node equal those of the
+ *                     reference's single-threaded DynBVH::update(0, 1) from
+ *                     the same tree; the costs a tree starts from are those
+ *                     the reference's rebuild leaves (computeCost<true>), for
+ *                     imported trees too.  Needs a tree whose leaves hold
+ *                     every triangle once.
+ *   RQ_UPDATE_REFIT   boxes only, the tree's topology kept (the reference
+ *                     built with TREE_ROT 0).
+ * Not for two-level scenes (update the inner scenes, then create the
+ * two-level scene again).
+ */
+#define RQ_UPDATE_REFIT 0
+#define RQ_UPDATE_ROTATE 1
+RQ_API int rq_scene_update_vertices_ex(rq_scene* scene, const float* vertices, int n_vertices,
+                                       int mode);
+
+/* rq_scene_update_vertices_ex(..., RQ_UPDATE_REFIT). */
 RQ_API int rq_scene_update_vertices(rq_scene* scene, const float* vertices, int n_vertices);
+
+/*
+ * The state the next RQ_UPDATE_ROTATE starts from (DynBVH::costs and
+ * DynBVH::nextFree, DynBVH.h:105, 382): *next_free, and when `costs` is
+ * not NULL the first *next_free per-node costs (capacity >= *next_free).
+ * RQ_ERR_STATE before the scene's first rotating update.
+ */
+RQ_API int rq_scene_update_state(const rq_scene* scene, float* costs, int capacity,
+                                 int* next_free);
 
 /*
  * Mesh files.  rq_mesh_read_ply reads a PLY file (ascii or binary) the way
@@ -138,6 +167,7 @@ RQ_API int rq_mesh_copy(const rq_mesh* mesh, float* vertices, uint32_t* indices,
                         uint32_t* face_material);
 RQ_API int rq_mesh_destroy(rq_mesh* mesh);
 
+/* SAH cost of the scene's tree, DynBVH::computeCost<>(0) with C_isec=C_trav=1. */
 RQ_API int rq_scene_sah_cost(const rq_scene* scene, double* cost);
 
 /* Counts: internal records, leaves, maximum traversal depth. */

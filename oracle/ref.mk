@@ -160,11 +160,11 @@ $(OUT)/obj_sse/harness.o: $(HERE)ref_harness.cc $(OUT)/gen_sse/include/.stamp
 
 REPO := $(abspath $(HERE)..)
 
-$(OUT)/obj_nosse/harness_dropin.o: $(HERE)ref_harness.cc $(OUT)/gen_nosse/include/.stamp
+$(OUT)/obj_nosse/harness_dropin.o: $(HERE)ref_harness.cc $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(OUT)/gen_nosse/include/.stamp
 	@mkdir -p $(dir $@)
 	$(CXX) $(COMMON_FLAGS) -DMREF_DROPIN $(INC_NOSSE) -I$(REPO) -c $< -o $@
 
-$(OUT)/obj_nosse/GpuDynBVH.o: $(REPO)/rfmanta_b200/manta/GpuDynBVH.cc $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(OUT)/gen_nosse/include/.stamp
+$(OUT)/obj_nosse/GpuDynBVH.o: $(REPO)/rfmanta_b200/manta/GpuDynBVH.cc $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(REPO)/include/rfmanta_b200.h $(OUT)/gen_nosse/include/.stamp
 	@mkdir -p $(dir $@)
 	$(CXX) $(COMMON_FLAGS) $(INC_NOSSE) -I$(REPO) -c $< -o $@
 

@@ -298,6 +298,10 @@ int mref_scene_update_vertices(void* h, const float* verts, int nverts) {
     if (w) w->update();
   }
   s->bvh->update(0, 1);
+#ifdef MREF_DROPIN
+  // a scene rendering through the drop-in updates that tree as well
+  if (GpuDynBVH* g = dynamic_cast<GpuDynBVH*>(s->object)) g->update(0, 1);
+#endif
   return 0;
 }
 

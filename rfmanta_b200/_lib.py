@@ -27,6 +27,8 @@ RQ_TRI_KS = 1
 RQ_INST_TRANSLATE = 0
 RQ_PATH_EXTEND = 2
 RQ_PATH_SHADE = 3
+RQ_UPDATE_REFIT = 0
+RQ_UPDATE_ROTATE = 1
 RQ_INST_NESTED = 1
 RQ_CLOSEST = 0
 RQ_ANYHIT = 1
@@ -151,6 +153,8 @@ def _load():
         "rq_server_destroy": ([vp], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
         "rq_scene_update_vertices": ([vp, vp, i], i),
+        "rq_scene_update_vertices_ex": ([vp, vp, i, i], i),
+        "rq_scene_update_state": ([vp, vp, i, vp], i),
         "rq_mesh_read_ply": ([C.c_char_p, vp, C.c_uint32, C.POINTER(vp)], i),
         "rq_mesh_info": ([vp, C.POINTER(i), C.POINTER(i)], i),
         "rq_mesh_copy": ([vp, vp, vp, vp], i),

@@ -39,8 +39,9 @@ __device__ __forceinline__ void leaf_box(const float* __restrict__ verts,
       const float* p = verts + 3 * (size_t)__ldg(idx + 3 * (size_t)obj + k);
       for (int c = 0; c < 3; ++c) {
         const float x = __ldg(p + c);
-        lo[c] = init ? fminf(lo[c], x) : x;
-        hi[c] = init ? fmaxf(hi[c], x) : x;
+        // BBox::extendByPoint / extendByBox: Min(a, b) = a < b ? a : b
+        lo[c] = init ? (lo[c] < x ? lo[c] : x) : x;
+        hi[c] = init ? (hi[c] > x ? hi[c] : x) : x;
       }
       init = true;
     }
@@ -57,12 +58,13 @@ __device__ __forceinline__ void child_box(const float4* nodes, const float* vert
   }
   const float4* p = nodes + 4 * (size_t)ref;
   const float4 q0 = p[0], q1 = p[1], q2 = p[2];
-  lo[0] = fminf(q0.x, q1.z);
-  lo[1] = fminf(q0.y, q1.w);
-  lo[2] = fminf(q0.z, q2.x);
-  hi[0] = fmaxf(q0.w, q2.y);
-  hi[1] = fmaxf(q1.x, q2.z);
-  hi[2] = fmaxf(q1.y, q2.w);
+  // reset, extendByBox(left), extendByBox(right) with the reference's Min/Max
+  lo[0] = q0.x < q1.z ? q0.x : q1.z;
+  lo[1] = q0.y < q1.w ? q0.y : q1.w;
+  lo[2] = q0.z < q2.x ? q0.z : q2.x;
+  hi[0] = q0.w > q2.y ? q0.w : q2.y;
+  hi[1] = q1.x > q2.z ? q1.x : q2.z;
+  hi[2] = q1.y > q2.w ? q1.y : q2.w;
 }
 
 __global__ void refit_level_kernel(float4* nodes, const int32_t* __restrict__ level_recs,
@@ -99,6 +101,13 @@ __global__ void refit_root_kernel(const float4* nodes, int root_ref, const float
 
 int Scene::refresh_tree() const {
   if (!tree_stale) return RQ_OK;
+  if (tree_from_dyn) {
+    const int rc = refresh_tree_from_dyn(this);
+    if (rc != RQ_OK) return rc;
+    tree_from_dyn = false;
+    tree_stale = false;
+    return RQ_OK;
+  }
   std::vector<float4> recs((size_t)n_records * 4);
   if (n_records > 0 &&
       cudaMemcpy(recs.data(), d_nodes, recs.size() * sizeof(float4), cudaMemcpyDeviceToHost) !=
@@ -134,10 +143,19 @@ int Scene::refresh_tree() const {
 
 extern "C" int rq_scene_update_vertices(rq_scene* scene, const float* vertices,
                                         int n_vertices) {
+  return rq_scene_update_vertices_ex(scene, vertices, n_vertices, RQ_UPDATE_REFIT);
+}
+
+extern "C" int rq_scene_update_vertices_ex(rq_scene* scene, const float* vertices,
+                                           int n_vertices, int mode) {
   using namespace rq;
   Scene* s = scene;
   if (!s || !vertices) {
     set_error("NULL argument");
+    return RQ_ERR_ARG;
+  }
+  if (mode != RQ_UPDATE_REFIT && mode != RQ_UPDATE_ROTATE) {
+    set_error("unknown update mode");
     return RQ_ERR_ARG;
   }
   if (s->instanced) {
@@ -157,13 +175,23 @@ extern "C" int rq_scene_update_vertices(rq_scene* scene, const float* vertices,
     return RQ_ERR_CUDA;
   }
   std::lock_guard<std::mutex> g(s->frame_mu);
+  // a topology-keeping refit writes its boxes into the host tree's shape,
+  // which must be current if rotations changed it
+  if (mode == RQ_UPDATE_REFIT && s->tree_stale && s->tree_from_dyn) {
+    const int rc = s->refresh_tree();
+    if (rc != RQ_OK) return rc;
+  }
   const size_t nb = 3 * (size_t)n_vertices * sizeof(float);
   std::memcpy(s->verts.data(), vertices, nb);
-  float* d_root = nullptr;
   cudaError_t e = cudaMemcpy(s->d_verts, vertices, nb, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = launch_tri_setup(s->tri_kind, s->d_verts, s->d_idx, s->d_perm, s->n_leaf_tris,
-                         s->d_tris, 0);
+  if (e != cudaSuccess) {
+    set_error(std::string("refit: ") + cudaGetErrorString(e));
+    return RQ_ERR_CUDA;
+  }
+  if (mode == RQ_UPDATE_ROTATE) return rotate_update(s);
+  float* d_root = nullptr;
+  e = launch_tri_setup(s->tri_kind, s->d_verts, s->d_idx, s->d_perm, s->n_leaf_tris,
+                       s->d_tris, 0);
   const int nlev = (int)s->level_offsets.size() - 1;
   for (int k = 0; e == cudaSuccess && k < nlev; ++k) {
     const int a = s->level_offsets[k], n = s->level_offsets[k + 1] - a;
@@ -190,5 +218,7 @@ extern "C" int rq_scene_update_vertices(rq_scene* scene, const float* vertices,
     s->root_hi[c] = root[3 + c];
   }
   s->tree_stale = true;
+  s->tree_from_dyn = false;
+  if (s->dyn) rq::mark_dyn_bounds_stale(s->dyn);
   return RQ_OK;
 }

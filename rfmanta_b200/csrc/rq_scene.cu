@@ -80,6 +80,14 @@ void Scene::free_tree() {
   d_level_recs = nullptr;
   level_offsets.clear();
   rec_node.clear();
+  rec_depth.clear();
+  rec_size.clear();
+  rec_capacity = 0;
+  tree_costs.clear();
+  tree_next_free = 0;
+  destroy_dyn_tree(dyn);
+  dyn = nullptr;
+  tree_from_dyn = false;
   tree_stale = false;
   has_tree = false;
 }
@@ -172,6 +180,14 @@ int layout_tree(const HostTree& t, int n_objects, TreeLayout& L) {
   }
   L.rec_node = order;
   L.n_records = (int)order.size();
+  // subtree record counts: children come after their parent in pre-order
+  L.rec_size.assign(order.size(), 1);
+  for (size_t r = order.size(); r-- > 0;) {
+    int4 q3;
+    std::memcpy(&q3, &recs[4 * r + 3], sizeof(q3));
+    if (q3.x >= 0) L.rec_size[r] += L.rec_size[q3.x];
+    if (q3.y >= 0) L.rec_size[r] += L.rec_size[q3.y];
+  }
   L.n_leaves = 0;
   for (int i = 0; i < nn; ++i)
     if (seen[i] && t.children[i] != 0) ++L.n_leaves;
@@ -230,7 +246,12 @@ int Scene::set_tree(const HostTree& t) {
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return cuda_fail(e, "triangle setup");
   rec_node = L.rec_node;
+  rec_depth = L.rec_depth;
+  rec_size = L.rec_size;
+  rec_capacity = L.n_records;
   tree = t;
+  tree_sah_cost(t, &tree_costs);
+  tree_next_free = (int)t.children.size();
   n_records = L.n_records;
   n_leaf_tris = (int)perm.size();
   n_leaves = L.n_leaves;
@@ -259,7 +280,7 @@ static float box_area(const float* b) {
 
 // DynBVH::computeCost (DynBVH.cc:3389-3416) with C_isec = C_trav = 1,
 // bottom-up over the pre-order so no recursion is needed.
-double tree_sah_cost(const HostTree& t) {
+double tree_sah_cost(const HostTree& t, std::vector<float>* costs) {
   const int nn = (int)t.children.size();
   std::vector<int> order;
   std::vector<int> st(1, 0);
@@ -289,6 +310,7 @@ double tree_sah_cost(const HostTree& t) {
       cost[n] = 1.f + q;
     }
   }
+  if (costs) *costs = cost;
   return cost[0];
 }
 

@@ -20,6 +20,8 @@ struct PathScratch;
 void destroy_path_scratch(PathScratch* p);
 struct SampleScratch;
 void destroy_sample_scratch(SampleScratch* p);
+struct DynTree;
+void destroy_dyn_tree(DynTree* d);
 struct Scene;
 struct HostTree;
 cudaError_t launch_trace2(const Scene& s, const RayArgs& a, bool anyhit, int32_t* inst,
@@ -36,7 +38,9 @@ struct HostTree {
   std::vector<int32_t> ids;  // object_ids, one per triangle
 };
 
-double tree_sah_cost(const HostTree& t);
+// DynBVH::computeCost (DynBVH.cc:3389-3416); with `costs`, every reachable
+// node's cost as computeCost<true> leaves it (others 0).
+double tree_sah_cost(const HostTree& t, std::vector<float>* costs = nullptr);
 
 // A validated tree laid out for the kernels: node records (4 float4 each,
 // depth-first pre-order) and the leaf-ordered object permutation (bit 31 on
@@ -46,6 +50,7 @@ struct TreeLayout {
   std::vector<int32_t> perm;
   std::vector<int32_t> rec_node;   // DynBVH node id of each record
   std::vector<int32_t> rec_depth;  // depth of each record (root = 0)
+  std::vector<int32_t> rec_size;   // records in each record's subtree
   int n_records = 0;
   int n_leaves = 0;
   int root_ref = 0;
@@ -90,6 +95,15 @@ struct Scene {
   int32_t* d_level_recs = nullptr;
   std::vector<int> level_offsets;
   std::vector<int32_t> rec_node;
+  std::vector<int32_t> rec_depth;  // of the layout set_tree made
+  std::vector<int32_t> rec_size;
+  int rec_capacity = 0;             // records d_nodes / d_level_recs hold
+  // rotating update (rq_rotate.cu): DynBVH::costs as a rebuild leaves them,
+  // DynBVH::nextFree, and the device node arrays once an update has run
+  std::vector<float> tree_costs;
+  int tree_next_free = 0;
+  DynTree* dyn = nullptr;
+  mutable bool tree_from_dyn = false;  // stale host tree: read dyn, not records
   float4* d_nodes = nullptr;
   float4* d_tris = nullptr;
   int n_records = 0;
@@ -143,6 +157,11 @@ struct Scene {
                    bool anyhit, float* t, int32_t* prim, float* u, float* v,
                    cudaStream_t st, int* counter);
 };
+
+int rotate_update(Scene* s);
+void mark_dyn_bounds_stale(DynTree* d);
+int refresh_tree_from_dyn(const Scene* s);
+int dyn_state(const Scene* s, float* costs, int cap, int* next_free);
 
 }  // namespace rq
 

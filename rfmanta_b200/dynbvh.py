@@ -18,7 +18,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import RQ_ANYHIT, RQ_CLOSEST, RQ_TRI_KS, RQ_TRI_WALD, check, lib
+from ._lib import (RQ_ANYHIT, RQ_CLOSEST, RQ_TRI_KS, RQ_TRI_WALD, RQ_UPDATE_REFIT,
+                   RQ_UPDATE_ROTATE, check, lib)
 from .scenes import Mesh
 
 T_EPSILON = np.float32(1.e-4)
@@ -114,14 +115,26 @@ class GpuDynBVH:
             self._upload()
         check(lib.rq_scene_build(self._h, bins))
 
-    def update(self) -> None:
-        """DynBVH::update: the group's vertices moved (same triangles); the
-        tree keeps its topology and is refitted on the GPU."""
+    def update(self, rotate: bool = True) -> None:
+        """DynBVH::update: the group's vertices moved (same triangles).
+        rotate=True is the reference's update as it ships (refit, leaf
+        re-splits and tree rotations, TREE_ROT 1); rotate=False refits the
+        boxes and keeps the topology (TREE_ROT 0).  Both run on the GPU."""
         if self._dirty or not self._h:
             self.rebuild()
             return
         v = np.ascontiguousarray(self._group.vertices, np.float32)
-        check(lib.rq_scene_update_vertices(self._h, _p(v), v.shape[0]))
+        mode = RQ_UPDATE_ROTATE if rotate else RQ_UPDATE_REFIT
+        check(lib.rq_scene_update_vertices_ex(self._h, _p(v), v.shape[0], mode))
+
+    def update_state(self):
+        """(costs, next_free): DynBVH::costs and DynBVH::nextFree, the state
+        the next rotating update starts from."""
+        nf = C.c_int()
+        check(lib.rq_scene_update_state(self._h, None, 0, C.byref(nf)))
+        costs = np.zeros(nf.value, np.float32)
+        check(lib.rq_scene_update_state(self._h, _p(costs), costs.shape[0], C.byref(nf)))
+        return costs, nf.value
 
     def importTree(self, tree) -> None:
         """Reference tree given field by field (oracle Tree or compatible)."""

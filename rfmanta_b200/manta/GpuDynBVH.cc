@@ -80,8 +80,9 @@ void GpuDynBVH::rebuild(int proc, int numProcs) {
   check(rq_scene_build(scene, 0), "build");
 }
 
-// DynBVH::update (DynBVH.cc:1574-1581): the mesh moved, the topology
-// stays; the device refits the tree to the new vertex positions.
+// DynBVH::update (DynBVH.cc:1574-1581): the mesh moved; the device refits
+// the tree and applies the reference's leaf re-splits and tree rotations
+// (TREE_ROT 1, rotateNode DynBVH.cc:3051-3348).
 void GpuDynBVH::update(int proc, int numProcs) {
   (void)numProcs;
   if (proc != 0) return;
@@ -93,7 +94,8 @@ void GpuDynBVH::update(int proc, int numProcs) {
   std::vector<float> v(3 * nv);
   for (size_t i = 0; i < nv; ++i)
     for (int c = 0; c < 3; ++c) v[3 * i + c] = mesh->vertices[i][c];
-  check(rq_scene_update_vertices(scene, v.empty() ? 0 : &v[0], (int)nv), "refit");
+  check(rq_scene_update_vertices_ex(scene, v.empty() ? 0 : &v[0], (int)nv, RQ_UPDATE_ROTATE),
+        "update");
 }
 
 bool GpuDynBVH::buildFromFile(const std::string& file) {

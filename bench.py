@@ -768,7 +768,91 @@ def rays_or(x):
     return max(int(x), 1)
 
 
+class AnimatedFrame(SmallFrame):
+    """The 512x512 Whitted frame of a moving mesh: every step first moves
+    the vertices (a periodic 8-frame wave, the positions resident on the
+    device) and updates the tree as DynBVH::update does (refit, leaf
+    re-splits, tree rotations), then renders."""
+    name = "animated_frame"
+    PERIOD = 8
+
+    def __init__(self):
+        super().__init__()
+        from rfmanta_b200 import scenes
+        self.v0 = self.sc.mesh.vertices.copy()
+        self.poses = [scenes.wave_vertices(self.v0, k, self.PERIOD) for k in range(self.PERIOD)]
+        self.k = 0
+
+    def config(self):
+        c = super().config()
+        c.update({"workload": self.name,
+                  "update": "DynBVH::update with tree rotations and leaf re-splits every frame",
+                  "animation": f"periodic wave, {self.PERIOD} poses, amplitude 0.01",
+                  "vertices": int(self.v0.shape[0])})
+        return c
+
+    def setup(self, bvh, dev):
+        import torch
+        super().setup(bvh, dev)
+        # (3 floats per vertex, row-major: the library reads a plain array)
+        self.dev_poses = [torch.from_numpy(np.ascontiguousarray(v)).to(dev).contiguous()
+                          for v in self.poses]
+        self.host_poses = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+                           for v in self.poses]
+        self.sc.mesh.vertices = self.poses[0]
+        bvh.update()
+        info = bvh.info()
+        # kernels per step: 2 for the frame; the update's object boxes, leaf
+        # boxes, re-splits, 2 scan kernels, relocation, rotations, frontier
+        # root, one relayout per tree level and the triangle records
+        self.launches = 2 + 9 + int(info.depth)
+
+    def frame(self, stream_ptr):
+        k = self.k % self.PERIOD
+        self.k += 1
+        self.sc.mesh.vertices = self.poses[k]
+        self.bvh.update_device(self.dev_poses[k].data_ptr(), rotate=True, stream=stream_ptr)
+        super().frame(stream_ptr)
+
+    def host_frame(self):
+        from rfmanta_b200 import _lib
+        k = self.k % self.PERIOD
+        self.k += 1
+        v = self.host_poses[k]
+        self.sc.mesh.vertices = self.poses[k]
+        _lib.check(_lib.lib.rq_scene_update_vertices_ex(self.bvh.handle, C.c_void_p(v.data_ptr()),
+                                                        v.shape[0], _lib.RQ_UPDATE_ROTATE))
+        h2d, d2h = super().host_frame()
+        return h2d + v.numel() * 4, d2h
+
+    def cpu_reference(self, seconds_budget, threads):
+        from oracle.pyoracle import Reference
+        sse = Reference.available(sse=True)
+        ref = Reference(sse=sse)
+        rs = ref.scene(self.sc.mesh, 0)
+        frames, secs, rays, upd = 0, 0.0, 0, 0.0
+        while frames < 2 or secs < seconds_budget:
+            v = self.poses[frames % self.PERIOD]
+            t0 = time.perf_counter()
+            rs.update_vertices(v)
+            du = time.perf_counter() - t0
+            self.sc.mesh.vertices = v
+            out = rs.render(self.sc, nthreads=threads, want_ids=False)
+            secs += du + out["seconds"]
+            upd += du
+            rays += self.sc.xres * self.sc.yres + out["shadow_rays"]
+            frames += 1
+        rs.close()
+        self.sc.mesh.vertices = self.v0
+        text = (f"{frames} full {self.sc.xres}x{self.sc.yres} animated frame(s): reference "
+                f"DynBVH::update(0, 1) (single-threaded, {1e3 * upd / frames:.1f} ms per frame) "
+                f"then Raytracer/DynBVH/WaldTriangle/Lambertian/HardShadows on {threads} "
+                f"thread(s) ({'MANTA_SSE' if sse else 'scalar'} build)")
+        return rays / secs / 1e6, threads, text, secs
+
+
 WORKLOADS = {"path_frame": PathFrame, "small_frame": SmallFrame,
+             "animated_frame": AnimatedFrame,
              "coherent_frame": CoherentFrame,
              "batched_queries": BatchedQueriesWL, "serving": ServingWL}
 

@@ -137,6 +137,13 @@ RQ_API int rq_scene_build(rq_scene* scene, int bins);
 RQ_API int rq_scene_update_vertices_ex(rq_scene* scene, const float* vertices, int n_vertices,
                                        int mode);
 
+/* rq_scene_update_vertices_ex with the new positions in device memory
+ * (3 * n_vertices floats on the scene's device), copied on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream); returns when the tree is
+ * updated. */
+RQ_API int rq_scene_update_vertices_device(rq_scene* scene, const float* d_vertices,
+                                           int n_vertices, int mode, void* stream);
+
 /* rq_scene_update_vertices_ex(..., RQ_UPDATE_REFIT). */
 RQ_API int rq_scene_update_vertices(rq_scene* scene, const float* vertices, int n_vertices);
 

@@ -154,6 +154,7 @@ def _load():
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
         "rq_scene_update_vertices": ([vp, vp, i], i),
         "rq_scene_update_vertices_ex": ([vp, vp, i, i], i),
+        "rq_scene_update_vertices_device": ([vp, vp, i, i, vp], i),
         "rq_scene_update_state": ([vp, vp, i, vp], i),
         "rq_mesh_read_ply": ([C.c_char_p, vp, C.c_uint32, C.POINTER(vp)], i),
         "rq_mesh_info": ([vp, C.POINTER(i), C.POINTER(i)], i),

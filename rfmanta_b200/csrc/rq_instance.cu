@@ -173,7 +173,9 @@ int rq_scene_create_instanced(rq_scene* const* inner, int n_inner, const int32_t
   std::vector<uint32_t> idx(3 * (size_t)n_instances);
   std::vector<float> vb(6 * (size_t)n_inner);
   for (int i = 0; i < n_inner; ++i) {
-    const std::vector<float>& v = inner[i]->verts;
+    const std::vector<float>* hv = inner[i]->host_vertices();
+    if (!hv) return ifail(RQ_ERR_CUDA, "reading an inner scene's vertices");
+    const std::vector<float>& v = *hv;
     for (int c = 0; c < 3; ++c) {
       vb[6 * i + c] = v[c];
       vb[6 * i + 3 + c] = v[c];

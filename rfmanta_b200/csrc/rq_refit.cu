@@ -141,15 +141,48 @@ int Scene::refresh_tree() const {
 
 }  // namespace rq
 
-extern "C" int rq_scene_update_vertices(rq_scene* scene, const float* vertices,
-                                        int n_vertices) {
-  return rq_scene_update_vertices_ex(scene, vertices, n_vertices, RQ_UPDATE_REFIT);
+namespace rq {
+namespace {
+
+// The update after the new positions are in the scene's device vertices.
+int update_tree(Scene* s, int mode) {
+  if (mode == RQ_UPDATE_ROTATE) return rotate_update(s);
+  cudaError_t e = launch_tri_setup(s->tri_kind, s->d_verts, s->d_idx, s->d_perm,
+                                   s->n_leaf_tris, s->d_tris, 0);
+  const int nlev = (int)s->level_offsets.size() - 1;
+  for (int k = 0; e == cudaSuccess && k < nlev; ++k) {
+    const int a = s->level_offsets[k], n = s->level_offsets[k + 1] - a;
+    if (n <= 0) continue;
+    refit_level_kernel<<<(n + 127) / 128, 128>>>(s->d_nodes, s->d_level_recs + a, n,
+                                                 s->d_verts, s->d_idx, s->d_perm);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && !s->d_root_box) e = cudaMalloc(&s->d_root_box, 6 * sizeof(float));
+  if (e == cudaSuccess) {
+    refit_root_kernel<<<1, 1>>>(s->d_nodes, s->root_ref, s->d_verts, s->d_idx, s->d_perm,
+                                s->d_root_box);
+    e = cudaGetLastError();
+  }
+  float root[6];
+  if (e == cudaSuccess)
+    e = cudaMemcpy(root, s->d_root_box, sizeof(root), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    set_error(std::string("refit: ") + cudaGetErrorString(e));
+    return RQ_ERR_CUDA;
+  }
+  for (int c = 0; c < 3; ++c) {
+    s->root_lo[c] = root[c];
+    s->root_hi[c] = root[3 + c];
+  }
+  s->tree_stale = true;
+  s->tree_from_dyn = false;
+  if (s->dyn) mark_dyn_bounds_stale(s->dyn);
+  return RQ_OK;
 }
 
-extern "C" int rq_scene_update_vertices_ex(rq_scene* scene, const float* vertices,
-                                           int n_vertices, int mode) {
-  using namespace rq;
-  Scene* s = scene;
+// Argument and state checks shared by both entry points; takes the lock
+// and brings the host tree up to date where a refit needs it.
+int update_begin(Scene* s, const void* vertices, int n_vertices, int mode) {
   if (!s || !vertices) {
     set_error("NULL argument");
     return RQ_ERR_ARG;
@@ -174,51 +207,61 @@ extern "C" int rq_scene_update_vertices_ex(rq_scene* scene, const float* vertice
     set_error("cudaSetDevice");
     return RQ_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> g(s->frame_mu);
   // a topology-keeping refit writes its boxes into the host tree's shape,
   // which must be current if rotations changed it
-  if (mode == RQ_UPDATE_REFIT && s->tree_stale && s->tree_from_dyn) {
-    const int rc = s->refresh_tree();
-    if (rc != RQ_OK) return rc;
+  if (mode == RQ_UPDATE_REFIT && s->tree_stale && s->tree_from_dyn) return s->refresh_tree();
+  return RQ_OK;
+}
+
+}  // namespace
+}  // namespace rq
+
+extern "C" int rq_scene_update_vertices(rq_scene* scene, const float* vertices,
+                                        int n_vertices) {
+  return rq_scene_update_vertices_ex(scene, vertices, n_vertices, RQ_UPDATE_REFIT);
+}
+
+extern "C" int rq_scene_update_vertices_ex(rq_scene* scene, const float* vertices,
+                                           int n_vertices, int mode) {
+  using namespace rq;
+  Scene* s = scene;
+  if (!s) {
+    set_error("NULL argument");
+    return RQ_ERR_ARG;
   }
+  std::lock_guard<std::mutex> g(s->frame_mu);
+  int rc = update_begin(s, vertices, n_vertices, mode);
+  if (rc != RQ_OK) return rc;
   const size_t nb = 3 * (size_t)n_vertices * sizeof(float);
   std::memcpy(s->verts.data(), vertices, nb);
-  cudaError_t e = cudaMemcpy(s->d_verts, vertices, nb, cudaMemcpyHostToDevice);
+  s->verts_stale = false;
+  const cudaError_t e = cudaMemcpy(s->d_verts, vertices, nb, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
-    set_error(std::string("refit: ") + cudaGetErrorString(e));
+    set_error(std::string("update: ") + cudaGetErrorString(e));
     return RQ_ERR_CUDA;
   }
-  if (mode == RQ_UPDATE_ROTATE) return rotate_update(s);
-  float* d_root = nullptr;
-  e = launch_tri_setup(s->tri_kind, s->d_verts, s->d_idx, s->d_perm, s->n_leaf_tris,
-                       s->d_tris, 0);
-  const int nlev = (int)s->level_offsets.size() - 1;
-  for (int k = 0; e == cudaSuccess && k < nlev; ++k) {
-    const int a = s->level_offsets[k], n = s->level_offsets[k + 1] - a;
-    if (n <= 0) continue;
-    refit_level_kernel<<<(n + 127) / 128, 128>>>(s->d_nodes, s->d_level_recs + a, n,
-                                                 s->d_verts, s->d_idx, s->d_perm);
-    e = cudaGetLastError();
+  return update_tree(s, mode);
+}
+
+extern "C" int rq_scene_update_vertices_device(rq_scene* scene, const float* d_vertices,
+                                               int n_vertices, int mode, void* stream) {
+  using namespace rq;
+  Scene* s = scene;
+  if (!s) {
+    set_error("NULL argument");
+    return RQ_ERR_ARG;
   }
-  if (e == cudaSuccess) e = cudaMalloc(&d_root, 6 * sizeof(float));
-  if (e == cudaSuccess) {
-    refit_root_kernel<<<1, 1>>>(s->d_nodes, s->root_ref, s->d_verts, s->d_idx, s->d_perm,
-                                d_root);
-    e = cudaGetLastError();
-  }
-  float root[6];
-  if (e == cudaSuccess) e = cudaMemcpy(root, d_root, sizeof(root), cudaMemcpyDeviceToHost);
-  cudaFree(d_root);
+  std::lock_guard<std::mutex> g(s->frame_mu);
+  int rc = update_begin(s, d_vertices, n_vertices, mode);
+  if (rc != RQ_OK) return rc;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t nb = 3 * (size_t)n_vertices * sizeof(float);
+  cudaError_t e = cudaMemcpyAsync(s->d_verts, d_vertices, nb, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
-    set_error(std::string("refit: ") + cudaGetErrorString(e));
+    set_error(std::string("update: ") + cudaGetErrorString(e));
     return RQ_ERR_CUDA;
   }
-  for (int c = 0; c < 3; ++c) {
-    s->root_lo[c] = root[c];
-    s->root_hi[c] = root[3 + c];
-  }
-  s->tree_stale = true;
-  s->tree_from_dyn = false;
-  if (s->dyn) rq::mark_dyn_bounds_stale(s->dyn);
-  return RQ_OK;
+  s->verts_stale = true;
+  return update_tree(s, mode);
 }

@@ -69,7 +69,19 @@ Scene::~Scene() {
   if (prev >= 0) cudaSetDevice(prev);
 }
 
+const std::vector<float>* Scene::host_vertices() const {
+  if (verts_stale) {
+    if (cudaMemcpy(verts.data(), d_verts, verts.size() * sizeof(float),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      return nullptr;
+    verts_stale = false;
+  }
+  return &verts;
+}
+
 void Scene::free_tree() {
+  if (d_root_box) cudaFree(d_root_box);
+  d_root_box = nullptr;
   if (d_nodes) cudaFree(d_nodes);
   if (d_tris) cudaFree(d_tris);
   if (d_perm) cudaFree(d_perm);

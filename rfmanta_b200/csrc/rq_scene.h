@@ -77,7 +77,8 @@ struct Scene {
   int n_tris = 0;
   int n_verts = 0;
   int num_sms = 148;
-  std::vector<float> verts;
+  mutable std::vector<float> verts;  // host mirror; stale after a device-side update
+  mutable bool verts_stale = false;
   std::vector<uint32_t> idx;
   std::vector<uint32_t> face_mat;
   float* d_verts = nullptr;
@@ -106,6 +107,7 @@ struct Scene {
   mutable bool tree_from_dyn = false;  // stale host tree: read dyn, not records
   float4* d_nodes = nullptr;
   float4* d_tris = nullptr;
+  float* d_root_box = nullptr;  // refit output: the root's box
   int n_records = 0;
   int n_leaves = 0;
   int n_leaf_tris = 0;
@@ -149,6 +151,7 @@ struct Scene {
   void free_tree();
   int set_tree(const HostTree& t);
   int refresh_tree() const;  // host tree bounds from the device records
+  const std::vector<float>* host_vertices() const;  // NULL on a copy failure
   DevScene dev() const;
   Staging* acquire(size_t bytes_in, size_t bytes_out);
   void release(Staging* s);

@@ -127,6 +127,17 @@ class GpuDynBVH:
         mode = RQ_UPDATE_ROTATE if rotate else RQ_UPDATE_REFIT
         check(lib.rq_scene_update_vertices_ex(self._h, _p(v), v.shape[0], mode))
 
+    def update_device(self, vertices_ptr: int, rotate: bool = True, stream: int = 0) -> None:
+        """update() with the new vertex positions already in device memory:
+        a row-major array of 3 floats per vertex of the group (for a torch
+        tensor, pass .contiguous().data_ptr())."""
+        if self._dirty or not self._h:
+            raise _lib.RQError(_lib.RQ_ERR_STATE, "no scene on the device to update")
+        mode = RQ_UPDATE_ROTATE if rotate else RQ_UPDATE_REFIT
+        check(lib.rq_scene_update_vertices_device(self._h, C.c_void_p(vertices_ptr),
+                                                  self._group.vertices.shape[0], mode,
+                                                  C.c_void_p(stream)))
+
     def update_state(self):
         """(costs, next_free): DynBVH::costs and DynBVH::nextFree, the state
         the next rotating update starts from."""

@@ -260,8 +260,17 @@ def animated_vertices(v0: np.ndarray, frame: int, amplitude: float = 0.04,
     plus per-vertex noise (the animated-mesh refit workload)."""
     rng = np.random.default_rng(seed + frame)
     w = np.sin(3.0 * v0[:, [1, 2, 0]] + 0.7 * frame).astype(np.float32)
-    return (v0 + np.float32(amplitude * (1 + frame)) * w +
-            rng.normal(scale=jitter, size=v0.shape)).astype(np.float32)
+    return np.ascontiguousarray(v0 + np.float32(amplitude * (1 + frame)) * w +
+                                rng.normal(scale=jitter, size=v0.shape), np.float32)
+
+
+def wave_vertices(v0: np.ndarray, frame: int, period: int = 8,
+                  amplitude: float = 0.01) -> np.ndarray:
+    """Frame `frame` of a periodic non-rigid animation (a travelling sine
+    displacement, `period` frames long) for benchmarking animated scenes."""
+    ph = np.float32(2.0 * np.pi * (frame % period) / period)
+    w = np.sin(np.float32(3.0) * v0[:, [1, 2, 0]] + ph).astype(np.float32)
+    return np.ascontiguousarray(v0 + np.float32(amplitude) * w, np.float32)
 
 
 def random_rays(n: int, lo: np.ndarray, hi: np.ndarray, seed: int,

@@ -222,3 +222,34 @@ def test_dropin_renders_after_update(tmp_path):
         assert got["shadow_rays"] == want["shadow_rays"]
         assert np.array_equal(got["prim"], want["prim"])
         assert np.array_equal(_bits(got["rgb"]), _bits(want["rgb"]))
+
+
+def test_update_from_device_vertices_equals_host_update():
+    """rq_scene_update_vertices_device gives the tree the host-pointer call
+    gives, and the scene's host copy of the vertices follows (it feeds the
+    instance boxes of a two-level scene built on it)."""
+    import torch
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH, InstancedBVH
+    sc = scenes.tiny_frame_scene()
+    v0 = sc.mesh.vertices.copy()
+    from oracle.pyoracle import Tree
+    from rfmanta_b200.treeio import parse_dynbvh_blob
+    a, b = GpuDynBVH(), GpuDynBVH()
+    a.setGroup(sc.mesh)
+    a.rebuild()
+    f0 = parse_dynbvh_blob(a.exportBlob(), sc.mesh.n_tris)
+    b.setGroup(sc.mesh)
+    b.importTree(Tree(f0.bounds, f0.child, f0.children, f0.axis, f0.left_cheaper, f0.ids))
+    for k in (1, 2, 3):
+        v = scenes.animated_vertices(v0, k)
+        sc.mesh.vertices = v
+        a.update(rotate=k != 2)
+        dv = torch.from_numpy(v).cuda()
+        b.update_device(dv.data_ptr(), rotate=k != 2)
+        torch.cuda.synchronize()
+        assert a.exportBlob() == b.exportBlob()
+    top = InstancedBVH([b], np.array([0], np.int32), np.zeros((1, 3), np.float32))
+    top.rebuild()
+    t = parse_dynbvh_blob(top.exportBlob(), 1)
+    assert np.array_equal(t.bounds[0, :3], v.min(0)) and np.array_equal(t.bounds[0, 3:], v.max(0))

@@ -801,11 +801,11 @@ class AnimatedFrame(SmallFrame):
                            for v in self.poses]
         self.sc.mesh.vertices = self.poses[0]
         bvh.update()
-        info = bvh.info()
-        # kernels per step: 2 for the frame; the update's object boxes, leaf
-        # boxes, re-splits, 2 scan kernels, relocation, rotations, frontier
-        # root, one relayout per tree level and the triangle records
-        self.launches = 2 + 9 + int(info.depth)
+        # kernels per step: 2 for the frame; the update's state reset, object
+        # boxes, leaf boxes, re-splits, 2 scan kernels, relocation, next-free
+        # advance, rotations, parents, 1 + 9 pointer-jumping rounds, records
+        # and the triangle records
+        self.launches = 2 + 21
 
     def frame(self, stream_ptr):
         k = self.k % self.PERIOD

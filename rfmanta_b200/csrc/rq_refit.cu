@@ -207,9 +207,16 @@ int update_begin(Scene* s, const void* vertices, int n_vertices, int mode) {
     set_error("cudaSetDevice");
     return RQ_ERR_CUDA;
   }
-  // a topology-keeping refit writes its boxes into the host tree's shape,
-  // which must be current if rotations changed it
-  if (mode == RQ_UPDATE_REFIT && s->tree_stale && s->tree_from_dyn) return s->refresh_tree();
+  // a topology-keeping refit writes its boxes into the host tree's shape and
+  // walks the records level by level: both must be current if rotations
+  // changed the tree
+  if (mode == RQ_UPDATE_REFIT) {
+    if (s->tree_stale && s->tree_from_dyn) {
+      const int rc = s->refresh_tree();
+      if (rc != RQ_OK) return rc;
+    }
+    return sync_layout_host(s);
+  }
   return RQ_OK;
 }
 

@@ -52,6 +52,15 @@
 
 namespace rq {
 
+// Results of an update on the device, read back once at its end.
+struct UpdState {
+  int next_free;
+  int error;  // 1: node capacity, 2: deeper than the traversal stack, 3: record capacity
+  int n_records;
+  int depth;
+  float root[6];
+};
+
 // Device state of the rotating update: the reference's node array with
 // room for `cap` nodes, per-node costs and subtree counts, object boxes,
 // re-split scratch, and the record metadata of the current layout.
@@ -92,10 +101,10 @@ struct DynTree {
   int32_t* rec_node = nullptr;
   int32_t* rec_depth = nullptr;
   int32_t* rec_size = nullptr;
-  int32_t* fr_pos = nullptr;
-  int32_t* fr_rec = nullptr;
-  int32_t* fr_off = nullptr;
-  int32_t* counter = nullptr;
+  int32_t* tpos = nullptr;  // the tree's positions before the re-splits
+  int32_t* jump[8] = {};     // pointer-jumping buffers (anc, rec, off, dep) x 2
+  UpdState* st = nullptr;
+  bool layout_host_stale = false;  // host rec_node / level lists behind the device
   void* scan_tmp = nullptr;
   size_t scan_bytes = 0;
   std::vector<void*> allocs;
@@ -209,8 +218,10 @@ __device__ void leaf_bounds(DynView V, int c) {
 }
 
 // One thread per (record, side): the child's parent, and its box if a leaf.
-__global__ void leaf_pass_kernel(DynView V, const int32_t* __restrict__ rec_node, int n_records) {
+__global__ void leaf_pass_kernel(DynView V, const int32_t* __restrict__ rec_node, int n_records,
+                                 int32_t* tpos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) tpos[0] = 0;
   if (n_records == 0) {
     if (i == 0) {
       leaf_bounds(V, 0);
@@ -221,6 +232,7 @@ __global__ void leaf_pass_kernel(DynView V, const int32_t* __restrict__ rec_node
   if (i >= 2 * n_records) return;
   const int node = rec_node[i >> 1];
   const int c = V.child[node] + (i & 1);
+  tpos[i + 1] = c;
   V.parent[c] = node;
   if ((i & 1) == 0) V.arrive[node] = 0;
   if (node == 0 && (i & 1) == 0) V.parent[0] = -1;
@@ -493,7 +505,8 @@ __global__ void relocate_kernel(DynView V, Scratch S, const int32_t* __restrict_
                                 const int32_t* __restrict__ slot_count,
                                 const int32_t* __restrict__ slot_off,
                                 const int32_t* __restrict__ split_axis,
-                                const int32_t* __restrict__ split_nint, int next_free) {
+                                const int32_t* __restrict__ split_nint, int next_free,
+                                int cap, UpdState* st) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 2 * n_records) return;
   const int r = i >> 1, side = i & 1;
@@ -501,6 +514,10 @@ __global__ void relocate_kernel(DynView V, Scratch S, const int32_t* __restrict_
   const int count = slot_count[key];
   if (count == 0) return;
   const int base = next_free + slot_off[key];
+  if ((long long)base + count > cap) {
+    st->error = 1;
+    return;
+  }
   const int node = rec_node[r];
   const int c = V.child[node] + side;
   const int b = V.child[c];
@@ -785,71 +802,156 @@ __global__ void rotate_kernel(DynView D, const float4* __restrict__ recs,
 }
 
 // ------------------------------------------------- 5. relayout ---------
+//
+// The records are numbered in pre-order of the internal nodes and the
+// leaves' objects placed in pre-order, both known from the subtree counts:
+// a node's record number is the sum over the edges from the root of
+// 1 (+ the internal nodes of the left sibling for a right child), its first
+// object the sum of the left siblings' object counts.  Those sums along the
+// path to the root are formed by pointer jumping (each round adds the
+// ancestor's partial sum and jumps to the ancestor's ancestor), so the whole
+// layout takes a fixed number of launches and no host round trip.
+// The tree's positions: 0, the children of the records before the update,
+// and the pairs the re-splits added (next_free before .. after).
 
-// One tree level: each internal node of the frontier writes its record
-// (pre-order number known from the subtree counts), places its leaf
-// children's objects and queues its internal children.
-__global__ void relayout_level_kernel(DynView V, const int32_t* __restrict__ fr_pos,
-                                      const int32_t* __restrict__ fr_rec,
-                                      const int32_t* __restrict__ fr_off, int n, int depth,
-                                      int32_t* next_pos, int32_t* next_rec, int32_t* next_off,
-                                      int* next_count, int next_room, float4* recs,
-                                      int32_t* perm, int n_objs, int32_t* rec_node,
-                                      int32_t* rec_depth, int32_t* rec_size, int rec_cap) {
-  // next_room: frontier slots left after this level; a tree whose counts
-  // disagree with its shape is caught on the host (record total)
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int pos = fr_pos[i], rec = fr_rec[i], off = fr_off[i];
-  const int L = V.child[pos];
-  int ref[2];
-  int r_next = rec + 1, o_next = off;
-  for (int s = 0; s < 2; ++s) {
-    const int c = L + s;
-    const int k = V.children[c];
-    if (k != 0) {
-      const int first = V.child[c];
-      for (int j = 0; j < k && o_next + j < n_objs; ++j) {
-        const int obj = V.ids[first + j];
-        perm[o_next + j] = j == k - 1 ? (int32_t)(obj | 0x80000000u) : obj;
-      }
-      ref[s] = ~o_next;
-    } else {
-      ref[s] = r_next;
-      const int q = atomicAdd(next_count, 1);
-      if (q < next_room) {
-        next_pos[q] = c;
-        next_rec[q] = r_next;
-        next_off[q] = o_next;
-      }
-      r_next += V.n_int[c];
-    }
-    o_next += V.n_obj[c];
+struct Jump {
+  int32_t* anc;
+  int32_t* rec;
+  int32_t* off;
+  int32_t* dep;
+};
+
+__device__ __forceinline__ int tree_position(int i, const int32_t* __restrict__ tpos, int m_old,
+                                             int nf_old, const UpdState* st) {
+  if (i < m_old) return tpos[i];
+  const int p = nf_old + (i - m_old);
+  return p < st->next_free ? p : -1;
+}
+
+__global__ void init_state_kernel(UpdState* st, int next_free) {
+  st->next_free = next_free;
+  st->error = 0;
+  st->n_records = 0;
+  st->depth = 0;
+}
+
+// The re-splits' pairs land after next_free; advance it (one thread).
+__global__ void advance_kernel(const int32_t* __restrict__ slot_count,
+                               const int32_t* __restrict__ slot_off, int n_slots, int cap,
+                               UpdState* st) {
+  const long long total =
+      n_slots > 0 ? (long long)slot_off[n_slots - 1] + slot_count[n_slots - 1] : 0;
+  if (st->next_free + total > cap) {
+    st->error = 1;
+    return;
   }
-  if (rec >= rec_cap) return;
-  const float* bl = V.bounds + 6 * (size_t)L;
-  const float* br = V.bounds + 6 * (size_t)(L + 1);
-  float4* p = recs + 4 * (size_t)rec;
-  p[0] = make_float4(bl[0], bl[1], bl[2], bl[3]);
-  p[1] = make_float4(bl[4], bl[5], br[0], br[1]);
-  p[2] = make_float4(br[2], br[3], br[4], br[5]);
-  const int meta = (V.axis[pos] & 3) | ((V.lc[pos] & 1) << 2);
-  reinterpret_cast<int4*>(p)[3] = make_int4(ref[0], ref[1], meta, 0);
-  rec_node[rec] = pos;
-  rec_depth[rec] = depth;
-  rec_size[rec] = V.n_int[pos];
+  st->next_free += (int)total;
 }
 
-// A tree that is a single leaf: all objects in its order.
-__global__ void leaf_root_perm_kernel(const int32_t* __restrict__ ids, int n, int32_t* perm) {
+__global__ void parent_pass_kernel(DynView V, const int32_t* __restrict__ tpos, int m_old,
+                                   int nf_old, const UpdState* st, int m_max) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) perm[i] = i == n - 1 ? (int32_t)(ids[i] | 0x80000000u) : ids[i];
+  if (i >= m_max) return;
+  const int p = tree_position(i, tpos, m_old, nf_old, st);
+  if (p < 0) return;
+  if (p == 0) V.parent[0] = -1;
+  if (V.children[p] == 0) {
+    const int c = V.child[p];
+    V.parent[c] = p;
+    V.parent[c + 1] = p;
+  }
 }
 
-__global__ void frontier_root_kernel(int32_t* fr_pos, int32_t* fr_rec, int32_t* fr_off) {
-  fr_pos[0] = 0;
-  fr_rec[0] = 0;
-  fr_off[0] = 0;
+__global__ void jump_init_kernel(DynView V, const int32_t* __restrict__ tpos, int m_old,
+                                 int nf_old, const UpdState* st, int m_max, Jump J) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m_max) return;
+  const int p = tree_position(i, tpos, m_old, nf_old, st);
+  if (p < 0) return;
+  if (p == 0) {
+    J.anc[0] = -1;
+    J.rec[0] = J.off[0] = J.dep[0] = 0;
+    return;
+  }
+  const int y = V.parent[p];
+  const int left = V.child[y];
+  const bool right = p == left + 1;
+  J.anc[p] = y;
+  J.rec[p] = 1 + (right ? V.n_int[left] : 0);
+  J.off[p] = right ? V.n_obj[left] : 0;
+  J.dep[p] = 1;
+}
+
+__global__ void jump_kernel(const int32_t* __restrict__ tpos, int m_old, int nf_old,
+                            const UpdState* st, int m_max, Jump S, Jump D) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m_max) return;
+  const int p = tree_position(i, tpos, m_old, nf_old, st);
+  if (p < 0) return;
+  const int a = S.anc[p];
+  if (a < 0) {
+    D.anc[p] = -1;
+    D.rec[p] = S.rec[p];
+    D.off[p] = S.off[p];
+    D.dep[p] = S.dep[p];
+  } else {
+    D.anc[p] = S.anc[a];
+    D.rec[p] = S.rec[p] + S.rec[a];
+    D.off[p] = S.off[p] + S.off[a];
+    D.dep[p] = S.dep[p] + S.dep[a];
+  }
+}
+
+// Records, leaf object order, depth and root box from the summed paths.
+__global__ void emit_kernel(DynView V, const int32_t* __restrict__ tpos, int m_old, int nf_old,
+                            UpdState* st, int m_max, Jump J, float4* recs, int rec_cap,
+                            int32_t* perm, int n_objs, int32_t* rec_node, int32_t* rec_depth,
+                            int32_t* rec_size) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m_max) return;
+  const int p = tree_position(i, tpos, m_old, nf_old, st);
+  if (p < 0) return;
+  if (J.anc[p] >= 0) {  // deeper than the rounds reach
+    st->error = 2;
+    return;
+  }
+  const int rec = J.rec[p], off = J.off[p], dep = J.dep[p];
+  if (p == 0) {
+    st->n_records = V.children[0] == 0 ? V.n_int[0] : 0;
+    for (int q = 0; q < 6; ++q) st->root[q] = V.bounds[q];
+  }
+  const int k = V.children[p];
+  if (k != 0) {
+    atomicMax(&st->depth, dep);
+    const int first = V.child[p];
+    for (int j = 0; j < k; ++j) {
+      if (off + j >= n_objs) {
+        st->error = 3;
+        break;
+      }
+      const int obj = V.ids[first + j];
+      perm[off + j] = j == k - 1 ? (int32_t)(obj | 0x80000000u) : obj;
+    }
+    return;
+  }
+  if (rec >= rec_cap) {
+    st->error = 3;
+    return;
+  }
+  const int L = V.child[p], R = L + 1;
+  const int ref_l = V.children[L] != 0 ? ~off : rec + 1;
+  const int ref_r = V.children[R] != 0 ? ~(off + V.n_obj[L]) : rec + 1 + V.n_int[L];
+  const float* bl = V.bounds + 6 * (size_t)L;
+  const float* br = V.bounds + 6 * (size_t)R;
+  float4* q = recs + 4 * (size_t)rec;
+  q[0] = make_float4(bl[0], bl[1], bl[2], bl[3]);
+  q[1] = make_float4(bl[4], bl[5], br[0], br[1]);
+  q[2] = make_float4(br[2], br[3], br[4], br[5]);
+  const int meta = (V.axis[p] & 3) | ((V.lc[p] & 1) << 2);
+  reinterpret_cast<int4*>(q)[3] = make_int4(ref_l, ref_r, meta, 0);
+  rec_node[rec] = p;
+  rec_depth[rec] = dep;
+  rec_size[rec] = V.n_int[p];
 }
 
 inline int blocks(long long n, int t) { return (int)std::max<long long>(1, (n + t - 1) / t); }
@@ -969,10 +1071,9 @@ int dyn_sync(Scene* s) {
   A(&d->rec_node, nr);
   A(&d->rec_depth, nr);
   A(&d->rec_size, nr);
-  A(&d->fr_pos, nr);
-  A(&d->fr_rec, nr);
-  A(&d->fr_off, nr);
-  A(&d->counter, 4);
+  A(&d->tpos, 2 * n);
+  for (int k = 0; k < 8; ++k) A(&d->jump[k], cap);
+  A(&d->st, 1);
   if (e == cudaSuccess)
     e = cub::DeviceScan::ExclusiveSum(nullptr, d->scan_bytes, d->slot_count, d->slot_off,
                                       (int)(2 * nr));
@@ -1022,8 +1123,10 @@ int rotate_update(Scene* s) {
   const int N = s->n_tris;
   const int T = 256;
   const int nrec = s->n_records;
+  const int nf_old = d.next_free;
+  init_state_kernel<<<1, 1>>>(d.st, nf_old);
   obj_box_kernel<<<blocks(N, T), T>>>(s->d_verts, s->d_idx, N, d.obj_bounds, d.obj_cent);
-  leaf_pass_kernel<<<blocks(2LL * nrec, T), T>>>(V, d.rec_node, nrec);
+  leaf_pass_kernel<<<blocks(2LL * nrec, T), T>>>(V, d.rec_node, nrec, d.tpos);
   DY_CUDA(cudaGetLastError(), "leaf boxes");
   if (nrec > 0) {
     const Scratch S{d.sc_bounds, d.sc_child, d.sc_children, d.sc_axis,
@@ -1036,87 +1139,90 @@ int rotate_update(Scene* s) {
     DY_CUDA(cub::DeviceScan::ExclusiveSum(d.scan_tmp, bytes, d.slot_count, d.slot_off,
                                           2 * nrec),
             "split offsets");
-    int last[2];
-    DY_CUDA(cudaMemcpy(&last[0], d.slot_off + 2 * nrec - 1, sizeof(int), cudaMemcpyDeviceToHost),
-            "split offsets");
-    DY_CUDA(cudaMemcpy(&last[1], d.slot_count + 2 * nrec - 1, sizeof(int),
-                       cudaMemcpyDeviceToHost),
-            "split offsets");
-    const long long total = (long long)last[0] + last[1];
-    if (d.next_free + total > d.cap)
-      return fail(RQ_ERR_CAPACITY, "leaf re-splits need more nodes than the tree holds");
     relocate_kernel<<<blocks(2LL * nrec, T), T>>>(V, S, d.rec_node, d.rec_depth, d.rec_size,
                                                   nrec, d.slot_count, d.slot_off, d.split_axis,
-                                                  d.split_nint, d.next_free);
-    DY_CUDA(cudaGetLastError(), "relocating re-splits");
-    d.next_free += (int)total;
+                                                  d.split_nint, nf_old, d.cap, d.st);
+    advance_kernel<<<1, 1>>>(d.slot_count, d.slot_off, 2 * nrec, d.cap, d.st);
     rotate_kernel<<<blocks(2LL * nrec, T), T>>>(V, s->d_nodes, d.rec_node, nrec);
     DY_CUDA(cudaGetLastError(), "rotations");
   }
-  // layout of the rotated tree
-  int new_nrec = 0;
-  if (nrec > 0)
-    DY_CUDA(cudaMemcpy(&new_nrec, d.n_int, sizeof(int), cudaMemcpyDeviceToHost), "record count");
-  if (new_nrec < 0 || new_nrec > s->rec_capacity || new_nrec > N - 1)
-    return fail(RQ_ERR_STATE, "rotated tree's record count is out of range");
-  std::vector<int> lvl_start(1, 0), lvl_count;
-  if (new_nrec > 0) {
-    frontier_root_kernel<<<1, 1>>>(d.fr_pos, d.fr_rec, d.fr_off);
-    int a = 0, n = 1, depth = 0;
-    while (n > 0) {
-      if (depth >= kMaxDepth)
-        return fail(RQ_ERR_CAPACITY, "rotated tree is deeper than the traversal stack limit");
-      DY_CUDA(cudaMemset(d.counter, 0, sizeof(int)), "relayout");
-      relayout_level_kernel<<<blocks(n, T), T>>>(
-          V, d.fr_pos + a, d.fr_rec + a, d.fr_off + a, n, depth, d.fr_pos + a + n,
-          d.fr_rec + a + n, d.fr_off + a + n, d.counter, new_nrec - (a + n), s->d_nodes,
-          s->d_perm, N, d.rec_node, d.rec_depth, d.rec_size, new_nrec);
-      DY_CUDA(cudaGetLastError(), "relayout");
-      int m = 0;
-      DY_CUDA(cudaMemcpy(&m, d.counter, sizeof(int), cudaMemcpyDeviceToHost), "relayout");
-      if (a + n + m > new_nrec) return fail(RQ_ERR_STATE, "rotated tree's records do not add up");
-      lvl_count.push_back(n);
-      a += n;
-      lvl_start.push_back(a);
-      n = m;
-      ++depth;
-    }
-    if (a != new_nrec) return fail(RQ_ERR_STATE, "rotated tree's records do not add up");
-  } else {
-    leaf_root_perm_kernel<<<blocks(N, T), T>>>(d.ids, N, s->d_perm);
-    DY_CUDA(cudaGetLastError(), "relayout");
+  // layout of the updated tree: the positions before the re-splits and the
+  // pairs they added (at most 2 (N - 1 - records) more)
+  const int m_old = 2 * nrec + 1;
+  const int m_max = m_old + 2 * std::max(N - 1 - nrec, 0);
+  parent_pass_kernel<<<blocks(m_max, T), T>>>(V, d.tpos, m_old, nf_old, d.st, m_max);
+  Jump J[2] = {{d.jump[0], d.jump[1], d.jump[2], d.jump[3]},
+               {d.jump[4], d.jump[5], d.jump[6], d.jump[7]}};
+  jump_init_kernel<<<blocks(m_max, T), T>>>(V, d.tpos, m_old, nf_old, d.st, m_max, J[0]);
+  int cur = 0;
+  for (int round = 0; (1 << round) < kMaxDepth; ++round) {
+    jump_kernel<<<blocks(m_max, T), T>>>(d.tpos, m_old, nf_old, d.st, m_max, J[cur],
+                                         J[cur ^ 1]);
+    cur ^= 1;
   }
-  // records grouped by level, deepest first, for the topology-keeping refit
-  const int nlev = (int)lvl_count.size();
-  std::vector<int> offsets(1, 0);
-  for (int k = nlev - 1; k >= 0; --k) {
-    DY_CUDA(cudaMemcpy(s->d_level_recs + offsets.back(), d.fr_rec + lvl_start[k],
-                       (size_t)lvl_count[k] * sizeof(int32_t), cudaMemcpyDeviceToDevice),
-            "levels");
-    offsets.push_back(offsets.back() + lvl_count[k]);
-  }
+  emit_kernel<<<blocks(m_max, T), T>>>(V, d.tpos, m_old, nf_old, d.st, m_max, J[cur],
+                                       s->d_nodes, s->rec_capacity, s->d_perm, N, d.rec_node,
+                                       d.rec_depth, d.rec_size);
+  DY_CUDA(cudaGetLastError(), "relayout");
   DY_CUDA(launch_tri_setup(s->tri_kind, s->d_verts, s->d_idx, s->d_perm, N, s->d_tris, 0),
           "triangle records");
-  std::vector<int32_t> rn((size_t)new_nrec);
-  if (new_nrec > 0)
-    DY_CUDA(cudaMemcpy(rn.data(), d.rec_node, (size_t)new_nrec * sizeof(int32_t),
-                       cudaMemcpyDeviceToHost),
-            "records");
-  float root[6];
-  DY_CUDA(cudaMemcpy(root, d.bounds, sizeof(root), cudaMemcpyDeviceToHost), "root box");
-  DY_CUDA(cudaDeviceSynchronize(), "rotating update");
-  s->n_records = new_nrec;
-  s->n_leaves = new_nrec + 1;
-  s->rec_node.swap(rn);
-  s->level_offsets.swap(offsets);
-  s->root_ref = new_nrec > 0 ? 0 : ~0;
-  for (int c = 0; c < 3; ++c) {
-    s->root_lo[c] = root[c];
-    s->root_hi[c] = root[3 + c];
+  UpdState out;
+  DY_CUDA(cudaMemcpy(&out, d.st, sizeof(out), cudaMemcpyDeviceToHost), "update state");
+  if (out.error != 0) {
+    // the device tree is no longer consistent: drop it
+    s->free_tree();
+    return fail(out.error == 2 ? RQ_ERR_CAPACITY : RQ_ERR_STATE,
+                out.error == 1   ? "leaf re-splits need more nodes than the tree holds"
+                : out.error == 2 ? "updated tree is deeper than the traversal stack limit"
+                                 : "updated tree's records exceed the record buffer");
   }
-  s->depth = std::max(nlev, 1);
+  d.next_free = out.next_free;
+  d.layout_host_stale = true;
+  s->n_records = out.n_records;
+  s->n_leaves = out.n_records + 1;
+  s->root_ref = out.n_records > 0 ? 0 : ~0;
+  for (int c = 0; c < 3; ++c) {
+    s->root_lo[c] = out.root[c];
+    s->root_hi[c] = out.root[3 + c];
+  }
+  s->depth = std::max(out.depth, 1);
   s->tree_stale = true;
   s->tree_from_dyn = true;
+  return RQ_OK;
+}
+
+// After rotating updates the host's record list and the records grouped by
+// level (the topology-keeping refit's bottom-up order) are brought up to
+// date only when a refit needs them.
+int sync_layout_host(Scene* s) {
+  if (!s->dyn || !s->dyn->layout_host_stale) return RQ_OK;
+  DynTree& d = *s->dyn;
+  const int n = s->n_records;
+  std::vector<int32_t> rn((size_t)n), rd((size_t)n);
+  if (n > 0) {
+    DY_CUDA(cudaMemcpy(rn.data(), d.rec_node, (size_t)n * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost),
+            "records");
+    DY_CUDA(cudaMemcpy(rd.data(), d.rec_depth, (size_t)n * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost),
+            "records");
+  }
+  int maxd = 0;
+  for (int x : rd) maxd = std::max(maxd, x);
+  std::vector<int> count(maxd + 1, 0), start(maxd + 2, 0);
+  for (int x : rd) ++count[x];
+  for (int x = maxd; x >= 0; --x) start[maxd - x + 1] = start[maxd - x] + count[x];
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  std::vector<int32_t> by_level((size_t)n);
+  for (int r = 0; r < n; ++r) by_level[fill[maxd - rd[r]]++] = r;
+  if (n > 0)
+    DY_CUDA(cudaMemcpy(s->d_level_recs, by_level.data(), (size_t)n * sizeof(int32_t),
+                       cudaMemcpyHostToDevice),
+            "levels");
+  s->level_offsets.assign(start.begin(), start.end());
+  if (n == 0) s->level_offsets.assign(1, 0);
+  s->rec_node.swap(rn);
+  d.layout_host_stale = false;
   return RQ_OK;
 }
 

@@ -162,6 +162,7 @@ struct Scene {
 };
 
 int rotate_update(Scene* s);
+int sync_layout_host(Scene* s);
 void mark_dyn_bounds_stale(DynTree* d);
 int refresh_tree_from_dyn(const Scene* s);
 int dyn_state(const Scene* s, float* costs, int cap, int* next_free);

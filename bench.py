@@ -8,7 +8,8 @@ Prints ONE JSON line (rank 0).  A step is one frame of the named workload:
   path_frame   (default) incoherent path tracing: 1280x720, 16 spp
                stratified jitter, diffuse bounces to depth 4 with cosine
                hemisphere sampling from per-path PCG32 streams, Russian
-               roulette from bounce 2, one parallelogram area light sampled
+               roulette from depth 1 as KajiyaPathtracer does (survivors
+               unscaled, as in the reference), one parallelogram area light sampled
                with a shadow ray at every bounce, over a 512x1024 fBm
                heightfield (1,048,576 triangles) plus 32 displaced level-4
                icospheres (163,840 triangles).  Rays per step = camera +

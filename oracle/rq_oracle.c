@@ -803,11 +803,13 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
       }
       if (depth + 1 >= maxd) break;
       if (depth >= rrd && depth != maxd - 1) {
+        /* russian_roulette_full (KajiyaPathtracer.cc:389-478): killed when
+           rr > max(reflectance); the reference's 1/max scale loop runs over
+           the killed rays past newEnd (468-475), so survivors keep their
+           importance unscaled */
         const float rr = pcg_float(&rng);
         const float mx = fmaxf(fmaxf(kd[0], kd[1]), kd[2]);
         if (rr > mx) break;
-        const float sc = 1.f / mx;
-        for (int c = 0; c < 3; ++c) imp[c] = imp[c] * sc;
       }
       for (int c = 0; c < 3; ++c) {
         r.o[c] = hp[c];

@@ -17,7 +17,8 @@
 //              the same thread, direct light weighted by the face-forward
 //              geometric normal (KajiyaPathtracer.cc:222-234), Russian
 //              roulette (russian_roulette_full, KajiyaPathtracer.cc:389-478:
-//              kill when rr > max(reflectance), else scale by 1/max), and
+//              kill when rr > max(reflectance); survivors are not rescaled,
+//              as in the reference), and
 //              compaction of the survivors into the next queue
 //   resolve    per pixel, the mean of its samples in sample order
 //

@@ -260,15 +260,13 @@ __device__ __forceinline__ bool shade_begin(const DevScene& S, const PathParams&
   }
   alive = !last_depth;
   if (alive && do_rr) {
+    // russian_roulette_full (KajiyaPathtracer.cc:389-478) kills a path when
+    // rr > max(reflectance) and then applies its 1/max scale to the killed
+    // rays it moved past newEnd, not to the survivors: a surviving path keeps
+    // its importance unscaled, and so does it here
     const float rr = pcg32_float(rng);
     const float mx = fmaxf(fmaxf(refl[0], refl[1]), refl[2]);
-    if (rr > mx) {
-      alive = false;
-    } else {
-      const float sc = fdiv(1.f, mx);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) imp[c] = fmul(imp[c], sc);
-    }
+    if (rr > mx) alive = false;
   }
   if (alive) {
 #pragma unroll

@@ -315,12 +315,14 @@ class PathScene:
 
 def path_scene(hf_nx: int = 512, hf_nz: int = 1024, n_spheres: int = 32,
                sphere_level: int = 4, xres: int = 1280, yres: int = 720, spp: int = 16,
-               max_depth: int = 4, rr_depth: int = 2, seed: int = 17) -> PathScene:
+               max_depth: int = 4, rr_depth: int = 1, seed: int = 17) -> PathScene:
     """Incoherent path-tracing frame: an hf_nx x hf_nz fBm heightfield
     (2*hf_nx*hf_nz triangles, 5 octaves, amplitude 0.2) plus n_spheres
     displaced icospheres at seeded positions on it, one parallelogram area
     light above, diffuse bounces to max_depth with Russian roulette from
-    rr_depth on.  Defaults: 1280x720, 16 spp, depth 4, RR after bounce 2,
+    rr_depth on (depth 0 = the camera ray's hit; the reference's
+    KajiyaPathtracer applies roulette from depth 1).  Defaults: 1280x720,
+    16 spp, depth 4, RR from depth 1,
     1,048,576 + 32 x 5,120 = 1,212,416 triangles."""
     rng = np.random.default_rng(seed)
     ext = 8.0
@@ -345,7 +347,7 @@ def path_scene(hf_nx: int = 512, hf_nz: int = 1024, n_spheres: int = 32,
 def tiny_path_scene(xres: int = 40, yres: int = 30, spp: int = 4) -> PathScene:
     """The path-tracing layout scaled down for committed checks."""
     return path_scene(hf_nx=16, hf_nz=16, n_spheres=3, sphere_level=2, xres=xres,
-                      yres=yres, spp=spp, max_depth=4, rr_depth=2, seed=5)
+                      yres=yres, spp=spp, max_depth=4, rr_depth=1, seed=5)
 
 
 def sphere_set(n: int, level: int, seed: int, extent: float = 6.0) -> Mesh:

@@ -25,7 +25,9 @@ Raytracer colours for the 4-spp jittered samples of a 48x40 frame, and
 ply_cases.npz: Manta::readPlyFile's vertices, triangles and face materials
 for the PLY files the tests write (tests/test_mesh_io.py), and
 tree_update.npz: DynBVH::update with its tree rotations over four frames of a
-seeded animation (the tree, per-node costs and nextFree after every frame).
+seeded animation (the tree, per-node costs and nextFree after every frame),
+and path_stats.npz: KajiyaPathtracer images of the tiny path scene for 16
+seeds at 4096 samples per pixel (the expectation the path tracer must match).
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -198,6 +200,29 @@ def write_tree_update() -> None:
     print(path, os.path.getsize(path), "bytes")
 
 
+PATH_STATS = dict(xres=16, yres=12, spp=4096, seeds=16)
+
+
+def write_path_stats() -> None:
+    """KajiyaPathtracer frames (one thread, so each seed is reproducible) of
+    the tiny path scene for several seeds: the reference's estimator that
+    the path tracer's images must match in expectation."""
+    ref = Reference()
+    p = PATH_STATS
+    sc = scenes.tiny_path_scene(xres=p["xres"], yres=p["yres"], spp=p["spp"])
+    rs = ref.scene(sc.mesh, 0)
+    imgs = []
+    for s in range(p["seeds"]):
+        sc.seed = 2000 + s
+        imgs.append(rs.render_path(sc, nthreads=1)["rgb"].reshape(p["yres"], p["xres"], 3))
+    rs.close()
+    path = os.path.join(OUT, "path_stats.npz")
+    np.savez_compressed(path, images=np.array(imgs, np.float32),
+                        seed_values=np.arange(2000, 2000 + p["seeds"]),
+                        **{k: np.int64(v) for k, v in p.items()})
+    print(path, os.path.getsize(path), "bytes")
+
+
 def sah_scenes():
     """Scenes whose reference SAH cost pins the GPU builder (2% bound)."""
     out = {"small_frame": scenes.small_frame_scene().mesh,
@@ -234,11 +259,15 @@ if __name__ == "__main__":
     elif "--ply" in sys.argv:
         write_ply_cases()
         write_tree_update()
+        write_path_stats()
     elif "--update" in sys.argv:
         write_tree_update()
+    elif "--path" in sys.argv:
+        write_path_stats()
     else:
         main()
         write_sah_costs()
         write_instanced()
         write_ply_cases()
         write_tree_update()
+        write_path_stats()

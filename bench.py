@@ -223,12 +223,12 @@ class PathFrame:
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per extension
     # ray of path_extend_persistent_kernel, from one ncu capture of bounce 0
     # of this workload at 640x360 x 4 spp (921,600 rays, same scene).
-    DRAM_BYTES_PER_RAY = 78.0
+    DRAM_BYTES_PER_RAY = 76.6
 
     def traffic(self, rays):
         ext, _ = rays
         per_launch = self.DRAM_BYTES_PER_RAY * ext / self.sc.max_depth
-        return per_launch, ("ncu DRAM bytes per extension ray at 640x360x4 spp (78.0 B) x "
+        return per_launch, ("ncu DRAM bytes per extension ray at 640x360x4 spp (76.6 B) x "
                             "extension rays per launch (all bounces / depth)")
 
     def group_stages(self, stage_ms):

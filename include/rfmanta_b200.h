@@ -174,6 +174,31 @@ RQ_API int rq_mesh_copy(const rq_mesh* mesh, float* vertices, uint32_t* indices,
                         uint32_t* face_material);
 RQ_API int rq_mesh_destroy(rq_mesh* mesh);
 
+/*
+ * rq_mesh_read_obj reads a Wavefront OBJ file (and its mtllib) the way
+ * Manta::ObjGroup does over its glm reader (Model/Groups/ObjGroup.cc:176-320,
+ * Model/Readers/glm/glm.cc): vertices, triangles (polygons as fans, groups
+ * newest first), each face's material index into the material table, and
+ * degenerate triangles removed.  The material table is ObjGroup's: entry 0
+ * its default material, entry i + 1 the library's material i (entry 1 being
+ * glm's "NO_ASSIGNED_MATERIAL"), each classified as ObjGroup classifies it.
+ * Texture maps are not loaded (their constant colours stand).  A missing
+ * file or library is RQ_ERR_NOTFOUND, malformed data RQ_ERR_FORMAT.
+ */
+#define RQ_MAT_LAMBERTIAN 0  /* Lambertian(Kd) */
+#define RQ_MAT_PHONG 1       /* Phong(Kd, Ks, int(Ns), reflectivity) */
+#define RQ_MAT_DIELECTRIC 2  /* Ni not 0 or 1 */
+#define RQ_MAT_TRANSPARENT 3 /* Tf / Tr not white, or d < 1 */
+#define RQ_MAT_DEFAULT 4     /* ObjGroup's default (Lambertian of the normal) */
+RQ_API int rq_mesh_read_obj(const char* path, rq_mesh** out);
+/* Entries in the mesh's material table (0 for PLY meshes). */
+RQ_API int rq_mesh_material_count(const rq_mesh* mesh, int* n);
+/* Per entry: kind, diffuse and specular rgb, Phong exponent, reflectivity,
+ * refraction index, alpha, filter rgb; any output may be NULL. */
+RQ_API int rq_mesh_materials(const rq_mesh* mesh, int32_t* kind, float* diffuse,
+                             float* specular, int32_t* exponent, float* reflectivity,
+                             float* refraction, float* alpha, float* filter);
+
 /* SAH cost of the scene's tree, DynBVH::computeCost<>(0) with C_isec=C_trav=1. */
 RQ_API int rq_scene_sah_cost(const rq_scene* scene, double* cost);
 

@@ -435,6 +435,7 @@ class Reference:
         L.mref_tree_export.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 6
         L.mref_tree_save.argtypes = [C.c_void_p, C.c_char_p]
         L.mref_tree_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.mref_read_obj.argtypes = [C.c_char_p, C.c_int] + [C.c_void_p] * 8 + [C.c_int] * 3
         L.mref_tree_cost.argtypes = [C.c_void_p]
         L.mref_tree_cost.restype = C.c_double
         L.mref_intersect.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
@@ -473,6 +474,28 @@ class Reference:
         """Top-level DynBVH over InstanceT (kind 0) / nested DynBVH (kind 1)
         objects of the inner RefScenes."""
         return RefScene(self, None, 0, inner=(inner, inst_scene, translation, kind))
+
+    def read_obj(self, path, tri_kind=0):
+        """Manta::ObjGroup over glm: (vertices, indices, face_material,
+        material kinds, material values [n, 13]: Kd rgb, Ks rgb, Ns, Ni, d,
+        filter rgb, reflectivity), or None when the reader fails."""
+        nv, nt, nm = C.c_int(), C.c_int(), C.c_int()
+        L = self.lib
+        rc = L.mref_read_obj(str(path).encode(), tri_kind, C.byref(nv), C.byref(nt), C.byref(nm),
+                             None, None, None, None, None, 0, 0, 0)
+        if rc != 0:
+            return None
+        v = np.zeros((nv.value, 3), np.float32)
+        ix = np.zeros((nt.value, 3), np.uint32)
+        fm = np.zeros(nt.value, np.uint32)
+        kind = np.zeros(nm.value, np.int32)
+        vals = np.zeros((nm.value, 13), np.float32)
+        rc = L.mref_read_obj(str(path).encode(), tri_kind, C.byref(nv), C.byref(nt), C.byref(nm),
+                             _ptr(v), _ptr(ix), _ptr(fm), _ptr(kind), _ptr(vals), v.shape[0],
+                             ix.shape[0], kind.shape[0])
+        if rc != 0:
+            return None
+        return v, ix, fm, kind, vals
 
     def read_ply(self, path, transform=None, tri_kind=0):
         """Manta::readPlyFile into a fresh Mesh: (vertices, indices,

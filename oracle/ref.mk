@@ -71,7 +71,10 @@ MODEL_SRC := \
   Model/Lights/AreaLight.cc Model/Primitives/Parallelogram.cc \
   Model/Primitives/PrimitiveCommon.cc Model/TexCoordMappers/UniformMapper.cc \
   Model/Instances/InstanceT.cc Model/Instances/InstanceMaterial.cc \
-  Model/Readers/PlyReader.cc
+  Model/Readers/PlyReader.cc \
+  Model/Groups/ObjGroup.cc Model/Readers/glm/glm.cc \
+  Model/Materials/Dielectric.cc Model/Materials/Transparent.cc Model/Materials/Flat.cc \
+  Model/Textures/NormalTexture.cc Model/Primitives/MovingKSTriangle.cc
 
 ENGINE_SRC := \
   Engine/Shadows/HardShadows.cc Engine/Renderers/Raytracer.cc \

@@ -53,6 +53,11 @@
 #include <Model/Materials/Lambertian.h>
 #include <Model/Materials/Phong.h>
 #include <Model/Readers/PlyReader.h>
+#include <Model/Groups/ObjGroup.h>
+#include <Model/Materials/Dielectric.h>
+#include <Model/Materials/Transparent.h>
+#include <Model/Readers/glm/glm.h>
+#include <Model/Textures/ImageTexture.h>
 #include <Model/Primitives/KenslerShirleyTriangle.h>
 #include <Model/Primitives/MeshTriangle.h>
 #include <Model/Primitives/WaldTriangle.h>
@@ -71,6 +76,15 @@
 #include <vector>
 
 using namespace Manta;
+
+namespace Manta {
+// No image readers are built into the checker: an OBJ material's texture
+// map fails to load and ObjGroup keeps its constant colour
+// (Model/Groups/ObjGroup.cc:38-64).
+ImageTexture<Color>* LoadColorImageTexture(const std::string& file_name, std::ostream*, bool) {
+  throw InputError("image textures are not built into the checker: " + file_name);
+}
+}  // namespace Manta
 
 namespace {
 
@@ -334,6 +348,63 @@ int mref_read_ply(const char* path, const float* transform, int tri_kind, int* n
   } catch (...) {
     return 1;
   }
+}
+
+// Manta::ObjGroup (Model/Groups/ObjGroup.cc:176-320) reading an OBJ file:
+// counts, and when the arrays are large enough the vertices, triangles, face
+// materials and, per entry of ObjGroup's material table, the kind of
+// material it made (0 Lambertian, 1 Phong, 2 Dielectric, 3 Transparent,
+// 4 for entry 0, ObjGroup's default) with the glm material values it was
+// made from (diffuse rgb, specular rgb, Ns, Ni, d, filter rgb,
+// reflectivity; glm_reader's model, read once more with glmReadOBJ).
+// 0 = ok, 1 = the reader failed, 2 = arrays too small.
+int mref_read_obj(const char* path, int tri_kind, int* nv, int* nt, int* nm, float* verts,
+                  unsigned* idx, unsigned* fmat, int* kind, float* mvals, int cap_v,
+                  int cap_t, int cap_m) {
+  ObjGroup* g = 0;
+  try {
+    g = new ObjGroup(path, NULL, tri_kind == 0 ? MeshTriangle::WALD_TRI
+                                                : MeshTriangle::KENSLER_SHIRLEY_TRI);
+  } catch (...) {
+    return 1;
+  }
+  *nv = (int)g->vertices.size();
+  *nt = (int)(g->vertex_indices.size() / 3);
+  *nm = (int)g->materials.size();
+  if (!verts) return 0;
+  if (*nv > cap_v || *nt > cap_t || *nm > cap_m) return 2;
+  for (int i = 0; i < *nv; ++i)
+    for (int c = 0; c < 3; ++c) verts[3 * i + c] = g->vertices[i][c];
+  for (int i = 0; i < 3 * *nt; ++i) idx[i] = g->vertex_indices[i];
+  for (int i = 0; i < *nt; ++i) fmat[i] = g->face_material[i];
+  Glm::GLMmodel* model = Glm::glmReadOBJ(path);
+  for (int i = 0; i < *nm; ++i) {
+    const Material* m = g->materials[i];
+    int k = 0;
+    if (i == 0) k = 4;
+    else if (dynamic_cast<const Dielectric*>(m)) k = 2;
+    else if (dynamic_cast<const Transparent*>(m)) k = 3;
+    else if (dynamic_cast<const Phong*>(m)) k = 1;
+    else if (dynamic_cast<const Lambertian*>(m)) k = 0;
+    else k = -1;
+    kind[i] = k;
+    float* q = mvals + 13 * i;
+    for (int c = 0; c < 13; ++c) q[c] = 0;
+    if (i > 0 && model && (unsigned)(i - 1) < model->nummaterials) {
+      const Glm::GLMmaterial& gm = model->materials[i - 1];
+      for (int c = 0; c < 3; ++c) {
+        q[c] = gm.diffuse[c];
+        q[3 + c] = gm.specular[c];
+        q[9 + c] = gm.filter[c];
+      }
+      q[6] = gm.shininess;
+      q[7] = gm.refraction;
+      q[8] = gm.alpha;
+      q[12] = gm.reflectivity;
+    }
+  }
+  if (model) Glm::glmDelete(model);
+  return 0;
 }
 
 void mref_scene_destroy(void* h) {

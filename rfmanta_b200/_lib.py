@@ -27,6 +27,11 @@ RQ_TRI_KS = 1
 RQ_INST_TRANSLATE = 0
 RQ_PATH_EXTEND = 2
 RQ_PATH_SHADE = 3
+RQ_MAT_LAMBERTIAN = 0
+RQ_MAT_PHONG = 1
+RQ_MAT_DIELECTRIC = 2
+RQ_MAT_TRANSPARENT = 3
+RQ_MAT_DEFAULT = 4
 RQ_UPDATE_REFIT = 0
 RQ_UPDATE_ROTATE = 1
 RQ_INST_NESTED = 1
@@ -160,6 +165,9 @@ def _load():
         "rq_mesh_info": ([vp, C.POINTER(i), C.POINTER(i)], i),
         "rq_mesh_copy": ([vp, vp, vp, vp], i),
         "rq_mesh_destroy": ([vp], i),
+        "rq_mesh_read_obj": ([C.c_char_p, C.POINTER(vp)], i),
+        "rq_mesh_material_count": ([vp, C.POINTER(i)], i),
+        "rq_mesh_materials": ([vp] * 9, i),
         "rq_scene_create_instanced": ([vp, i, vp, vp, vp, i, C.POINTER(vp)], i),
         "rq_trace_device_ex": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp, vp, vp], i),
         "rq_render_frame": ([vp, C.POINTER(FrameParams), vp, C.POINTER(C.c_uint64)], i),

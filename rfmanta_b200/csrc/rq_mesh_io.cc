@@ -35,16 +35,12 @@
 #include <vector>
 
 #include "../../include/rfmanta_b200.h"
+#include "rq_mesh.h"
 
 namespace rq {
 void set_error(const std::string& msg);
 }
 
-struct rq_mesh {
-  std::vector<float> vertices;     // 3 per vertex
-  std::vector<uint32_t> indices;   // 3 per triangle
-  std::vector<uint32_t> face_material;
-};
 
 namespace {
 
@@ -254,8 +250,10 @@ struct PlyBuild {
   }
 };
 
+}  // namespace
+
 // Mesh::removeDegenerateTriangles.
-void remove_degenerate(rq_mesh* m) {
+void rq_mesh_remove_degenerate(rq_mesh* m) {
   std::vector<uint32_t>& vi = m->indices;
   const float* v = m->vertices.data();
   for (size_t i = 0; i < vi.size(); i += 3) {
@@ -279,8 +277,6 @@ void remove_degenerate(rq_mesh* m) {
     }
   }
 }
-
-}  // namespace
 
 extern "C" {
 
@@ -350,7 +346,7 @@ int rq_mesh_read_ply(const char* path, const float* transform, uint32_t material
   const size_t nv = mesh->vertices.size() / 3;
   for (uint32_t i : mesh->indices)
     if (i >= nv) return fail(RQ_ERR_FORMAT, "PLY face refers to a missing vertex");
-  remove_degenerate(mesh.get());
+  rq_mesh_remove_degenerate(mesh.get());
   *out = mesh.release();
   return RQ_OK;
 }
@@ -369,6 +365,32 @@ int rq_mesh_copy(const rq_mesh* m, float* vertices, uint32_t* indices, uint32_t*
   if (face_material)
     std::memcpy(face_material, m->face_material.data(),
                 m->face_material.size() * sizeof(uint32_t));
+  return RQ_OK;
+}
+
+int rq_mesh_material_count(const rq_mesh* m, int* n) {
+  if (!m || !n) return fail(RQ_ERR_ARG, "NULL argument");
+  *n = (int)m->materials.size();
+  return RQ_OK;
+}
+
+int rq_mesh_materials(const rq_mesh* m, int32_t* kind, float* diffuse, float* specular,
+                      int32_t* exponent, float* reflectivity, float* refraction, float* alpha,
+                      float* filter) {
+  if (!m) return fail(RQ_ERR_ARG, "NULL mesh");
+  for (size_t i = 0; i < m->materials.size(); ++i) {
+    const rq_mesh_material& q = m->materials[i];
+    if (kind) kind[i] = q.kind;
+    for (int c = 0; c < 3; ++c) {
+      if (diffuse) diffuse[3 * i + c] = q.diffuse[c];
+      if (specular) specular[3 * i + c] = q.specular[c];
+      if (filter) filter[3 * i + c] = q.filter[c];
+    }
+    if (exponent) exponent[i] = q.exponent;
+    if (reflectivity) reflectivity[i] = q.reflectivity;
+    if (refraction) refraction[i] = q.refraction;
+    if (alpha) alpha[i] = q.alpha;
+  }
   return RQ_OK;
 }
 

@@ -27,7 +27,9 @@ for the PLY files the tests write (tests/test_mesh_io.py), and
 tree_update.npz: DynBVH::update with its tree rotations over four frames of a
 seeded animation (the tree, per-node costs and nextFree after every frame),
 and path_stats.npz: KajiyaPathtracer images of the tiny path scene for 16
-seeds at 4096 samples per pixel (the expectation the path tracer must match).
+seeds at 4096 samples per pixel (the expectation the path tracer must match),
+and obj_cases.npz: Manta::ObjGroup's vertices, triangles, face materials and
+material table for the OBJ files the tests write.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -135,6 +137,34 @@ def write_instanced() -> None:
         out[f"inner{i}_indices"] = m.indices
         out[f"inner{i}_face_material"] = m.face_material
     path = os.path.join(OUT, "tiny_instanced.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
+def write_obj_cases() -> None:
+    """Manta::ObjGroup's results for the OBJ files tests/test_mesh_io.py
+    writes (vertices, triangles, face materials, material kinds and glm
+    values)."""
+    import pathlib
+    import tempfile
+    sys.path.insert(0, os.path.dirname(OUT))
+    from test_mesh_io import obj_cases
+    ref = Reference()
+    out = {"names": np.array([n for n, _, _ in obj_cases()])}
+    with tempfile.TemporaryDirectory() as td:
+        for name, files, obj in obj_cases():
+            d = pathlib.Path(td) / name
+            d.mkdir()
+            for fn, text in files.items():
+                (d / fn).write_text(text)
+            v, ix, fm, kind, vals = ref.read_obj(d / obj)
+            out[f"{name}_bytes"] = np.frombuffer((d / obj).read_bytes(), np.uint8)
+            out[f"{name}_vertices"] = v
+            out[f"{name}_indices"] = ix
+            out[f"{name}_face_material"] = fm
+            out[f"{name}_kind"] = kind
+            out[f"{name}_values"] = vals
+    path = os.path.join(OUT, "obj_cases.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")
 
@@ -260,10 +290,13 @@ if __name__ == "__main__":
         write_ply_cases()
         write_tree_update()
         write_path_stats()
+        write_obj_cases()
     elif "--update" in sys.argv:
         write_tree_update()
     elif "--path" in sys.argv:
         write_path_stats()
+    elif "--obj" in sys.argv:
+        write_obj_cases()
     else:
         main()
         write_sah_costs()
@@ -271,3 +304,4 @@ if __name__ == "__main__":
         write_ply_cases()
         write_tree_update()
         write_path_stats()
+        write_obj_cases()

@@ -233,3 +233,206 @@ def test_ply_mesh_traces(tmp_path):
     r = RayBatch(o, d)
     bvh.intersect(r)
     assert np.all(r.hitPrim >= 0)
+
+
+# ----------------------------------------------------------------- OBJ ---
+
+MTL_MAIN = """# materials
+newmtl red
+Kd 0.9 0.1 0.1
+Ka 0.1 0.1 0.1
+illum 2
+newmtl shiny
+Kd 0.2 0.3 0.4
+Ks 0.5 0.5 0.5
+Ns 32.7
+map_Kd -s 2 2 tex.png
+newmtl glass
+Ni 1.5
+newmtl fog
+d 0.5
+newmtl tinted
+Tf 0.9 1 1
+newmtl clear
+Tr 1
+Ns 8
+newmtl two words
+Kd 0.25 0.5 0.75
+"""
+
+
+def obj_cases():
+    """(name, {file name: text}, obj file) of the OBJ parity cases."""
+    rng = np.random.default_rng(11)
+    pts = rng.normal(size=(24, 3)).round(4)
+    vlines = "".join(f"v {x!r} {y!r} {z!r}\n" for x, y, z in pts.tolist())
+    faces = [[int(i) + 1 for i in rng.choice(24, size=int(rng.integers(3, 7)), replace=False)]
+             for _ in range(30)]
+    flines = "".join("f " + " ".join(str(i) for i in f) + "\n" for f in faces)
+    basic = ("# groups, materials, fans, relative indices, v/t/n forms\n"
+             "mtllib main.mtl\n" + vlines +
+             "vt 0 0\nvt 1 0\nvt 1 1\nvn 0 0 1\nvn 0 1 0\n"
+             "g first\nusemtl red\nf 1 2 3 4\n"
+             "g second\nusemtl shiny\nf 1/1/1 2/2/2 5/3/1\nf -1 -2 -3\n"
+             "usemtl unknown\nf 2//1 3//2 6//1 7//2\n"
+             "g first\nf 3 4 6\nusemtl glass\nf 4 1 6\n"
+             "o third\nusemtl fog\nf 1/1 3/2 5/3\n"
+             "s 1\nl 1 2\ng fourth\nusemtl tinted\nf 7 8 9\nusemtl clear\nf 9 10 11\n"
+             "usemtl x two\nf 10 11 12\n")
+    plain = "# no material library, no groups\n" + vlines + flines
+    grid = "".join(f"v {x} {y} 0\n" for y in range(4) for x in range(4))
+    degen = ("mtllib main.mtl\n" + grid + "v 0 0 0\n"
+             "usemtl red\nf 1 2 3\nf 1 1 5\nf 1 2 5\n"  # collinear / repeated
+             "g quad\nf 1 2 6 5\nf 17 1 2\nf 5 6 7 8\nf 2 3 4\n")
+    mtl_pre = "Kd 0.3 0.3 0.3\nnewmtl only\nKd 0.6 0.7 0.8\n"
+    defaults = ("mtllib pre.mtl\n" + grid + "g a\nf 1 2 6\nusemtl NO_ASSIGNED_MATERIAL\n"
+                "f 2 3 7\ng b\nusemtl only\nf 3 4 8\ng c\nf 5 6 10\n")
+    two_libs = ("mtllib pre.mtl\nmtllib main.mtl\n" + grid +
+                "usemtl only\nf 1 2 6\nusemtl red\nf 2 3 7\n")
+    return [
+        ("basic", {"main.mtl": MTL_MAIN, "basic.obj": basic}, "basic.obj"),
+        ("plain", {"plain.obj": plain}, "plain.obj"),
+        ("degenerate", {"main.mtl": MTL_MAIN, "degen.obj": degen}, "degen.obj"),
+        ("defaults", {"pre.mtl": mtl_pre, "defaults.obj": defaults}, "defaults.obj"),
+        ("two_libs", {"pre.mtl": mtl_pre, "main.mtl": MTL_MAIN, "two.obj": two_libs}, "two.obj"),
+    ]
+
+
+def _write_case(d, files):
+    for name, text in files.items():
+        (d / name).write_text(text)
+
+
+def _obj_product(path):
+    from rfmanta_b200.meshio import read_obj
+    m, mats = read_obj(path)
+    vals = np.concatenate([mats.diffuse, mats.specular, mats.exponent[:, None].astype(np.float32),
+                           mats.refraction[:, None], mats.alpha[:, None], mats.filter,
+                           mats.reflectivity[:, None]], axis=1)
+    return m.vertices, m.indices, m.face_material, mats.kind, vals, mats
+
+
+def _obj_same(got, exp, name):
+    v, ix, fm, kind, vals, mats = got
+    ev, eix, efm, ekind, evals = exp
+    assert np.array_equal(v.view(np.uint32), np.ascontiguousarray(ev, np.float32).view(np.uint32)), name
+    assert np.array_equal(ix, eix), f"{name}: triangles differ"
+    assert np.array_equal(fm, efm), f"{name}: face materials differ"
+    assert np.array_equal(kind, ekind), f"{name}: material kinds differ"
+    # the reference reports glm's values for library materials (entries 1..)
+    ev = np.array(evals, np.float32)
+    if len(kind) > 1:
+        assert np.array_equal(mats.diffuse[1:], ev[1:, 0:3]), name
+        assert np.array_equal(mats.specular[1:], ev[1:, 3:6]), name
+        assert np.array_equal(mats.exponent[1:], ev[1:, 6].astype(np.int32)), name
+        assert np.array_equal(mats.refraction[1:], ev[1:, 7]), name
+        assert np.array_equal(mats.alpha[1:], ev[1:, 8]), name
+        assert np.array_equal(mats.filter[1:], ev[1:, 9:12]), name
+        assert np.array_equal(mats.reflectivity[1:], ev[1:, 12]), name
+
+
+def test_obj_fixture_cases(tmp_path):
+    z = np.load(os.path.join(GOLDEN, "obj_cases.npz"))
+    names = [n for n, _, _ in obj_cases()]
+    assert sorted(str(x) for x in z["names"]) == sorted(names)
+    for name, files, obj in obj_cases():
+        d = tmp_path / name
+        d.mkdir()
+        _write_case(d, files)
+        assert (d / obj).read_bytes() == bytes(z[f"{name}_bytes"]), f"{name}: writer changed"
+        exp = tuple(z[f"{name}_{k}"] for k in ("vertices", "indices", "face_material", "kind",
+                                                "values"))
+        _obj_same(_obj_product(d / obj), exp, name)
+
+
+def test_obj_live_reference(tmp_path):
+    from oracle.pyoracle import Reference
+    if not Reference.available():
+        pytest.skip("reference library not built")
+    ref = Reference()
+    for name, files, obj in obj_cases():
+        d = tmp_path / name
+        d.mkdir()
+        _write_case(d, files)
+        exp = ref.read_obj(d / obj)
+        assert exp is not None, name
+        _obj_same(_obj_product(d / obj), exp, name)
+
+
+def test_obj_rules(tmp_path):
+    """The behaviours the parity cases pin, stated directly."""
+    from rfmanta_b200._lib import RQ_MAT_DEFAULT, RQ_MAT_PHONG
+    cases = {n: (f, o) for n, f, o in obj_cases()}
+    d = tmp_path / "basic"
+    d.mkdir()
+    _write_case(d, cases["basic"][0])
+    v, ix, fm, kind, vals, mats = _obj_product(d / "basic.obj")
+    # entry 0 ObjGroup's default, 1 glm's NO_ASSIGNED_MATERIAL, then the
+    # library in order: red, shiny, glass, fog, tinted, clear, words
+    assert kind[0] == RQ_MAT_DEFAULT
+    assert list(kind[1:]) == [0, 0, 1, 2, 3, 3, 1, 0]  # "clear": Tr 1 is white, Ns 8
+    assert mats.exponent[3] == 32  # int(Ns 32.7)
+    # "newmtl two words" names the material "words" and "usemtl x two"
+    # selects "two" (each takes its line's second word), which the library
+    # lacks, so glm's material 0: the newest group's face has material 1
+    assert fm[0] == 1
+    assert np.array_equal(mats.diffuse[8], np.array([0.25, 0.5, 0.75], np.float32))
+    d = tmp_path / "plain"
+    d.mkdir()
+    _write_case(d, cases["plain"][0])
+    v, ix, fm, kind, vals, mats = _obj_product(d / "plain.obj")
+    assert np.all(fm == 0) and list(kind) == [RQ_MAT_DEFAULT]
+
+
+def test_obj_errors(tmp_path):
+    from rfmanta_b200._lib import RQ_ERR_FORMAT, RQ_ERR_NOTFOUND, RQError
+    from rfmanta_b200.meshio import read_obj
+    with pytest.raises(RQError) as e:
+        read_obj(tmp_path / "missing.obj")
+    assert e.value.code == RQ_ERR_NOTFOUND
+    (tmp_path / "nolib.obj").write_text("mtllib nothere.mtl\nv 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
+    with pytest.raises(RQError) as e:
+        read_obj(tmp_path / "nolib.obj")
+    assert e.value.code == RQ_ERR_NOTFOUND
+    (tmp_path / "range.obj").write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 4\n")
+    with pytest.raises(RQError) as e:
+        read_obj(tmp_path / "range.obj")
+    assert e.value.code == RQ_ERR_FORMAT
+    (tmp_path / "w.obj").write_text("v 0 0 0 1\nv 1 0 0 1\nv 0 1 0 1\nf 1 2 3\n")
+    with pytest.raises(RQError) as e:
+        read_obj(tmp_path / "w.obj")
+    assert e.value.code == RQ_ERR_FORMAT
+
+
+@pytest.mark.gpu
+def test_obj_mesh_renders(tmp_path, restatement):
+    """An OBJ mesh with its material table goes into a device scene and a
+    supersampled frame (Phong entries with their exponents) equals the
+    restatement's."""
+    from oracle.pyoracle import Tree
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    from rfmanta_b200.meshio import read_obj
+    from rfmanta_b200.treeio import parse_dynbvh_blob
+    name, files, obj = obj_cases()[0]
+    _write_case(tmp_path, files)
+    mesh, mats = read_obj(tmp_path / obj)
+    bvh = GpuDynBVH()
+    bvh.setGroup(mesh)
+    bvh.rebuild()
+    sc = scenes.tiny_frame_scene(xres=32, yres=24)
+    sc.mesh = mesh
+    sc.spp, sc.seed = 4, 7
+    sc.specpow = mats.specpow()
+    sc.specular = mats.specular
+    sc.camera = scenes.Camera(eye=(0.5, -2.5, 3.0), lookat=(0.0, 0.0, 0.0), up=(0.0, 0.0, 1.0),
+                              hfov=60.0, vfov=45.0)
+    out = bvh.render_frame(sc, mesh.materials)
+    f = parse_dynbvh_blob(bvh.exportBlob(), mesh.n_tris)
+    W = restatement.world(Tree(f.bounds, f.child, f.children, f.axis, f.left_cheaper, f.ids),
+                          mesh)
+    exp = restatement.render_frame(W, sc, mesh.materials, specular=mats.specular,
+                                   specpow=sc.specpow)
+    assert out["shadow_rays"] == exp["shadow_rays"]
+    assert np.array_equal(out["rgb"].view(np.uint32), exp["rgb"].view(np.uint32))
+    assert np.count_nonzero(out["rgb"].sum(1)) > 0

@@ -190,6 +190,14 @@ struct rq_batch_plan {
   cudaStream_t cap_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // the scenes' descriptors as captured, and their generations: a scene
+  // updated since (refit, rotations, new tree) gets its descriptor copied
+  // in again before the next launch
+  std::vector<const rq::Scene*> scenes;
+  std::vector<uint64_t> generations;
+  std::vector<rq::DevScene> host_scenes;
+  int stack_depth = 1;
+  int num_sms = 148;
   ~rq_batch_plan() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -215,6 +223,49 @@ rq_batch_config default_batch_config() {
   c.refill_threshold = 8;
   c.reg_stack = 2;
   return c;
+}
+
+// Sizes the traversal stack for the plan's deepest tree and captures
+// counter reset + persistent launch in a graph (again after a scene's tree
+// grew deeper).
+int capture_plan(rq_batch_plan* p) {
+  using namespace rq;
+  const rq_batch_config& cfg = p->cfg;
+  BatchArgs& A = p->args;
+  A.stack_depth = p->stack_depth;
+  p->smem = (size_t)p->stack_depth * cfg.block_threads * sizeof(int2);
+  const bool stats = A.stats != nullptr;
+  const void* f = nullptr;
+  batch_dispatch(p->tri_kind, cfg.reg_stack, stats, false, 0, 0, 0, A, nullptr, &f);
+  if (p->smem > 48 * 1024 &&
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem) !=
+          cudaSuccess)
+    return bfail(RQ_ERR_CAPACITY, "traversal stack does not fit in shared memory");
+  int bps = cfg.blocks_per_sm;
+  if (bps <= 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, f, cfg.block_threads, p->smem) !=
+            cudaSuccess ||
+        bps <= 0)
+      bps = 1;
+  }
+  const long long warps_needed = A.total_chunks;  // at most one chunk per warp to start
+  const long long max_blocks =
+      std::max(1LL, (warps_needed * 32 + cfg.block_threads - 1) / cfg.block_threads);
+  p->grid = (int)std::max(1LL, std::min((long long)bps * p->num_sms, max_blocks));
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->exec = nullptr;
+  p->graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(p->d_counter, 0, sizeof(int), p->cap_stream);
+    batch_dispatch(p->tri_kind, cfg.reg_stack, stats, true, p->grid, cfg.block_threads, p->smem,
+                   A, p->cap_stream, nullptr);
+    e = cudaStreamEndCapture(p->cap_stream, &p->graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+  if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+  return RQ_OK;
 }
 
 }  // namespace
@@ -292,22 +343,6 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
       cudaMemcpy(p->d_batches, bd.data(), sizeof(BatchDesc) * n_batches,
                  cudaMemcpyHostToDevice) != cudaSuccess)
     return bfail(RQ_ERR_CUDA, "plan table upload");
-  p->smem = (size_t)depth * cfg.block_threads * sizeof(int2);
-  const bool stats = s0->stats != nullptr;
-  const void* f = nullptr;
-  batch_dispatch(p->tri_kind, cfg.reg_stack, stats, false, 0, 0, 0, p->args, nullptr, &f);
-  if (p->smem > 48 * 1024)
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
-  int bps = cfg.blocks_per_sm;
-  if (bps <= 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, f, cfg.block_threads, p->smem) !=
-            cudaSuccess ||
-        bps <= 0)
-      bps = 1;
-  }
-  const int warps_needed = chunks;  // at most one chunk per warp to start
-  const int max_blocks = std::max(1, (warps_needed * 32 + cfg.block_threads - 1) / cfg.block_threads);
-  p->grid = std::max(1, std::min(bps * s0->num_sms, max_blocks));
   BatchArgs& A = p->args;
   A.scenes = p->d_scenes;
   A.n_scenes = n_scenes;
@@ -316,21 +351,20 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
   A.total_chunks = chunks;
   A.chunk_rays = cfg.chunk_rays;
   A.refill = cfg.refill_threshold;
-  A.stack_depth = depth;
   A.counter = p->d_counter;
   A.stats = s0->stats;
-  // capture counter reset + launch in a graph
+  p->num_sms = s0->num_sms;
+  p->stack_depth = depth;
+  p->host_scenes = ds;
+  for (int i = 0; i < n_scenes; ++i) {
+    const Scene* s = reinterpret_cast<const Scene*>(scenes[i]);
+    p->scenes.push_back(s);
+    p->generations.push_back(s->generation);
+  }
   if (cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
     return bfail(RQ_ERR_CUDA, "stream");
-  cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    cudaMemsetAsync(p->d_counter, 0, sizeof(int), p->cap_stream);
-    batch_dispatch(p->tri_kind, cfg.reg_stack, stats, true, p->grid, cfg.block_threads, p->smem,
-                   A, p->cap_stream, nullptr);
-    e = cudaStreamEndCapture(p->cap_stream, &p->graph);
-  }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
-  if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+  const int rc = capture_plan(p.get());
+  if (rc != RQ_OK) return rc;
   *out = p.release();
   return RQ_OK;
 }
@@ -338,6 +372,33 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
 int rq_batch_plan_launch(rq_batch_plan* plan, void* stream) {
   if (!plan) return bfail(RQ_ERR_ARG, "NULL plan");
   if (cudaSetDevice(plan->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
+  bool changed = false;
+  for (size_t i = 0; i < plan->scenes.size(); ++i) {
+    const rq::Scene* s = plan->scenes[i];
+    if (s->generation == plan->generations[i]) continue;
+    if (!s->has_tree) return bfail(RQ_ERR_STATE, "a scene of the plan has no tree");
+    plan->host_scenes[i] = s->dev();
+    plan->generations[i] = s->generation;
+    changed = true;
+  }
+  if (changed) {
+    int depth = 1;
+    for (const rq::DevScene& d : plan->host_scenes) depth = std::max(depth, d.depth);
+    if (depth > plan->stack_depth) {
+      // a deeper tree: a larger stack, captured again (after the launches
+      // already queued, which still use the old graph)
+      plan->stack_depth = depth;
+      const int rc = capture_plan(plan);
+      if (rc != RQ_OK) return rc;
+    }
+    // ordered before this launch on its stream (pageable source: the copy
+    // is staged before the call returns)
+    const cudaError_t c =
+        cudaMemcpyAsync(plan->d_scenes, plan->host_scenes.data(),
+                        sizeof(rq::DevScene) * plan->host_scenes.size(), cudaMemcpyHostToDevice,
+                        static_cast<cudaStream_t>(stream));
+    if (c != cudaSuccess) return bfail(RQ_ERR_CUDA, "scene table");
+  }
   const cudaError_t e = cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
   return RQ_OK;

@@ -124,6 +124,7 @@ int set_instance_tree(Scene* s, const HostTree& t) {
   }
   s->depth = L.depth;
   s->has_tree = true;
+  ++s->generation;
   return RQ_OK;
 }
 
@@ -207,7 +208,10 @@ int rq_scene_create_instanced(rq_scene* const* inner, int n_inner, const int32_t
   s->verts = verts;
   s->idx = idx;
   s->instanced = true;
-  for (int i = 0; i < n_inner; ++i) s->blas.push_back(inner[i]);
+  for (int i = 0; i < n_inner; ++i) {
+    s->blas.push_back(inner[i]);
+    s->blas_generation.push_back(inner[i]->generation);
+  }
   s->inst_blas.assign(inst_scene, inst_scene + n_instances);
   s->inst_translation.assign(inst_translation, inst_translation + 3 * (size_t)n_instances);
   s->inst_kind.assign(n_instances, RQ_INST_TRANSLATE);
@@ -590,6 +594,10 @@ int frame_prepare(rq::Scene* s, const rq_frame_params* fp, rq::FrameParams& P,
     for (uint32_t id : m->face_mat)
       if ((int)id >= p->n_materials) return ifail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return ifail(RQ_ERR_STATE, "scene has no tree");
+  if (s->instanced) {
+    const int rc = s->check_inner_current();
+    if (rc != RQ_OK) return rc;
+  }
   std::memset(&P, 0, sizeof(P));
   camera_basis(p->eye, p->lookat, p->up, p->hfov, p->vfov, P.cam);
   P.xres = p->xres;

@@ -177,6 +177,7 @@ int update_tree(Scene* s, int mode) {
   s->tree_stale = true;
   s->tree_from_dyn = false;
   if (s->dyn) mark_dyn_bounds_stale(s->dyn);
+  ++s->generation;
   return RQ_OK;
 }
 

@@ -1188,6 +1188,7 @@ int rotate_update(Scene* s) {
   s->depth = std::max(out.depth, 1);
   s->tree_stale = true;
   s->tree_from_dyn = true;
+  ++s->generation;
   return RQ_OK;
 }
 

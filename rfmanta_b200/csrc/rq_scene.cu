@@ -274,6 +274,15 @@ int Scene::set_tree(const HostTree& t) {
   }
   depth = L.depth;
   has_tree = true;
+  ++generation;
+  return RQ_OK;
+}
+
+int Scene::check_inner_current() const {
+  for (size_t i = 0; i < blas.size(); ++i)
+    if (i >= blas_generation.size() || blas[i]->generation != blas_generation[i])
+      return fail(RQ_ERR_STATE, "an inner scene changed after the two-level scene was made; "
+                                "create the two-level scene again");
   return RQ_OK;
 }
 
@@ -386,6 +395,10 @@ int Scene::trace_device(int n, const float* org, const float* dir,
                         const float* tmax, bool anyhit, float* t, int32_t* prim,
                         float* u, float* v, cudaStream_t st, int* counter) {
   if (!has_tree) return fail(RQ_ERR_STATE, "scene has no tree");
+  if (instanced) {
+    const int rc = check_inner_current();
+    if (rc != RQ_OK) return rc;
+  }
   RayArgs a{n, org, dir, tmax, t, prim, u, v};
   LaunchPlan p = plan(anyhit, n, counter);
   if (p.persistent) {

@@ -128,6 +128,13 @@ struct Scene {
   DevScene* d_blas = nullptr;
   int max_blas_depth = 0;
 
+  // bumped whenever the device tree or the descriptor dev() returns changes
+  // (a new tree, an update); users that keep copies of dev() (batch plans,
+  // servers, two-level scenes) compare it before they launch
+  uint64_t generation = 0;
+  std::vector<uint64_t> blas_generation;  // two-level: inner generations at creation
+  int check_inner_current() const;
+
   rq_launch_config cfg[4];  // RQ_CLOSEST, RQ_ANYHIT, RQ_PATH_EXTEND, RQ_PATH_SHADE
   int* d_counter = nullptr;  // persistent-launch counters for rq_trace_device
 

@@ -368,6 +368,11 @@ struct rq_server {
   long long steps = 0;
   int grid = 1;
   size_t smem = 0;
+  // the scenes' descriptors as uploaded and their generations: a scene
+  // updated since (refit, rotations, new tree) gets its descriptor copied in
+  // again before the next step
+  std::vector<uint64_t> generations;
+  std::vector<rq::DevScene> host_scenes;
 
   ~rq_server() {
     cudaSetDevice(device);
@@ -514,6 +519,8 @@ int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capac
   s->smem = (size_t)s->depth * 128 * sizeof(int2);
   s->grid = std::max(1, serve_blocks_per_sm(s->tri_kind, s->smem) * s->num_sms);
   s->table.assign(s->max_active, 0);
+  s->host_scenes = ds;
+  for (Scene* sc : s->scenes) s->generations.push_back(sc->generation);
   *out = s.release();
   return RQ_OK;
 }
@@ -554,6 +561,30 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
   if (!s) return sfail(RQ_ERR_ARG, "NULL server");
   if (scheduled_paths) *scheduled_paths = 0;
   if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  // scenes updated since the last step: new descriptors (ordered on the
+  // server's stream before this step) and a stack for the deepest tree
+  bool changed = false;
+  for (size_t i = 0; i < s->scenes.size(); ++i) {
+    const Scene* sc = s->scenes[i];
+    if (sc->generation == s->generations[i]) continue;
+    if (!sc->has_tree) return sfail(RQ_ERR_STATE, "a scene of the server has no tree");
+    s->host_scenes[i] = sc->dev();
+    s->generations[i] = sc->generation;
+    changed = true;
+  }
+  if (changed) {
+    int depth = 1;
+    for (const DevScene& d : s->host_scenes) depth = std::max(depth, d.depth);
+    if (cudaMemcpyAsync(s->d_scenes, s->host_scenes.data(),
+                        sizeof(DevScene) * s->host_scenes.size(), cudaMemcpyHostToDevice,
+                        s->stream) != cudaSuccess)
+      return sfail(RQ_ERR_CUDA, "scene table");
+    if (depth != s->depth) {
+      s->depth = depth;
+      s->smem = (size_t)depth * 128 * sizeof(int2);
+      s->grid = std::max(1, serve_blocks_per_sm(s->tri_kind, s->smem) * s->num_sms);
+    }
+  }
   // admission in arrival order while the budget allows
   while (!s->pending.empty()) {
     HostReq& r = *s->reqs[s->pending.front()];

@@ -114,3 +114,32 @@ def test_plan_errors(setup):
     assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, None, C.byref(plan)) == _lib.RQ_ERR_ARG
     arr[0].scene = 0
     assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, None, C.byref(plan)) == _lib.RQ_ERR_ARG
+
+
+def test_plan_follows_scene_updates():
+    """A plan made before a scene's mesh moved (rotating update, new tree
+    layout, possibly a deeper tree) launches on the updated scene: the plan
+    copies in the scene's new descriptor, and its results equal tracing the
+    updated scene alone."""
+    import torch
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.batch import BatchedQueries, QueryBatch
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    mesh = scenes.small_frame_scene(level=3, grid=10).mesh
+    bvh = GpuDynBVH()
+    bvh.setGroup(mesh)
+    bvh.rebuild()
+    lo, hi = mesh.bounds()
+    o, d, tm, _ = scenes.random_rays(5000, lo - 0.3, hi + 0.3, seed=3)
+    tm = np.full(o.shape[1], 1e19, np.float32)
+    batch = QueryBatch(0, torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda(),
+                       torch.from_numpy(tm).cuda(), False, want_uv=True)
+    bq = BatchedQueries([bvh], [batch], dict(reg_stack=0))
+    bq.launch()
+    v0 = mesh.vertices.copy()
+    for k, rotate in ((1, True), (2, False), (3, True)):
+        mesh.vertices = scenes.animated_vertices(v0, k, amplitude=0.05)
+        bvh.update(rotate=rotate)
+        bq.launch()
+        _check(bq, _expected([bvh], [(0, o, d, tm, False)]))
+    bq.close()

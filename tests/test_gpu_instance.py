@@ -225,3 +225,24 @@ def test_bad_instance_arguments():
     with pytest.raises(RQError):  # unknown kind
         InstancedBVH(inner, np.array([0], np.int32), np.zeros((1, 3), np.float32),
                      np.array([7], np.int32)).rebuild()
+
+
+def test_two_level_scene_refuses_updated_inner_scenes():
+    """Instance boxes and inner descriptors are taken when the two-level
+    scene is made; after an inner scene's mesh moves the two-level scene
+    refuses to trace until it is made again."""
+    from rfmanta_b200._lib import RQ_ERR_STATE, RQError
+    from rfmanta_b200.dynbvh import InstancedBVH, RayBatch
+    g = load_instanced()
+    top, inner = _device_scene(g, import_trees=False)
+    rays = RayBatch(g["rand_org"], g["rand_dir"])
+    top.intersect(rays)
+    m = inner[0].getGroup()
+    m.vertices = (m.vertices * np.float32(1.01)).astype(np.float32)
+    inner[0].update()
+    with pytest.raises(RQError) as e:
+        top.intersect(RayBatch(g["rand_org"], g["rand_dir"]))
+    assert e.value.code == RQ_ERR_STATE
+    again = InstancedBVH(inner, g["inst_scene"], g["translation"], g["kind"])
+    again.rebuild()
+    again.intersect(RayBatch(g["rand_org"], g["rand_dir"]))

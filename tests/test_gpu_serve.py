@@ -105,3 +105,32 @@ def test_admission_waits_for_budget(scenes3):
         srv.submit(reqs[3])
     assert e.value.code == _lib.RQ_ERR_CAPACITY
     srv.close()
+
+
+def test_server_follows_scene_updates():
+    """A server keeps serving a scene whose mesh moved (rotating update,
+    new layout, possibly a deeper tree): the next step copies in the new
+    descriptor, and a request after the update equals the frame path
+    tracer on the updated scene."""
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    from rfmanta_b200.serve import RenderServer, request_for_scene
+    mesh = scenes.tiny_path_scene().mesh
+    bvh = GpuDynBVH()
+    bvh.setGroup(mesh)
+    bvh.rebuild()
+    srv = RenderServer([bvh], path_capacity=1 << 15, chunk_pixels=500)
+    r = request_for_scene(0, mesh, 40, 30, 4, 4, seed=7)
+    _run(srv, [r])
+    v0 = mesh.vertices.copy()
+    for k in (1, 2):
+        mesh.vertices = scenes.animated_vertices(v0, k, amplitude=0.05)
+        bvh.update()
+        img = _run(srv, [r])[0]
+        ps = scenes.PathScene(mesh, scenes.Camera(r.eye, r.lookat, r.up, r.hfov, r.vfov),
+                              scenes.AreaLightSpec(r.light_anchor, r.light_v1, r.light_v2,
+                                                   r.light_color),
+                              r.background, r.xres, r.yres, r.spp, r.max_depth, r.rr_depth,
+                              r.seed)
+        assert np.array_equal(_bits(img), _bits(bvh.render_path(ps)["rgb"]))
+    srv.close()

@@ -360,6 +360,7 @@ typedef struct {
   uint64_t seed;
   float light_anchor[3], light_v1[3], light_v2[3], light_color[3];
   float background[3];
+  float ambient[3];                /* as in rq_path_params */
   int n_materials;
   const float* material_rgb;       /* host, copied on submit */
 } rq_serve_request;
@@ -486,6 +487,9 @@ typedef struct {
   float light_v2[3];
   float light_color[3];
   float background[3];
+  float ambient[3];               /* ConstantAmbient, added where a path
+                                     reaches max_depth (KajiyaPathtracer's
+                                     do_ambient_on_maxdepth) */
   int n_materials;
   const float* material_rgb;      /* host: n_materials x (r, g, b) */
   int chunk_paths;                /* paths per wavefront pass, 0 = 4Mi */

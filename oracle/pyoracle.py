@@ -275,7 +275,9 @@ class Restatement:
         fp = np.concatenate([basis, np.asarray(L.anchor, np.float32),
                              np.asarray(L.v1, np.float32), np.asarray(L.v2, np.float32),
                              np.asarray(L.color, np.float32),
-                             np.asarray(scene.background, np.float32)]).astype(np.float32)
+                             np.asarray(scene.background, np.float32),
+                             np.asarray(getattr(scene, "ambient", (0.0, 0.0, 0.0)),
+                                        np.float32)]).astype(np.float32)
         ip = np.array([scene.xres, scene.yres, scene.spp, scene.max_depth, scene.rr_depth],
                       np.int32)
         total = scene.xres * scene.yres * scene.spp
@@ -702,7 +704,8 @@ class RefScene:
                         [cam.hfov, cam.vfov], np.float32)
         L = scene.light
         light = np.array(list(L.anchor) + list(L.v1) + list(L.v2) + list(L.color), np.float32)
-        bg = np.asarray(scene.background, np.float32)
+        bg = np.asarray(list(scene.background) +
+                        list(getattr(scene, "ambient", (0.0, 0.0, 0.0))), np.float32)
         rgb = np.zeros((scene.xres * scene.yres, 3), np.float32)
         secs = C.c_double()
         rays = C.c_longlong()

@@ -1018,7 +1018,9 @@ static void* path_worker(void* p) {
 
 // Path-traced frame through KajiyaPathtracer::traceEyeRays
 // (Engine/Renderers/KajiyaPathtracer.cc:113-302) with its default modes,
-// HardShadows and one Parallelogram AreaLight; rows of 64-ray packets on N
+// HardShadows, one Parallelogram AreaLight and a ConstantAmbient
+// (background[0..2] then the ambient colour in background[3..5]); rows of
+// 64-ray packets on N
 // pthreads, spp stratified-jitter packets per pixel row segment.  *rays =
 // every unmasked ray handed to DynBVH::intersect (camera, bounce, shadow).
 int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
@@ -1043,7 +1045,7 @@ int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
   args.push_back("-normalizeRays");
   ExposedCamera camera(args);
   LightSet* ls = new LightSet();
-  ls->setAmbientLight(new ConstantAmbient(Color(RGB(0, 0, 0))));
+  ls->setAmbientLight(new ConstantAmbient(Color(RGB(background[3], background[4], background[5]))));
   Parallelogram* emitter = new Parallelogram(s->materials[0],
       Vector(light12[0], light12[1], light12[2]), Vector(light12[3], light12[4], light12[5]),
       Vector(light12[6], light12[7], light12[8]));

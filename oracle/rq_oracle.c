@@ -665,7 +665,7 @@ void orq_sincos_2pi(const float* u, int n, float* c, float* s) {
 }
 
 /* params (float): cam[12], light_anchor[3], light_v1[3], light_v2[3],
- * light_color[3], background[3]; iparams: xres, yres, spp, max_depth,
+ * light_color[3], background[3], ambient[3]; iparams: xres, yres, spp, max_depth,
  * rr_depth.  Writes rgb per pixel, ray counts[2] (extension, shadow), and
  * optionally prim[max_depth][n_paths] (-2 where a path had ended). */
 void orq_render_path(const float* bounds, const int* child, const int* children,
@@ -683,6 +683,7 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
   const float* lv2 = fp + 18;
   const float* lcol = fp + 21;
   const float* bg = fp + 24;
+  const float* amb = fp + 27;
   const int xres = ip[0], yres = ip[1], spp = ip[2], maxd = ip[3], rrd = ip[4];
   int strata = 1;
   while (strata * strata < spp) ++strata;
@@ -767,6 +768,11 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
       for (int c = 0; c < 3; ++c) nd[c] = ffn[c] * costheta + v1[c] * cosphi + v2[c] * sinphi;
       const float* kd = mat_rgb + 3 * face_mat[r.prim];
       for (int c = 0; c < 3; ++c) imp[c] = imp[c] * kd[c];
+      /* do_ambient_on_maxdepth (KajiyaPathtracer.cc:259-279): ambient * kd
+         times the importance (which holds this kd) where the path reaches
+         its last bounce */
+      if (depth + 1 >= maxd)
+        for (int c = 0; c < 3; ++c) rad[c] = rad[c] + (amb[c] * kd[c]) * imp[c];
       const float lr1 = pcg_float(&rng);
       const float lr2 = pcg_float(&rng);
       float ld[3];

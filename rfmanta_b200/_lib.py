@@ -75,8 +75,8 @@ class PathParams(C.Structure):
                 ("seed", C.c_uint64), ("light_anchor", C.c_float * 3),
                 ("light_v1", C.c_float * 3), ("light_v2", C.c_float * 3),
                 ("light_color", C.c_float * 3), ("background", C.c_float * 3),
-                ("n_materials", C.c_int), ("material_rgb", C.c_void_p),
-                ("chunk_paths", C.c_int)]
+                ("ambient", C.c_float * 3), ("n_materials", C.c_int),
+                ("material_rgb", C.c_void_p), ("chunk_paths", C.c_int)]
 
 
 class Batch(C.Structure):
@@ -101,7 +101,8 @@ class ServeRequest(C.Structure):
                 ("rr_depth", C.c_int), ("seed", C.c_uint64), ("light_anchor", C.c_float * 3),
                 ("light_v1", C.c_float * 3), ("light_v2", C.c_float * 3),
                 ("light_color", C.c_float * 3), ("background", C.c_float * 3),
-                ("n_materials", C.c_int), ("material_rgb", C.c_void_p)]
+                ("ambient", C.c_float * 3), ("n_materials", C.c_int),
+                ("material_rgb", C.c_void_p)]
 
 
 class LaunchConfig(C.Structure):

@@ -29,6 +29,7 @@ struct PathParams {
   float light_inv_area;   // 1 / |Cross(v1, v2)|
   float light_color[3];
   float background[3];
+  float ambient[3];        // added at max_depth (do_ambient_on_maxdepth)
   const float* materials;  // device, rgb per material id
 };
 

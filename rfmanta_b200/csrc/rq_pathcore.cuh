@@ -219,6 +219,15 @@ __device__ __forceinline__ bool shade_begin(const DevScene& S, const PathParams&
     refl[c] = __ldg(kd + c);
     imp[c] = fmul(imp[c], refl[c]);
   }
+  if (last_depth) {
+    // do_ambient_on_maxdepth (KajiyaPathtracer.cc:259-279): a path still
+    // alive after its last bounce is shaded by its material with ambient
+    // light only (Lambertian: ambient * kd) times its importance, which
+    // already holds this surface's reflectance
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      B.rad[c * C + p] = fadd(B.rad[c * C + p], fmul(fmul(P.ambient[c], refl[c]), imp[c]));
+  }
   // one area-light sample
   const float lr1 = pcg32_float(rng);
   const float lr2 = pcg32_float(rng);

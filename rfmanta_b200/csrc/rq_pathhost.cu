@@ -83,6 +83,7 @@ static int path_prepare(Scene* s, const rq_path_params* p, PathParams& P, long l
     P.light_v2[c] = p->light_v2[c];
     P.light_color[c] = p->light_color[c];
     P.background[c] = p->background[c];
+    P.ambient[c] = p->ambient[c];
   }
   // Parallelogram constructor (Model/Primitives/Parallelogram.cc:26-35)
   float n[3] = {p->light_v1[1] * p->light_v2[2] - p->light_v1[2] * p->light_v2[1],

@@ -440,6 +440,7 @@ void request_params(const rq_serve_request& q, rq::PathParams& P) {
     P.light_v2[c] = q.light_v2[c];
     P.light_color[c] = q.light_color[c];
     P.background[c] = q.background[c];
+    P.ambient[c] = q.ambient[c];
   }
   const float* v1 = q.light_v1;
   const float* v2 = q.light_v2;

@@ -355,6 +355,7 @@ class GpuDynBVH:
         p.light_v2[:] = L.v2
         p.light_color[:] = L.color
         p.background[:] = scene.background
+        p.ambient[:] = getattr(scene, "ambient", (0.0, 0.0, 0.0))
         mats = np.ascontiguousarray(scene.mesh.materials, np.float32)
         p.n_materials = mats.shape[0]
         p.material_rgb = mats.ctypes.data

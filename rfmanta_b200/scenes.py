@@ -311,6 +311,7 @@ class PathScene:
     max_depth: int
     rr_depth: int
     seed: int = 1
+    ambient: tuple = (0.0, 0.0, 0.0)  # ConstantAmbient, added at max_depth
 
 
 def path_scene(hf_nx: int = 512, hf_nz: int = 1024, n_spheres: int = 32,

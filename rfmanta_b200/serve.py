@@ -36,6 +36,7 @@ class RenderRequest:
     light_color: tuple
     background: tuple
     materials: np.ndarray = field(default_factory=lambda: np.full((1, 3), 0.7, np.float32))
+    ambient: tuple = (0.0, 0.0, 0.0)
 
     def to_c(self) -> _lib.ServeRequest:
         q = _lib.ServeRequest()
@@ -47,6 +48,7 @@ class RenderRequest:
         q.light_anchor[:], q.light_v1[:], q.light_v2[:] = (self.light_anchor, self.light_v1,
                                                            self.light_v2)
         q.light_color[:], q.background[:] = self.light_color, self.background
+        q.ambient[:] = self.ambient
         m = np.ascontiguousarray(self.materials, np.float32)
         q.n_materials = m.shape[0]
         q.material_rgb = m.ctypes.data

@@ -27,7 +27,8 @@ for the PLY files the tests write (tests/test_mesh_io.py), and
 tree_update.npz: DynBVH::update with its tree rotations over four frames of a
 seeded animation (the tree, per-node costs and nextFree after every frame),
 and path_stats.npz: KajiyaPathtracer images of the tiny path scene for 16
-seeds at 4096 samples per pixel (the expectation the path tracer must match),
+seeds at 4096 samples per pixel, at depth 4 and at depth 2 with a constant
+ambient light (the expectation the path tracer must match),
 and obj_cases.npz: Manta::ObjGroup's vertices, triangles, face materials and
 material table for the OBJ files the tests write.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
@@ -231,6 +232,7 @@ def write_tree_update() -> None:
 
 
 PATH_STATS = dict(xres=16, yres=12, spp=4096, seeds=16)
+PATH_AMBIENT = (0.3, 0.4, 0.5)
 
 
 def write_path_stats() -> None:
@@ -241,13 +243,19 @@ def write_path_stats() -> None:
     p = PATH_STATS
     sc = scenes.tiny_path_scene(xres=p["xres"], yres=p["yres"], spp=p["spp"])
     rs = ref.scene(sc.mesh, 0)
-    imgs = []
+    imgs, amb = [], []
     for s in range(p["seeds"]):
         sc.seed = 2000 + s
+        sc.ambient = (0.0, 0.0, 0.0)
         imgs.append(rs.render_path(sc, nthreads=1)["rgb"].reshape(p["yres"], p["xres"], 3))
+        sc.ambient, sc.max_depth = PATH_AMBIENT, 2  # most paths reach the last bounce
+        amb.append(rs.render_path(sc, nthreads=1)["rgb"].reshape(p["yres"], p["xres"], 3))
+        sc.max_depth = 4
     rs.close()
     path = os.path.join(OUT, "path_stats.npz")
     np.savez_compressed(path, images=np.array(imgs, np.float32),
+                        images_ambient=np.array(amb, np.float32),
+                        ambient=np.array(PATH_AMBIENT, np.float32),
                         seed_values=np.arange(2000, 2000 + p["seeds"]),
                         **{k: np.int64(v) for k, v in p.items()})
     print(path, os.path.getsize(path), "bytes")

@@ -104,3 +104,36 @@ def test_medium_frame_sampled_paths(restatement):
             acc = (acc + r[:, s]).astype(np.float32)
         acc = (acc * np.float32(1.0 / sc.spp)).astype(np.float32)
         assert np.array_equal(_bits(out["rgb"][pix0:pix0 + 40]), _bits(acc))
+
+
+@pytest.mark.parametrize("max_depth", [2, 4])
+def test_ambient_at_max_depth_bit_exact(tiny, restatement, max_depth):
+    """With a ConstantAmbient light the paths that reach their last bounce
+    add ambient * kd times their importance (do_ambient_on_maxdepth):
+    device and restatement agree bit for bit, in a served request too."""
+    import dataclasses
+    from rfmanta_b200.serve import RenderServer, request_for_scene
+    kind, sc, bvh, tree = tiny
+    s2 = dataclasses.replace(sc, ambient=(0.3, 0.4, 0.5), max_depth=max_depth)
+    out = bvh.render_path(s2)
+    exp = restatement.render_path(tree, s2, tri_kind=kind)
+    assert out["rays"] == exp["rays"]
+    assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))
+    plain = bvh.render_path(dataclasses.replace(s2, ambient=(0.0, 0.0, 0.0)))
+    assert np.all(out["rgb"].sum(0) > plain["rgb"].sum(0))
+    srv = RenderServer([bvh], path_capacity=1 << 15, chunk_pixels=300)
+    q = request_for_scene(0, sc.mesh, s2.xres, s2.yres, s2.spp, max_depth, seed=s2.seed)
+    q = dataclasses.replace(q, eye=s2.camera.eye, lookat=s2.camera.lookat, up=s2.camera.up,
+                            hfov=s2.camera.hfov, vfov=s2.camera.vfov, rr_depth=s2.rr_depth,
+                            light_anchor=s2.light.anchor, light_v1=s2.light.v1,
+                            light_v2=s2.light.v2, light_color=s2.light.color,
+                            background=s2.background, ambient=s2.ambient,
+                            materials=sc.mesh.materials)
+    rid = srv.submit(q)
+    for _ in range(10000):
+        srv.step()
+        if rid in srv.poll():
+            break
+    img, _, _ = srv.result(rid, q.xres, q.yres)
+    srv.close()
+    assert np.array_equal(_bits(img), _bits(out["rgb"]))

@@ -36,13 +36,21 @@ def _z(a, b):
     return (a.mean(0) - b.mean(0)) / np.sqrt(va + vb + 1e-30)
 
 
-def test_images_match_reference_in_expectation(restatement):
+import pytest
+
+
+@pytest.mark.parametrize("with_ambient", [False, True])
+def test_images_match_reference_in_expectation(restatement, with_ambient):
+    """At depth 4, and at depth 2 with a ConstantAmbient light (added where
+    a path reaches its last bounce, do_ambient_on_maxdepth)."""
     from oracle.pyoracle import Tree
     from rfmanta_b200 import scenes
     z = np.load(os.path.join(GOLDEN, "path_stats.npz"))
-    ref = z["images"].astype(np.float64)
+    ref = z["images_ambient" if with_ambient else "images"].astype(np.float64)
     xres, yres, spp = int(z["xres"]), int(z["yres"]), int(z["spp"])
     sc = scenes.tiny_path_scene(xres=xres, yres=yres, spp=spp)
+    if with_ambient:  # depth 2: most paths reach the last bounce
+        sc.ambient, sc.max_depth = tuple(float(x) for x in z["ambient"]), 2
     assert ref.shape[1:] == (yres, xres, 3)
     # the image's expectation does not depend on the tree, so any valid tree
     # over the mesh serves (a median split, built here without a GPU)
@@ -57,6 +65,10 @@ def test_images_match_reference_in_expectation(restatement):
     # the check has the power to see a 0.1% bias
     biased = _z((ours * 1.001).mean((1, 2)), ref.mean((1, 2)))
     assert np.all(np.abs(biased) > 4.0), biased
+    if with_ambient:  # and the ambient term is there to be seen
+        sc.ambient = (0.0, 0.0, 0.0)
+        dark = _ours(restatement, tree, sc, range(4000, 4008))
+        assert np.all(np.abs(_z(dark.mean((1, 2)), ref.mean((1, 2)))) > 8.0)
 
 
 def _median_tree(mesh):

@@ -450,15 +450,23 @@ RQ_API int rq_trace_device_ex(rq_scene* scene, int n, const float* d_org,
  * averaged in sample order; spp = 1 samples pixel centres and equals
  * rq_render_whitted.  Materials are Lambertian (Model/Materials/
  * Lambertian.cc) unless material_specpow[m] >= 0: then material m is a Phong
- * without reflection (Model/Materials/Phong.cc:130-410, refl = 0) with
- * diffuse material_rgb[m], specular material_specular[m] and that
- * exponent.  Both Phong arrays NULL = all Lambertian. */
+ * (Model/Materials/Phong.cc:130-540) with diffuse material_rgb[m], specular
+ * material_specular[m], that exponent and reflectivity
+ * material_reflectivity[m] (NULL = none): a reflective Phong hit at depth
+ * d < max_depth traces the mirrored ray with importance x reflectivity when
+ * that importance's luminance exceeds importance_cutoff, and adds its colour
+ * x reflectivity (Raytracer::traceRays recursion; the reference's
+ * RenderParameters default to max_depth 15, importance_cutoff 0.01).  Both
+ * Phong arrays NULL = all Lambertian. */
 typedef struct {
   rq_whitted_params whitted;
   int spp;        /* 1, 4, 16, ... */
   uint64_t seed;
   const float* material_specular;   /* 3 per material, or NULL */
   const int32_t* material_specpow;  /* 1 per material, or NULL */
+  const float* material_reflectivity; /* 1 per material, or NULL */
+  int max_depth;                    /* 0..32, with material_reflectivity */
+  float importance_cutoff;
 } rq_frame_params;
 
 RQ_API int rq_render_frame(rq_scene* scene, const rq_frame_params* params, float* rgb,

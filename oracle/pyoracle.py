@@ -196,7 +196,8 @@ class Restatement:
                                       [C.c_void_p] * 6)
         L.orq_sample_coords.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_longlong,
                                         C.c_longlong, C.c_void_p, C.c_void_p]
-        L.orq_render_frame.argtypes = ([C.c_void_p] * 5 + [C.c_int] * 3 + [C.c_uint64] +
+        L.orq_render_frame.argtypes = ([C.c_void_p] * 5 + [C.c_int, C.c_float, C.c_void_p] +
+                                       [C.c_int] * 3 + [C.c_uint64] +
                                        [C.c_void_p, C.c_int] + [C.c_void_p] * 2 +
                                        [C.c_int, C.c_int] + [C.c_void_p] * 4)
         L.orq_render_frame.restype = C.c_longlong
@@ -228,10 +229,12 @@ class Restatement:
         return px, py
 
     def render_frame(self, world: World, scene, materials, rows=None, per_sample=False,
-                     specular=None, specpow=None):
+                     specular=None, specpow=None, reflectivity=None, max_depth=15,
+                     cutoff=0.01):
         """Supersampled Whitted frame (any scene with camera, lights,
         ambient, background, xres, yres, spp, seed) over a world; materials
-        with specpow >= 0 are Phong with the given specular colour."""
+        with specpow >= 0 are Phong with the given specular colour and
+        reflectivity (RenderParameters maxDepth / importanceCutoff)."""
         basis = self.camera_basis(scene.camera)
         xres, yres, spp = scene.xres, scene.yres, scene.spp
         y0, y1 = rows if rows else (0, yres)
@@ -247,8 +250,9 @@ class Restatement:
         srgb = np.zeros((npx * spp, 3), np.float32) if per_sample else None
         st = np.zeros(npx * spp, np.float32) if per_sample else None
         sp = np.zeros(npx * spp, np.int32) if per_sample else None
-        ns = self.lib.orq_render_frame(world.ptr, _ptr(mats), _ptr(spec), _ptr(spow),
-                                       _ptr(basis), xres, yres, spp,
+        refl = None if reflectivity is None else np.ascontiguousarray(reflectivity, np.float32)
+        ns = self.lib.orq_render_frame(world.ptr, _ptr(mats), _ptr(spec), _ptr(spow), _ptr(refl),
+                                       int(max_depth), float(cutoff), _ptr(basis), xres, yres, spp,
                                        int(scene.seed), _ptr(lights), lights.shape[0],
                                        _ptr(amb), _ptr(bg), y0, y1, _ptr(rgb), _ptr(srgb),
                                        _ptr(st), _ptr(sp))
@@ -458,7 +462,8 @@ class Reference:
         L.mref_scene_create_instanced.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
                                                   [C.c_int])
         L.mref_scene_create_instanced.restype = C.c_void_p
-        L.mref_scene_set_phong.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.mref_scene_set_phong.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_float]
+        L.mref_scene_set_render_parameters.argtypes = [C.c_void_p, C.c_int, C.c_float]
         L.mref_read_ply.argtypes = ([C.c_char_p, C.c_void_p, C.c_int] + [C.c_void_p] * 5 +
                                     [C.c_int, C.c_int])
         L.mref_scene_update_vertices.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
@@ -554,12 +559,17 @@ class RefScene:
         if not self.h:
             raise RuntimeError("reference scene build failed")
 
-    def set_phong(self, material: int, specular, specpow: int) -> None:
-        """Material `material` becomes a Phong (no reflection) with its
-        diffuse colour and the given specular colour and exponent."""
+    def set_phong(self, material: int, specular, specpow: int, reflectivity: float = 0.0) -> None:
+        """Material `material` becomes a Phong with its diffuse colour and
+        the given specular colour, exponent and reflectivity (0: none)."""
         sp = np.ascontiguousarray(specular, np.float32)
-        if self.ref.lib.mref_scene_set_phong(self.h, material, _ptr(sp), int(specpow)) != 0:
+        if self.ref.lib.mref_scene_set_phong(self.h, material, _ptr(sp), int(specpow),
+                                             float(reflectivity)) != 0:
             raise RuntimeError("mref_scene_set_phong failed")
+
+    def set_render_parameters(self, max_depth: int, cutoff: float) -> None:
+        """RenderParameters maxDepth / importanceCutoff of later renders."""
+        self.ref.lib.mref_scene_set_render_parameters(self.h, int(max_depth), float(cutoff))
 
     def update_vertices(self, vertices) -> None:
         """Animated mesh: new vertex positions, WaldTriangle::update and

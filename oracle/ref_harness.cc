@@ -280,10 +280,20 @@ void* mref_scene_create(const float* verts, int nverts, const unsigned* idx,
   }
 }
 
+// RenderParameters::maxDepth and importanceCutoff of the scene's renders
+// (Interface/RenderParameters.h: 15 and 0.01 unless set).
+int mref_scene_set_render_parameters(void* h, int max_depth, float cutoff) {
+  RefScene* s = static_cast<RefScene*>(h);
+  if (!s->scene) s->scene = new Scene();
+  s->scene->getRenderParameters().maxDepth = max_depth;
+  s->scene->getRenderParameters().importanceCutoff = cutoff;
+  return 0;
+}
+
 // Makes material k of a scene a Phong (Model/Materials/Phong.cc) with the
-// material's diffuse colour, the given specular colour and exponent and no
-// reflection, in place of its Lambertian.
-int mref_scene_set_phong(void* h, int k, const float* specular, int specpow) {
+// material's diffuse colour, the given specular colour, exponent and
+// reflectivity (0: no reflection), in place of its Lambertian.
+int mref_scene_set_phong(void* h, int k, const float* specular, int specpow, float refl) {
   RefScene* s = static_cast<RefScene*>(h);
   if (!s->mesh || k < 0 || k >= (int)s->mesh->materials.size()) return 1;
   Material* old = s->mesh->materials[k];
@@ -291,7 +301,7 @@ int mref_scene_set_phong(void* h, int k, const float* specular, int specpow) {
   if (!lam) return 2;
   const float* kd = s->diffuse.data() + 3 * k;
   Material* ph = new Phong(Color(RGB(kd[0], kd[1], kd[2])),
-                           Color(RGB(specular[0], specular[1], specular[2])), specpow, 0);
+                           Color(RGB(specular[0], specular[1], specular[2])), specpow, refl);
   s->mesh->materials[k] = ph;
   for (size_t i = 0; i < s->materials.size(); ++i)
     if (s->materials[i] == old) s->materials[i] = ph;

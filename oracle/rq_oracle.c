@@ -989,52 +989,57 @@ static float ipow_f(float x, int p) {
 /* Material m is a Phong (Model/Materials/Phong.cc:130-410, scalar branch,
  * no reflection) when mat_pow is given and mat_pow[m] >= 0, else a
  * Lambertian. */
-static long long whitted_sample(const orq_world* W, const float* mat_rgb,
-                                const float* mat_spec, const int* mat_pow, const float* cam,
-                                float px, float py, const float* lights, int nl,
-                                const float* ambient, const float* background,
-                                float* rgb, float* tprim, int* prim) {
-  Ray r;
-  const float* dir = cam + 3;
-  const float* cu = cam + 6;
-  const float* cv = cam + 9;
-  for (int c = 0; c < 3; ++c) {
-    r.o[c] = cam[c];
-    r.d[c] = cv[c] * px + cu[c] * py + dir[c];
-  }
-  v_normalize(r.d);
-  for (int c = 0; c < 3; ++c) r.inv[c] = (float)1 / r.d[c];
-  r.minT = MAXT;
-  r.hit = 0;
-  r.prim = -1;
-  r.u = r.v = 0.f;
-  r.anyhit = 0;
-  r.node_tests = r.tri_tests = 0;
+/* How a frame shades: material tables, lights, and the recursion limits of
+ * reflective Phong (RenderParameters::maxDepth / importanceCutoff,
+ * Interface/RenderParameters.h:11-15). */
+typedef struct {
+  const float* mat_rgb;
+  const float* mat_spec;
+  const int* mat_pow;    /* >= 0: Phong with that exponent */
+  const float* mat_refl; /* Phong reflectivity (NULL = none) */
+  const float* lights;
+  int nl;
+  const float* ambient;
+  const float* background;
+  int max_depth;
+  float cutoff;
+} Shading;
+
+/* Raytracer::traceRays for one ray (Engine/Renderers/Raytracer.cc:49-97):
+ * the closest hit shaded by its material - Lambertian::shade, or
+ * Phong::shade (Model/Materials/Phong.cc:130-540, scalar branches) whose
+ * reflection, when its reflectivity is not 0 and depth < maxDepth, traces
+ * the mirrored ray d - N (2 N.d) from the hit point with importance x
+ * reflectivity if that importance's luminance exceeds the cutoff (else its
+ * colour is black) and adds its colour x reflectivity - with HardShadows
+ * shadow rays to every point light; the background where nothing is hit.
+ * Returns the shadow rays sent; *kout is the hit instance. */
+static long long trace_color(const orq_world* W, const Shading* S, Ray* r, int depth,
+                             const float* imp, float* rgb, int* kout) {
   int k;
-  world_trace(W, &r, &k);
-  *tprim = r.minT;
-  *prim = r.hit ? r.prim : -1;
-  if (!r.hit) {
-    for (int c = 0; c < 3; ++c) rgb[c] = background[c];
+  world_trace(W, r, &k);
+  *kout = k;
+  if (!r->hit) {
+    for (int c = 0; c < 3; ++c) rgb[c] = S->background[c];
     return 0;
   }
   const orq_tree* HT = W->inner ? &W->inner[W->inst_scene[k]] : W->top;
   const Tree T = as_tree(HT);
-  const unsigned m = HT->face_mat[r.prim];
-  const float* kd = mat_rgb + 3 * m;
-  const int phong = mat_pow && mat_pow[m] >= 0;
+  const unsigned m = HT->face_mat[r->prim];
+  const float* kd = S->mat_rgb + 3 * m;
+  const int phong = S->mat_pow && S->mat_pow[m] >= 0;
   float spec[3] = {0.f, 0.f, 0.f};
   float nrm[3];
-  tri_normal(&T, r.prim, nrm);
+  tri_normal(&T, r->prim, nrm);
   float ffn[3];
-  const float dn = nrm[0] * r.d[0] + nrm[1] * r.d[1] + nrm[2] * r.d[2];
+  const float dn = nrm[0] * r->d[0] + nrm[1] * r->d[1] + nrm[2] * r->d[2];
   for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0) ? nrm[c] : -nrm[c];
-  float total[3] = {ambient[0], ambient[1], ambient[2]};
+  float total[3] = {S->ambient[0], S->ambient[1], S->ambient[2]};
   float hp[3];
-  for (int c = 0; c < 3; ++c) hp[c] = r.o[c] + r.d[c] * r.minT;
+  for (int c = 0; c < 3; ++c) hp[c] = r->o[c] + r->d[c] * r->minT;
   long long shadow_rays = 0;
-  for (int j = 0; j < nl; ++j) {
-    const float* L = lights + 6 * j;
+  for (int j = 0; j < S->nl; ++j) {
+    const float* L = S->lights + 6 * j;
     float sd[3] = {L[0] - hp[0], L[1] - hp[1], L[2] - hp[2]};
     if (!(sd[0] * ffn[0] + sd[1] * ffn[1] + sd[2] * ffn[2] > 0)) continue;
     Ray s;
@@ -1060,35 +1065,89 @@ static long long whitted_sample(const orq_world* W, const float* mat_rgb,
     const float cos_theta = sd[0] * ffn[0] + sd[1] * ffn[1] + sd[2] * ffn[2];
     for (int c = 0; c < 3; ++c) total[c] += L[3 + c] * cos_theta;
     if (phong) {
-      const float H[3] = {sd[0] - r.d[0], sd[1] - r.d[1], sd[2] - r.d[2]};
+      const float H[3] = {sd[0] - r->d[0], sd[1] - r->d[1], sd[2] - r->d[2]};
       const float cos_alpha = H[0] * ffn[0] + H[1] * ffn[1] + H[2] * ffn[2];
       if (cos_alpha > 0) {
         const float length = sqrtf(H[0] * H[0] + H[1] * H[1] + H[2] * H[2]);
-        const float scale = ipow_f(cos_alpha / length, mat_pow[m]);
+        const float scale = ipow_f(cos_alpha / length, S->mat_pow[m]);
         for (int c = 0; c < 3; ++c) spec[c] += L[3 + c] * scale;
       }
     }
   }
   if (phong) {
-    const float* ks = mat_spec + 3 * m;
+    const float* ks = S->mat_spec + 3 * m;
     for (int c = 0; c < 3; ++c) rgb[c] = spec[c] * ks[c] + total[c] * kd[c];
   } else {
     for (int c = 0; c < 3; ++c) rgb[c] = total[c] * kd[c];
   }
+  const float refl = (phong && S->mat_refl) ? S->mat_refl[m] : 0.f;
+  if (refl != 0.f && depth < S->max_depth) {
+    float cimp[3], child[3] = {0.f, 0.f, 0.f};
+    for (int c = 0; c < 3; ++c) cimp[c] = imp[c] * refl;
+    const float lum = cimp[0] * 0.3f + cimp[1] * 0.59f + cimp[2] * 0.11f;
+    if (lum > S->cutoff) {
+      Ray q;
+      const float s2 = 2 * (ffn[0] * r->d[0] + ffn[1] * r->d[1] + ffn[2] * r->d[2]);
+      for (int c = 0; c < 3; ++c) {
+        q.o[c] = hp[c];
+        q.d[c] = r->d[c] - ffn[c] * s2;
+        q.inv[c] = (float)1 / q.d[c];
+      }
+      q.minT = MAXT;
+      q.hit = 0;
+      q.prim = -1;
+      q.u = q.v = 0.f;
+      q.anyhit = 0;
+      q.node_tests = q.tri_tests = 0;
+      int qk;
+      shadow_rays += trace_color(W, S, &q, depth + 1, cimp, child, &qk);
+    }
+    for (int c = 0; c < 3; ++c) rgb[c] = rgb[c] + child[c] * refl;
+  }
   return shadow_rays;
 }
 
-/* Supersampled Whitted frame over a world (Lambertian or non-reflective
- * Phong materials, see whitted_sample), pixel rows [y0, y1): per pixel
+/* One image sample: the camera ray through (px, py) traced and shaded. */
+static long long whitted_sample(const orq_world* W, const Shading* S, const float* cam,
+                                float px, float py, float* rgb, float* tprim, int* prim) {
+  Ray r;
+  const float* dir = cam + 3;
+  const float* cu = cam + 6;
+  const float* cv = cam + 9;
+  for (int c = 0; c < 3; ++c) {
+    r.o[c] = cam[c];
+    r.d[c] = cv[c] * px + cu[c] * py + dir[c];
+  }
+  v_normalize(r.d);
+  for (int c = 0; c < 3; ++c) r.inv[c] = (float)1 / r.d[c];
+  r.minT = MAXT;
+  r.hit = 0;
+  r.prim = -1;
+  r.u = r.v = 0.f;
+  r.anyhit = 0;
+  r.node_tests = r.tri_tests = 0;
+  const float one[3] = {1.f, 1.f, 1.f};
+  int k;
+  const long long n = trace_color(W, S, &r, 0, one, rgb, &k);
+  *tprim = r.minT;
+  *prim = r.hit ? r.prim : -1;
+  return n;
+}
+
+/* Supersampled Whitted frame over a world (Lambertian and Phong materials,
+ * reflective ones up to max_depth, see trace_color), pixel rows [y0, y1): per pixel
  * the spp samples' colours summed in sample order and scaled by 1/spp.
  * Optional per-sample outputs (indexed by item - y0 * xres * spp): colour,
  * primary t and triangle id.  Returns the shadow rays sent. */
 long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float* mat_spec,
-                           const int* mat_pow, const float* cam,
+                           const int* mat_pow, const float* mat_refl, int max_depth,
+                           float cutoff, const float* cam,
                            int xres, int yres, int spp, unsigned long long seed,
                            const float* lights, int nl, const float* ambient,
                            const float* background, int y0, int y1, float* rgb,
                            float* sample_rgb, float* sample_t, int* sample_prim) {
+  const Shading S = {mat_rgb, mat_spec, mat_pow, mat_refl, lights, nl, ambient, background,
+                     max_depth, cutoff};
   long long shadow = 0;
   const float inv = (float)1 / (float)spp;
   for (int y = y0; y < y1; ++y)
@@ -1101,8 +1160,7 @@ long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float
         float px, py, c[3], t;
         int p;
         sample_coords(xres, yres, spp, seed, item, &px, &py);
-        shadow += whitted_sample(W, mat_rgb, mat_spec, mat_pow, cam, px, py, lights, nl,
-                                 ambient, background, c, &t, &p);
+        shadow += whitted_sample(W, &S, cam, px, py, c, &t, &p);
         for (int j = 0; j < 3; ++j) acc[j] += c[j];
         if (sample_rgb)
           for (int j = 0; j < 3; ++j) sample_rgb[3 * o + j] = c[j];

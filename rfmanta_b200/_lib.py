@@ -65,7 +65,9 @@ class WhittedParams(C.Structure):
 
 class FrameParams(C.Structure):
     _fields_ = [("whitted", WhittedParams), ("spp", C.c_int), ("seed", C.c_uint64),
-                ("material_specular", C.c_void_p), ("material_specpow", C.c_void_p)]
+                ("material_specular", C.c_void_p), ("material_specpow", C.c_void_p),
+                ("material_reflectivity", C.c_void_p), ("max_depth", C.c_int),
+                ("importance_cutoff", C.c_float)]
 
 
 class PathParams(C.Structure):

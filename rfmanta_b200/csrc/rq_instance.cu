@@ -390,14 +390,108 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// Shades one hit the way Lambertian::shade / Phong::shade do (ambient plus
+// every unshadowed point light; Phong adds its specular highlight): the
+// local colour in col, the face-forward normal and hit point for a
+// reflection.  Returns the material's reflectivity (0 unless a reflective
+// Phong).
 template <int KIND, bool TWO, bool STATS>
+__device__ __forceinline__ float shade_hit(const DevScene& S, const DevScene* blas,
+                                           const FrameParams& P, const Ray& r, float t,
+                                           int prim, int pos, int bh, int2* stk, int stride,
+                                           Counts* cnt, int& nshadow, float* col, float* ffn,
+                                           float* hp) {
+  const float shadow_tmax = fsub(1.f, kTEpsilon);
+  const DevScene& HS = TWO ? blas[bh] : S;
+  const int mat = (int)__ldg(HS.face_material + prim);
+  float ks[3] = {0.f, 0.f, 0.f};
+  int specpow = -1;
+  if (P.phong) {
+    const float4 ph = __ldg(reinterpret_cast<const float4*>(P.phong) + mat);
+    ks[0] = ph.x;
+    ks[1] = ph.y;
+    ks[2] = ph.z;
+    specpow = __float_as_int(ph.w);
+  }
+  float spec[3] = {0.f, 0.f, 0.f};
+  float nrm[3];
+  record_normal<KIND>(HS, pos, nrm);
+  const float dn = dot3(nrm, r.d);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ffn[c] = (dn <= 0.f) ? nrm[c] : -nrm[c];
+    hp[c] = fadd(r.o[c], fmul(r.d[c], t));
+  }
+  float total[3] = {P.ambient[0], P.ambient[1], P.ambient[2]};
+  for (int j = 0; j < P.n_lights; ++j) {
+    const float* L = P.lights + 6 * j;
+    float sd[3] = {fsub(L[0], hp[0]), fsub(L[1], hp[1]), fsub(L[2], hp[2])};
+    if (!(dot3(sd, ffn) > 0.f)) continue;
+    Ray s;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      s.o[c] = hp[c];
+      s.d[c] = sd[c];
+      s.inv[c] = fdiv(1.f, sd[c]);
+    }
+    s.minT = shadow_tmax;
+    ++nshadow;
+    Hit sh;
+    int sb;
+    scene_trace<KIND, TWO, true, STATS>(S, blas, s, sh, sb, stk, stride, cnt);
+    if (sh.id >= 0) continue;
+    const float sum = fadd(fadd(fmul(sd[0], sd[0]), fmul(sd[1], sd[1])), fmul(sd[2], sd[2]));
+    const float scale = fdiv(1.f, __fsqrt_rn(sum));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sd[c] = fmul(sd[c], scale);
+    const float cos_theta = dot3(sd, ffn);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) total[c] = fadd(total[c], fmul(L[3 + c], cos_theta));
+    if (specpow >= 0) {
+      // Phong::shade scalar branch (Phong.cc:367-383): H = L - d,
+      // ipow(Dot(H, N) / |H|, exponent) (Core/Math/ipow.h:21-31)
+      const float H[3] = {fsub(sd[0], r.d[0]), fsub(sd[1], r.d[1]), fsub(sd[2], r.d[2])};
+      const float cos_alpha = dot3(H, ffn);
+      if (cos_alpha > 0.f) {
+        const float len = __fsqrt_rn(dot3(H, H));
+        float x = fdiv(cos_alpha, len), sc = 1.f;
+        for (int pw = specpow; pw; pw >>= 1) {
+          if (pw & 1) sc = fmul(sc, x);
+          x = fmul(x, x);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) spec[c] = fadd(spec[c], fmul(L[3 + c], sc));
+      }
+    }
+  }
+  const float* kd = P.materials + 3 * (size_t)mat;
+  if (specpow >= 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) col[c] = fadd(fmul(spec[c], ks[c]), fmul(total[c], __ldg(kd + c)));
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) col[c] = fmul(total[c], __ldg(kd + c));
+  }
+  return (specpow >= 0 && P.refl) ? __ldg(P.refl + mat) : 0.f;
+}
+
+// Shades the queued primary hits.  REFL: reflective Phong materials are
+// followed (Phong.cc:438-540): while the material reflects, depth <
+// maxDepth and the reflected importance's luminance (0.3 r + 0.59 g +
+// 0.11 b, Core/Color/RGBTraits.h:43-45) exceeds the cutoff, the mirrored
+// ray d - N (2 N.d) is traced from the hit point and shaded in turn; the
+// chain is then folded from its end, colour = local + child x reflectivity,
+// in the reference's order (a reflection cut off by importance adds black
+// x reflectivity).
+template <int KIND, bool TWO, bool STATS, bool REFL>
 __global__ void __launch_bounds__(128)
     frame_shade_kernel(DevScene S, const DevScene* blas, FrameParams P, SampleParams Q,
                        SampleBufs B, unsigned long long* stats) {
   extern __shared__ int2 smem_stack[];
   const int nq = *(volatile const int*)&B.counters[0];
   const unsigned lane = threadIdx.x & 31u;
-  const float shadow_tmax = fsub(1.f, kTEpsilon);
+  int2* stk = smem_stack + threadIdx.x;
+  const int stride = blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
     const int qi = base + threadIdx.x;
     int nshadow = 0;
@@ -406,80 +500,67 @@ __global__ void __launch_bounds__(128)
       const int it = B.queue[qi];
       Ray r;
       sample_ray(P, Q, it, r);
-      const float t = B.t[it];
-      const int bh = B.blas[it];
-      const DevScene& HS = TWO ? blas[bh] : S;
-      const int mat = (int)__ldg(HS.face_material + B.prim[it]);
-      float ks[3] = {0.f, 0.f, 0.f};
-      int specpow = -1;
-      if (P.phong) {
-        const float4 ph = __ldg(reinterpret_cast<const float4*>(P.phong) + mat);
-        ks[0] = ph.x;
-        ks[1] = ph.y;
-        ks[2] = ph.z;
-        specpow = __float_as_int(ph.w);
-      }
-      float spec[3] = {0.f, 0.f, 0.f};
-      float nrm[3];
-      record_normal<KIND>(HS, B.pos[it], nrm);
-      const float dn = dot3(nrm, r.d);
-      float ffn[3], hp[3];
+      float col[3], ffn[3], hp[3];
+      const float refl = shade_hit<KIND, TWO, STATS>(S, blas, P, r, B.t[it], B.prim[it],
+                                                     B.pos[it], B.blas[it], stk, stride, &cnt,
+                                                     nshadow, col, ffn, hp);
+      if (!REFL || refl == 0.f || P.max_depth <= 0) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        ffn[c] = (dn <= 0.f) ? nrm[c] : -nrm[c];
-        hp[c] = fadd(r.o[c], fmul(r.d[c], t));
-      }
-      float total[3] = {P.ambient[0], P.ambient[1], P.ambient[2]};
-      for (int j = 0; j < P.n_lights; ++j) {
-        const float* L = P.lights + 6 * j;
-        float sd[3] = {fsub(L[0], hp[0]), fsub(L[1], hp[1]), fsub(L[2], hp[2])};
-        if (!(dot3(sd, ffn) > 0.f)) continue;
-        Ray s;
+        for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = col[c];
+      } else {
+        float loc[kMaxReflectDepth + 1][3];
+        float rf[kMaxReflectDepth + 1];
+        for (int c = 0; c < 3; ++c) loc[0][c] = col[c];
+        rf[0] = refl;
+        float imp[3] = {1.f, 1.f, 1.f};
+        float d[3] = {r.d[0], r.d[1], r.d[2]};
+        int depth = 0;
+        bool black = false;
+        for (;;) {
+          if (rf[depth] == 0.f || depth >= P.max_depth) break;
+          float ci[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          s.o[c] = hp[c];
-          s.d[c] = sd[c];
-          s.inv[c] = fdiv(1.f, sd[c]);
-        }
-        s.minT = shadow_tmax;
-        ++nshadow;
-        Hit sh;
-        int sb;
-        scene_trace<KIND, TWO, true, STATS>(S, blas, s, sh, sb, smem_stack + threadIdx.x,
-                                            blockDim.x, &cnt);
-        if (sh.id >= 0) continue;
-        const float sum = fadd(fadd(fmul(sd[0], sd[0]), fmul(sd[1], sd[1])), fmul(sd[2], sd[2]));
-        const float scale = fdiv(1.f, __fsqrt_rn(sum));
-#pragma unroll
-        for (int c = 0; c < 3; ++c) sd[c] = fmul(sd[c], scale);
-        const float cos_theta = dot3(sd, ffn);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) total[c] = fadd(total[c], fmul(L[3 + c], cos_theta));
-        if (specpow >= 0) {
-          // Phong::shade scalar branch (Phong.cc:367-383): H = L - d,
-          // ipow(Dot(H, N) / |H|, exponent) (Core/Math/ipow.h:21-31)
-          const float H[3] = {fsub(sd[0], r.d[0]), fsub(sd[1], r.d[1]), fsub(sd[2], r.d[2])};
-          const float cos_alpha = dot3(H, ffn);
-          if (cos_alpha > 0.f) {
-            const float len = __fsqrt_rn(dot3(H, H));
-            float x = fdiv(cos_alpha, len), sc = 1.f;
-            for (int pw = specpow; pw; pw >>= 1) {
-              if (pw & 1) sc = fmul(sc, x);
-              x = fmul(x, x);
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) spec[c] = fadd(spec[c], fmul(L[3 + c], sc));
+          for (int c = 0; c < 3; ++c) ci[c] = fmul(imp[c], rf[depth]);
+          const float lum = fadd(fadd(fmul(ci[0], 0.3f), fmul(ci[1], 0.59f)), fmul(ci[2], 0.11f));
+          if (!(lum > P.cutoff)) {
+            black = true;
+            break;
           }
+          Ray q;
+          const float s2 = fmul(2.f, dot3(ffn, d));
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            q.o[c] = hp[c];
+            q.d[c] = fsub(d[c], fmul(ffn[c], s2));
+            q.inv[c] = fdiv(1.f, q.d[c]);
+          }
+          q.minT = kMaxT;
+          Hit qh;
+          int qb;
+          scene_trace<KIND, TWO, false, STATS>(S, blas, q, qh, qb, stk, stride, &cnt);
+          ++depth;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) imp[c] = ci[c];
+          if (qh.id < 0) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) loc[depth][c] = P.background[c];
+            rf[depth] = 0.f;
+            break;
+          }
+          rf[depth] = shade_hit<KIND, TWO, STATS>(S, blas, P, q, qh.t, qh.id, qh.pos, qb, stk,
+                                                  stride, &cnt, nshadow, loc[depth], ffn, hp);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) d[c] = q.d[c];
         }
-      }
-      const float* kd = P.materials + 3 * (size_t)mat;
-      if (specpow >= 0) {
+        float c3[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          B.col[3 * (size_t)it + c] = fadd(fmul(spec[c], ks[c]), fmul(total[c], __ldg(kd + c)));
-      } else {
+          c3[c] = black ? fadd(loc[depth][c], fmul(0.f, rf[depth])) : loc[depth][c];
+        for (int k = depth - 1; k >= 0; --k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = fmul(total[c], __ldg(kd + c));
+          for (int c = 0; c < 3; ++c) c3[c] = fadd(loc[k][c], fmul(c3[c], rf[k]));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = c3[c];
       }
     }
     int tot = nshadow;
@@ -506,8 +587,10 @@ static cudaError_t frame_go(const Scene& s, const FrameParams& P, const SamplePa
   const DevScene S = s.dev();
   const int bs = 128;
   const size_t smem = (size_t)(S.depth + (TWO ? s.max_blas_depth : 0) + 1) * bs * sizeof(int2);
+  const bool refl = P.refl != nullptr;
   const void* f1 = (const void*)frame_primary_kernel<KIND, TWO, STATS>;
-  const void* f2 = (const void*)frame_shade_kernel<KIND, TWO, STATS>;
+  const void* f2 = refl ? (const void*)frame_shade_kernel<KIND, TWO, STATS, true>
+                        : (const void*)frame_shade_kernel<KIND, TWO, STATS, false>;
   if (smem > 48 * 1024) {
     cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -525,7 +608,12 @@ static cudaError_t frame_go(const Scene& s, const FrameParams& P, const SamplePa
       <<<std::max(1, std::min(grid, (n_items + bs - 1) / bs)), bs, smem, st>>>(
           S, s.d_blas, P, Q, B, n_items, s.stats);
   if (nev > 1) cudaEventRecord(ev[1], st);
-  frame_shade_kernel<KIND, TWO, STATS><<<grid, bs, smem, st>>>(S, s.d_blas, P, Q, B, s.stats);
+  if (refl)
+    frame_shade_kernel<KIND, TWO, STATS, true><<<grid, bs, smem, st>>>(S, s.d_blas, P, Q, B,
+                                                                      s.stats);
+  else
+    frame_shade_kernel<KIND, TWO, STATS, false><<<grid, bs, smem, st>>>(S, s.d_blas, P, Q, B,
+                                                                       s.stats);
   if (nev > 2) cudaEventRecord(ev[2], st);
   frame_resolve_kernel<<<std::max(1, std::min(grid, (npix + 255) / 256)), 256, 0, st>>>(Q, B, npix, rgb);
   if (nev > 3) cudaEventRecord(ev[3], st);
@@ -549,6 +637,8 @@ struct SampleScratch {
   std::vector<float> host_materials;
   float4* phong = nullptr;
   std::vector<float4> host_phong;
+  float* refl = nullptr;
+  std::vector<float> host_refl;
   float* d_rgb = nullptr;
   size_t rgb_pix = 0;
   cudaStream_t stream = nullptr;
@@ -565,6 +655,7 @@ struct SampleScratch {
     cudaFree(B.shadow);
     cudaFree(materials);
     cudaFree(phong);
+    cudaFree(refl);
     cudaFree(d_rgb);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -658,6 +749,27 @@ int frame_prepare(rq::Scene* s, const rq_frame_params* fp, rq::FrameParams& P,
       x->host_phong = ph;
     }
     P.phong = reinterpret_cast<const float*>(x->phong);
+  }
+  P.refl = nullptr;
+  P.max_depth = 0;
+  P.cutoff = 0.f;
+  if (fp->material_reflectivity) {
+    if (!fp->material_specpow) return ifail(RQ_ERR_ARG, "material_reflectivity needs Phong materials");
+    if (fp->max_depth < 0 || fp->max_depth > kMaxReflectDepth)
+      return ifail(RQ_ERR_ARG, "max_depth must be in [0, 32]");
+    std::vector<float> rf(fp->material_reflectivity, fp->material_reflectivity + p->n_materials);
+    if (x->host_refl != rf) {
+      cudaFree(x->refl);
+      x->refl = nullptr;
+      if (cudaMalloc(&x->refl, rf.size() * sizeof(float)) != cudaSuccess ||
+          cudaMemcpy(x->refl, rf.data(), rf.size() * sizeof(float), cudaMemcpyHostToDevice) !=
+              cudaSuccess)
+        return ifail(RQ_ERR_OOM, "reflectivity table");
+      x->host_refl = rf;
+    }
+    P.refl = x->refl;
+    P.max_depth = fp->max_depth;
+    P.cutoff = fp->importance_cutoff;
   }
   return RQ_OK;
 }

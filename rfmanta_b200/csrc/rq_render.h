@@ -10,6 +10,7 @@
 namespace rq {
 
 constexpr int kMaxLights = 16;
+constexpr int kMaxReflectDepth = 32;  // reflective Phong recursion limit
 
 enum FrameCounter { kCntQueue = 0, kCntWork = 1, kNumCounters = 4 };
 
@@ -26,6 +27,12 @@ struct FrameParams {
   // specular rgb + exponent bits; exponent < 0 = Lambertian.  NULL = all
   // Lambertian.
   const float* phong;
+  // optional (rq_render_frame): reflectivity per material id of the Phong
+  // materials (NULL = none), with RenderParameters maxDepth and
+  // importanceCutoff
+  const float* refl;
+  int max_depth;
+  float cutoff;
 };
 
 // Device buffers of one frame.  rgb/t/prim are outputs; pos, queue and the

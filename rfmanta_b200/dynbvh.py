@@ -299,6 +299,14 @@ class GpuDynBVH:
             p.material_specular = ks.ctypes.data
             p.material_specpow = sp.ctypes.data
             keep += [sp, ks]
+            refl = getattr(scene, "reflectivity", None)
+            if refl is not None:
+                rf = np.ascontiguousarray(refl, np.float32)
+                p.material_reflectivity = rf.ctypes.data
+                # RenderParameters defaults (Interface/RenderParameters.h)
+                p.max_depth = int(getattr(scene, "max_depth", 15))
+                p.importance_cutoff = float(getattr(scene, "importance_cutoff", 0.01))
+                keep.append(rf)
         p._keep = keep
         return p
 

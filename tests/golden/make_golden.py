@@ -29,8 +29,9 @@ seeded animation (the tree, per-node costs and nextFree after every frame),
 and path_stats.npz: KajiyaPathtracer images of the tiny path scene for 16
 seeds at 4096 samples per pixel, at depth 4 and at depth 2 with a constant
 ambient light (the expectation the path tracer must match),
-and obj_cases.npz: Manta::ObjGroup's vertices, triangles, face materials and
-material table for the OBJ files the tests write.
+obj_cases.npz: Manta::ObjGroup's vertices, triangles, face materials and
+material table for the OBJ files the tests write, and tiny_reflect.npz: the
+reference's sample colours of frames with reflective Phong materials.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -138,6 +139,52 @@ def write_instanced() -> None:
         out[f"inner{i}_indices"] = m.indices
         out[f"inner{i}_face_material"] = m.face_material
     path = os.path.join(OUT, "tiny_instanced.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
+REFLECT = dict(flat_refl=(0.9, 0.8), flat_specpow=(20, 8), instanced_refl=0.6)
+
+
+def write_reflect() -> None:
+    """Reflective Phong (Phong.cc:438-540, Raytracer recursion with the
+    default maxDepth 15 and importance cutoff 0.01): the reference's
+    per-sample colours of a 40x32, 4-spp frame of the tiny frame scene with
+    both materials reflective, and of the tiny two-level scene's frame with
+    its Phong spheres reflective (trees: tiny_instanced.npz)."""
+    ref = Reference()
+    restated = Restatement()
+    out = {}
+    sc = scenes.tiny_frame_scene(xres=40, yres=32)
+    sc.spp, sc.seed = 4, 5
+    m = sc.mesh
+    rs = ref.scene(m, 0)
+    nm = m.materials.shape[0]
+    for k in range(nm):
+        rs.set_phong(k, np.full(3, 0.4, np.float32), REFLECT["flat_specpow"][k],
+                     REFLECT["flat_refl"][k])
+    px, py = restated.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed)
+    img = rs.render_coords(sc, px, py)
+    t = rs.tree()
+    for f in ("bounds", "child", "children", "axis", "left_cheaper", "ids"):
+        out[f"flat_{f}"] = getattr(t, f)
+    out.update(flat_vertices=m.vertices, flat_indices=m.indices,
+               flat_face_material=m.face_material, flat_materials=m.materials,
+               flat_sample_rgb=img["rgb"], flat_sample_t=img["t"], flat_sample_prim=img["prim"],
+               flat_shadow_rays=np.int64(img["shadow_rays"]))
+    rs.close()
+    sc = scenes.tiny_coherent_scene()
+    inner = [ref.scene(mm, 0) for mm in sc.inner]
+    for r in inner:
+        for k, sp in enumerate(sc.specpow):
+            if sp >= 0:
+                r.set_phong(k, sc.specular[k], int(sp), REFLECT["instanced_refl"])
+    top = ref.instanced(inner, sc.inst_scene, sc.translation, sc.kind)
+    px, py = restated.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed)
+    img = top.render_coords(sc, px, py)
+    out.update(inst_sample_rgb=img["rgb"], inst_sample_t=img["t"],
+               inst_sample_prim=img["prim"], inst_shadow_rays=np.int64(img["shadow_rays"]))
+    path = os.path.join(OUT, "tiny_reflect.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")
 
@@ -299,12 +346,16 @@ if __name__ == "__main__":
         write_tree_update()
         write_path_stats()
         write_obj_cases()
+        write_reflect()
     elif "--update" in sys.argv:
         write_tree_update()
     elif "--path" in sys.argv:
         write_path_stats()
     elif "--obj" in sys.argv:
         write_obj_cases()
+        write_reflect()
+    elif "--reflect" in sys.argv:
+        write_reflect()
     else:
         main()
         write_sah_costs()
@@ -313,3 +364,4 @@ if __name__ == "__main__":
         write_tree_update()
         write_path_stats()
         write_obj_cases()
+        write_reflect()

@@ -246,3 +246,66 @@ def test_two_level_scene_refuses_updated_inner_scenes():
     again = InstancedBVH(inner, g["inst_scene"], g["translation"], g["kind"])
     again.rebuild()
     again.intersect(RayBatch(g["rand_org"], g["rand_dir"]))
+
+
+def _pixels_from_samples(sample_rgb, spp):
+    r = sample_rgb.reshape(-1, spp, 3)
+    acc = np.zeros((r.shape[0], 3), np.float32)
+    for s in range(spp):
+        acc = (acc + r[:, s]).astype(np.float32)
+    return (acc * np.float32(np.float32(1.0) / np.float32(spp))).astype(np.float32)
+
+
+def test_reflective_phong_matches_reference_fixture():
+    """Reflective Phong frames (Phong.cc:438-540 recursion) against the
+    reference's samples: a flat scene whose materials reflect each other
+    and the two-level scene with reflective InstanceT spheres."""
+    import os
+    import sys
+    from conftest import GOLDEN
+    sys.path.insert(0, GOLDEN)
+    from make_golden import REFLECT
+    from test_oracle_reflect import flat_case, load_reflect
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    r = load_reflect()
+    tree, mesh, sc, spec, specpow, refl = flat_case(r)
+    bvh = GpuDynBVH()
+    bvh.setGroup(mesh)
+    bvh.importTree(tree)
+    sc.specular, sc.specpow, sc.reflectivity = spec, specpow, refl
+    out = bvh.render_frame(sc, mesh.materials)
+    assert out["shadow_rays"] == int(r["flat_shadow_rays"])
+    exp = _pixels_from_samples(r["flat_sample_rgb"], sc.spp)
+    assert np.array_equal(_bits(out["rgb"]), _bits(exp))
+    g = load_instanced()
+    top, inner = _device_scene(g)
+    sc = tiny_scene_from_golden(g)
+    sc.reflectivity = np.where(g["specpow"] >= 0, np.float32(REFLECT["instanced_refl"]),
+                               np.float32(0)).astype(np.float32)
+    out = top.render_frame(sc, g["materials"])
+    assert out["shadow_rays"] == int(r["inst_shadow_rays"])
+    assert np.array_equal(_bits(out["rgb"]), _bits(_pixels_from_samples(r["inst_sample_rgb"],
+                                                                         sc.spp)))
+
+
+@pytest.mark.parametrize("max_depth,cutoff", [(15, 0.01), (3, 0.01), (15, 0.3), (0, 0.01)])
+def test_reflective_phong_gpu_built_matches_restatement(restatement, max_depth, cutoff):
+    from oracle.pyoracle import Tree
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    from rfmanta_b200.treeio import parse_dynbvh_blob
+    from test_oracle_reflect import flat_case, load_reflect
+    r = load_reflect()
+    _, mesh, sc, spec, specpow, refl = flat_case(r)
+    bvh = GpuDynBVH(tri_kind=1)
+    bvh.setGroup(mesh)
+    bvh.rebuild()
+    f = parse_dynbvh_blob(bvh.exportBlob(), mesh.n_tris)
+    W = restatement.world(Tree(f.bounds, f.child, f.children, f.axis, f.left_cheaper, f.ids),
+                          mesh, tri_kind=1)
+    sc.specular, sc.specpow, sc.reflectivity = spec, specpow, refl
+    sc.max_depth, sc.importance_cutoff = max_depth, cutoff
+    out = bvh.render_frame(sc, mesh.materials)
+    exp = restatement.render_frame(W, sc, mesh.materials, specular=spec, specpow=specpow,
+                                   reflectivity=refl, max_depth=max_depth, cutoff=cutoff)
+    assert out["shadow_rays"] == exp["shadow_rays"]
+    assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))

@@ -134,6 +134,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def pinned(shape, dtype=np.float32):
+    """A host array in pinned (page-locked) memory, where the end-to-end
+    numbers read each step's result."""
+    import torch
+    t = torch.empty(shape, dtype={np.float32: torch.float32, np.int32: torch.int32}[dtype],
+                    pin_memory=True)
+    return t.numpy()
+
+
 def _dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -203,7 +212,7 @@ class PathFrame:
         from rfmanta_b200 import _lib
         sc = self.sc
         if not hasattr(self, "_host_rgb"):
-            self._host_rgb = np.empty((sc.xres * sc.yres, 3), np.float32)
+            self._host_rgb = pinned((sc.xres * sc.yres, 3))
             self._host_counts = (C.c_uint64 * 2)()
         _lib.check(_lib.lib.rq_render_path(self.bvh.handle, C.byref(self.params),
                                            self._host_rgb.ctypes.data, self._host_counts))
@@ -300,8 +309,7 @@ class SmallFrame:
         from rfmanta_b200 import _lib
         npx = self.sc.xres * self.sc.yres
         if not hasattr(self, "_h"):
-            self._h = (np.empty((npx, 3), np.float32), np.empty(npx, np.float32),
-                       np.empty(npx, np.int32), C.c_uint64())
+            self._h = (pinned((npx, 3)), pinned(npx), pinned(npx, np.int32), C.c_uint64())
         rgb, t, p, ns = self._h
         _lib.check(_lib.lib.rq_render_whitted(self.bvh.handle, C.byref(self.params),
                                               rgb.ctypes.data, t.ctypes.data, p.ctypes.data,
@@ -409,7 +417,7 @@ class CoherentFrame:
         from rfmanta_b200 import _lib
         npx = self.sc.xres * self.sc.yres
         if not hasattr(self, "_h"):
-            self._h = (np.empty((npx, 3), np.float32), C.c_uint64())
+            self._h = (pinned((npx, 3)), C.c_uint64())
         rgb, ns = self._h
         _lib.check(_lib.lib.rq_render_frame(self.bvh.handle, C.byref(self.params),
                                             rgb.ctypes.data, C.byref(ns)))

@@ -98,9 +98,8 @@ static int prepare(Scene* s, const rq_whitted_params* p, FrameParams& P) {
   if (p->n_lights < 0 || p->n_lights > kMaxLights || (p->n_lights > 0 && !p->lights))
     return set_fail(RQ_ERR_ARG, "0..16 point lights");
   if (p->n_materials <= 0 || !p->material_rgb) return set_fail(RQ_ERR_ARG, "no materials");
-  for (uint32_t m : s->face_mat)
-    if ((int)m >= p->n_materials)
-      return set_fail(RQ_ERR_ARG, "face_material refers past n_materials");
+  if (s->max_face_material >= p->n_materials)
+    return set_fail(RQ_ERR_ARG, "face_material refers past n_materials");
   if (!s->has_tree) return set_fail(RQ_ERR_STATE, "scene has no tree");
   if (s->instanced) return set_fail(RQ_ERR_ARG, "instanced scene: render it with rq_render_frame");
   std::memset(&P, 0, sizeof(P));

@@ -682,8 +682,8 @@ int frame_prepare(rq::Scene* s, const rq_frame_params* fp, rq::FrameParams& P,
   if (p->n_materials <= 0 || !p->material_rgb) return ifail(RQ_ERR_ARG, "no materials");
   const std::vector<Scene*> meshes = s->instanced ? s->blas : std::vector<Scene*>{s};
   for (const Scene* m : meshes)
-    for (uint32_t id : m->face_mat)
-      if ((int)id >= p->n_materials) return ifail(RQ_ERR_ARG, "face_material past n_materials");
+    if (m->max_face_material >= p->n_materials)
+      return ifail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return ifail(RQ_ERR_STATE, "scene has no tree");
   if (s->instanced) {
     const int rc = s->check_inner_current();

@@ -94,8 +94,8 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
                        std::to_string(kNoAllocMaxMaterials) + " materials");
   if (p->n_lights < 0 || p->n_lights > kMaxLights || (p->n_lights > 0 && !p->lights))
     return na_fail(RQ_ERR_ARG, "0..16 point lights");
-  for (uint32_t m : s->face_mat)
-    if ((int)m >= p->n_materials) return na_fail(RQ_ERR_ARG, "face_material past n_materials");
+  if (s->max_face_material >= p->n_materials)
+    return na_fail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return na_fail(RQ_ERR_STATE, "scene has no tree");
   if (s->instanced) return na_fail(RQ_ERR_ARG, "instanced scene: render it with rq_render_frame");
   if (cudaSetDevice(s->device) != cudaSuccess) return na_fail(RQ_ERR_CUDA, "cudaSetDevice");

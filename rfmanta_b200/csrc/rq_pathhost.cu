@@ -64,8 +64,8 @@ static int path_prepare(Scene* s, const rq_path_params* p, PathParams& P, long l
   if (p->max_depth < 1 || p->max_depth > kMaxPathDepth)
     return pfail(RQ_ERR_ARG, "max_depth must be in [1, 16]");
   if (p->n_materials <= 0 || !p->material_rgb) return pfail(RQ_ERR_ARG, "no materials");
-  for (uint32_t m : s->face_mat)
-    if ((int)m >= p->n_materials) return pfail(RQ_ERR_ARG, "face_material past n_materials");
+  if (s->max_face_material >= p->n_materials)
+    return pfail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return pfail(RQ_ERR_STATE, "scene has no tree");
   if (s->instanced) return pfail(RQ_ERR_ARG, "path tracing takes triangle scenes");
   std::memset(&P, 0, sizeof(P));

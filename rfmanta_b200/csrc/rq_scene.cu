@@ -457,6 +457,7 @@ int rq_scene_create(const float* vertices, int n_vertices,
     s->face_mat.assign(face_material, face_material + n_tris);
   else
     s->face_mat.assign(n_tris, 0u);
+  for (uint32_t m : s->face_mat) s->max_face_material = std::max<int64_t>(s->max_face_material, m);
   RQ_CUDA(cudaSetDevice(device));
   RQ_CUDA(cudaMalloc(&s->d_verts, s->verts.size() * sizeof(float)));
   RQ_CUDA(cudaMalloc(&s->d_idx, s->idx.size() * sizeof(uint32_t)));

@@ -81,6 +81,7 @@ struct Scene {
   mutable bool verts_stale = false;
   std::vector<uint32_t> idx;
   std::vector<uint32_t> face_mat;
+  int64_t max_face_material = -1;  // largest face material id (-1: no faces)
   float* d_verts = nullptr;
   uint32_t* d_idx = nullptr;
   uint32_t* d_face_mat = nullptr;

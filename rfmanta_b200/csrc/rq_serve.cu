@@ -536,8 +536,8 @@ int rq_server_submit(rq_server* s, const rq_serve_request* q, int* request_id) {
     return sfail(RQ_ERR_CAPACITY, "a chunk of this request does not fit the path pool");
   if (q->max_depth < 1 || q->max_depth > rq::kMaxPathDepth) return sfail(RQ_ERR_ARG, "max_depth in [1, 16]");
   if (q->n_materials <= 0 || !q->material_rgb) return sfail(RQ_ERR_ARG, "no materials");
-  for (uint32_t m : s->scenes[q->scene]->face_mat)
-    if ((int)m >= q->n_materials) return sfail(RQ_ERR_ARG, "face_material past n_materials");
+  if (s->scenes[q->scene]->max_face_material >= q->n_materials)
+    return sfail(RQ_ERR_ARG, "face_material past n_materials");
   const size_t bytes = (size_t)q->xres * q->yres * 12;
   if (bytes + (size_t)q->n_materials * 12 > s->budget)
     return sfail(RQ_ERR_CAPACITY, "request larger than the server's HBM budget");

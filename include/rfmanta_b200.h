@@ -256,6 +256,27 @@ RQ_API int rq_get_launch_config(const rq_scene* scene, int flags,
                          rq_launch_config* cfg);
 
 /*
+ * Ambient light and background of a frame beyond the constant forms.  The
+ * frame's `ambient` colour is ConstantAmbient's colour, or EyeAmbient's
+ * (Model/AmbientLights/EyeAmbient.cc:29-44: ambient x (0.5 - 0.5 d.N_ff)
+ * for ray direction d and face-forward normal N_ff).  The frame's
+ * `background` colour is ConstantBackground's, or LinearBackground's `cup`
+ * (Model/Backgrounds/LinearBackground.cc:15-40: cup x t + cdown x (1 - t),
+ * t = 0.5 (1 + d.up), `up` normalised as the constructor does).  An all-zero
+ * rq_environment selects the constant forms.
+ */
+#define RQ_AMBIENT_CONSTANT 0
+#define RQ_AMBIENT_EYE 1
+#define RQ_BACKGROUND_CONSTANT 0
+#define RQ_BACKGROUND_LINEAR 1
+typedef struct {
+  int ambient_kind;          /* RQ_AMBIENT_* */
+  int background_kind;       /* RQ_BACKGROUND_* */
+  float background_down[3];  /* LinearBackground cdown */
+  float background_up[3];    /* LinearBackground up (any nonzero length) */
+} rq_environment;
+
+/*
  * Whitted frame (Raytracer::traceEyeRays, Engine/Renderers/Raytracer.cc:41-97,
  * with PinholeCamera -normalizeRays, Lambertian, HardShadows and point
  * lights): the frame the reference's render workers produce tile by tile,
@@ -271,6 +292,7 @@ typedef struct {
   float background[3];            /* ConstantBackground colour */
   int n_materials;                /* Lambertian diffuse colours by material id */
   const float* material_rgb;      /* host: n_materials x (r, g, b) */
+  rq_environment environment;     /* zero = constant ambient and background */
 } rq_whitted_params;
 
 /* PinholeCamera::setup basis (Model/Cameras/PinholeCamera.cc:167-198):
@@ -363,6 +385,7 @@ typedef struct {
   float ambient[3];                /* as in rq_path_params */
   int n_materials;
   const float* material_rgb;       /* host, copied on submit */
+  rq_environment environment;      /* as in rq_path_params */
 } rq_serve_request;
 
 typedef struct rq_server rq_server;
@@ -501,6 +524,10 @@ typedef struct {
   int n_materials;
   const float* material_rgb;      /* host: n_materials x (r, g, b) */
   int chunk_paths;                /* paths per wavefront pass, 0 = 4Mi */
+  rq_environment environment;     /* zero = constant ambient and background;
+                                     EyeAmbient at the last bounce sees the
+                                     direction sampled there, as the
+                                     reference's packet holds it by then */
 } rq_path_params;
 
 /* Renders into HOST rgb (3 per pixel); ray_counts[0] = camera + bounce rays

@@ -34,6 +34,24 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
+class _Env(C.Structure):
+    """orq_env: ambient / background kinds, LinearBackground cdown and up."""
+    _fields_ = [("ambient_kind", C.c_int), ("background_kind", C.c_int),
+                ("down", C.c_float * 3), ("up", C.c_float * 3)]
+
+
+def _env(scene):
+    """orq_env for a scene's optional `environment` (None = constant forms)."""
+    env = getattr(scene, "environment", None)
+    if env is None:
+        return None
+    e = _Env()
+    e.ambient_kind, e.background_kind = env.kinds()
+    e.down[:] = env.background_down
+    e.up[:] = env.background_up
+    return C.byref(e)
+
+
 @dataclass
 class Tree:
     """Reference DynBVH node array, field by field (DynBVH.h:37-79)."""
@@ -186,12 +204,12 @@ class Restatement:
         L.orq_primary_rays.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.orq_render_whitted.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 6 +
                                          [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
-                                          C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5)
+                                          C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 6)
         L.orq_render_whitted.restype = C.c_longlong
         L.orq_sincos_2pi.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.orq_render_path.argtypes = ([C.c_void_p] * 6 + [C.c_int] + [C.c_void_p] * 7 +
                                       [C.c_uint64, C.c_longlong, C.c_longlong] +
-                                      [C.c_void_p] * 3)
+                                      [C.c_void_p] * 4)
         L.orq_trace_world.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 + [C.c_int] +
                                       [C.c_void_p] * 6)
         L.orq_sample_coords.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_longlong,
@@ -199,7 +217,7 @@ class Restatement:
         L.orq_render_frame.argtypes = ([C.c_void_p] * 5 + [C.c_int, C.c_float, C.c_void_p] +
                                        [C.c_int] * 3 + [C.c_uint64] +
                                        [C.c_void_p, C.c_int] + [C.c_void_p] * 2 +
-                                       [C.c_int, C.c_int] + [C.c_void_p] * 4)
+                                       [C.c_int, C.c_int] + [C.c_void_p] * 5)
         L.orq_render_frame.restype = C.c_longlong
 
     def world(self, top_tree, top_mesh=None, inner=None, inst_scene=None, translation=None,
@@ -255,7 +273,7 @@ class Restatement:
                                        int(max_depth), float(cutoff), _ptr(basis), xres, yres, spp,
                                        int(scene.seed), _ptr(lights), lights.shape[0],
                                        _ptr(amb), _ptr(bg), y0, y1, _ptr(rgb), _ptr(srgb),
-                                       _ptr(st), _ptr(sp))
+                                       _ptr(st), _ptr(sp), _env(scene))
         out = dict(rgb=rgb, shadow_rays=int(ns))
         if per_sample:
             out.update(sample_rgb=srgb, sample_t=st, sample_prim=sp)
@@ -292,7 +310,8 @@ class Restatement:
         fm = np.ascontiguousarray(mesh.face_material, np.uint32)
         mats = np.ascontiguousarray(mesh.materials, np.float32)
         self.lib.orq_render_path(*args, _ptr(fm), _ptr(mats), _ptr(fp), _ptr(ip),
-                                 int(scene.seed), p0, p1, _ptr(rad), _ptr(counts), _ptr(dbg))
+                                 int(scene.seed), p0, p1, _ptr(rad), _ptr(counts), _ptr(dbg),
+                                 _env(scene))
         out = dict(rad=rad, rays=int(counts[0]), shadow_rays=int(counts[1]), prim=dbg)
         if paths is None:
             r = rad.reshape(-1, scene.spp, 3)
@@ -415,7 +434,7 @@ class Restatement:
         ns = self.lib.orq_render_whitted(*args, _ptr(fm), _ptr(mats), _ptr(basis), xres, yres,
                                          _ptr(lights), len(scene.lights), _ptr(amb), _ptr(bg),
                                          y0, y1, _ptr(rgb), _ptr(tp), _ptr(pr), _ptr(lit),
-                                         _ptr(counts))
+                                         _ptr(counts), _env(scene))
         return dict(rgb=rgb, t=tp, prim=pr, lit=lit, shadow_rays=int(ns),
                     primary_node_tests=int(counts[0]), primary_tri_tests=int(counts[1]),
                     shadow_node_tests=int(counts[2]), shadow_tri_tests=int(counts[3]))
@@ -464,6 +483,8 @@ class Reference:
         L.mref_scene_create_instanced.restype = C.c_void_p
         L.mref_scene_set_phong.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_float]
         L.mref_scene_set_render_parameters.argtypes = [C.c_void_p, C.c_int, C.c_float]
+        L.mref_scene_set_environment.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                                 C.c_void_p]
         L.mref_read_ply.argtypes = ([C.c_char_p, C.c_void_p, C.c_int] + [C.c_void_p] * 5 +
                                     [C.c_int, C.c_int])
         L.mref_scene_update_vertices.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
@@ -570,6 +591,17 @@ class RefScene:
     def set_render_parameters(self, max_depth: int, cutoff: float) -> None:
         """RenderParameters maxDepth / importanceCutoff of later renders."""
         self.ref.lib.mref_scene_set_render_parameters(self.h, int(max_depth), float(cutoff))
+
+    def set_environment(self, env) -> None:
+        """EyeAmbient / LinearBackground for later renders (a
+        scenes.Environment; None = ConstantAmbient / ConstantBackground)."""
+        if env is None:
+            self.ref.lib.mref_scene_set_environment(self.h, 0, 0, None, None)
+            return
+        a, b = env.kinds()
+        down = np.asarray(env.background_down, np.float32)
+        up = np.asarray(env.background_up, np.float32)
+        self.ref.lib.mref_scene_set_environment(self.h, a, b, _ptr(down), _ptr(up))
 
     def update_vertices(self, vertices) -> None:
         """Animated mesh: new vertex positions, WaldTriangle::update and

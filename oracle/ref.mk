@@ -66,7 +66,9 @@ MODEL_SRC := \
   Model/Textures/Constant.cc \
   Model/Lights/PointLight.cc \
   Model/AmbientLights/ConstantAmbient.cc \
+  Model/AmbientLights/EyeAmbient.cc \
   Model/Backgrounds/ConstantBackground.cc \
+  Model/Backgrounds/LinearBackground.cc \
   Model/Cameras/PinholeCamera.cc \
   Model/Lights/AreaLight.cc Model/Primitives/Parallelogram.cc \
   Model/Primitives/PrimitiveCommon.cc Model/TexCoordMappers/UniformMapper.cc \

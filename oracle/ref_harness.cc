@@ -42,7 +42,9 @@
 #include <Interface/RayPacket.h>
 #include <Interface/Scene.h>
 #include <Model/AmbientLights/ConstantAmbient.h>
+#include <Model/AmbientLights/EyeAmbient.h>
 #include <Model/Backgrounds/ConstantBackground.h>
+#include <Model/Backgrounds/LinearBackground.h>
 #include <Model/Cameras/PinholeCamera.h>
 #include <Model/Groups/DynBVH.h>
 #include <Model/Groups/Group.h>
@@ -184,7 +186,27 @@ struct RefScene {
   Scene* scene;
   // two-level scenes: instance index of each top-level InstanceT object
   std::map<const Primitive*, int> instance_of;
+  // renders' ambient light and background: kinds (0 constant, 1 EyeAmbient /
+  // LinearBackground) and LinearBackground's cdown and up
+  int env_ambient, env_background;
+  float env_down[3], env_up[3];
 };
+
+// The ambient light and background a render of this scene uses: the given
+// colours as ConstantAmbient / ConstantBackground, or EyeAmbient and
+// LinearBackground(cup = colour, cdown, up) when the scene asks for them.
+AmbientLight* make_ambient(const RefScene* s, const float* c) {
+  if (s->env_ambient == 1) return new EyeAmbient(Color(RGB(c[0], c[1], c[2])));
+  return new ConstantAmbient(Color(RGB(c[0], c[1], c[2])));
+}
+
+Background* make_background(const RefScene* s, const float* c) {
+  if (s->env_background == 1)
+    return new LinearBackground(Color(RGB(c[0], c[1], c[2])),
+                                Color(RGB(s->env_down[0], s->env_down[1], s->env_down[2])),
+                                Vector(s->env_up[0], s->env_up[1], s->env_up[2]));
+  return new ConstantBackground(Color(RGB(c[0], c[1], c[2])));
+}
 
 // Triangle id (and instance index, -1 for none) of a hit: a hit on an
 // InstanceT carries the inner primitive in its MPT scratchpad
@@ -282,6 +304,19 @@ void* mref_scene_create(const float* verts, int nverts, const unsigned* idx,
 
 // RenderParameters::maxDepth and importanceCutoff of the scene's renders
 // (Interface/RenderParameters.h: 15 and 0.01 unless set).
+// Ambient light and background kinds for this scene's later renders.
+int mref_scene_set_environment(void* h, int ambient_kind, int background_kind,
+                               const float* down, const float* up) {
+  RefScene* s = static_cast<RefScene*>(h);
+  s->env_ambient = ambient_kind;
+  s->env_background = background_kind;
+  for (int c = 0; c < 3; ++c) {
+    s->env_down[c] = down ? down[c] : 0.f;
+    s->env_up[c] = up ? up[c] : 0.f;
+  }
+  return 0;
+}
+
 int mref_scene_set_render_parameters(void* h, int max_depth, float cutoff) {
   RefScene* s = static_cast<RefScene*>(h);
   if (!s->scene) s->scene = new Scene();
@@ -745,7 +780,7 @@ int mref_render(void* h, int xres, int yres, const float* cam12_args,
   ExposedCamera camera(args);
 
   LightSet* ls = new LightSet();
-  ls->setAmbientLight(new ConstantAmbient(Color(RGB(ambient[0], ambient[1], ambient[2]))));
+  ls->setAmbientLight(make_ambient(s, ambient));
   for (int k = 0; k < nlights; ++k) {
     const float* L = lights + 6 * k;
     ls->add(new PointLight(Vector(L[0], L[1], L[2]), Color(RGB(L[3], L[4], L[5]))));
@@ -755,8 +790,7 @@ int mref_render(void* h, int xres, int yres, const float* cam12_args,
   for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
   if (!s->scene) s->scene = new Scene();
   s->scene->setObject(s->object);
-  s->scene->setBackground(new ConstantBackground(
-      Color(RGB(background[0], background[1], background[2]))));
+  s->scene->setBackground(make_background(s, background));
   s->scene->setLights(ls);
 
   Raytracer renderer;
@@ -917,7 +951,7 @@ int mref_render_coords(void* h, int n, const float* px, const float* py,
   args.push_back("-normalizeRays");
   ExposedCamera camera(args);
   LightSet* ls = new LightSet();
-  ls->setAmbientLight(new ConstantAmbient(Color(RGB(ambient[0], ambient[1], ambient[2]))));
+  ls->setAmbientLight(make_ambient(s, ambient));
   for (int k = 0; k < nlights; ++k) {
     const float* L = lights + 6 * k;
     ls->add(new PointLight(Vector(L[0], L[1], L[2]), Color(RGB(L[3], L[4], L[5]))));
@@ -927,8 +961,7 @@ int mref_render_coords(void* h, int n, const float* px, const float* py,
   for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
   if (!s->scene) s->scene = new Scene();
   s->scene->setObject(s->object);
-  s->scene->setBackground(new ConstantBackground(
-      Color(RGB(background[0], background[1], background[2]))));
+  s->scene->setBackground(make_background(s, background));
   s->scene->setLights(ls);
   Raytracer renderer;
   ConstantSampleGenerator sampler(0.f);
@@ -1055,7 +1088,7 @@ int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
   args.push_back("-normalizeRays");
   ExposedCamera camera(args);
   LightSet* ls = new LightSet();
-  ls->setAmbientLight(new ConstantAmbient(Color(RGB(background[3], background[4], background[5]))));
+  ls->setAmbientLight(make_ambient(s, background + 3));
   Parallelogram* emitter = new Parallelogram(s->materials[0],
       Vector(light12[0], light12[1], light12[2]), Vector(light12[3], light12[4], light12[5]),
       Vector(light12[6], light12[7], light12[8]));
@@ -1065,8 +1098,7 @@ int mref_render_path(void* h, int xres, int yres, const float* cam11, int spp,
   for (size_t k = 0; k < s->materials.size(); ++k) s->materials[k]->preprocess(pctx);
   if (!s->scene) s->scene = new Scene();
   s->scene->setObject(s->object);
-  s->scene->setBackground(new ConstantBackground(
-      Color(RGB(background[0], background[1], background[2]))));
+  s->scene->setBackground(make_background(s, background));
   s->scene->setLights(ls);
   s->scene->getRenderParameters().maxDepth = max_depth;
   std::vector<std::string> none;

@@ -404,6 +404,61 @@ static void v_cross(const float* a, const float* b, float* o) {
   o[2] = a[0] * b[1] - a[1] * b[0];
 }
 
+/* -------------------------------------------- ambient and background --- */
+
+/* A frame's ambient light and background beyond the constant forms:
+ * ambient_kind 1 = EyeAmbient, background_kind 1 = LinearBackground with
+ * cup = the frame's background colour, cdown = down, and up as given (the
+ * constructor normalises it).  NULL or zero kinds = ConstantAmbient /
+ * ConstantBackground. */
+typedef struct {
+  int ambient_kind;
+  int background_kind;
+  float down[3];
+  float up[3];
+} orq_env;
+
+/* Vector Dot (Core/Geometry/VectorT.h:443-449): result = 0, then += a[i]b[i]. */
+static float v_dot(const float* a, const float* b) {
+  float r = 0;
+  for (int i = 0; i < 3; ++i) r += a[i] * b[i];
+  return r;
+}
+
+/* EyeAmbient::computeAmbient (Model/AmbientLights/EyeAmbient.cc:29-44):
+ * cos_theta = -Dot(eyeDir, ffnormal) * (1 - minLighting) + minLighting with
+ * minLighting 0.5, ambient = colour * cos_theta; ConstantAmbient copies the
+ * colour. */
+static void env_ambient(const orq_env* E, const float* color, const float* d,
+                        const float* ffn, float* out) {
+  if (E && E->ambient_kind == 1) {
+    const float min_lighting = 0.5f;
+    const float cos_theta = -v_dot(d, ffn) * (1 - min_lighting) + min_lighting;
+    for (int c = 0; c < 3; ++c) out[c] = color[c] * cos_theta;
+  } else {
+    for (int c = 0; c < 3; ++c) out[c] = color[c];
+  }
+}
+
+/* LinearBackground (Model/Backgrounds/LinearBackground.cc:15-40): the
+ * constructor's up.normalize() (VectorT::normalize, VectorT.h:324-333), then
+ * t = 0.5 * (1 + Dot(d, up)) and colour = cup * t + cdown * (1 - t);
+ * ConstantBackground returns cup. */
+static void env_background(const orq_env* E, const float* cup, const float* d, float* out) {
+  if (E && E->background_kind == 1) {
+    float up[3] = {E->up[0], E->up[1], E->up[2]};
+    float sum = 0;
+    for (int i = 0; i < 3; ++i) sum += up[i] * up[i];
+    const float l = sqrtf(sum);
+    const float scale = 1 / l;
+    for (int i = 0; i < 3; ++i) up[i] *= scale;
+    const float t = 0.5f * (1 + v_dot(d, up));
+    for (int c = 0; c < 3; ++c) out[c] = cup[c] * t + E->down[c] * (1 - t);
+  } else {
+    for (int c = 0; c < 3; ++c) out[c] = cup[c];
+  }
+}
+
 /* PinholeCamera::setup (PinholeCamera.cc:167-198): out = eye, direction, u, v. */
 void orq_camera_basis(const float* eye, const float* lookat, const float* up_in,
                       float hfov, float vfov, float* out12) {
@@ -514,7 +569,7 @@ long long orq_render_whitted(const float* bounds, const int* child,
                              const float* lights, int nl, const float* ambient,
                              const float* background, int y0, int y1,
                              float* rgb, float* tprim, int* prim,
-                             int* lit_bits, long long* counts) {
+                             int* lit_bits, long long* counts, const orq_env* env) {
   Tree T = {bounds, child, children, axis, left_cheaper, ids,
             tri_kind, verts, idx, wald};
   long long shadow_rays = 0;
@@ -539,8 +594,8 @@ long long orq_render_whitted(const float* bounds, const int* child,
       prim[pix] = r.hit ? r.prim : -1;
       if (lit_bits) lit_bits[pix] = 0;
       if (!r.hit) {
-        /* ConstantBackground::shade */
-        for (int c = 0; c < 3; ++c) rgb[3 * pix + c] = background[c];
+        /* Background::shade */
+        env_background(env, background, r.d, rgb + 3 * pix);
         continue;
       }
       /* Lambertian::shade.  Directions are already unit length
@@ -554,7 +609,8 @@ long long orq_render_whitted(const float* bounds, const int* child,
       for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0) ? nrm[c] : -nrm[c];
       /* geometric normal == shading normal for both triangle kinds here */
       const float* ffg = ffn;
-      float total[3] = {ambient[0], ambient[1], ambient[2]};
+      float total[3];
+      env_ambient(env, ambient, r.d, ffn, total);
       float hp[3];
       for (int c = 0; c < 3; ++c) hp[c] = r.o[c] + r.d[c] * r.minT;
       for (int j = 0; j < nl; ++j) {
@@ -674,7 +730,7 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
                      const unsigned* idx, const float* wald, const unsigned* face_mat,
                      const float* mat_rgb, const float* fp, const int* ip,
                      unsigned long long seed, long long p0, long long p1, float* rad_out,
-                     long long* counts, int* dbg_prim) {
+                     long long* counts, int* dbg_prim, const orq_env* env) {
   Tree T = {bounds, child, children, axis, left_cheaper, ids,
             tri_kind, verts, idx, wald};
   const float* cam = fp;
@@ -731,7 +787,9 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
       counts[0]++;
       if (dbg_prim) dbg_prim[(size_t)depth * npaths + g] = r.hit ? r.prim : -1;
       if (!r.hit) {
-        for (int c = 0; c < 3; ++c) rad[c] = rad[c] + bg[c] * imp[c];
+        float bgc[3];
+        env_background(env, bg, r.d, bgc);
+        for (int c = 0; c < 3; ++c) rad[c] = rad[c] + bgc[c] * imp[c];
         break;
       }
       float hp[3], ng[3], ffn[3];
@@ -771,8 +829,17 @@ void orq_render_path(const float* bounds, const int* child, const int* children,
       /* do_ambient_on_maxdepth (KajiyaPathtracer.cc:259-279): ambient * kd
          times the importance (which holds this kd) where the path reaches
          its last bounce */
-      if (depth + 1 >= maxd)
-        for (int c = 0; c < 3; ++c) rad[c] = rad[c] + (amb[c] * kd[c]) * imp[c];
+      if (depth + 1 >= maxd) {
+        /* By then sampleBSDF has written nd into the packet, and
+           Lambertian::shade recomputes the face-forward normals against it
+           (RayPacket::computeFFNormals, RayPacket.cc:205-233; the flag
+           sampleBSDF set lived in a sub-packet), which EyeAmbient reads. */
+        float fn[3], a[3];
+        const float dd = ng[0] * nd[0] + ng[1] * nd[1] + ng[2] * nd[2];
+        for (int c = 0; c < 3; ++c) fn[c] = (dd <= 0.f) ? ng[c] : -ng[c];
+        env_ambient(env, amb, nd, fn, a);
+        for (int c = 0; c < 3; ++c) rad[c] = rad[c] + (a[c] * kd[c]) * imp[c];
+      }
       const float lr1 = pcg_float(&rng);
       const float lr2 = pcg_float(&rng);
       float ld[3];
@@ -1003,6 +1070,7 @@ typedef struct {
   const float* background;
   int max_depth;
   float cutoff;
+  const orq_env* env;
 } Shading;
 
 /* Raytracer::traceRays for one ray (Engine/Renderers/Raytracer.cc:49-97):
@@ -1020,7 +1088,7 @@ static long long trace_color(const orq_world* W, const Shading* S, Ray* r, int d
   world_trace(W, r, &k);
   *kout = k;
   if (!r->hit) {
-    for (int c = 0; c < 3; ++c) rgb[c] = S->background[c];
+    env_background(S->env, S->background, r->d, rgb);
     return 0;
   }
   const orq_tree* HT = W->inner ? &W->inner[W->inst_scene[k]] : W->top;
@@ -1034,7 +1102,8 @@ static long long trace_color(const orq_world* W, const Shading* S, Ray* r, int d
   float ffn[3];
   const float dn = nrm[0] * r->d[0] + nrm[1] * r->d[1] + nrm[2] * r->d[2];
   for (int c = 0; c < 3; ++c) ffn[c] = (dn <= 0) ? nrm[c] : -nrm[c];
-  float total[3] = {S->ambient[0], S->ambient[1], S->ambient[2]};
+  float total[3];
+  env_ambient(S->env, S->ambient, r->d, ffn, total);
   float hp[3];
   for (int c = 0; c < 3; ++c) hp[c] = r->o[c] + r->d[c] * r->minT;
   long long shadow_rays = 0;
@@ -1145,9 +1214,10 @@ long long orq_render_frame(const orq_world* W, const float* mat_rgb, const float
                            int xres, int yres, int spp, unsigned long long seed,
                            const float* lights, int nl, const float* ambient,
                            const float* background, int y0, int y1, float* rgb,
-                           float* sample_rgb, float* sample_t, int* sample_prim) {
+                           float* sample_rgb, float* sample_t, int* sample_prim,
+                           const orq_env* env) {
   const Shading S = {mat_rgb, mat_spec, mat_pow, mat_refl, lights, nl, ambient, background,
-                     max_depth, cutoff};
+                     max_depth, cutoff, env};
   long long shadow = 0;
   const float inv = (float)1 / (float)spp;
   for (int y = y0; y < y1; ++y)

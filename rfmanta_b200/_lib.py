@@ -55,12 +55,21 @@ class RQError(RuntimeError):
         self.code = code
 
 
+RQ_AMBIENT_CONSTANT, RQ_AMBIENT_EYE = 0, 1
+RQ_BACKGROUND_CONSTANT, RQ_BACKGROUND_LINEAR = 0, 1
+
+
+class EnvironmentParams(C.Structure):
+    _fields_ = [("ambient_kind", C.c_int), ("background_kind", C.c_int),
+                ("background_down", C.c_float * 3), ("background_up", C.c_float * 3)]
+
+
 class WhittedParams(C.Structure):
     _fields_ = [("eye", C.c_float * 3), ("lookat", C.c_float * 3), ("up", C.c_float * 3),
                 ("hfov", C.c_float), ("vfov", C.c_float), ("xres", C.c_int), ("yres", C.c_int),
                 ("n_lights", C.c_int), ("lights", C.c_void_p), ("ambient", C.c_float * 3),
                 ("background", C.c_float * 3), ("n_materials", C.c_int),
-                ("material_rgb", C.c_void_p)]
+                ("material_rgb", C.c_void_p), ("environment", EnvironmentParams)]
 
 
 class FrameParams(C.Structure):
@@ -78,7 +87,8 @@ class PathParams(C.Structure):
                 ("light_v1", C.c_float * 3), ("light_v2", C.c_float * 3),
                 ("light_color", C.c_float * 3), ("background", C.c_float * 3),
                 ("ambient", C.c_float * 3), ("n_materials", C.c_int),
-                ("material_rgb", C.c_void_p), ("chunk_paths", C.c_int)]
+                ("material_rgb", C.c_void_p), ("chunk_paths", C.c_int),
+                ("environment", EnvironmentParams)]
 
 
 class Batch(C.Structure):
@@ -104,7 +114,7 @@ class ServeRequest(C.Structure):
                 ("light_v1", C.c_float * 3), ("light_v2", C.c_float * 3),
                 ("light_color", C.c_float * 3), ("background", C.c_float * 3),
                 ("ambient", C.c_float * 3), ("n_materials", C.c_int),
-                ("material_rgb", C.c_void_p)]
+                ("material_rgb", C.c_void_p), ("environment", EnvironmentParams)]
 
 
 class LaunchConfig(C.Structure):

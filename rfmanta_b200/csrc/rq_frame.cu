@@ -55,6 +55,29 @@ void camera_basis(const float* eye, const float* lookat, const float* up_in,
   }
 }
 
+bool environment_from(const rq_environment& in, Environment& out) {
+  std::memset(&out, 0, sizeof(out));
+  if (in.ambient_kind != RQ_AMBIENT_CONSTANT && in.ambient_kind != RQ_AMBIENT_EYE)
+    return false;
+  if (in.background_kind != RQ_BACKGROUND_CONSTANT &&
+      in.background_kind != RQ_BACKGROUND_LINEAR)
+    return false;
+  out.ambient_kind = in.ambient_kind == RQ_AMBIENT_EYE ? kAmbientEye : kAmbientConstant;
+  out.background_kind =
+      in.background_kind == RQ_BACKGROUND_LINEAR ? kBackgroundLinear : kBackgroundConstant;
+  if (out.background_kind == kBackgroundLinear) {
+    // LinearBackground's constructor: up.normalize() (VectorT::normalize)
+    float up[3] = {in.background_up[0], in.background_up[1], in.background_up[2]};
+    hnormalize(up);
+    for (int c = 0; c < 3; ++c) {
+      if (!std::isfinite(up[c])) return false;
+      out.up[c] = up[c];
+      out.down[c] = in.background_down[c];
+    }
+  }
+  return true;
+}
+
 // Scratch of the frame path, owned by the scene and grown on demand.
 struct FrameScratch {
   size_t npix = 0;
@@ -110,6 +133,8 @@ static int prepare(Scene* s, const rq_whitted_params* p, FrameParams& P) {
   std::memcpy(P.lights, p->lights, sizeof(float) * 6 * p->n_lights);
   std::memcpy(P.ambient, p->ambient, sizeof(P.ambient));
   std::memcpy(P.background, p->background, sizeof(P.background));
+  if (!environment_from(p->environment, P.env))
+    return set_fail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   if (!s->frame) s->frame = new FrameScratch();
   FrameScratch* f = s->frame;
   const size_t npix = (size_t)p->xres * p->yres;

@@ -375,8 +375,11 @@ __global__ void __launch_bounds__(128)
       B.pos[it] = h.pos;
       B.blas[it] = bh;
       hit = h.id >= 0;
-      if (!hit)
-        for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = P.background[c];
+      if (!hit) {
+        float bg[3];
+        background_color(P.env, P.background, r.d, bg);
+        for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = bg[c];
+      }
     }
     const unsigned m = __ballot_sync(0xffffffffu, hit);
     if (m) {
@@ -422,7 +425,8 @@ __device__ __forceinline__ float shade_hit(const DevScene& S, const DevScene* bl
     ffn[c] = (dn <= 0.f) ? nrm[c] : -nrm[c];
     hp[c] = fadd(r.o[c], fmul(r.d[c], t));
   }
-  float total[3] = {P.ambient[0], P.ambient[1], P.ambient[2]};
+  float total[3];
+  ambient_light(P.env, P.ambient, r.d, ffn, total);
   for (int j = 0; j < P.n_lights; ++j) {
     const float* L = P.lights + 6 * j;
     float sd[3] = {fsub(L[0], hp[0]), fsub(L[1], hp[1]), fsub(L[2], hp[2])};
@@ -542,8 +546,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
           for (int c = 0; c < 3; ++c) imp[c] = ci[c];
           if (qh.id < 0) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) loc[depth][c] = P.background[c];
+            background_color(P.env, P.background, q.d, loc[depth]);
             rf[depth] = 0.f;
             break;
           }
@@ -697,6 +700,8 @@ int frame_prepare(rq::Scene* s, const rq_frame_params* fp, rq::FrameParams& P,
   std::memcpy(P.lights, p->lights, sizeof(float) * 6 * p->n_lights);
   std::memcpy(P.ambient, p->ambient, sizeof(P.ambient));
   std::memcpy(P.background, p->background, sizeof(P.background));
+  if (!environment_from(p->environment, P.env))
+    return ifail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   Q.spp = fp->spp;
   Q.strata = strata;
   Q.seed = fp->seed;

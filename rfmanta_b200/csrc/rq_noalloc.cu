@@ -113,6 +113,8 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
   std::memcpy(P.lights, p->lights, sizeof(float) * 6 * p->n_lights);
   std::memcpy(P.ambient, p->ambient, sizeof(P.ambient));
   std::memcpy(P.background, p->background, sizeof(P.background));
+  if (!environment_from(p->environment, P.env))
+    return na_fail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   float* mats = reinterpret_cast<float*>(base + kOffMaterials);
   cudaError_t e = cudaMemcpyAsync(mats, p->material_rgb, sizeof(float) * 3 * p->n_materials,
                                   cudaMemcpyHostToDevice, st);

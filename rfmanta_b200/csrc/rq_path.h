@@ -6,6 +6,7 @@
 #include <cstdint>
 
 #include "rq_device.cuh"
+#include "rq_env.cuh"
 
 namespace rq {
 
@@ -30,6 +31,7 @@ struct PathParams {
   float light_color[3];
   float background[3];
   float ambient[3];        // added at max_depth (do_ambient_on_maxdepth)
+  Environment env;         // ambient and background kinds
   const float* materials;  // device, rgb per material id
 };
 

@@ -162,9 +162,11 @@ __device__ __forceinline__ bool shade_begin(const DevScene& S, const PathParams&
   }
   const int prim = B.prim[p];
   if (prim < 0) {
+    float bg[3];
+    background_color(P.env, P.background, d, bg);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      B.rad[c * C + p] = fadd(B.rad[c * C + p], fmul(P.background[c], imp[c]));
+      B.rad[c * C + p] = fadd(B.rad[c * C + p], fmul(bg[c], imp[c]));
     return false;
   }
   Pcg32 rng;
@@ -223,10 +225,24 @@ __device__ __forceinline__ bool shade_begin(const DevScene& S, const PathParams&
     // do_ambient_on_maxdepth (KajiyaPathtracer.cc:259-279): a path still
     // alive after its last bounce is shaded by its material with ambient
     // light only (Lambertian: ambient * kd) times its importance, which
-    // already holds this surface's reflectance
+    // already holds this surface's reflectance.  By then sampleBSDF has
+    // written the new direction into the packet and the packet's
+    // face-forward normals are recomputed against it (the ones sampleBSDF
+    // computed lived in a sub-packet's flags), which an EyeAmbient sees.
+    float amb[3];
+    if (P.env.ambient_kind == kAmbientEye) {
+      float fn[3];
+      const float dd = dot3(ng, nd);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) fn[c] = (dd <= 0.f) ? ng[c] : -ng[c];
+      ambient_light(P.env, P.ambient, nd, fn, amb);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) amb[c] = P.ambient[c];
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      B.rad[c * C + p] = fadd(B.rad[c * C + p], fmul(fmul(P.ambient[c], refl[c]), imp[c]));
+      B.rad[c * C + p] = fadd(B.rad[c * C + p], fmul(fmul(amb[c], refl[c]), imp[c]));
   }
   // one area-light sample
   const float lr1 = pcg32_float(rng);

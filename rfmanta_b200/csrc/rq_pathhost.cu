@@ -85,6 +85,8 @@ static int path_prepare(Scene* s, const rq_path_params* p, PathParams& P, long l
     P.background[c] = p->background[c];
     P.ambient[c] = p->ambient[c];
   }
+  if (!environment_from(p->environment, P.env))
+    return pfail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   // Parallelogram constructor (Model/Primitives/Parallelogram.cc:26-35)
   float n[3] = {p->light_v1[1] * p->light_v2[2] - p->light_v1[2] * p->light_v2[1],
                 p->light_v1[2] * p->light_v2[0] - p->light_v1[0] * p->light_v2[2],

@@ -65,9 +65,10 @@ __global__ void __launch_bounds__(128)
       B.pos[pix] = h.pos;
       hit = h.id >= 0;
       if (!hit) {
-        B.rgb[3 * (size_t)pix + 0] = P.background[0];
-        B.rgb[3 * (size_t)pix + 1] = P.background[1];
-        B.rgb[3 * (size_t)pix + 2] = P.background[2];
+        float bg[3];
+        background_color(P.env, P.background, r.d, bg);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) B.rgb[3 * (size_t)pix + c] = bg[c];
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -146,7 +147,8 @@ __global__ void __launch_bounds__(128)
       float hp[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) hp[c] = fadd(r.o[c], fmul(r.d[c], t));
-      float total[3] = {P.ambient[0], P.ambient[1], P.ambient[2]};
+      float total[3];
+      ambient_light(P.env, P.ambient, r.d, ffn, total);
       for (int j = 0; j < P.n_lights; ++j) {
         const float* L = P.lights + 6 * j;
         float sd[3] = {fsub(L[0], hp[0]), fsub(L[1], hp[1]), fsub(L[2], hp[2])};

@@ -5,7 +5,9 @@
 
 #include <cstdint>
 
+#include "../../include/rfmanta_b200.h"
 #include "rq_device.cuh"
+#include "rq_env.cuh"
 
 namespace rq {
 
@@ -22,6 +24,7 @@ struct FrameParams {
   float lights[6 * kMaxLights];  // position xyz, colour rgb
   float ambient[3];
   float background[3];
+  Environment env;         // ambient and background kinds
   const float* materials;  // device, 3 floats per material id
   // optional (rq_render_frame): Phong materials, 4 per material id =
   // specular rgb + exponent bits; exponent < 0 = Lambertian.  NULL = all
@@ -87,5 +90,9 @@ int whitted_blocks_per_sm(int tri_kind, size_t smem);
 // PinholeCamera::setup (Model/Cameras/PinholeCamera.cc:167-198) on the host.
 void camera_basis(const float* eye, const float* lookat, const float* up,
                   float hfov, float vfov, float* out12);
+
+// Checks the C ABI's environment and fills the device form (LinearBackground's
+// up normalised as its constructor does); false on a bad kind or a zero up.
+bool environment_from(const rq_environment& in, Environment& out);
 
 }  // namespace rq

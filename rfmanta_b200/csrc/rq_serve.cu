@@ -442,6 +442,7 @@ void request_params(const rq_serve_request& q, rq::PathParams& P) {
     P.background[c] = q.background[c];
     P.ambient[c] = q.ambient[c];
   }
+  rq::environment_from(q.environment, P.env);  // checked on submit
   const float* v1 = q.light_v1;
   const float* v2 = q.light_v2;
   float n[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2],
@@ -538,6 +539,9 @@ int rq_server_submit(rq_server* s, const rq_serve_request* q, int* request_id) {
   if (q->n_materials <= 0 || !q->material_rgb) return sfail(RQ_ERR_ARG, "no materials");
   if (s->scenes[q->scene]->max_face_material >= q->n_materials)
     return sfail(RQ_ERR_ARG, "face_material past n_materials");
+  rq::Environment env;
+  if (!rq::environment_from(q->environment, env))
+    return sfail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   const size_t bytes = (size_t)q->xres * q->yres * 12;
   if (bytes + (size_t)q->n_materials * 12 > s->budget)
     return sfail(RQ_ERR_CAPACITY, "request larger than the server's HBM budget");

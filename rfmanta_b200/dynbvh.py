@@ -26,6 +26,15 @@ T_EPSILON = np.float32(1.e-4)
 MAXT = np.float32(1.e19)
 
 
+def fill_environment(dst: "_lib.EnvironmentParams", env) -> None:
+    """rq_environment from a scenes.Environment (None = the constant forms)."""
+    if env is None:
+        return
+    dst.ambient_kind, dst.background_kind = env.kinds()
+    dst.background_down[:] = env.background_down
+    dst.background_up[:] = env.background_up
+
+
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
@@ -259,6 +268,7 @@ class GpuDynBVH:
         p.background[:] = scene.background
         p.n_materials = mats.shape[0]
         p.material_rgb = mats.ctypes.data
+        fill_environment(p.environment, getattr(scene, "environment", None))
         p._keep = (lights, mats)
         return p
 
@@ -368,6 +378,7 @@ class GpuDynBVH:
         p.n_materials = mats.shape[0]
         p.material_rgb = mats.ctypes.data
         p.chunk_paths = chunk_paths
+        fill_environment(p.environment, getattr(scene, "environment", None))
         p._keep = (mats,)
         return p
 

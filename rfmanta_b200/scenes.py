@@ -220,6 +220,25 @@ class PointLightSpec:
 
 
 @dataclass
+class Environment:
+    """Ambient light and background beyond the constant forms: ambient
+    "constant" (ConstantAmbient) or "eye" (EyeAmbient, Model/AmbientLights/
+    EyeAmbient.cc), background "constant" (ConstantBackground) or "linear"
+    (LinearBackground, Model/Backgrounds/LinearBackground.cc, with the
+    scene's background colour as cup).  The colours stay in the scene's
+    `ambient` and `background`."""
+    ambient: str = "constant"
+    background: str = "constant"
+    background_down: tuple = (0.0, 0.0, 0.0)
+    background_up: tuple = (0.0, 1.0, 0.0)
+
+    def kinds(self) -> tuple:
+        amb = {"constant": 0, "eye": 1}[self.ambient]
+        bg = {"constant": 0, "linear": 1}[self.background]
+        return amb, bg
+
+
+@dataclass
 class WhittedScene:
     mesh: Mesh
     camera: Camera
@@ -228,6 +247,7 @@ class WhittedScene:
     background: tuple
     xres: int
     yres: int
+    environment: Environment | None = None
 
 
 def small_frame_scene(level: int = 6, grid: int = 100, xres: int = 512,
@@ -312,6 +332,7 @@ class PathScene:
     rr_depth: int
     seed: int = 1
     ambient: tuple = (0.0, 0.0, 0.0)  # ConstantAmbient, added at max_depth
+    environment: Environment | None = None
 
 
 def path_scene(hf_nx: int = 512, hf_nz: int = 1024, n_spheres: int = 32,
@@ -437,6 +458,7 @@ class InstancedFrameScene:
     # colour per material and exponent, specpow < 0 = Lambertian
     specular: np.ndarray | None = None
     specpow: np.ndarray | None = None
+    environment: Environment | None = None
 
     @property
     def n_tris(self) -> int:

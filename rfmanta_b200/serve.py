@@ -14,6 +14,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, lib
+from .dynbvh import fill_environment
 
 
 @dataclass
@@ -37,6 +38,7 @@ class RenderRequest:
     background: tuple
     materials: np.ndarray = field(default_factory=lambda: np.full((1, 3), 0.7, np.float32))
     ambient: tuple = (0.0, 0.0, 0.0)
+    environment: object = None  # scenes.Environment, None = constant forms
 
     def to_c(self) -> _lib.ServeRequest:
         q = _lib.ServeRequest()
@@ -49,6 +51,7 @@ class RenderRequest:
                                                            self.light_v2)
         q.light_color[:], q.background[:] = self.light_color, self.background
         q.ambient[:] = self.ambient
+        fill_environment(q.environment, self.environment)
         m = np.ascontiguousarray(self.materials, np.float32)
         q.n_materials = m.shape[0]
         q.material_rgb = m.ctypes.data

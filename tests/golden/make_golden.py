@@ -30,8 +30,11 @@ and path_stats.npz: KajiyaPathtracer images of the tiny path scene for 16
 seeds at 4096 samples per pixel, at depth 4 and at depth 2 with a constant
 ambient light (the expectation the path tracer must match),
 obj_cases.npz: Manta::ObjGroup's vertices, triangles, face materials and
-material table for the OBJ files the tests write, and tiny_reflect.npz: the
-reference's sample colours of frames with reflective Phong materials.
+material table for the OBJ files the tests write, tiny_reflect.npz: the
+reference's sample colours of frames with reflective Phong materials, and
+tiny_env.npz: frames and path-traced images lit by EyeAmbient over a
+LinearBackground.  One flag (--instanced, --ply, --update, --path, --obj,
+--reflect, --env) regenerates that fixture alone.
 The fixtures pin the CPU restatement (oracle/rq_oracle.c) and the device
 path to the reference without needing the reference at test time.
 """
@@ -189,6 +192,69 @@ def write_reflect() -> None:
     print(path, os.path.getsize(path), "bytes")
 
 
+# EyeAmbient and LinearBackground (cup = the scene's background colour)
+ENVIRONMENT = dict(down=(0.9, 0.3, 0.1), up=(0.2, 1.0, 0.3), path_ambient=(0.3, 0.4, 0.5),
+                   path_background=(0.2, 0.3, 0.6), path_depths=(1, 2), seeds=16)
+
+
+def environment():
+    return scenes.Environment(ambient="eye", background="linear",
+                              background_down=ENVIRONMENT["down"],
+                              background_up=ENVIRONMENT["up"])
+
+
+def write_environment() -> None:
+    """EyeAmbient (Model/AmbientLights/EyeAmbient.cc) and LinearBackground
+    (Model/Backgrounds/LinearBackground.cc): the reference's Whitted frame of
+    the tiny frame scene (48x40, Raytracer::traceEyeRays), its per-sample
+    colours of the 40x32 4-spp reflective Phong frame (materials as in
+    tiny_reflect.npz), and KajiyaPathtracer images of the tiny path scene at
+    depths 1 and 2 (16 seeds each, 16x12 at 4096 spp, one thread), all with
+    both."""
+    ref = Reference()
+    restated = Restatement()
+    env = environment()
+    out = {}
+    sc = scenes.tiny_frame_scene(xres=48, yres=40)
+    sc.environment = env
+    m = sc.mesh
+    rs = ref.scene(m, 0)
+    rs.set_environment(env)
+    img = rs.render(sc)
+    t = rs.tree()
+    for f in ("bounds", "child", "children", "axis", "left_cheaper", "ids"):
+        out[f"tree_{f}"] = getattr(t, f)
+    out.update(whitted_rgb=img["rgb"], whitted_t=img["t"], whitted_prim=img["prim"],
+               whitted_shadow_rays=np.int64(img["shadow_rays"]))
+    nm = m.materials.shape[0]
+    for k in range(nm):
+        rs.set_phong(k, np.full(3, 0.4, np.float32), REFLECT["flat_specpow"][k],
+                     REFLECT["flat_refl"][k])
+    sc.xres, sc.yres, sc.spp, sc.seed = 40, 32, 4, 5
+    px, py = restated.sample_coords(sc.xres, sc.yres, sc.spp, sc.seed)
+    img = rs.render_coords(sc, px, py)
+    out.update(frame_sample_rgb=img["rgb"], frame_sample_prim=img["prim"],
+               frame_shadow_rays=np.int64(img["shadow_rays"]))
+    rs.close()
+    p = PATH_STATS
+    ps = scenes.tiny_path_scene(xres=p["xres"], yres=p["yres"], spp=p["spp"])
+    ps.ambient, ps.background = ENVIRONMENT["path_ambient"], ENVIRONMENT["path_background"]
+    ps.environment = env
+    rp = ref.scene(ps.mesh, 0)
+    rp.set_environment(env)
+    for depth in ENVIRONMENT["path_depths"]:
+        ps.max_depth = depth
+        imgs = []
+        for s in range(ENVIRONMENT["seeds"]):
+            ps.seed = 5000 + 100 * depth + s
+            imgs.append(rp.render_path(ps, nthreads=1)["rgb"].reshape(p["yres"], p["xres"], 3))
+        out[f"path_images_d{depth}"] = np.array(imgs, np.float32)
+    rp.close()
+    path = os.path.join(OUT, "tiny_env.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 def write_obj_cases() -> None:
     """Manta::ObjGroup's results for the OBJ files tests/test_mesh_io.py
     writes (vertices, triangles, face materials, material kinds and glm
@@ -339,29 +405,15 @@ def write_sah_costs() -> None:
 
 
 if __name__ == "__main__":
-    if "--instanced" in sys.argv:
-        write_instanced()
-    elif "--ply" in sys.argv:
-        write_ply_cases()
-        write_tree_update()
-        write_path_stats()
-        write_obj_cases()
-        write_reflect()
-    elif "--update" in sys.argv:
-        write_tree_update()
-    elif "--path" in sys.argv:
-        write_path_stats()
-    elif "--obj" in sys.argv:
-        write_obj_cases()
-        write_reflect()
-    elif "--reflect" in sys.argv:
-        write_reflect()
+    ONE = {"--instanced": write_instanced, "--ply": write_ply_cases,
+           "--update": write_tree_update, "--path": write_path_stats,
+           "--obj": write_obj_cases, "--reflect": write_reflect, "--env": write_environment}
+    chosen = [f for flag, f in ONE.items() if flag in sys.argv]
+    if chosen:
+        for f in chosen:
+            f()
     else:
         main()
         write_sah_costs()
-        write_instanced()
-        write_ply_cases()
-        write_tree_update()
-        write_path_stats()
-        write_obj_cases()
-        write_reflect()
+        for f in ONE.values():
+            f()

@@ -294,9 +294,9 @@ class SmallFrame:
         self.t = torch.empty(npx, device=dev)
         self.prim = torch.empty(npx, dtype=torch.int32, device=dev)
         self.nshadow = torch.zeros(1, dtype=torch.int64, device=dev)
-        self.n_events = 3
-        self.stage_names = ["whitted_primary_kernel", "whitted_shade_kernel"]
-        self.launches = 2
+        self.n_events = 2
+        self.stage_names = ["whitted_fused_kernel"]
+        self.launches = 1
 
     def frame(self, stream_ptr):
         self.bvh.render_whitted_device(self.params, self.rgb.data_ptr(), self.t.data_ptr(),
@@ -322,20 +322,23 @@ class SmallFrame:
         b_s, t_s = stats[2] / max(shadow, 1), stats[3] / max(shadow, 1)
         per_ray = {"primary_box_tests": round(b_p, 3), "primary_tri_tests": round(t_p, 3),
                    "shadow_box_tests": round(b_s, 3), "shadow_tri_tests": round(t_s, 3)}
-        return (prim * (32 + 16 + 32 * b_p + 48 * t_p),
-                shadow * (32 + 4 + 32 * b_s + 48 * t_s)), per_ray
+        # one kernel traces both kinds of ray
+        return (prim * (32 + 16 + 32 * b_p + 48 * t_p) +
+                shadow * (32 + 4 + 32 * b_s + 48 * t_s),), per_ray
 
-    # DRAM bytes per primary ray of whitted_primary_kernel, from one ncu
-    # capture of this workload at full size (262,144 rays, 3.97 MB).
-    DRAM_BYTES_PER_RAY = 15.1
+    # DRAM bytes per pixel of whitted_fused_kernel, from one ncu capture of
+    # this workload at full size (262,144 pixels: 4.84 MB read, 0.02 MB
+    # written).
+    DRAM_BYTES_PER_PIXEL = 18.6
 
     def traffic(self, rays):
         prim, _ = rays
-        return self.DRAM_BYTES_PER_RAY * prim, ("ncu DRAM bytes of one whitted_primary_kernel "
-                                                "launch at full size (15.1 B per ray)")
+        return self.DRAM_BYTES_PER_PIXEL * prim, (
+            f"ncu DRAM bytes of one whitted_fused_kernel launch at full size "
+            f"({self.DRAM_BYTES_PER_PIXEL} B per pixel)")
 
     def group_stages(self, stage_ms):
-        return self.stage_names, [stage_ms[0], stage_ms[1]]
+        return self.stage_names, [stage_ms[0]]
 
     def cpu_reference(self, seconds_budget, threads):
         from oracle.pyoracle import Reference
@@ -816,11 +819,11 @@ class AnimatedFrame(SmallFrame):
                            for v in self.poses]
         self.sc.mesh.vertices = self.poses[0]
         bvh.update()
-        # kernels per step: 2 for the frame; the update's state reset, object
+        # kernels per step: 1 for the frame; the update's state reset, object
         # boxes, leaf boxes, re-splits, 2 scan kernels, relocation, next-free
         # advance, rotations, parents, 1 + 9 pointer-jumping rounds, records
         # and the triangle records
-        self.launches = 2 + 21
+        self.launches = 1 + 21
 
     def frame(self, stream_ptr):
         k = self.k % self.PERIOD

@@ -416,11 +416,11 @@ RQ_API int rq_server_destroy(rq_server* server);
  * has no counterpart in the reference.  It is for callers that cannot call
  * cudaMalloc: a process whose device memory is already handed out to another
  * allocator, or a render thread that must not make calls which can
- * synchronise the whole device.  The frame's scratch (hit record per pixel,
- * compaction queue, counters, material table) lives in a fixed array inside
- * the library, so the call allocates nothing; the caller still passes the
- * outputs.  Limits: xres * yres <= 1,048,576 pixels and n_materials <= 1024;
- * larger frames return RQ_ERR_CAPACITY.  The first call on a device looks up
+ * synchronise the whole device.  The frame's scratch (work counters, shadow
+ * counter, material table) lives in a fixed array inside the library, so the
+ * call allocates nothing; the caller still passes the outputs.  Limit:
+ * n_materials <= 1024 (more return RQ_ERR_CAPACITY); any resolution
+ * rq_render_whitted_device takes is accepted.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress, with that device
  * current) and caches it; make that first call before any stream capture.
  * All calls on a device share the array: calls whose work overlaps on the
@@ -552,8 +552,8 @@ RQ_API int rq_set_path_debug(rq_scene* scene, int32_t* d_prim, float* d_org,
  * Profiling hook (the role of DynBVH's COLLECT_STATS counters,
  * Model/Groups/DynBVH.h:314-374): when `events` (n cudaEvent_t handles
  * created by the caller, up to 16) is set, the frame paths record events[0]
- * before their first stage and events[k] after stage k: Whitted frames have
- * two stages (primary, shade); path-traced frames record, for their last
+ * before their first stage and events[k] after stage k: Whitted frames
+ * (rq_render_whitted*) run as one stage; path-traced frames record, for their last
  * chunk, extend and shade of every bounce (events[1 + 2d], events[2 + 2d])
  * and the resolve after them.  NULL turns it off.
  */

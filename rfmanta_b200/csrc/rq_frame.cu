@@ -80,9 +80,6 @@ bool environment_from(const rq_environment& in, Environment& out) {
 
 // Scratch of the frame path, owned by the scene and grown on demand.
 struct FrameScratch {
-  size_t npix = 0;
-  int32_t* pos = nullptr;
-  int32_t* queue = nullptr;
   int32_t* counters = nullptr;
   unsigned long long* shadow = nullptr;
   float* materials = nullptr;
@@ -95,8 +92,6 @@ struct FrameScratch {
   int32_t* d_prim = nullptr;
   cudaStream_t stream = nullptr;
   ~FrameScratch() {
-    cudaFree(pos);
-    cudaFree(queue);
     cudaFree(counters);
     cudaFree(shadow);
     cudaFree(materials);
@@ -137,16 +132,6 @@ static int prepare(Scene* s, const rq_whitted_params* p, FrameParams& P) {
     return set_fail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   if (!s->frame) s->frame = new FrameScratch();
   FrameScratch* f = s->frame;
-  const size_t npix = (size_t)p->xres * p->yres;
-  if (f->npix < npix) {
-    cudaFree(f->pos);
-    cudaFree(f->queue);
-    f->pos = f->queue = nullptr;
-    if (cudaMalloc(&f->pos, npix * 4) != cudaSuccess ||
-        cudaMalloc(&f->queue, npix * 4) != cudaSuccess)
-      return set_fail(RQ_ERR_OOM, "frame scratch allocation failed");
-    f->npix = npix;
-  }
   if (!f->counters) {
     if (cudaMalloc(&f->counters, kNumCounters * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&f->shadow, sizeof(unsigned long long)) != cudaSuccess)
@@ -176,18 +161,15 @@ static int launch(Scene* s, const FrameParams& P, float* rgb, float* t, int32_t*
   B.rgb = rgb;
   B.t = t;
   B.prim = prim;
-  B.pos = f->pos;
-  B.queue = f->queue;
   B.counters = f->counters;
   B.shadow_rays_ptr = shadow ? shadow : f->shadow;
   B.stats = s->stats;
   const DevScene S = s->dev();
   const size_t smem = (size_t)S.depth * 128 * sizeof(int2);
   const int bps = whitted_blocks_per_sm(s->tri_kind, smem);
-  const int grid = std::max(1, bps * s->num_sms);
   const int npix = P.xres * P.yres;
-  const int grid1 = std::min(grid, (npix + 127) / 128);
-  cudaError_t e = launch_whitted(S, P, B, grid1, grid, st, s->stage_events, s->n_stage_events);
+  const int grid = std::max(1, std::min(bps * s->num_sms, (npix + 127) / 128));
+  cudaError_t e = launch_whitted(S, P, B, grid, st, s->stage_events, s->n_stage_events);
   if (e != cudaSuccess) return set_fail(RQ_ERR_CUDA, std::string("whitted launch: ") +
                                                          cudaGetErrorString(e));
   return RQ_OK;

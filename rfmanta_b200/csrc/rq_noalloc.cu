@@ -4,11 +4,11 @@
 // allocator, or a host thread that may not call cudaMalloc/cudaFree because
 // those calls can synchronise the device in the middle of its work.
 //
-// The frame's scratch - per-pixel hit record index, the compacted queue of
-// hit pixels, the stage counters, the shadow-ray counter and the material
-// table - lives in one file-scope __device__ array of fixed size instead of
-// buffers the scene allocates on first use.  Limits: at most
-// kNoAllocMaxPixels pixels and kNoAllocMaxMaterials materials per frame.
+// The frame's scratch - the work counters, the shadow-ray counter and the
+// material table - lives in one file-scope __device__ array of fixed size
+// instead of buffers the scene allocates on first use.  The frame kernel
+// keeps no per-pixel scratch, so any resolution the allocating entry point
+// takes is accepted; the limit is kNoAllocMaxMaterials materials per frame.
 //
 // Host code cannot use the array's name as a device address (on the host it
 // names a host-side stand-in).  The device address is looked up with
@@ -32,13 +32,10 @@
 
 namespace rq {
 
-constexpr size_t kNoAllocMaxPixels = size_t(1) << 20;  // 1,048,576 (1280x720 fits)
 constexpr int kNoAllocMaxMaterials = 1024;
 
 // Byte offsets inside the array (each region 256-byte aligned).
-constexpr size_t kOffPos = 0;
-constexpr size_t kOffQueue = kOffPos + 4 * kNoAllocMaxPixels;
-constexpr size_t kOffCounters = kOffQueue + 4 * kNoAllocMaxPixels;
+constexpr size_t kOffCounters = 0;
 constexpr size_t kOffShadow = kOffCounters + 256;
 constexpr size_t kOffMaterials = kOffShadow + 256;
 constexpr size_t kNoAllocBytes = kOffMaterials + 12 * (size_t)kNoAllocMaxMaterials;
@@ -82,11 +79,7 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
   if (!s || !p || !d_rgb || !d_t || !d_prim) return na_fail(RQ_ERR_ARG, "NULL argument");
   if (p->xres <= 0 || p->yres <= 0) return na_fail(RQ_ERR_ARG, "bad resolution");
   const size_t npix = (size_t)p->xres * (size_t)p->yres;
-  if (npix > kNoAllocMaxPixels)
-    return na_fail(RQ_ERR_CAPACITY,
-                   "rq_render_whitted_device_noalloc: " + std::to_string(npix) +
-                       " pixels exceed its fixed scratch of " +
-                       std::to_string(kNoAllocMaxPixels) + " pixels");
+  if (npix > (size_t(1) << 30)) return na_fail(RQ_ERR_ARG, "bad resolution");
   if (p->n_materials <= 0 || !p->material_rgb) return na_fail(RQ_ERR_ARG, "no materials");
   if (p->n_materials > kNoAllocMaxMaterials)
     return na_fail(RQ_ERR_CAPACITY,
@@ -125,18 +118,16 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
   B.rgb = d_rgb;
   B.t = d_t;
   B.prim = d_prim;
-  B.pos = reinterpret_cast<int32_t*>(base + kOffPos);
-  B.queue = reinterpret_cast<int32_t*>(base + kOffQueue);
   B.counters = reinterpret_cast<int32_t*>(base + kOffCounters);
   B.shadow_rays_ptr = d_shadow_rays ? reinterpret_cast<unsigned long long*>(d_shadow_rays)
                                     : reinterpret_cast<unsigned long long*>(base + kOffShadow);
   B.stats = s->stats;
   const DevScene S = s->dev();
   const size_t smem = (size_t)S.depth * 128 * sizeof(int2);
-  const int grid = std::max(1, whitted_blocks_per_sm(s->tri_kind, smem) * s->num_sms);
-  const int grid1 = std::min(grid, (int)((npix + 127) / 128));
-  // launch_whitted clears the stage counters and the shadow counter first
-  e = launch_whitted(S, P, B, grid1, grid, st, nullptr, 0);
+  const int grid = std::max(1, std::min(whitted_blocks_per_sm(s->tri_kind, smem) * s->num_sms,
+                                        (int)((npix + 127) / 128)));
+  // launch_whitted clears the work counters and the shadow counter first
+  e = launch_whitted(S, P, B, grid, st, nullptr, 0);
   if (e != cudaSuccess) return na_fail(RQ_ERR_CUDA, std::string("whitted launch: ") + cudaGetErrorString(e));
   return RQ_OK;
 }

@@ -14,7 +14,7 @@ namespace rq {
 constexpr int kMaxLights = 16;
 constexpr int kMaxReflectDepth = 32;  // reflective Phong recursion limit
 
-enum FrameCounter { kCntQueue = 0, kCntWork = 1, kNumCounters = 4 };
+enum FrameCounter { kCntWork = 0, kNumCounters = 4 };  // kCntWork: pixels handed out
 
 // Per-frame constants (passed by value as a kernel parameter).
 struct FrameParams {
@@ -38,14 +38,12 @@ struct FrameParams {
   float cutoff;
 };
 
-// Device buffers of one frame.  rgb/t/prim are outputs; pos, queue and the
-// counters are scratch.
+// Device buffers of one frame.  rgb/t/prim are outputs; the counters are
+// scratch.
 struct FrameBuffers {
   float* rgb;       // 3 per pixel
   float* t;         // primary hit distance per pixel
   int32_t* prim;    // primary triangle id per pixel (-1 = miss)
-  int32_t* pos;     // scratch: triangle record index of the primary hit
-  int32_t* queue;   // scratch: compacted hit pixels
   int32_t* counters;                 // scratch: kNumCounters ints
   unsigned long long* shadow_rays_ptr;  // shadow rays sent this frame
   // optional statistics (NULL = off): box tests and triangle tests of the
@@ -82,9 +80,11 @@ __device__ __forceinline__ void primary_ray(const FrameParams& P, int x, int y,
   r.minT = kMaxT;
 }
 
+// The frame's one persistent kernel on `grid` blocks of 128 threads; records
+// ev[0] before it and ev[1] after it when given.
 cudaError_t launch_whitted(const DevScene& S, const FrameParams& P,
-                           const FrameBuffers& B, int grid1, int grid2,
-                           cudaStream_t st, const cudaEvent_t* ev, int nev);
+                           const FrameBuffers& B, int grid, cudaStream_t st,
+                           const cudaEvent_t* ev, int nev);
 int whitted_blocks_per_sm(int tri_kind, size_t smem);
 
 // PinholeCamera::setup (Model/Cameras/PinholeCamera.cc:167-198) on the host.

@@ -58,19 +58,38 @@ def test_noalloc_frame_matches_allocating_entry_point():
     assert free[1] == free[0]
 
 
-def test_noalloc_rejects_frames_beyond_its_scratch():
+def test_noalloc_large_frames_and_material_limit():
+    """The frame kernel keeps no per-pixel scratch, so a 2048x1024 frame
+    renders through the fixed array as through the allocating entry point;
+    a material table beyond the array's 1,024 entries is refused."""
+    import torch
     from rfmanta_b200 import _lib, scenes
     from rfmanta_b200.dynbvh import GpuDynBVH
     sc = scenes.small_frame_scene(level=2, grid=4, xres=2048, yres=1024)
     bvh = GpuDynBVH()
     bvh.setGroup(sc.mesh)
     bvh.rebuild()
-    import torch
     p = bvh.whitted_params(sc)
-    tiny = torch.zeros(4, device="cuda")
+    npx = sc.xres * sc.yres
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    outs = []
+    for fn in (_lib.lib.rq_render_whitted_device, _lib.lib.rq_render_whitted_device_noalloc):
+        rgb = torch.zeros(npx * 3, device="cuda")
+        t = torch.zeros(npx, device="cuda")
+        prim = torch.zeros(npx, dtype=torch.int32, device="cuda")
+        _lib.check(fn(bvh.handle, C.byref(p), C.c_void_p(rgb.data_ptr()),
+                      C.c_void_p(t.data_ptr()), C.c_void_p(prim.data_ptr()), None, stream))
+        torch.cuda.synchronize()
+        outs.append((rgb.cpu().numpy(), prim.cpu().numpy()))
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(_bits(outs[0][0]), _bits(outs[1][0]))
+    mats = np.full((1025, 3), 0.5, np.float32)
+    p.n_materials = mats.shape[0]
+    p.material_rgb = mats.ctypes.data
+    tiny = torch.zeros(npx * 3, device="cuda")
     rc = _lib.lib.rq_render_whitted_device_noalloc(bvh.handle, C.byref(p),
                                                    C.c_void_p(tiny.data_ptr()),
                                                    C.c_void_p(tiny.data_ptr()),
                                                    C.c_void_p(tiny.data_ptr()), None, None)
     assert rc == _lib.RQ_ERR_CAPACITY
-    assert b"exceed" in _lib.lib.rq_last_error()
+    assert b"materials" in _lib.lib.rq_last_error()

@@ -20,8 +20,10 @@
 # RAYPACKET_MAXSIZE 64, SCRATCHPAD_MAXSIZE 128, MAXCACHELINESIZE 128,
 # DynBVH ports/approximate/lazy all off.  Nothing is written outside _ref/.
 
-REF ?= /root/reference
+# The reference checkout: REF=..., else $RFMANTA_REFERENCE, else a checkout
+# named `reference` beside this repository.
 HERE := $(dir $(lastword $(MAKEFILE_LIST)))
+REF ?= $(if $(RFMANTA_REFERENCE),$(RFMANTA_REFERENCE),$(abspath $(HERE)../../reference))
 OUT := $(HERE)_ref
 # The system compiler driver links libstdc++ as a shared library, so the
 # checker shares one C++ runtime with the Python process that loads it.

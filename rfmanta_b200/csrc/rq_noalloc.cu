@@ -87,11 +87,17 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
                        std::to_string(kNoAllocMaxMaterials) + " materials");
   if (p->n_lights < 0 || p->n_lights > kMaxLights || (p->n_lights > 0 && !p->lights))
     return na_fail(RQ_ERR_ARG, "0..16 point lights");
+  if (s->instanced) return na_fail(RQ_ERR_ARG, "instanced scene: render it with rq_render_frame");
+  if (cudaSetDevice(s->device) != cudaSuccess) return na_fail(RQ_ERR_CUDA, "cudaSetDevice");
+  // The scene's tree, statistics pointer and material maximum may be
+  // replaced by an update on another host thread (an update can free and
+  // reallocate the node records); the same per-scene lock as the allocating
+  // entry point keeps this frame's snapshot of them valid.  A host mutex
+  // makes no device call.
+  std::lock_guard<std::mutex> g(s->frame_mu);
   if (s->max_face_material >= p->n_materials)
     return na_fail(RQ_ERR_ARG, "face_material past n_materials");
   if (!s->has_tree) return na_fail(RQ_ERR_STATE, "scene has no tree");
-  if (s->instanced) return na_fail(RQ_ERR_ARG, "instanced scene: render it with rq_render_frame");
-  if (cudaSetDevice(s->device) != cudaSuccess) return na_fail(RQ_ERR_CUDA, "cudaSetDevice");
   unsigned char* base = nullptr;
   int rc = scratch_address(s->device, &base);
   if (rc != RQ_OK) return rc;
@@ -109,8 +115,11 @@ extern "C" int rq_render_whitted_device_noalloc(rq_scene* scene,
   if (!environment_from(p->environment, P.env))
     return na_fail(RQ_ERR_ARG, "bad environment (kind, or a zero background up)");
   float* mats = reinterpret_cast<float*>(base + kOffMaterials);
+  // cudaMemcpyDefault: the table may sit in pinned host memory (an
+  // asynchronous copy) or in device memory; a pageable host table is
+  // accepted too, but the driver then stages it and the call may block.
   cudaError_t e = cudaMemcpyAsync(mats, p->material_rgb, sizeof(float) * 3 * p->n_materials,
-                                  cudaMemcpyHostToDevice, st);
+                                  cudaMemcpyDefault, st);
   if (e != cudaSuccess) return na_fail(RQ_ERR_CUDA, std::string("materials: ") + cudaGetErrorString(e));
   P.materials = mats;
 

@@ -5,9 +5,11 @@ calls such as cudaMalloc).  Its scratch is a fixed array inside the library,
 so it is checked here against the allocating entry point
 rq_render_whitted_device: two calls in a row, each equal to the allocating
 call bit for bit (the tolerance all frame tests use: none), and no change in
-free device memory between the first and the second call.  The file name
-makes pytest collect it last."""
+free device memory from before the first no-alloc call to after the second.
+A threaded test runs no-alloc frames beside tree updates of the same scene
+on another host thread.  The file name makes pytest collect it last."""
 import ctypes as C
+import threading
 
 import numpy as np
 import pytest
@@ -42,7 +44,8 @@ def test_noalloc_frame_matches_allocating_entry_point():
         C.c_void_p(want[2].data_ptr()), C.c_void_p(want[3].data_ptr()), C.c_void_p(stream)))
     torch.cuda.synchronize()
     outs = [buffers(), buffers()]
-    free = []
+    torch.cuda.synchronize()
+    free = [torch.cuda.mem_get_info()[0]]
     for got in outs:
         _lib.check(_lib.lib.rq_render_whitted_device_noalloc(
             bvh.handle, C.byref(p), C.c_void_p(got[0].data_ptr()),
@@ -55,7 +58,7 @@ def test_noalloc_frame_matches_allocating_entry_point():
         assert np.array_equal(got[2].cpu().numpy(), want[2].cpu().numpy())
         assert np.array_equal(_bits(got[1].cpu().numpy()), _bits(want[1].cpu().numpy()))
         assert np.array_equal(_bits(got[0].cpu().numpy()), _bits(want[0].cpu().numpy()))
-    assert free[1] == free[0]
+    assert free[1] == free[0] and free[2] == free[0], free
 
 
 def test_noalloc_large_frames_and_material_limit():
@@ -93,3 +96,61 @@ def test_noalloc_large_frames_and_material_limit():
                                                    C.c_void_p(tiny.data_ptr()), None, None)
     assert rc == _lib.RQ_ERR_CAPACITY
     assert b"materials" in _lib.lib.rq_last_error()
+
+
+def test_noalloc_frames_beside_updates_on_another_thread():
+    """Manta's workers call into one scene from several host threads.  One
+    thread renders no-alloc frames while another updates the same scene's
+    tree (with rotations, which can replace the node records); both use the
+    legacy default stream, so the GPU runs their work in launch order, and
+    the scene's lock keeps every frame's snapshot of the tree valid.  After
+    both finish, the no-alloc frame equals the allocating one."""
+    import torch
+    from rfmanta_b200 import _lib, scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    sc = scenes.small_frame_scene(level=4, grid=30, xres=256, yres=256)
+    bvh = GpuDynBVH()
+    bvh.setGroup(sc.mesh)
+    bvh.rebuild()
+    p = bvh.whitted_params(sc)
+    npx = sc.xres * sc.yres
+    v0 = sc.mesh.vertices.copy()
+    poses = [np.ascontiguousarray(scenes.wave_vertices(v0, k, 4)) for k in range(4)]
+    rgb = torch.zeros(npx * 3, device="cuda")
+    t = torch.zeros(npx, device="cuda")
+    prim = torch.zeros(npx, dtype=torch.int32, device="cuda")
+    errors = []
+
+    def frames():
+        for _ in range(40):
+            rc = _lib.lib.rq_render_whitted_device_noalloc(
+                bvh.handle, C.byref(p), C.c_void_p(rgb.data_ptr()), C.c_void_p(t.data_ptr()),
+                C.c_void_p(prim.data_ptr()), None, None)
+            if rc != _lib.RQ_OK:
+                errors.append(("frame", rc))
+
+    def updates():
+        for k in range(40):
+            v = poses[k % 4]
+            rc = _lib.lib.rq_scene_update_vertices_ex(bvh.handle, C.c_void_p(v.ctypes.data),
+                                                      v.shape[0], _lib.RQ_UPDATE_ROTATE)
+            if rc != _lib.RQ_OK:
+                errors.append(("update", rc))
+
+    th = [threading.Thread(target=frames), threading.Thread(target=updates)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    torch.cuda.synchronize()
+    assert not errors, errors
+    outs = []
+    for fn in (_lib.lib.rq_render_whitted_device, _lib.lib.rq_render_whitted_device_noalloc):
+        o = (torch.zeros(npx * 3, device="cuda"), torch.zeros(npx, dtype=torch.int32, device="cuda"))
+        _lib.check(fn(bvh.handle, C.byref(p), C.c_void_p(o[0].data_ptr()),
+                      C.c_void_p(t.data_ptr()), C.c_void_p(o[1].data_ptr()), None, None))
+        torch.cuda.synchronize()
+        outs.append((o[0].cpu().numpy(), o[1].cpu().numpy()))
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(_bits(outs[0][0]), _bits(outs[1][0]))
+    assert (outs[1][1] >= 0).any()

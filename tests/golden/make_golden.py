@@ -374,30 +374,56 @@ def write_path_stats() -> None:
     print(path, os.path.getsize(path), "bytes")
 
 
+def sah_scene_makers():
+    """Scenes whose reference SAH cost pins the GPU builder (2% bound), as
+    name -> generator.  The first three are small; the rest are the
+    benchmark scenes at full size: the path-tracing frame (1,212,416
+    triangles), the coherent frame's 1024x1024 heightfield (2,097,152), and
+    the two largest batched-query scenes (3,276,800 and 5,120,000)."""
+    def soup():
+        rng = np.random.default_rng(23)
+        n = 20000
+        c = rng.uniform(-2, 2, (n, 1, 3))
+        tri = (c + rng.normal(scale=0.05, size=(n, 3, 3))).reshape(-1, 3).astype(np.float32)
+        return scenes.Mesh(tri, np.arange(3 * n, dtype=np.uint32).reshape(-1, 3),
+                           np.zeros(n, np.uint32), np.ones((1, 3), np.float32))
+
+    return {
+        "small_frame": lambda: scenes.small_frame_scene().mesh,
+        "heightfield_256": lambda: scenes.merge(
+            [scenes.heightfield(256, 256, seed=21, extent=4.0, y=-1.1),
+             scenes.displaced_icosphere(4, seed=22, center=(0.5, 0.0, -0.5), radius=0.6)],
+            np.array([[0.5, 0.5, 0.5]], np.float32)),
+        "random_soup": soup,
+        "path_frame": lambda: scenes.path_scene().mesh,
+        "coherent_heightfield": lambda: scenes.coherent_scene().inner[0],
+        "query_scene_6": lambda: scenes.query_scene(6),
+        "query_scene_7": lambda: scenes.query_scene(7),
+    }
+
+
 def sah_scenes():
-    """Scenes whose reference SAH cost pins the GPU builder (2% bound)."""
-    out = {"small_frame": scenes.small_frame_scene().mesh,
-           "heightfield_256": scenes.merge(
-               [scenes.heightfield(256, 256, seed=21, extent=4.0, y=-1.1),
-                scenes.displaced_icosphere(4, seed=22, center=(0.5, 0.0, -0.5), radius=0.6)],
-               np.array([[0.5, 0.5, 0.5]], np.float32))}
-    rng = np.random.default_rng(23)
-    n = 20000
-    c = rng.uniform(-2, 2, (n, 1, 3))
-    tri = (c + rng.normal(scale=0.05, size=(n, 3, 3))).reshape(-1, 3).astype(np.float32)
-    out["random_soup"] = scenes.Mesh(tri, np.arange(3 * n, dtype=np.uint32).reshape(-1, 3),
-                                     np.zeros(n, np.uint32), np.ones((1, 3), np.float32))
-    return out
+    """The small SAH scenes, generated."""
+    mk = sah_scene_makers()
+    return {k: mk[k]() for k in ("small_frame", "heightfield_256", "random_soup")}
 
 
 def write_sah_costs() -> None:
+    """DynBVH::rebuild (the reference's exact-sweep SAH build) of every SAH
+    scene and DynBVH::computeCost of the result (Model/Groups/DynBVH.cc:
+    1699-1857, 3389-3416), with the reference's build time."""
     import json
+    import time
     ref = Reference()
-    costs = {}
-    for name, mesh in sah_scenes().items():
+    costs, secs = {}, {}
+    for name, make in sah_scene_makers().items():
+        mesh = make()
+        t0 = time.perf_counter()
         rs = ref.scene(mesh, 0)
+        secs[name] = round(time.perf_counter() - t0, 2)
         costs[name] = rs.sah_cost()
         rs.close()
+        print(name, mesh.n_tris, costs[name], secs[name], "s", flush=True)
     path = os.path.join(OUT, "sah_costs.json")
     with open(path, "w") as f:
         json.dump(costs, f, indent=1, sort_keys=True)
@@ -407,13 +433,13 @@ def write_sah_costs() -> None:
 if __name__ == "__main__":
     ONE = {"--instanced": write_instanced, "--ply": write_ply_cases,
            "--update": write_tree_update, "--path": write_path_stats,
-           "--obj": write_obj_cases, "--reflect": write_reflect, "--env": write_environment}
+           "--obj": write_obj_cases, "--reflect": write_reflect, "--env": write_environment,
+           "--sah": write_sah_costs}
     chosen = [f for flag, f in ONE.items() if flag in sys.argv]
     if chosen:
         for f in chosen:
             f()
     else:
         main()
-        write_sah_costs()
         for f in ONE.values():
             f()

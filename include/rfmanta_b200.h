@@ -242,11 +242,14 @@ typedef struct {
   int blocks_per_sm;    /* resident blocks per SM, 0 = occupancy maximum */
   int refill_threshold; /* idle lanes in a warp before it fetches new rays */
   int persistent;       /* 0 = one thread per ray, 1 = persistent */
+  int reg_stack;        /* traversal-stack entries kept in registers (0, 1, 2, 4);
+                           the rest spill to shared memory.  Path stages only. */
 } rq_launch_config;
 
 /* rq_set_launch_config / rq_get_launch_config also take these flags for the
  * path tracer's two persistent stages (rq_render_path*): block_threads,
- * blocks_per_sm and refill_threshold apply, `persistent` is ignored. */
+ * blocks_per_sm, refill_threshold and reg_stack apply, `persistent` is
+ * ignored. */
 #define RQ_PATH_EXTEND 2
 #define RQ_PATH_SHADE 3
 
@@ -411,6 +414,37 @@ RQ_API int rq_server_stats(rq_server* server, uint64_t* ray_counts, long long* s
                            int* pending, int* active, size_t* bytes_in_use);
 RQ_API int rq_server_destroy(rq_server* server);
 
+/* Runs a timed arrival stream through the server on the calling thread (the
+ * request loop a serving front end runs; the analogue of RTRT's frame loop
+ * handing out WorkQueue assignments, Engine/Control/RTRT.cc:668-1028,
+ * Core/Thread/WorkQueue.cc:61-69).  Request k is submitted once
+ * arrival_s[k] seconds have passed since the call began (any order), the
+ * engine is stepped while it has work, and finished requests are collected
+ * and released.  On return latency_s[k] and queue_s[k] hold each request's
+ * latency (submit to completion observed on the host) and admission wait;
+ * images (NULL, or n host pointers of which any may be NULL) receive the
+ * finished images; *wall_s = first submit to last completion.  Gives up with
+ * RQ_ERR_TIMEOUT after timeout_s seconds. */
+RQ_API int rq_server_run_stream(rq_server* server, const rq_serve_request* requests,
+                                const double* arrival_s, int n, float* const* images,
+                                double* latency_s, double* queue_s, double* wall_s,
+                                double timeout_s);
+
+/* Per-step records (the server's COLLECT_STATS): with profiling on, every
+ * step records the requests, chunks and distinct scenes it packed, its path
+ * count, its deepest request and its device time (CUDA events on the
+ * server's stream).  rq_server_profile copies up to max_steps records of
+ * steps that have finished and clears them. */
+typedef struct {
+  int requests, chunks, scenes, max_depth;
+  long long paths;
+  float gpu_ms;
+  double t_enqueue_s;  /* host time of the enqueue, since profiling began */
+} rq_server_step_record;
+RQ_API int rq_server_set_profile(rq_server* server, int on);
+RQ_API int rq_server_profile(rq_server* server, rq_server_step_record* records,
+                             int max_steps, int* n_steps);
+
 /*
  * rq_render_whitted_device without any device allocation.  This entry point
  * has no counterpart in the reference.  It is for callers that cannot call
@@ -425,6 +459,12 @@ RQ_API int rq_server_destroy(rq_server* server);
  * current) and caches it; make that first call before any stream capture.
  * All calls on a device share the array: calls whose work overlaps on the
  * GPU race and must be ordered by the caller (one stream, or events).
+ * params->material_rgb is copied into the array on `stream` each call; give
+ * it in pinned host memory or device memory so the copy is asynchronous (a
+ * pageable host table is accepted, but the driver stages it and the call can
+ * block).  Calls on one scene take the scene's lock, like the other frame
+ * entry points, so an update on another host thread never frees the tree
+ * under a frame being launched.
  */
 RQ_API int rq_render_whitted_device_noalloc(rq_scene* scene,
                                             const rq_whitted_params* params,

@@ -106,6 +106,15 @@ class BatchConfig(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServerStepRecord(C.Structure):
+    _fields_ = [("requests", C.c_int), ("chunks", C.c_int), ("scenes", C.c_int),
+                ("max_depth", C.c_int), ("paths", C.c_longlong), ("gpu_ms", C.c_float),
+                ("t_enqueue_s", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class ServeRequest(C.Structure):
     _fields_ = [("scene", C.c_int), ("eye", C.c_float * 3), ("lookat", C.c_float * 3),
                 ("up", C.c_float * 3), ("hfov", C.c_float), ("vfov", C.c_float),
@@ -119,7 +128,8 @@ class ServeRequest(C.Structure):
 
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
-                ("refill_threshold", C.c_int), ("persistent", C.c_int)]
+                ("refill_threshold", C.c_int), ("persistent", C.c_int),
+                ("reg_stack", C.c_int)]
 
 
 def _load():
@@ -169,6 +179,10 @@ def _load():
         "rq_server_stats": ([vp, vp, C.POINTER(C.c_longlong), C.POINTER(i), C.POINTER(i),
                              C.POINTER(sz)], i),
         "rq_server_destroy": ([vp], i),
+        "rq_server_run_stream": ([vp, vp, vp, i, vp, vp, vp, C.POINTER(C.c_double), C.c_double],
+                                 i),
+        "rq_server_set_profile": ([vp, i], i),
+        "rq_server_profile": ([vp, vp, i, C.POINTER(i)], i),
         "rq_scene_build_seconds": ([vp, C.POINTER(C.c_double)], i),
         "rq_scene_update_vertices": ([vp, vp, i], i),
         "rq_scene_update_vertices_ex": ([vp, vp, i, i], i),

@@ -222,6 +222,7 @@ int rq_scene_create_instanced(rq_scene* const* inner, int n_inner, const int32_t
     s->cfg[k].blocks_per_sm = 0;
     s->cfg[k].refill_threshold = 8;
     s->cfg[k].persistent = 0;
+    s->cfg[k].reg_stack = 0;
   }
   if (cudaMalloc(&s->d_verts, verts.size() * 4) != cudaSuccess ||
       cudaMalloc(&s->d_idx, idx.size() * 4) != cudaSuccess ||

@@ -51,13 +51,19 @@ __device__ __forceinline__ int queue_count(const PathBuffers& B, int depth, int 
 // work counter and the idle lanes start them.  Lanes stay busy while a
 // warp's rays finish at different times; results do not depend on the
 // schedule.
-template <int KIND, bool STATS>
+//
+// R = traversal-stack entries kept in registers (0, 1, 2 or 4): the newest
+// pending children stay in registers and only older ones go to this
+// thread's shared-memory column, which holds depth - R entries.
+template <int KIND, bool STATS, int R>
 __global__ void __launch_bounds__(256)
     path_extend_persistent_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0,
                                   int refill) {
   extern __shared__ int2 smem_stack[];
   int2* stk = smem_stack + threadIdx.x;
   const int stride = blockDim.x;
+  RegStack<R> st;
+  st.init(stk, stride);
   const int nq = queue_count(B, depth, n0);
   const int* qin = B.queue[depth & 1];
   int* counter = &B.counters[kFetchBase + depth];
@@ -68,7 +74,7 @@ __global__ void __launch_bounds__(256)
   Counts cnt;
   Ray r;
   Hit h;
-  int ref = kDone, sp = 0;
+  int ref = kDone;
   for (;;) {
     const bool idle = (p < 0) && !exhausted;
     const unsigned m = __ballot_sync(0xffffffffu, idle);
@@ -83,7 +89,8 @@ __global__ void __launch_bounds__(256)
         if (qi < nq) {
           p = depth == 0 ? qi : qin[qi];
           load_extension_ray(B, p, r);
-          start_ray(S, r, h, ref, sp);
+          start_ray(S, r, h, ref, st.sp);
+          st.nreg = 0;
           if (STATS) cnt.boxes += 1;
         } else {
           exhausted = true;
@@ -92,7 +99,7 @@ __global__ void __launch_bounds__(256)
     }
     if (__all_sync(0xffffffffu, exhausted)) break;
     if (p >= 0) {
-      if (ref != kDone) step<KIND, false, STATS>(S, r, h, ref, sp, stk, stride, &cnt);
+      if (ref != kDone) step_dyn<KIND, R, STATS>(S, r, h, ref, st, false, &cnt);
       if (ref == kDone) {
         store_extension(P, B, depth, p, r, h);
         p = -1;
@@ -117,13 +124,15 @@ __global__ void __launch_bounds__(256)
 // steps its shadow ray's any-hit traversal; when the ray is done (or none was
 // needed) it applies shade_finish and the survivors are compacted into the
 // next queue at the warp's common point, one atomic per warp.
-template <int KIND, bool STATS>
+template <int KIND, bool STATS, int R>
 __global__ void __launch_bounds__(256)
     path_shade_persistent_kernel(DevScene S, PathParams P, PathBuffers B, int depth, int n0,
                                  int refill) {
   extern __shared__ int2 smem_stack[];
   int2* stk = smem_stack + threadIdx.x;
   const int stride = blockDim.x;
+  RegStack<R> st;
+  st.init(stk, stride);
   const int nq = queue_count(B, depth, n0);
   const int* qin = B.queue[depth & 1];
   int* qout = B.queue[(depth + 1) & 1];
@@ -137,7 +146,7 @@ __global__ void __launch_bounds__(256)
   float contrib[3];
   Ray sr;
   Hit sh;
-  int ref = kDone, sp = 0;
+  int ref = kDone;
   for (;;) {
     const bool idle = (p < 0) && !exhausted;
     const unsigned m = __ballot_sync(0xffffffffu, idle);
@@ -155,7 +164,8 @@ __global__ void __launch_bounds__(256)
           ref = kDone;
           if (traced) {
             ++nshadow;
-            start_ray(S, sr, sh, ref, sp);
+            start_ray(S, sr, sh, ref, st.sp);
+            st.nreg = 0;
             if (STATS) cnt.boxes += 1;
           }
         } else {
@@ -166,7 +176,7 @@ __global__ void __launch_bounds__(256)
     if (__all_sync(0xffffffffu, exhausted)) break;
     bool fin = false;
     if (p >= 0) {
-      if (ref != kDone) step<KIND, true, STATS>(S, sr, sh, ref, sp, stk, stride, &cnt);
+      if (ref != kDone) step_dyn<KIND, R, STATS>(S, sr, sh, ref, st, true, &cnt);
       if (ref == kDone) {
         if (traced && sh.id < 0) shade_finish(B, p, contrib);
         fin = true;
@@ -327,25 +337,49 @@ static int stage_grid(const void* f, int block, int blocks_per_sm, size_t smem) 
   return std::max(1, b * sms);
 }
 
+// Shared-memory stack bytes per block: the column holds the entries that do
+// not fit in the R registers (at least one, so the column is never empty).
+static size_t stack_smem(int depth, int block, int regs) {
+  return (size_t)std::max(1, depth - regs) * block * sizeof(int2);
+}
+
+template <int KIND, bool STATS>
+static const void* extend_fn(int regs) {
+  return regs == 4 ? (const void*)path_extend_persistent_kernel<KIND, STATS, 4>
+       : regs == 2 ? (const void*)path_extend_persistent_kernel<KIND, STATS, 2>
+       : regs == 1 ? (const void*)path_extend_persistent_kernel<KIND, STATS, 1>
+                   : (const void*)path_extend_persistent_kernel<KIND, STATS, 0>;
+}
+
+template <int KIND, bool STATS>
+static const void* shade_fn(int regs) {
+  return regs == 4 ? (const void*)path_shade_persistent_kernel<KIND, STATS, 4>
+       : regs == 2 ? (const void*)path_shade_persistent_kernel<KIND, STATS, 2>
+       : regs == 1 ? (const void*)path_shade_persistent_kernel<KIND, STATS, 1>
+                   : (const void*)path_shade_persistent_kernel<KIND, STATS, 0>;
+}
+
 template <int KIND, bool STATS>
 static void launch_bounces(const DevScene& S, const PathParams& P, const PathBuffers& B,
                            int n, const PathLaunch& L, cudaStream_t st,
                            const cudaEvent_t* ev, int nev) {
   const int eb = L.block_threads[0], sb = L.block_threads[1];
-  const size_t esm = (size_t)S.depth * eb * sizeof(int2);
-  const size_t ssm = (size_t)S.depth * sb * sizeof(int2);
-  const int egrid = stage_grid((const void*)path_extend_persistent_kernel<KIND, STATS>, eb,
-                               L.blocks_per_sm[0], esm);
-  const int sgrid = stage_grid((const void*)path_shade_persistent_kernel<KIND, STATS>, sb,
-                               L.blocks_per_sm[1], ssm);
+  const size_t esm = stack_smem(S.depth, eb, L.reg_stack[0]);
+  const size_t ssm = stack_smem(S.depth, sb, L.reg_stack[1]);
+  const void* ef = extend_fn<KIND, STATS>(L.reg_stack[0]);
+  const void* sf = shade_fn<KIND, STATS>(L.reg_stack[1]);
+  const int egrid = stage_grid(ef, eb, L.blocks_per_sm[0], esm);
+  const int sgrid = stage_grid(sf, sb, L.blocks_per_sm[1], ssm);
   for (int depth = 0; depth < P.max_depth; ++depth) {
     path_count_kernel<<<1, 32, 0, st>>>(B, depth, n);
-    path_extend_persistent_kernel<KIND, STATS><<<egrid, eb, esm, st>>>(S, P, B, depth, n,
-                                                                       L.refill[0]);
+    void* eargs[] = {(void*)&S, (void*)&P, (void*)&B, (void*)&depth, (void*)&n,
+                     (void*)&L.refill[0]};
+    cudaLaunchKernel(ef, dim3(egrid), dim3(eb), eargs, esm, st);
     if (nev > 1 + 2 * depth) cudaEventRecord(ev[1 + 2 * depth], st);
     if (B.alive) cudaMemsetAsync(B.alive, 0, (size_t)n, st);
-    path_shade_persistent_kernel<KIND, STATS><<<sgrid, sb, ssm, st>>>(S, P, B, depth, n,
-                                                                      L.refill[1]);
+    void* sargs[] = {(void*)&S, (void*)&P, (void*)&B, (void*)&depth, (void*)&n,
+                     (void*)&L.refill[1]};
+    cudaLaunchKernel(sf, dim3(sgrid), dim3(sb), sargs, ssm, st);
     if (B.alive) launch_ordered_compaction(B, n, depth, st);
     if (nev > 2 + 2 * depth) cudaEventRecord(ev[2 + 2 * depth], st);
   }
@@ -376,10 +410,10 @@ cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffer
 }
 
 int path_blocks_per_sm(int tri_kind, size_t smem) {
-  const void* fs[4] = {(const void*)path_shade_persistent_kernel<kWald, false>,
-                       (const void*)path_shade_persistent_kernel<kWald, true>,
-                       (const void*)path_shade_persistent_kernel<kKS, false>,
-                       (const void*)path_shade_persistent_kernel<kKS, true>};
+  const void* fs[4] = {(const void*)path_shade_persistent_kernel<kWald, false, 0>,
+                       (const void*)path_shade_persistent_kernel<kWald, true, 0>,
+                       (const void*)path_shade_persistent_kernel<kKS, false, 0>,
+                       (const void*)path_shade_persistent_kernel<kKS, true, 0>};
   if (smem > 48 * 1024)
     for (const void* f : fs)
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -66,6 +66,7 @@ struct PathLaunch {
   int block_threads[2];
   int blocks_per_sm[2];  // 0 = occupancy maximum
   int refill[2];
+  int reg_stack[2];      // traversal-stack entries in registers: 0, 2 or 4
 };
 
 cudaError_t launch_path_chunk(const DevScene& S, const PathParams& P, PathBuffers B,

@@ -153,6 +153,7 @@ static int path_run(Scene* s, const PathParams& P, long long total, int chunk, f
     L.block_threads[k] = c.block_threads;
     L.blocks_per_sm[k] = c.blocks_per_sm;
     L.refill[k] = c.refill_threshold;
+    L.reg_stack[k] = c.reg_stack;
   }
   cudaError_t e = cudaMemsetAsync(B.ray_counts, 0, 2 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return pfail(RQ_ERR_CUDA, cudaGetErrorString(e));

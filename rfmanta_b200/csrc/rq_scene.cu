@@ -473,6 +473,7 @@ int rq_scene_create(const float* vertices, int n_vertices,
     s->cfg[k].blocks_per_sm = 0;
     s->cfg[k].refill_threshold = 8;
     s->cfg[k].persistent = 1;
+    s->cfg[k].reg_stack = 0;
   }
   // path stages: refill thresholds from a sweep of the 1280x720x16 path
   // frame (block 64/128/256 x refill 4..24)
@@ -690,6 +691,8 @@ int rq_set_launch_config(rq_scene* s, int flags, const rq_launch_config* cfg) {
     return fail(RQ_ERR_ARG, "blocks_per_sm out of range");
   if (cfg->refill_threshold < 1 || cfg->refill_threshold > 32)
     return fail(RQ_ERR_ARG, "refill_threshold must be in [1, 32]");
+  if (cfg->reg_stack < 0 || cfg->reg_stack > 4 || cfg->reg_stack == 3)
+    return fail(RQ_ERR_ARG, "reg_stack must be 0, 1, 2 or 4");
   s->cfg[flags] = *cfg;
   return RQ_OK;
 }

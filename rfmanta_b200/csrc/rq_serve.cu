@@ -26,6 +26,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rfmanta_b200.h"
@@ -373,6 +374,29 @@ struct rq_server {
   // again before the next step
   std::vector<uint64_t> generations;
   std::vector<rq::DevScene> host_scenes;
+  // per-step records (rq_server_set_profile): timing events around each
+  // step's kernels, the record of the step in each ring slot until its end
+  // event has been seen, finished records
+  bool profile = false;
+  double prof_t0 = 0;
+  cudaEvent_t prof_start[kRing] = {};
+  cudaEvent_t prof_end[kRing] = {};
+  rq_server_step_record prof_slot[kRing] = {};
+  bool prof_open[kRing] = {};
+  std::vector<rq_server_step_record> prof_done;
+
+  // Moves the record of ring slot `slot` to the finished list once its
+  // end event has completed (blocking if `wait`).
+  void close_profile(int slot, bool wait) {
+    if (!prof_open[slot]) return;
+    if (!wait && cudaEventQuery(prof_end[slot]) != cudaSuccess) return;
+    if (wait) cudaEventSynchronize(prof_end[slot]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, prof_start[slot], prof_end[slot]);
+    prof_slot[slot].gpu_ms = ms;
+    prof_done.push_back(prof_slot[slot]);
+    prof_open[slot] = false;
+  }
 
   ~rq_server() {
     cudaSetDevice(device);
@@ -393,6 +417,8 @@ struct rq_server {
       cudaFreeHost(h_chunks[i]);
       if (ring_ev[i]) cudaEventDestroy(ring_ev[i]);
       if (end_ev[i]) cudaEventDestroy(end_ev[i]);
+      if (prof_start[i]) cudaEventDestroy(prof_start[i]);
+      if (prof_end[i]) cudaEventDestroy(prof_end[i]);
     }
     if (stream) cudaStreamDestroy(stream);
   }
@@ -651,6 +677,23 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
     e = cudaMemcpyAsync(s->d_chunks, hch, sizeof(ServeChunk) * n_chunks, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaEventRecord(s->ring_ev[slot], st);
   s->ring_used[slot] = true;
+  if (s->profile) {
+    s->close_profile(slot, true);
+    std::vector<int> seen;
+    for (int i = 0; i < n_req; ++i)
+      if (std::find(seen.begin(), seen.end(), hreq[i].scene) == seen.end())
+        seen.push_back(hreq[i].scene);
+    rq_server_step_record& pr = s->prof_slot[slot];
+    pr.requests = n_req;
+    pr.chunks = n_chunks;
+    pr.scenes = (int)seen.size();
+    pr.max_depth = max_depth;
+    pr.paths = slots;
+    pr.gpu_ms = 0.f;
+    pr.t_enqueue_s = now_s() - s->prof_t0;
+    s->prof_open[slot] = true;
+    if (e == cudaSuccess) e = cudaEventRecord(s->prof_start[slot], st);
+  }
   ServeArgs A;
   A.scenes = s->d_scenes;
   A.n_scenes = s->n_scenes;
@@ -670,6 +713,7 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
     if (r.scheduled_all) cudaEventRecord(r.done_ev, st);
   }
   cudaEventRecord(s->end_ev[slot], st);
+  if (s->profile) cudaEventRecord(s->prof_end[slot], st);
   ++s->steps;
   if (scheduled_paths) *scheduled_paths = (int)slots;
   // keep at most two steps in flight: wait for the end of the step before
@@ -762,6 +806,87 @@ int rq_server_stats(rq_server* s, uint64_t* ray_counts, long long* steps, int* p
 
 int rq_server_destroy(rq_server* s) {
   delete s;
+  return RQ_OK;
+}
+
+int rq_server_set_profile(rq_server* s, int on) {
+  if (!s) return sfail(RQ_ERR_ARG, "NULL server");
+  if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  if (on && !s->prof_start[0]) {
+    for (int i = 0; i < rq_server::kRing; ++i)
+      if (cudaEventCreate(&s->prof_start[i]) != cudaSuccess ||
+          cudaEventCreate(&s->prof_end[i]) != cudaSuccess)
+        return sfail(RQ_ERR_CUDA, "profile events");
+  }
+  if (!on)
+    for (int i = 0; i < rq_server::kRing; ++i) s->close_profile(i, true);
+  s->profile = on != 0;
+  s->prof_t0 = now_s();
+  return RQ_OK;
+}
+
+int rq_server_profile(rq_server* s, rq_server_step_record* out, int max_steps, int* n_steps) {
+  if (!s || !n_steps || (max_steps > 0 && !out)) return sfail(RQ_ERR_ARG, "NULL argument");
+  if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  for (int i = 0; i < rq_server::kRing; ++i) s->close_profile(i, false);
+  const int n = std::min<int>(max_steps, (int)s->prof_done.size());
+  std::copy(s->prof_done.begin(), s->prof_done.begin() + n, out);
+  s->prof_done.erase(s->prof_done.begin(), s->prof_done.begin() + n);
+  *n_steps = n;
+  return RQ_OK;
+}
+
+int rq_server_run_stream(rq_server* s, const rq_serve_request* requests,
+                         const double* arrival_s, int n, float* const* images,
+                         double* latency_s, double* queue_s, double* wall_s, double timeout_s) {
+  if (!s || (n > 0 && (!requests || !arrival_s || !latency_s))) return sfail(RQ_ERR_ARG, "NULL argument");
+  if (n < 0) return sfail(RQ_ERR_ARG, "negative request count");
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return arrival_s[a] < arrival_s[b]; });
+  std::map<int, int> index_of;  // request id -> position in `requests`
+  std::vector<int> done_ids(1024);
+  const double t0 = now_s();
+  double first = -1, last = t0;
+  int k = 0, done = 0;
+  while (done < n) {
+    const double now = now_s() - t0;
+    if (now > timeout_s) return sfail(RQ_ERR_TIMEOUT, "serving stream did not finish in time");
+    while (k < n && arrival_s[order[k]] <= now) {
+      int id = 0;
+      const int rc = rq_server_submit(s, &requests[order[k]], &id);
+      if (rc != RQ_OK) return rc;
+      if (first < 0) first = now_s();
+      index_of[id] = order[k++];
+    }
+    int scheduled = 0;
+    int rc = rq_server_step(s, &scheduled);
+    if (rc != RQ_OK) return rc;
+    int nd = 0;
+    rc = rq_server_poll(s, done_ids.data(), (int)done_ids.size(), &nd);
+    if (rc != RQ_OK) return rc;
+    for (int j = 0; j < nd; ++j) {
+      const int i = index_of[done_ids[j]];
+      double lat = 0, qs = 0;
+      rc = rq_server_result(s, done_ids[j], images ? images[i] : nullptr, &lat, &qs);
+      if (rc != RQ_OK) return rc;
+      latency_s[i] = lat;
+      if (queue_s) queue_s[i] = qs;
+      rc = rq_server_release(s, done_ids[j]);
+      if (rc != RQ_OK) return rc;
+      last = now_s();
+      ++done;
+    }
+    if (scheduled == 0 && nd == 0) {
+      // nothing new to enqueue: sleep until the next arrival or a short
+      // interval (steps in flight finish meanwhile)
+      double wait = 2e-5;
+      if (k < n && s->active.empty()) wait = std::max(0.0, arrival_s[order[k]] - (now_s() - t0));
+      std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 5e-4)));
+    }
+  }
+  if (wall_s) *wall_s = n > 0 ? last - first : 0.0;
   return RQ_OK;
 }
 

@@ -143,12 +143,18 @@ __device__ __forceinline__ void store_hit(const RayArgs& a, int i,
 
 namespace rq {
 
-// Traversal stack whose top R entries (0 or 2) stay in registers and whose
-// older entries spill to this thread's shared-memory column.  LIFO order is
-// kept: registers hold the newest entries, the shared column the older ones.
+// Traversal stack whose newest R entries (R = 0, 1, 2 or 4) stay in registers
+// and whose older entries spill to this thread's shared-memory column (the
+// short register stack of a while-while traversal).  LIFO order is kept:
+// registers hold the newest entries (r[0] the oldest of them), the shared
+// column the older ones.  A spill only happens when all R registers are in
+// use, so with at most `depth` pending entries the column never holds more
+// than depth - R of them.  Register slots are addressed by selects so the
+// array never leaves registers.
 template <int R>
 struct RegStack {
-  int2 r0, r1;
+  static_assert(R == 0 || R == 1 || R == 2 || R == 4, "0, 1, 2 or 4 register entries");
+  int2 r0, r1, r2, r3;
   int nreg;
   int sp;
   int2* col;
@@ -163,28 +169,36 @@ struct RegStack {
     if (R == 0) {
       col[sp * stride] = e;
       ++sp;
-    } else if (nreg == 2) {
+      return;
+    }
+    if (nreg == R) {
       col[sp * stride] = r0;
       ++sp;
+      if (R == 1) {
+        r0 = e;
+        return;
+      }
       r0 = r1;
-      r1 = e;
-    } else if (nreg == 1) {
-      r1 = e;
-      nreg = 2;
-    } else {
-      r0 = e;
-      nreg = 1;
+      if (R == 2) {
+        r1 = e;
+      } else {
+        r1 = r2;
+        r2 = r3;
+        r3 = e;
+      }
+      return;
     }
+    if (nreg == 0) r0 = e;
+    if (R >= 2 && nreg == 1) r1 = e;
+    if (R == 4 && nreg == 2) r2 = e;
+    if (R == 4 && nreg == 3) r3 = e;
+    ++nreg;
   }
   __device__ __forceinline__ bool pop(int2& e) {
-    if (R != 0 && nreg == 2) {
-      e = r1;
-      nreg = 1;
-      return true;
-    }
-    if (R != 0 && nreg == 1) {
-      e = r0;
-      nreg = 0;
+    if (R != 0 && nreg > 0) {
+      --nreg;
+      e = (R == 1 || nreg == 0) ? r0 : r1;
+      if (R == 4 && nreg >= 2) e = nreg == 2 ? r2 : r3;
       return true;
     }
     if (sp > 0) {

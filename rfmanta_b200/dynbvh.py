@@ -232,10 +232,13 @@ class GpuDynBVH:
                                   C.c_void_p(stream or None)))
 
     def set_launch_config(self, anyhit: bool, block_threads=128, blocks_per_sm=0,
-                          refill_threshold=8, persistent=True, stage=None) -> None:
+                          refill_threshold=8, persistent=True, stage=None,
+                          reg_stack=0) -> None:
         """Launch shape of ray queries (closest / any hit), or with
-        stage=RQ_PATH_EXTEND / RQ_PATH_SHADE of a path-tracer stage."""
-        cfg = _lib.LaunchConfig(block_threads, blocks_per_sm, refill_threshold, int(persistent))
+        stage=RQ_PATH_EXTEND / RQ_PATH_SHADE of a path-tracer stage
+        (reg_stack: traversal-stack entries kept in registers, 0/1/2/4)."""
+        cfg = _lib.LaunchConfig(block_threads, blocks_per_sm, refill_threshold, int(persistent),
+                                reg_stack)
         flags = stage if stage is not None else (RQ_ANYHIT if anyhit else RQ_CLOSEST)
         check(lib.rq_set_launch_config(self._h, flags, C.byref(cfg)))
 
@@ -244,7 +247,8 @@ class GpuDynBVH:
         flags = stage if stage is not None else (RQ_ANYHIT if anyhit else RQ_CLOSEST)
         check(lib.rq_get_launch_config(self._h, flags, C.byref(cfg)))
         return dict(block_threads=cfg.block_threads, blocks_per_sm=cfg.blocks_per_sm,
-                    refill_threshold=cfg.refill_threshold, persistent=bool(cfg.persistent))
+                    refill_threshold=cfg.refill_threshold, persistent=bool(cfg.persistent),
+                    reg_stack=cfg.reg_stack)
 
     # -- frame path -----------------------------------------------------------
     @staticmethod

@@ -122,36 +122,46 @@ class RenderServer:
     def run_stream(self, stream: list[tuple[float, RenderRequest]], keep_images: bool = False,
                    timeout_s: float = 600.0) -> dict:
         """Submits each request at its arrival time (seconds from start),
-        steps until all are done.  Returns per-request latencies (s) and,
-        optionally, the images."""
-        order = sorted(range(len(stream)), key=lambda i: stream[i][0])
-        t0 = time.perf_counter()
-        ids, info = {}, {}
-        k = 0
-        done = 0
-        while done < len(stream):
-            now = time.perf_counter() - t0
-            if now > timeout_s:
-                raise TimeoutError("serving stream did not finish")
-            while k < len(order) and stream[order[k]][0] <= now:
-                i = order[k]
-                ids[self.submit(stream[i][1])] = i
-                k += 1
-            n = self.step()
-            for rid in self.poll():
-                i = ids[rid]
-                req = stream[i][1]
-                img, lat, qs = self.result(rid, req.xres, req.yres, copy=keep_images)
-                info[i] = dict(latency=lat, queue=qs, image=img)
-                self.release(rid)
-                done += 1
-            if n == 0 and k < len(order):
-                wait = stream[order[k]][0] - (time.perf_counter() - t0)
-                if wait > 0:
-                    time.sleep(min(wait, 0.0005))
-            elif n == 0:
-                time.sleep(0.0002)
-        return dict(info=info, wall_s=time.perf_counter() - t0)
+        steps until all are done (the loop runs in the library,
+        rq_server_run_stream).  Returns per-request latencies and admission
+        waits (s), the wall time from the first submit to the last
+        completion and, optionally, the images."""
+        n = len(stream)
+        reqs = (_lib.ServeRequest * max(n, 1))()
+        keep = []
+        for i, (_, r) in enumerate(stream):
+            q = r.to_c()
+            keep.append(q._keep)
+            reqs[i] = q
+        arr = np.ascontiguousarray([a for a, _ in stream], np.float64)
+        lat = np.zeros(n, np.float64)
+        qs = np.zeros(n, np.float64)
+        imgs = None
+        ptrs = None
+        if keep_images:
+            imgs = [np.empty((r.xres * r.yres, 3), np.float32) for _, r in stream]
+            ptrs = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in imgs])
+        wall = C.c_double()
+        check(lib.rq_server_run_stream(self._h, reqs, arr.ctypes.data, n, ptrs,
+                                       lat.ctypes.data, qs.ctypes.data, C.byref(wall),
+                                       float(timeout_s)))
+        info = {i: dict(latency=float(lat[i]), queue=float(qs[i]),
+                        image=imgs[i] if imgs else None) for i in range(n)}
+        return dict(info=info, wall_s=wall.value)
+
+    def set_profile(self, on: bool = True) -> None:
+        check(lib.rq_server_set_profile(self._h, int(on)))
+
+    def profile(self) -> list[dict]:
+        """Finished steps' records since the last call (profiling on)."""
+        out = []
+        buf = (_lib.ServerStepRecord * 4096)()
+        while True:
+            n = C.c_int()
+            check(lib.rq_server_profile(self._h, buf, 4096, C.byref(n)))
+            out += [buf[i].as_dict() for i in range(n.value)]
+            if n.value < 4096:
+                return out
 
 
 def request_for_scene(scene_index: int, mesh, xres: int, yres: int, spp: int,

@@ -137,3 +137,32 @@ def test_ambient_at_max_depth_bit_exact(tiny, restatement, max_depth):
     img, _, _ = srv.result(rid, q.xres, q.yres)
     srv.close()
     assert np.array_equal(_bits(img), _bits(out["rgb"]))
+
+
+@pytest.mark.parametrize("regs", [(1, 1), (2, 2), (4, 4), (4, 0), (0, 2)])
+def test_register_stack_entries_do_not_change_results(tiny, restatement, regs):
+    """The persistent stages keep 0, 1, 2 or 4 of the newest traversal-stack
+    entries in registers (the rest in the thread's shared-memory column);
+    image, ray counts and per-bounce ids are those of the restatement
+    whatever the split, also in a block shape with a small column."""
+    from rfmanta_b200._lib import RQ_PATH_EXTEND, RQ_PATH_SHADE
+    kind, sc, bvh, tree = tiny
+    old = [bvh.get_launch_config(False, stage=s) for s in (RQ_PATH_EXTEND, RQ_PATH_SHADE)]
+    try:
+        for stage, r in zip((RQ_PATH_EXTEND, RQ_PATH_SHADE), regs):
+            bvh.set_launch_config(False, block_threads=64, refill_threshold=8, stage=stage,
+                                  reg_stack=r)
+        out = bvh.render_path(sc)
+    finally:
+        for stage, c in zip((RQ_PATH_EXTEND, RQ_PATH_SHADE), old):
+            bvh.set_launch_config(False, stage=stage, **c)
+    exp = restatement.render_path(tree, sc, tri_kind=kind)
+    assert out["rays"] == exp["rays"] and out["shadow_rays"] == exp["shadow_rays"]
+    assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))
+
+
+def test_register_stack_entries_rejected_outside_0_1_2_4(tiny):
+    from rfmanta_b200._lib import RQ_PATH_EXTEND, RQError
+    kind, sc, bvh, tree = tiny
+    with pytest.raises(RQError):
+        bvh.set_launch_config(False, stage=RQ_PATH_EXTEND, reg_stack=3)

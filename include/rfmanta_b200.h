@@ -236,6 +236,40 @@ RQ_API int rq_trace_device(rq_scene* scene, int n, const float* d_org,
                     float* d_t, int32_t* d_prim, float* d_u, float* d_v,
                     void* stream);
 
+/*
+ * Submission queue for many host threads that each trace one small packet
+ * at a time and wait for it: Manta's render workers call
+ * DynBVH::intersect with 64-ray packets from every thread at once
+ * (Engine/Control/RTRT.cc:984-990).  rq_queue_trace is rq_trace (same
+ * arguments, same results) and may be called from any number of threads at
+ * once.  Packets that arrive while the device works on an earlier batch are
+ * gathered into the next batch, sent as one copy in, one launch and one
+ * copy out as soon as the earlier batch is back; a packet that finds the
+ * device idle goes out at once.  Each caller blocks until its own results
+ * are back.  Packets of up to max_rays rays are batched (larger ones go
+ * through rq_trace); closest-hit and any-hit packets form separate batches.
+ * The scene must outlive the queue, and must not be updated while queued
+ * traces run.
+ */
+typedef struct rq_queue rq_queue;
+RQ_API int rq_queue_create(rq_scene* scene, int max_rays, rq_queue** out);
+RQ_API int rq_queue_trace(rq_queue* queue, int n, const float* org, const float* dir,
+                          const float* tmax, int flags, float* t, int32_t* prim,
+                          float* u, float* v);
+/* Batches sent, packets and rays traced so far. */
+RQ_API int rq_queue_stats(const rq_queue* queue, long long* batches, long long* packets,
+                          long long* rays);
+RQ_API int rq_queue_destroy(rq_queue* queue);
+
+/* Node-record orders a traversal can read (same records, same results):
+ * the builder's depth-first pre-order, breadth-first from the root, or the
+ * top 16,384 records breadth-first followed by the rest depth-first.  Batch
+ * plans (rq_batch_config) and the path stages (rq_launch_config) use a
+ * reordered copy the scene keeps until its tree changes. */
+#define RQ_LAYOUT_DFS 0
+#define RQ_LAYOUT_BFS 1
+#define RQ_LAYOUT_BFS_TOP 2
+
 /* Traversal launch parameters (persistent kernel, warp-ballot ray fetch). */
 typedef struct {
   int block_threads;    /* threads per block (multiple of 32) */
@@ -244,12 +278,15 @@ typedef struct {
   int persistent;       /* 0 = one thread per ray, 1 = persistent */
   int reg_stack;        /* traversal-stack entries kept in registers (0, 1, 2, 4);
                            the rest spill to shared memory.  Path stages only. */
+  int node_layout;      /* order of the node records the path stages read
+                           (RQ_LAYOUT_*, taken from the RQ_PATH_EXTEND
+                           config for both stages).  Path stages only. */
 } rq_launch_config;
 
 /* rq_set_launch_config / rq_get_launch_config also take these flags for the
  * path tracer's two persistent stages (rq_render_path*): block_threads,
- * blocks_per_sm, refill_threshold and reg_stack apply, `persistent` is
- * ignored. */
+ * blocks_per_sm, refill_threshold, reg_stack and node_layout apply,
+ * `persistent` is ignored. */
 #define RQ_PATH_EXTEND 2
 #define RQ_PATH_SHADE 3
 
@@ -343,12 +380,16 @@ typedef struct {
   int blocks_per_sm;    /* 0 = occupancy maximum */
   int chunk_rays;       /* rays a warp claims per fetch (multiple of 32) */
   int refill_threshold; /* idle lanes before a warp refills, 1..32 */
-  int reg_stack;        /* traversal-stack entries kept in registers: 0 or 2 */
+  int reg_stack;        /* traversal-stack entries kept in registers: 0, 1, 2, 4 */
+  int node_layout;      /* order of the node records in HBM (RQ_LAYOUT_*) */
 } rq_batch_config;
+
+
 
 typedef struct rq_batch_plan rq_batch_plan;
 
-/* cfg NULL = defaults (128 threads, 128-ray chunks, refill 8, 2 registers). */
+/* cfg NULL = defaults (128 threads, 128-ray chunks, refill 8, no register
+ * stack entries, depth-first records). */
 RQ_API int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes,
                                 const rq_batch* batches, int n_batches,
                                 const rq_batch_config* cfg, rq_batch_plan** out);
@@ -358,9 +399,13 @@ RQ_API int rq_batch_plan_info(const rq_batch_plan* plan, rq_batch_config* cfg,
                               int* grid, long long* total_rays);
 RQ_API int rq_batch_plan_destroy(rq_batch_plan* plan);
 
-/* Times each candidate configuration (NULL = a built-in sweep over block
- * size, rays per warp chunk, refill threshold and register stack entries)
- * on these batches, `reps` graph replays each, and returns the fastest. */
+/* Times each candidate configuration on these batches, `reps` graph
+ * replays each, and returns the fastest.  candidates NULL = the built-in
+ * search: block size x rays per warp chunk x refill threshold (the
+ * compaction threshold of the persistent loop) with the stack in shared
+ * memory and depth-first records, then register-stack entries (0, 1, 2, 4)
+ * x node layout (RQ_LAYOUT_*) at the best of those, then chunk x refill
+ * again at the best stack and layout. */
 RQ_API int rq_batch_autotune(rq_scene* const* scenes, int n_scenes,
                              const rq_batch* batches, int n_batches,
                              const rq_batch_config* candidates, int n_candidates,

@@ -473,6 +473,8 @@ class Reference:
                                         [C.c_int, C.c_int] + [C.c_void_p] * 4)
         if hasattr(L, "mref_scene_use_gpu"):
             L.mref_scene_use_gpu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_char_p]
+            L.mref_scene_gpu_options.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            L.mref_scene_gpu_as_primitive.argtypes = [C.c_void_p]
         L.mref_render_path.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                         C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_uint,
                                         C.c_void_p, C.c_void_p, C.c_void_p])
@@ -616,6 +618,19 @@ class RefScene:
                                              tree_file.encode() if tree_file else None)
         if rc != 0:
             raise RuntimeError(f"mref_scene_use_gpu failed ({rc})")
+
+    def gpu_as_primitive(self):
+        """Drop-in library only: trace through a reference Group holding a
+        GpuMeshPrimitive (the Primitive surface) instead of the bare
+        GpuDynBVH."""
+        if self.ref.lib.mref_scene_gpu_as_primitive(self.h) != 0:
+            raise RuntimeError("mref_scene_gpu_as_primitive: the scene is not on the drop-in")
+
+    def gpu_options(self, batching=True, gpu_shadows=False):
+        """Drop-in library only: packets through the submission queue or one
+        round trip each; GpuHardShadows instead of HardShadows."""
+        if self.ref.lib.mref_scene_gpu_options(self.h, int(batching), int(gpu_shadows)) != 0:
+            raise RuntimeError("mref_scene_gpu_options: the scene is not on the drop-in")
 
     def close(self):
         if self.h:

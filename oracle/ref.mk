@@ -167,7 +167,7 @@ $(OUT)/obj_sse/harness.o: $(HERE)ref_harness.cc $(OUT)/gen_sse/include/.stamp
 
 REPO := $(abspath $(HERE)..)
 
-$(OUT)/obj_nosse/harness_dropin.o: $(HERE)ref_harness.cc $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(OUT)/gen_nosse/include/.stamp
+$(OUT)/obj_nosse/harness_dropin.o: $(HERE)ref_harness.cc $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(REPO)/rfmanta_b200/manta/GpuHardShadows.h $(REPO)/rfmanta_b200/manta/GpuMeshPrimitive.h $(OUT)/gen_nosse/include/.stamp
 	@mkdir -p $(dir $@)
 	$(CXX) $(COMMON_FLAGS) -DMREF_DROPIN $(INC_NOSSE) -I$(REPO) -c $< -o $@
 
@@ -175,8 +175,19 @@ $(OUT)/obj_nosse/GpuDynBVH.o: $(REPO)/rfmanta_b200/manta/GpuDynBVH.cc $(REPO)/rf
 	@mkdir -p $(dir $@)
 	$(CXX) $(COMMON_FLAGS) $(INC_NOSSE) -I$(REPO) -c $< -o $@
 
-$(OUT)/libmanta_dropin.so: $(OBJ_NOSSE) $(OUT)/obj_nosse/harness_dropin.o $(OUT)/obj_nosse/GpuDynBVH.o $(REPO)/rfmanta_b200/librfmanta_b200.so
-	$(CXX) -shared -pthread -o $@ $(OBJ_NOSSE) $(OUT)/obj_nosse/harness_dropin.o $(OUT)/obj_nosse/GpuDynBVH.o -L$(REPO)/rfmanta_b200 -lrfmanta_b200 -Wl,-rpath,'$$ORIGIN/../../rfmanta_b200' -Wl,--no-as-needed -lstdc++ -lm
+$(OUT)/obj_nosse/GpuHardShadows.o: $(REPO)/rfmanta_b200/manta/GpuHardShadows.cc $(REPO)/rfmanta_b200/manta/GpuHardShadows.h $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(REPO)/include/rfmanta_b200.h $(OUT)/gen_nosse/include/.stamp
+	@mkdir -p $(dir $@)
+	$(CXX) $(COMMON_FLAGS) $(INC_NOSSE) -I$(REPO) -c $< -o $@
+
+$(OUT)/obj_nosse/GpuMeshPrimitive.o: $(REPO)/rfmanta_b200/manta/GpuMeshPrimitive.cc $(REPO)/rfmanta_b200/manta/GpuMeshPrimitive.h $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(REPO)/include/rfmanta_b200.h $(OUT)/gen_nosse/include/.stamp
+	@mkdir -p $(dir $@)
+	$(CXX) $(COMMON_FLAGS) $(INC_NOSSE) -I$(REPO) -c $< -o $@
+
+DROPIN_OBJ := $(OUT)/obj_nosse/harness_dropin.o $(OUT)/obj_nosse/GpuDynBVH.o \
+  $(OUT)/obj_nosse/GpuHardShadows.o $(OUT)/obj_nosse/GpuMeshPrimitive.o
+
+$(OUT)/libmanta_dropin.so: $(OBJ_NOSSE) $(DROPIN_OBJ) $(REPO)/rfmanta_b200/librfmanta_b200.so
+	$(CXX) -shared -pthread -o $@ $(OBJ_NOSSE) $(DROPIN_OBJ) -L$(REPO)/rfmanta_b200 -lrfmanta_b200 -Wl,-rpath,'$$ORIGIN/../../rfmanta_b200' -Wl,--no-as-needed -lstdc++ -lm
 
 $(OUT)/libmanta_ref.so: $(OBJ_NOSSE) $(OUT)/obj_nosse/harness.o
 	$(CXX) -shared -pthread -o $@ $^ -Wl,--no-as-needed -lstdc++ -lm

@@ -66,6 +66,8 @@
 
 #ifdef MREF_DROPIN
 #include <rfmanta_b200/manta/GpuDynBVH.h>
+#include <rfmanta_b200/manta/GpuHardShadows.h>
+#include <rfmanta_b200/manta/GpuMeshPrimitive.h>
 #endif
 
 #include <pthread.h>
@@ -153,6 +155,23 @@ public:
   }
 };
 
+#ifdef MREF_DROPIN
+// GpuHardShadows that counts the shadow rays it hands out, as
+// CountingShadows does for HardShadows.
+class CountingGpuShadows : public GpuHardShadows {
+public:
+  explicit CountingGpuShadows(const GpuDynBVH* bvh) : GpuHardShadows(bvh), counter(0) {}
+  long long* counter;
+  void computeShadows(const RenderContext& context, StateBuffer& state,
+                      const LightSet* lights, RayPacket& source,
+                      RayPacket& shadow) {
+    GpuHardShadows::computeShadows(context, state, lights, source, shadow);
+    for (int i = shadow.begin(); i < shadow.end(); ++i)
+      if (!shadow.rayIsMasked(i)) ++*counter;
+  }
+};
+#endif
+
 // Hands a packet to an InstanceT with the derived-data flags cleared.
 // InstanceT::intersect (Model/Instances/InstanceT.cc:60-66) builds its local
 // packet from rays.getAllFlags(); HaveInverseDirections / HaveSigns set by
@@ -190,6 +209,9 @@ struct RefScene {
   // LinearBackground) and LinearBackground's cdown and up
   int env_ambient, env_background;
   float env_down[3], env_up[3];
+  // drop-in builds: Whitted renders use GpuHardShadows (all lights' shadow
+  // rays of a packet in one submission) instead of HardShadows
+  int gpu_shadows;
 };
 
 // The ambient light and background a render of this scene uses: the given
@@ -715,7 +737,23 @@ static void* render_worker(void* p) {
   RenderJob* j = a->job;
   CountingShadows shadows;  // per-thread (it carries the counter slot)
   shadows.counter = &j->shadow_rays[a->proc];
-  RenderContext ctx(0, 0, a->proc, j->nthreads, 0, 0, 0, j->renderer, &shadows,
+  ShadowAlgorithm* sa = &shadows;
+#ifdef MREF_DROPIN
+  CountingGpuShadows* gpu_shadows = 0;
+  if (j->s->gpu_shadows) {
+    GpuDynBVH* g = dynamic_cast<GpuDynBVH*>(j->s->object);
+    if (!g) {
+      Group* grp = dynamic_cast<Group*>(j->s->object);
+      GpuMeshPrimitive* p =
+          grp && grp->size() > 0 ? dynamic_cast<GpuMeshPrimitive*>(grp->get(0)) : 0;
+      g = p ? p->bvh() : 0;
+    }
+    gpu_shadows = new CountingGpuShadows(g);
+    gpu_shadows->counter = &j->shadow_rays[a->proc];
+    sa = gpu_shadows;
+  }
+#endif
+  RenderContext ctx(0, 0, a->proc, j->nthreads, 0, 0, 0, j->renderer, sa,
                     j->camera, j->s->scene, 0, 0, j->sampler);
   for (;;) {
     pthread_mutex_lock(&j->lock);
@@ -749,6 +787,9 @@ static void* render_worker(void* p) {
       }
     }
   }
+#ifdef MREF_DROPIN
+  delete gpu_shadows;
+#endif
   return 0;
 }
 
@@ -1162,6 +1203,37 @@ int mref_scene_use_gpu(void* h, int device, int tri_kind, const char* tree_file)
     fprintf(stderr, "mref_scene_use_gpu: %s\n", e.message());
     return 1;
   }
+  return 0;
+}
+
+// Options of a scene already swapped to the drop-in: batching of concurrent
+// packets through the submission queue (GpuDynBVH::setBatching), and
+// GpuHardShadows for Whitted renders.
+int mref_scene_gpu_options(void* h, int batching, int gpu_shadows) {
+  RefScene* s = static_cast<RefScene*>(h);
+  GpuDynBVH* g = dynamic_cast<GpuDynBVH*>(s->object);
+  if (!g) {
+    Group* grp = dynamic_cast<Group*>(s->object);
+    GpuMeshPrimitive* p =
+        grp && grp->size() > 0 ? dynamic_cast<GpuMeshPrimitive*>(grp->get(0)) : 0;
+    g = p ? p->bvh() : 0;
+  }
+  if (!g) return 1;
+  g->setBatching(batching != 0);
+  s->gpu_shadows = gpu_shadows;
+  return 0;
+}
+
+// The drop-in as a Primitive: the scene's object becomes a reference Group
+// holding one GpuMeshPrimitive over the scene's GpuDynBVH (after
+// mref_scene_use_gpu), traced through Group::intersect.
+int mref_scene_gpu_as_primitive(void* h) {
+  RefScene* s = static_cast<RefScene*>(h);
+  GpuDynBVH* g = dynamic_cast<GpuDynBVH*>(s->object);
+  if (!g) return 1;
+  Group* grp = new Group();
+  grp->add(new GpuMeshPrimitive(g));
+  s->object = grp;
   return 0;
 }
 #endif

@@ -25,6 +25,9 @@ RQ_ERR_NODEV = 8
 RQ_TRI_WALD = 0
 RQ_TRI_KS = 1
 RQ_INST_TRANSLATE = 0
+RQ_LAYOUT_DFS = 0
+RQ_LAYOUT_BFS = 1
+RQ_LAYOUT_BFS_TOP = 2
 RQ_PATH_EXTEND = 2
 RQ_PATH_SHADE = 3
 RQ_MAT_LAMBERTIAN = 0
@@ -100,7 +103,8 @@ class Batch(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
-                ("chunk_rays", C.c_int), ("refill_threshold", C.c_int), ("reg_stack", C.c_int)]
+                ("chunk_rays", C.c_int), ("refill_threshold", C.c_int), ("reg_stack", C.c_int),
+                ("node_layout", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -129,7 +133,7 @@ class ServeRequest(C.Structure):
 class LaunchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
                 ("refill_threshold", C.c_int), ("persistent", C.c_int),
-                ("reg_stack", C.c_int)]
+                ("reg_stack", C.c_int), ("node_layout", C.c_int)]
 
 
 def _load():
@@ -179,6 +183,11 @@ def _load():
         "rq_server_stats": ([vp, vp, C.POINTER(C.c_longlong), C.POINTER(i), C.POINTER(i),
                              C.POINTER(sz)], i),
         "rq_server_destroy": ([vp], i),
+        "rq_queue_create": ([vp, i, C.POINTER(vp)], i),
+        "rq_queue_trace": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp], i),
+        "rq_queue_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                            C.POINTER(C.c_longlong)], i),
+        "rq_queue_destroy": ([vp], i),
         "rq_server_run_stream": ([vp, vp, vp, i, vp, vp, vp, C.POINTER(C.c_double), C.c_double],
                                  i),
         "rq_server_set_profile": ([vp, i], i),

@@ -60,7 +60,8 @@ class BatchedQueries:
         c.blocks_per_sm = config.get("blocks_per_sm", 0)
         c.chunk_rays = config.get("chunk_rays", 128)
         c.refill_threshold = config.get("refill_threshold", 8)
-        c.reg_stack = config.get("reg_stack", 2)
+        c.reg_stack = config.get("reg_stack", 0)
+        c.node_layout = config.get("node_layout", 0)
         return c
 
     def make_plan(self, config: dict | None = None) -> None:

@@ -159,19 +159,32 @@ static cudaError_t batch_go(bool launch, int grid, int block, size_t smem, const
 
 // Resolves (triangle kind, register stack, statistics) to one kernel and
 // either returns its address or launches it.
+template <int KIND>
+static cudaError_t batch_dispatch_kind(int reg, bool stats, bool launch, int grid, int block,
+                                       size_t smem, const BatchArgs& A, cudaStream_t st,
+                                       const void** fn) {
+  switch (reg) {
+    case 1:
+      return stats ? batch_go<KIND, 1, true>(launch, grid, block, smem, A, st, fn)
+                   : batch_go<KIND, 1, false>(launch, grid, block, smem, A, st, fn);
+    case 2:
+      return stats ? batch_go<KIND, 2, true>(launch, grid, block, smem, A, st, fn)
+                   : batch_go<KIND, 2, false>(launch, grid, block, smem, A, st, fn);
+    case 4:
+      return stats ? batch_go<KIND, 4, true>(launch, grid, block, smem, A, st, fn)
+                   : batch_go<KIND, 4, false>(launch, grid, block, smem, A, st, fn);
+    default:
+      return stats ? batch_go<KIND, 0, true>(launch, grid, block, smem, A, st, fn)
+                   : batch_go<KIND, 0, false>(launch, grid, block, smem, A, st, fn);
+  }
+}
+
 static cudaError_t batch_dispatch(int kind, int reg, bool stats, bool launch, int grid,
                                   int block, size_t smem, const BatchArgs& A, cudaStream_t st,
                                   const void** fn) {
-  if (kind == kWald) {
-    if (reg) return stats ? batch_go<kWald, 2, true>(launch, grid, block, smem, A, st, fn)
-                          : batch_go<kWald, 2, false>(launch, grid, block, smem, A, st, fn);
-    return stats ? batch_go<kWald, 0, true>(launch, grid, block, smem, A, st, fn)
-                 : batch_go<kWald, 0, false>(launch, grid, block, smem, A, st, fn);
-  }
-  if (reg) return stats ? batch_go<kKS, 2, true>(launch, grid, block, smem, A, st, fn)
-                        : batch_go<kKS, 2, false>(launch, grid, block, smem, A, st, fn);
-  return stats ? batch_go<kKS, 0, true>(launch, grid, block, smem, A, st, fn)
-               : batch_go<kKS, 0, false>(launch, grid, block, smem, A, st, fn);
+  if (kind == kWald)
+    return batch_dispatch_kind<kWald>(reg, stats, launch, grid, block, smem, A, st, fn);
+  return batch_dispatch_kind<kKS>(reg, stats, launch, grid, block, smem, A, st, fn);
 }
 
 }  // namespace rq
@@ -193,7 +206,7 @@ struct rq_batch_plan {
   // the scenes' descriptors as captured, and their generations: a scene
   // updated since (refit, rotations, new tree) gets its descriptor copied
   // in again before the next launch
-  std::vector<const rq::Scene*> scenes;
+  std::vector<rq::Scene*> scenes;
   std::vector<uint64_t> generations;
   std::vector<rq::DevScene> host_scenes;
   int stack_depth = 1;
@@ -221,7 +234,8 @@ rq_batch_config default_batch_config() {
   c.blocks_per_sm = 0;
   c.chunk_rays = 128;
   c.refill_threshold = 8;
-  c.reg_stack = 2;
+  c.reg_stack = 0;
+  c.node_layout = RQ_LAYOUT_DFS;
   return c;
 }
 
@@ -233,7 +247,9 @@ int capture_plan(rq_batch_plan* p) {
   const rq_batch_config& cfg = p->cfg;
   BatchArgs& A = p->args;
   A.stack_depth = p->stack_depth;
-  p->smem = (size_t)p->stack_depth * cfg.block_threads * sizeof(int2);
+  // the shared-memory column holds what the register entries do not
+  p->smem = (size_t)std::max(1, p->stack_depth - cfg.reg_stack) * cfg.block_threads *
+            sizeof(int2);
   const bool stats = A.stats != nullptr;
   const void* f = nullptr;
   batch_dispatch(p->tri_kind, cfg.reg_stack, stats, false, 0, 0, 0, A, nullptr, &f);
@@ -287,26 +303,42 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
     return bfail(RQ_ERR_ARG, "chunk_rays must be a multiple of 32");
   if (cfg.refill_threshold < 1 || cfg.refill_threshold > 32)
     return bfail(RQ_ERR_ARG, "refill_threshold must be in [1, 32]");
-  if (cfg.reg_stack != 0 && cfg.reg_stack != 2) return bfail(RQ_ERR_ARG, "reg_stack is 0 or 2");
+  if (cfg.reg_stack != 0 && cfg.reg_stack != 1 && cfg.reg_stack != 2 && cfg.reg_stack != 4)
+    return bfail(RQ_ERR_ARG, "reg_stack is 0, 1, 2 or 4");
+  if (cfg.node_layout < RQ_LAYOUT_DFS || cfg.node_layout > RQ_LAYOUT_BFS_TOP)
+    return bfail(RQ_ERR_ARG, "node_layout is one of RQ_LAYOUT_*");
   const Scene* s0 = reinterpret_cast<const Scene*>(scenes[0]);
   if (!s0) return bfail(RQ_ERR_ARG, "NULL scene");
+  if (cudaSetDevice(s0->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
   std::vector<DevScene> ds(n_scenes);
   int depth = 1;
   for (int i = 0; i < n_scenes; ++i) {
-    const Scene* s = reinterpret_cast<const Scene*>(scenes[i]);
+    Scene* s = reinterpret_cast<Scene*>(scenes[i]);
     if (!s) return bfail(RQ_ERR_ARG, "NULL scene");
     if (!s->has_tree) return bfail(RQ_ERR_STATE, "scene " + std::to_string(i) + " has no tree");
     if (s->instanced) return bfail(RQ_ERR_ARG, "batched queries take triangle scenes");
     if (s->device != s0->device) return bfail(RQ_ERR_ARG, "all scenes must be on one device");
     if (s->tri_kind != s0->tri_kind) return bfail(RQ_ERR_ARG, "all scenes must use one triangle kind");
-    ds[i] = s->dev();
+    const int rc = s->node_layout(cfg.node_layout, ds[i]);
+    if (rc != RQ_OK) return rc;
     depth = std::max(depth, ds[i].depth);
   }
+  // Work order: scene by scene (closest-hit batches, then any-hit, each in
+  // submission order), so the warps resident at any moment mostly trace
+  // one scene and share its node and triangle records in L1/L2, as a
+  // plain per-batch launch does, instead of all scenes at once.
+  std::vector<int> order(n_batches);
+  for (int b = 0; b < n_batches; ++b) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    if (batches[a].scene != batches[b].scene) return batches[a].scene < batches[b].scene;
+    return batches[a].flags < batches[b].flags;
+  });
   std::vector<BatchDesc> bd(n_batches);
   int chunks = 0;
   long long rays = 0;
-  for (int b = 0; b < n_batches; ++b) {
-    const rq_batch& q = batches[b];
+  for (int k = 0; k < n_batches; ++k) {
+    const int b = k;
+    const rq_batch& q = batches[order[k]];
     if (q.scene < 0 || q.scene >= n_scenes) return bfail(RQ_ERR_ARG, "batch scene index out of range");
     if (q.n < 0 || (q.n > 0 && (!q.d_org || !q.d_dir || !q.d_tmax)))
       return bfail(RQ_ERR_ARG, "bad batch ray arrays");
@@ -357,7 +389,7 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
   p->stack_depth = depth;
   p->host_scenes = ds;
   for (int i = 0; i < n_scenes; ++i) {
-    const Scene* s = reinterpret_cast<const Scene*>(scenes[i]);
+    Scene* s = reinterpret_cast<Scene*>(scenes[i]);
     p->scenes.push_back(s);
     p->generations.push_back(s->generation);
   }
@@ -374,10 +406,12 @@ int rq_batch_plan_launch(rq_batch_plan* plan, void* stream) {
   if (cudaSetDevice(plan->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
   bool changed = false;
   for (size_t i = 0; i < plan->scenes.size(); ++i) {
-    const rq::Scene* s = plan->scenes[i];
+    rq::Scene* s = plan->scenes[i];
     if (s->generation == plan->generations[i]) continue;
     if (!s->has_tree) return bfail(RQ_ERR_STATE, "a scene of the plan has no tree");
-    plan->host_scenes[i] = s->dev();
+    // the plan's node layout of the new tree (made again on the device)
+    const int rc = s->node_layout(plan->cfg.node_layout, plan->host_scenes[i]);
+    if (rc != RQ_OK) return rc;
     plan->generations[i] = s->generation;
     changed = true;
   }
@@ -425,23 +459,6 @@ int rq_batch_autotune(rq_scene* const* scenes, int n_scenes, const rq_batch* bat
                       int n_batches, const rq_batch_config* candidates, int n_candidates,
                       int reps, rq_batch_config* best, float* best_ms) {
   if (!best) return bfail(RQ_ERR_ARG, "best is NULL");
-  std::vector<rq_batch_config> cand;
-  if (candidates && n_candidates > 0) {
-    cand.assign(candidates, candidates + n_candidates);
-  } else {
-    for (int bt : {64, 128, 256})
-      for (int cr : {32, 128, 512})
-        for (int rf : {1, 8, 24})
-          for (int rs : {0, 2}) {
-            rq_batch_config c;
-            c.block_threads = bt;
-            c.blocks_per_sm = 0;
-            c.chunk_rays = cr;
-            c.refill_threshold = rf;
-            c.reg_stack = rs;
-            cand.push_back(c);
-          }
-  }
   if (reps < 1) reps = 1;
   const rq::Scene* s0 = reinterpret_cast<const rq::Scene*>(scenes ? scenes[0] : nullptr);
   if (!s0) return bfail(RQ_ERR_ARG, "NULL scene");
@@ -454,10 +471,11 @@ int rq_batch_autotune(rq_scene* const* scenes, int n_scenes, const rq_batch* bat
   cudaEventCreate(&e1);
   float bms = 1e30f;
   int rc = RQ_OK;
-  for (const rq_batch_config& c : cand) {
+  // times one configuration; keeps it if it is the fastest so far
+  auto time_one = [&](const rq_batch_config& c) -> int {
     rq_batch_plan* p = nullptr;
-    rc = rq_batch_plan_create(scenes, n_scenes, batches, n_batches, &c, &p);
-    if (rc != RQ_OK) break;
+    int r = rq_batch_plan_create(scenes, n_scenes, batches, n_batches, &c, &p);
+    if (r != RQ_OK) return r;
     rq_batch_plan_launch(p, st);  // warm-up
     cudaEventRecord(e0, st);
     for (int k = 0; k < reps; ++k) rq_batch_plan_launch(p, st);
@@ -466,15 +484,49 @@ int rq_batch_autotune(rq_scene* const* scenes, int n_scenes, const rq_batch* bat
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     rq_batch_plan_destroy(p);
-    if (e != cudaSuccess) {
-      rc = bfail(RQ_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
-      break;
-    }
+    if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
     ms /= reps;
     if (ms < bms) {
       bms = ms;
       *best = c;
     }
+    return RQ_OK;
+  };
+  if (candidates && n_candidates > 0) {
+    for (int i = 0; i < n_candidates && rc == RQ_OK; ++i) rc = time_one(candidates[i]);
+  } else {
+    // 1. launch shape, rays per warp chunk and refill (compaction)
+    //    threshold, stack in shared memory, depth-first records
+    for (int bt : {64, 128, 256})
+      for (int cr : {32, 128, 512})
+        for (int rf : {1, 8, 24}) {
+          if (rc != RQ_OK) break;
+          rq_batch_config c = default_batch_config();
+          c.block_threads = bt;
+          c.chunk_rays = cr;
+          c.refill_threshold = rf;
+          rc = time_one(c);
+        }
+    // 2. register-stack entries x node layout at the best shape
+    const rq_batch_config shape = *best;
+    for (int rs : {0, 1, 2, 4})
+      for (int nl : {RQ_LAYOUT_DFS, RQ_LAYOUT_BFS, RQ_LAYOUT_BFS_TOP}) {
+        if (rc != RQ_OK || (rs == shape.reg_stack && nl == shape.node_layout)) continue;
+        rq_batch_config c = shape;
+        c.reg_stack = rs;
+        c.node_layout = nl;
+        rc = time_one(c);
+      }
+    // 3. chunk and refill again at the best stack and layout
+    const rq_batch_config mid = *best;
+    for (int cr : {64, 128, 256, 512})
+      for (int rf : {4, 8, 16, 24}) {
+        if (rc != RQ_OK || (cr == mid.chunk_rays && rf == mid.refill_threshold)) continue;
+        rq_batch_config c = mid;
+        c.chunk_rays = cr;
+        c.refill_threshold = rf;
+        rc = time_one(c);
+      }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(128)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   Ray r;
-  const int n = a.n;
+  const int n = a.stride ? a.stride : a.n;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     r.o[c] = __ldg(a.org + (size_t)c * n + i);
@@ -223,6 +223,7 @@ int rq_scene_create_instanced(rq_scene* const* inner, int n_inner, const int32_t
     s->cfg[k].refill_threshold = 8;
     s->cfg[k].persistent = 0;
     s->cfg[k].reg_stack = 0;
+    s->cfg[k].node_layout = RQ_LAYOUT_DFS;
   }
   if (cudaMalloc(&s->d_verts, verts.size() * 4) != cudaSuccess ||
       cudaMalloc(&s->d_idx, idx.size() * 4) != cudaSuccess ||

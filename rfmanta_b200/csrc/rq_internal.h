@@ -13,13 +13,14 @@ namespace rq {
 // Device pointers of one ray batch (SoA) and its outputs.
 struct RayArgs {
   int n;
-  const float* org;  // 3*n
-  const float* dir;  // 3*n
+  const float* org;  // 3 rows: org[c * stride + i]
+  const float* dir;  // 3 rows
   const float* tmax; // n
   float* t;
   int32_t* prim;
   float* u;
   float* v;
+  int stride = 0;    // elements between the rows of org/dir; 0 = n
 };
 
 struct LaunchPlan {

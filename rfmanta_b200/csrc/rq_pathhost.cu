@@ -144,7 +144,9 @@ static int path_run(Scene* s, const PathParams& P, long long total, int chunk, f
   if (B.dbg_prim && (long long)s->path_dbg_capacity < total)
     return pfail(RQ_ERR_ARG, "debug buffers smaller than the frame's path count");
   if (B.dbg_prim && chunk != total) return pfail(RQ_ERR_ARG, "debug dump needs a single chunk");
-  const DevScene S = s->dev();
+  DevScene S;
+  int lrc = s->node_layout(s->cfg[RQ_PATH_EXTEND].node_layout, S);
+  if (lrc != RQ_OK) return lrc;
   const size_t smem = (size_t)S.depth * 128 * sizeof(int2);
   const int grid = std::max(1, path_blocks_per_sm(s->tri_kind, smem) * s->num_sms);
   PathLaunch L;

@@ -47,6 +47,7 @@ static int cuda_fail(cudaError_t e, const char* what) {
 
 Staging::~Staging() {
   if (stream) cudaStreamDestroy(stream);
+  if (h_map) cudaFreeHost(h_map);
   if (h_buf) cudaFreeHost(h_buf);
   if (d_buf) cudaFree(d_buf);
   if (d_counter) cudaFree(d_counter);
@@ -57,6 +58,7 @@ Scene::~Scene() {
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   free_tree();
+  free_layouts();
   if (d_verts) cudaFree(d_verts);
   if (d_idx) cudaFree(d_idx);
   if (d_face_mat) cudaFree(d_face_mat);
@@ -393,14 +395,29 @@ LaunchPlan Scene::plan(bool anyhit, int n, int* counter) const {
 
 int Scene::trace_device(int n, const float* org, const float* dir,
                         const float* tmax, bool anyhit, float* t, int32_t* prim,
-                        float* u, float* v, cudaStream_t st, int* counter) {
+                        float* u, float* v, cudaStream_t st, int* counter, int stride,
+                        bool one_per_ray) {
   if (!has_tree) return fail(RQ_ERR_STATE, "scene has no tree");
   if (instanced) {
     const int rc = check_inner_current();
     if (rc != RQ_OK) return rc;
   }
-  RayArgs a{n, org, dir, tmax, t, prim, u, v};
-  LaunchPlan p = plan(anyhit, n, counter);
+  RayArgs a{n, org, dir, tmax, t, prim, u, v, stride};
+  LaunchPlan p;
+  if (one_per_ray) {
+    // a plain grid sized by the launch itself: no work counter, and no
+    // occupancy query on this per-packet path
+    const rq_launch_config& c = cfg[anyhit ? 1 : 0];
+    p.block_threads = c.block_threads;
+    p.grid = 1;
+    p.refill = 1;
+    p.persistent = false;
+    p.counter = nullptr;
+    const size_t smem = (size_t)std::max(depth, 1) * c.block_threads * sizeof(int2);
+    if (smem > 48 * 1024) max_blocks_per_sm(tri_kind, anyhit, false, c.block_threads, smem);
+  } else {
+    p = plan(anyhit, n, counter);
+  }
   if (p.persistent) {
     if (!counter) return fail(RQ_ERR_ARG, "persistent launch needs a counter");
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
@@ -474,6 +491,7 @@ int rq_scene_create(const float* vertices, int n_vertices,
     s->cfg[k].refill_threshold = 8;
     s->cfg[k].persistent = 1;
     s->cfg[k].reg_stack = 0;
+    s->cfg[k].node_layout = RQ_LAYOUT_DFS;
   }
   // path stages: refill thresholds from a sweep of the 1280x720x16 path
   // frame (block 64/128/256 x refill 4..24)
@@ -634,6 +652,41 @@ int rq_trace(rq_scene* s, int n, const float* org, const float* dir,
   const size_t out_bytes = 4 * (size_t)n * sizeof(float);
   rq::Staging* st = s->acquire(in_bytes, out_bytes);
   if (!st) return fail(RQ_ERR_OOM, "staging allocation failed");
+  if (n <= rq::kZeroCopyRays) {
+    // a packet-sized call: the kernel reads the rays from, and writes the
+    // hits to, mapped pinned host memory; one launch and one synchronise
+    if (!st->h_map) {
+      const size_t cap = 11 * (size_t)rq::kZeroCopyRays * sizeof(float);
+      if (cudaHostAlloc(&st->h_map, cap, cudaHostAllocMapped) != cudaSuccess ||
+          cudaHostGetDevicePointer(&st->d_map, st->h_map, 0) != cudaSuccess) {
+        s->release(st);
+        return fail(RQ_ERR_OOM, "mapped staging allocation failed");
+      }
+      st->map_cap = cap;
+    }
+    float* h = static_cast<float*>(st->h_map);
+    std::memcpy(h, org, 3 * (size_t)n * sizeof(float));
+    std::memcpy(h + 3 * (size_t)n, dir, 3 * (size_t)n * sizeof(float));
+    std::memcpy(h + 6 * (size_t)n, tmax, (size_t)n * sizeof(float));
+    float* d = static_cast<float*>(st->d_map);
+    float* d_out = d + 7 * (size_t)n;
+    int rc = s->trace_device(n, d, d + 3 * (size_t)n, d + 6 * (size_t)n, flags == RQ_ANYHIT,
+                             d_out, reinterpret_cast<int32_t*>(d_out + n), d_out + 2 * (size_t)n,
+                             d_out + 3 * (size_t)n, st->stream, st->d_counter, 0, true);
+    if (rc == RQ_OK) {
+      const cudaError_t e = cudaStreamSynchronize(st->stream);
+      if (e != cudaSuccess) rc = cuda_fail(e, "trace");
+    }
+    if (rc == RQ_OK) {
+      const float* o = h + 7 * (size_t)n;
+      if (t) std::memcpy(t, o, (size_t)n * sizeof(float));
+      if (prim) std::memcpy(prim, o + n, (size_t)n * sizeof(int32_t));
+      if (u) std::memcpy(u, o + 2 * (size_t)n, (size_t)n * sizeof(float));
+      if (v) std::memcpy(v, o + 3 * (size_t)n, (size_t)n * sizeof(float));
+    }
+    s->release(st);
+    return rc;
+  }
   float* h = static_cast<float*>(st->h_buf);
   std::memcpy(h, org, 3 * (size_t)n * sizeof(float));
   std::memcpy(h + 3 * (size_t)n, dir, 3 * (size_t)n * sizeof(float));
@@ -693,6 +746,8 @@ int rq_set_launch_config(rq_scene* s, int flags, const rq_launch_config* cfg) {
     return fail(RQ_ERR_ARG, "refill_threshold must be in [1, 32]");
   if (cfg->reg_stack < 0 || cfg->reg_stack > 4 || cfg->reg_stack == 3)
     return fail(RQ_ERR_ARG, "reg_stack must be 0, 1, 2 or 4");
+  if (cfg->node_layout < RQ_LAYOUT_DFS || cfg->node_layout > RQ_LAYOUT_BFS_TOP)
+    return fail(RQ_ERR_ARG, "node_layout must be one of RQ_LAYOUT_*");
   s->cfg[flags] = *cfg;
   return RQ_OK;
 }

@@ -61,6 +61,9 @@ struct TreeLayout {
 
 int layout_tree(const HostTree& t, int n_objects, TreeLayout& out);
 
+// Calls of up to this many rays trace straight from mapped host memory.
+constexpr int kZeroCopyRays = 4096;
+
 // Per-call resources for the host-array entry point.
 struct Staging {
   cudaStream_t stream = nullptr;
@@ -68,6 +71,11 @@ struct Staging {
   void* d_buf = nullptr;
   int* d_counter = nullptr;
   size_t cap = 0;
+  // small calls: pinned host memory mapped into the device's address space,
+  // read and written by the kernel directly (no copies)
+  void* h_map = nullptr;
+  void* d_map = nullptr;
+  size_t map_cap = 0;
   ~Staging();
 };
 
@@ -155,6 +163,19 @@ struct Scene {
   int n_stage_events = 0;
   std::mutex frame_mu;
 
+  // node records in another order (rq_layout.cu), per RQ_LAYOUT_*, made on
+  // first use and kept until the tree changes
+  struct AltLayout {
+    float4* nodes = nullptr;
+    int capacity = 0;
+    int root = 0;
+    uint64_t generation = ~0ull;
+  };
+  AltLayout alt_layout[3];
+  // dev() with the records in `layout` order
+  int node_layout(int layout, DevScene& out);
+  void free_layouts();
+
   ~Scene();
   void free_tree();
   int set_tree(const HostTree& t);
@@ -164,9 +185,12 @@ struct Scene {
   Staging* acquire(size_t bytes_in, size_t bytes_out);
   void release(Staging* s);
   LaunchPlan plan(bool anyhit, int n, int* counter) const;
+  // stride: elements between the x/y/z rows of org and dir (0 = n);
+  // one_per_ray: a plain grid of one thread per ray (no work counter to
+  // reset), for small batches
   int trace_device(int n, const float* org, const float* dir, const float* tmax,
                    bool anyhit, float* t, int32_t* prim, float* u, float* v,
-                   cudaStream_t st, int* counter);
+                   cudaStream_t st, int* counter, int stride = 0, bool one_per_ray = false);
 };
 
 int rotate_update(Scene* s);

@@ -361,6 +361,14 @@ struct rq_server {
   cudaEvent_t end_ev[kRing] = {};    // after a step's last kernel
   bool ring_used[kRing] = {};
   cudaStream_t stream = nullptr;
+  // result copies wait for their request's completion event on a stream of
+  // their own, so a copy never waits for steps enqueued after its request
+  cudaStream_t copy_stream = nullptr;
+  // request images come from the server's own memory pool, which keeps
+  // what it has mapped (release threshold = all): the device's default
+  // pool returns freed memory at every synchronisation, and mapping it
+  // again stalls the request loop
+  cudaMemPool_t pool = nullptr;
   std::map<int, std::unique_ptr<HostReq>> reqs;
   std::deque<int> pending;   // submitted, not admitted
   std::vector<int> active;   // admitted, not finished (admission order)
@@ -421,6 +429,8 @@ struct rq_server {
       if (prof_end[i]) cudaEventDestroy(prof_end[i]);
     }
     if (stream) cudaStreamDestroy(stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (pool) cudaMemPoolDestroy(pool);
   }
 
   bool admit(HostReq& r) {
@@ -428,8 +438,9 @@ struct rq_server {
     if ((int)active.size() >= max_active || used + need > budget) return false;
     // stream-ordered allocation: no device-wide synchronisation while
     // other steps are in flight
-    if (cudaMallocAsync(&r.d_out, r.bytes, stream) != cudaSuccess) return false;
-    if (cudaMallocAsync(&r.d_mat, r.materials.size() * sizeof(float), stream) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync(&r.d_out, r.bytes, pool, stream) != cudaSuccess) return false;
+    if (cudaMallocFromPoolAsync(&r.d_mat, r.materials.size() * sizeof(float), pool, stream) !=
+        cudaSuccess) {
       cudaFreeAsync(r.d_out, stream);
       r.d_out = nullptr;
       return false;
@@ -542,8 +553,28 @@ int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capac
   if (cudaMemset(s->counts, 0, 16) != cudaSuccess ||
       cudaMemcpy(s->d_scenes, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice) !=
           cudaSuccess ||
-      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
     return sfail(RQ_ERR_CUDA, "server setup");
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    uint64_t keep = ~0ull;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+      return sfail(RQ_ERR_CUDA, "server memory pool");
+    // map a first slice of the budget now, so early requests do not wait
+    // for the pool to grow
+    void* warm = nullptr;
+    const size_t first = std::min<size_t>(hbm_budget_bytes, size_t(2) << 30);
+    if (cudaMallocFromPoolAsync(&warm, first, s->pool, s->stream) == cudaSuccess)
+      cudaFreeAsync(warm, s->stream);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess)
+      return sfail(RQ_ERR_CUDA, "server memory pool");
+  }
   s->smem = (size_t)s->depth * 128 * sizeof(int2);
   s->grid = std::max(1, serve_blocks_per_sm(s->tri_kind, s->smem) * s->num_sms);
   s->table.assign(s->max_active, 0);
@@ -756,10 +787,10 @@ int rq_server_result(rq_server* s, int request_id, float* rgb, double* latency_s
   HostReq& r = *it->second;
   if (!r.done) return sfail(RQ_ERR_STATE, "request not finished");
   if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
-  if (rgb && (cudaMemcpyAsync(rgb, r.d_out, r.bytes, cudaMemcpyDeviceToHost, s->stream) !=
+  if (rgb && (cudaStreamWaitEvent(s->copy_stream, r.done_ev, 0) != cudaSuccess ||
+              cudaMemcpyAsync(rgb, r.d_out, r.bytes, cudaMemcpyDeviceToHost, s->copy_stream) !=
                   cudaSuccess ||
-              cudaEventSynchronize(r.done_ev) != cudaSuccess ||
-              cudaStreamSynchronize(s->stream) != cudaSuccess))
+              cudaStreamSynchronize(s->copy_stream) != cudaSuccess))
     return sfail(RQ_ERR_CUDA, "result copy failed");
   if (latency_s) *latency_s = r.t_done - r.t_submit;
   if (queue_s) *queue_s = r.t_admit - r.t_submit;

@@ -121,7 +121,7 @@ __device__ __forceinline__ void step(const DevScene& S, Ray& r, Hit& h,
 }
 
 __device__ __forceinline__ void load_ray(const RayArgs& a, int i, Ray& r) {
-  const int n = a.n;
+  const int n = a.stride ? a.stride : a.n;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     r.o[c] = __ldg(a.org + (size_t)c * n + i);

@@ -233,12 +233,13 @@ class GpuDynBVH:
 
     def set_launch_config(self, anyhit: bool, block_threads=128, blocks_per_sm=0,
                           refill_threshold=8, persistent=True, stage=None,
-                          reg_stack=0) -> None:
+                          reg_stack=0, node_layout=0) -> None:
         """Launch shape of ray queries (closest / any hit), or with
         stage=RQ_PATH_EXTEND / RQ_PATH_SHADE of a path-tracer stage
-        (reg_stack: traversal-stack entries kept in registers, 0/1/2/4)."""
+        (reg_stack: traversal-stack entries kept in registers, 0/1/2/4;
+        node_layout: RQ_LAYOUT_* order of the records the path stages read)."""
         cfg = _lib.LaunchConfig(block_threads, blocks_per_sm, refill_threshold, int(persistent),
-                                reg_stack)
+                                reg_stack, node_layout)
         flags = stage if stage is not None else (RQ_ANYHIT if anyhit else RQ_CLOSEST)
         check(lib.rq_set_launch_config(self._h, flags, C.byref(cfg)))
 
@@ -248,7 +249,7 @@ class GpuDynBVH:
         check(lib.rq_get_launch_config(self._h, flags, C.byref(cfg)))
         return dict(block_threads=cfg.block_threads, blocks_per_sm=cfg.blocks_per_sm,
                     refill_threshold=cfg.refill_threshold, persistent=bool(cfg.persistent),
-                    reg_stack=cfg.reg_stack)
+                    reg_stack=cfg.reg_stack, node_layout=cfg.node_layout)
 
     # -- frame path -----------------------------------------------------------
     @staticmethod

@@ -16,12 +16,19 @@
 
 using namespace Manta;
 
+// Rays per batch of the submission queue: 256 packets of 64 rays.
+static const int kQueueRays = 256 * RayPacket::MaxSize;
+
 GpuDynBVH::GpuDynBVH(int device_, int tri_kind_)
-    : group(0), mesh(0), scene(0), device(device_), tri_kind(tri_kind_), dirty(false) {}
+    : group(0), mesh(0), scene(0), queue(0), device(device_), tri_kind(tri_kind_), dirty(false),
+      batching(false) {}
 
 GpuDynBVH::~GpuDynBVH() {
+  if (queue) rq_queue_destroy(queue);
   if (scene) rq_scene_destroy(scene);
 }
+
+void GpuDynBVH::setBatching(bool on) { batching = on; }
 
 void GpuDynBVH::check(int rc, const char* what) const {
   if (rc != RQ_OK)
@@ -51,6 +58,10 @@ Interpolable::InterpErr GpuDynBVH::parallelInterpolate(const std::vector<keyfram
 // Mesh::vertices / vertex_indices / face_material (Model/Groups/Mesh.h:27-50).
 void GpuDynBVH::upload() {
   if (!mesh) throw InternalError("GpuDynBVH needs a Mesh group");
+  if (queue) {
+    rq_queue_destroy(queue);
+    queue = 0;
+  }
   if (scene) {
     rq_scene_destroy(scene);
     scene = 0;
@@ -64,6 +75,7 @@ void GpuDynBVH::upload() {
                         mesh->face_material.empty() ? 0 : &mesh->face_material[0], tri_kind,
                         device, &scene),
         "scene upload");
+  check(rq_queue_create(scene, kQueueRays, &queue), "submission queue");
   dirty = false;
 }
 
@@ -123,34 +135,40 @@ void GpuDynBVH::computeBounds(const PreprocessContext& context, BBox& bbox) cons
   group->computeBounds(context, bbox);
 }
 
-// DynBVH::intersect (Model/Groups/DynBVH.cc:101-404) for one packet: the
-// unmasked (and, for AnyHit, not yet hit) rays go to the device; hits come
-// back through RayPacket::hit with the real MeshTriangle, its material and
-// the scratchpad pair; occluded AnyHit rays are then treated as the
-// reference's opaque shadower path does (hit kept, minT = T_EPSILON).
-void GpuDynBVH::intersect(const RenderContext& context, RayPacket& rays) const {
-  const bool any = rays.getFlag(RayPacket::AnyHit);
-  const int MS = RayPacket::MaxSize;
-  int map[MS];
-  float org[3 * MS], dir[3 * MS], tmax[MS], t[MS], u[MS], v[MS];
-  int prim[MS];
+int GpuDynBVH::selectRays(const RayPacket& rays, bool any, int* map) const {
   int n = 0;
   for (int i = rays.begin(); i < rays.end(); ++i) {
     if (rays.rayIsMasked(i)) continue;
     if (any && rays.wasHit(i)) continue;
     map[n++] = i;
   }
-  if (n == 0) return;
+  return n;
+}
+
+void GpuDynBVH::packRays(const RayPacket& rays, const int* map, int n, int stride, int base,
+                         float* org, float* dir, float* tmax) {
   for (int k = 0; k < n; ++k) {
     const int i = map[k];
     for (int c = 0; c < 3; ++c) {
-      org[c * n + k] = rays.getOrigin(i, c);
-      dir[c * n + k] = rays.getDirection(i, c);
+      org[c * stride + base + k] = rays.getOrigin(i, c);
+      dir[c * stride + base + k] = rays.getDirection(i, c);
     }
-    tmax[k] = rays.getMinT(i);
+    tmax[base + k] = rays.getMinT(i);
   }
-  check(rq_trace(scene, n, org, dir, tmax, any ? RQ_ANYHIT : RQ_CLOSEST, t, prim, u, v),
-        "trace");
+}
+
+void GpuDynBVH::traceRays(int n, const float* org, const float* dir, const float* tmax, bool any,
+                          float* t, int* prim, float* u, float* v) const {
+  const int flags = any ? RQ_ANYHIT : RQ_CLOSEST;
+  if (batching && queue)
+    check(rq_queue_trace(queue, n, org, dir, tmax, flags, t, prim, u, v), "queued trace");
+  else
+    check(rq_trace(scene, n, org, dir, tmax, flags, t, prim, u, v), "trace");
+}
+
+void GpuDynBVH::applyHits(const RenderContext& context, RayPacket& rays, bool any,
+                          const int* map, int n, const float* t, const int* prim,
+                          const float* u, const float* v) const {
   for (int k = 0; k < n; ++k) {
     if (prim[k] < 0) continue;
     const int i = map[k];
@@ -171,4 +189,22 @@ void GpuDynBVH::intersect(const RenderContext& context, RayPacket& rays) const {
       }
     }
   }
+}
+
+// DynBVH::intersect (Model/Groups/DynBVH.cc:101-404) for one packet: the
+// unmasked (and, for AnyHit, not yet hit) rays go to the device; hits come
+// back through RayPacket::hit with the real MeshTriangle, its material and
+// the scratchpad pair; occluded AnyHit rays are then treated as the
+// reference's opaque shadower path does (hit kept, minT = T_EPSILON).
+void GpuDynBVH::intersect(const RenderContext& context, RayPacket& rays) const {
+  const bool any = rays.getFlag(RayPacket::AnyHit);
+  const int MS = RayPacket::MaxSize;
+  int map[MS];
+  float org[3 * MS], dir[3 * MS], tmax[MS], t[MS], u[MS], v[MS];
+  int prim[MS];
+  const int n = selectRays(rays, any, map);
+  if (n == 0) return;
+  packRays(rays, map, n, n, 0, org, dir, tmax);
+  traceRays(n, org, dir, tmax, any, t, prim, u, v);
+  applyHits(context, rays, any, map, n, t, prim, u, v);
 }

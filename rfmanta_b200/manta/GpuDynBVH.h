@@ -43,6 +43,32 @@ class GpuDynBVH : public AccelerationStructure {
 
   rq_scene* handle() const { return scene; }
 
+  // How a packet reaches the device.  Off (the default): every call is its
+  // own round trip (rq_trace: one launch on a private stream, rays read from
+  // and hits written to mapped host memory, one synchronise).  On: calls go
+  // through one submission queue (rq_queue_*), where packets that arrive
+  // while the device is busy are sent together as one batch.  On the
+  // measured host (16 cores, Manta's Raytracer, 16-256 workers) the queue
+  // is slower: waking the waiting workers costs more than the launches it
+  // saves.
+  void setBatching(bool on);
+
+  // Packet plumbing shared with GpuHardShadows.  selectRays lists the rays
+  // of `rays` the reference's DynBVH::intersect would trace (unmasked and,
+  // for AnyHit, not yet hit) into map[] and returns their count;
+  // packRays writes them as SoA rows (x, y, z of origin and direction, then
+  // minT) of length `stride` at column `base`; traceRays traces such rows;
+  // applyHits hands the hits back through RayPacket::hit with the real
+  // MeshTriangle, its material and the scratchpad pair, and for AnyHit
+  // applies the material's attenuateShadows as DynBVH does.
+  int selectRays(const RayPacket& rays, bool any, int* map) const;
+  static void packRays(const RayPacket& rays, const int* map, int n, int stride, int base,
+                       float* org, float* dir, float* tmax);
+  void traceRays(int n, const float* org, const float* dir, const float* tmax, bool any,
+                 float* t, int* prim, float* u, float* v) const;
+  void applyHits(const RenderContext& context, RayPacket& rays, bool any, const int* map,
+                 int n, const float* t, const int* prim, const float* u, const float* v) const;
+
  private:
   void upload();
   void check(int rc, const char* what) const;
@@ -50,9 +76,11 @@ class GpuDynBVH : public AccelerationStructure {
   Group* group;
   Mesh* mesh;
   rq_scene* scene;
+  rq_queue* queue;
   int device;
   int tri_kind;
   bool dirty;
+  bool batching;
 };
 
 }  // namespace Manta

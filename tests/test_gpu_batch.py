@@ -1,8 +1,8 @@
 """Batched multi-scene queries in one persistent, graph-captured launch:
 every configuration (block size, rays per warp chunk, refill threshold,
-register stack entries) and the autotuned one give, for every batch, the
-same bits as tracing that batch alone (rq_trace), which the other tests tie
-to the reference."""
+register stack entries, node-record layout) and the autotuned one give, for
+every batch, the same bits as tracing that batch alone (rq_trace), which the
+other tests tie to the reference."""
 import numpy as np
 import pytest
 
@@ -67,7 +67,11 @@ def _check(bq, exp):
                                  dict(block_threads=64, chunk_rays=32, refill_threshold=1, reg_stack=0),
                                  dict(block_threads=256, chunk_rays=512, refill_threshold=32, reg_stack=2),
                                  dict(block_threads=128, chunk_rays=96, refill_threshold=5, reg_stack=2,
-                                      blocks_per_sm=1)])
+                                      blocks_per_sm=1),
+                                 dict(block_threads=128, chunk_rays=64, refill_threshold=8, reg_stack=4,
+                                      node_layout=1),
+                                 dict(block_threads=64, chunk_rays=128, refill_threshold=16, reg_stack=1,
+                                      node_layout=2)])
 def test_batches_match_single_queries(setup, cfg):
     from rfmanta_b200.batch import BatchedQueries
     bvhs, batches, host = setup
@@ -86,6 +90,11 @@ def test_autotune_and_new_rays(setup):
     bq = BatchedQueries(bvhs, batches)
     cfg = bq.autotune(reps=1, candidates=[dict(chunk_rays=32), dict(chunk_rays=256, reg_stack=0)])
     assert cfg["chunk_rays"] in (32, 256)
+    # the built-in search (shape, then stack entries x node layout, then
+    # chunk x refill) returns a valid configuration
+    full = bq.autotune(reps=1)
+    assert full["reg_stack"] in (0, 1, 2, 4) and full["node_layout"] in (0, 1, 2)
+    _check(bq, _expected(bvhs, host))
     # write new rays into the same device arrays and replay the plan
     rng = np.random.default_rng(9)
     for b, h in zip(batches, host):
@@ -136,10 +145,15 @@ def test_plan_follows_scene_updates():
                        torch.from_numpy(tm).cuda(), False, want_uv=True)
     bq = BatchedQueries([bvh], [batch], dict(reg_stack=0))
     bq.launch()
+    # a plan over a breadth-first copy of the records follows the updates too
+    bq2 = BatchedQueries([bvh], [batch], dict(reg_stack=2, node_layout=1))
     v0 = mesh.vertices.copy()
     for k, rotate in ((1, True), (2, False), (3, True)):
         mesh.vertices = scenes.animated_vertices(v0, k, amplitude=0.05)
         bvh.update(rotate=rotate)
         bq.launch()
         _check(bq, _expected([bvh], [(0, o, d, tm, False)]))
+        bq2.launch()
+        _check(bq2, _expected([bvh], [(0, o, d, tm, False)]))
     bq.close()
+    bq2.close()

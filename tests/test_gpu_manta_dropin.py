@@ -45,3 +45,49 @@ def test_raytracer_through_gpu_dynbvh(kind, tmp_path):
     img = own.render(sc, nthreads=4)
     differ = (img["prim"] != want["prim"]).mean()
     assert differ < 1e-3, differ
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_gpu_hard_shadows_and_batched_packets(kind, tmp_path):
+    """GpuHardShadows (all lights' shadow rays of a packet in one
+    submission) and the submission queue (concurrent workers' packets
+    gathered into batches) under the reference's own Raytracer and
+    Lambertian, with three point lights and 32 worker threads: the frame,
+    the per-pixel hits and the shadow-ray count equal the reference's
+    DynBVH + HardShadows render bit for bit, with batching on and off."""
+    from rfmanta_b200 import scenes
+    sc = scenes.small_frame_scene(xres=192, yres=160)
+    sc.lights = list(sc.lights) + [scenes.PointLightSpec((-2.5, 2.0, 1.0), (0.3, 0.35, 0.4)),
+                                   scenes.PointLightSpec((0.0, -3.0, 0.5), (0.2, 0.2, 0.2))]
+    ref = Reference(path=DROPIN_SO)
+    cpu = ref.scene(sc.mesh, kind)
+    want = cpu.render(sc, nthreads=8)
+    gpu = ref.scene(sc.mesh, kind)
+    gpu.use_gpu(0, kind, tree_file=str(tmp_path / "tree.bvh"))
+    for batching, gpu_shadows in ((True, True), (False, True), (True, False)):
+        gpu.gpu_options(batching=batching, gpu_shadows=gpu_shadows)
+        got = gpu.render(sc, nthreads=32)
+        assert got["shadow_rays"] == want["shadow_rays"], (batching, gpu_shadows)
+        assert np.array_equal(got["prim"], want["prim"]), (batching, gpu_shadows)
+        assert np.array_equal(_bits(got["rgb"]), _bits(want["rgb"])), (batching, gpu_shadows)
+
+
+def test_gpu_mesh_as_primitive_in_a_group(tmp_path):
+    """The Primitive surface: a reference Group holding one GpuMeshPrimitive
+    over the drop-in, traced through Group::intersect, renders the frame of
+    the reference's DynBVH bit for bit (with HardShadows and with
+    GpuHardShadows)."""
+    from rfmanta_b200 import scenes
+    sc = scenes.small_frame_scene(xres=160, yres=128)
+    ref = Reference(path=DROPIN_SO)
+    cpu = ref.scene(sc.mesh, 0)
+    want = cpu.render(sc, nthreads=4)
+    gpu = ref.scene(sc.mesh, 0)
+    gpu.use_gpu(0, 0, tree_file=str(tmp_path / "tree.bvh"))
+    gpu.gpu_as_primitive()
+    for gpu_shadows in (False, True):
+        gpu.gpu_options(batching=True, gpu_shadows=gpu_shadows)
+        got = gpu.render(sc, nthreads=8)
+        assert got["shadow_rays"] == want["shadow_rays"]
+        assert np.array_equal(got["prim"], want["prim"])
+        assert np.array_equal(_bits(got["rgb"]), _bits(want["rgb"]))

@@ -166,3 +166,22 @@ def test_register_stack_entries_rejected_outside_0_1_2_4(tiny):
     kind, sc, bvh, tree = tiny
     with pytest.raises(RQError):
         bvh.set_launch_config(False, stage=RQ_PATH_EXTEND, reg_stack=3)
+
+
+@pytest.mark.parametrize("layout", [1, 2])
+def test_node_layouts_do_not_change_results(tiny, restatement, layout):
+    """The path stages can read a breadth-first (1) or hot-top (2) copy of
+    the node records; the records and the traversal order are unchanged, so
+    image, ray counts and per-bounce ids stay those of the restatement."""
+    from rfmanta_b200._lib import RQ_PATH_EXTEND
+    kind, sc, bvh, tree = tiny
+    old = bvh.get_launch_config(False, stage=RQ_PATH_EXTEND)
+    try:
+        bvh.set_launch_config(False, stage=RQ_PATH_EXTEND,
+                              **dict(old, node_layout=layout))
+        out = bvh.render_path(sc)
+    finally:
+        bvh.set_launch_config(False, stage=RQ_PATH_EXTEND, **old)
+    exp = restatement.render_path(tree, sc, tri_kind=kind)
+    assert out["rays"] == exp["rays"] and out["shadow_rays"] == exp["shadow_rays"]
+    assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))

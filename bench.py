@@ -567,15 +567,18 @@ class BatchedQueriesWL:
 
     name = "batched_queries"
 
-    def __init__(self):
+    def __init__(self, scale=1.0, plan_config=None):
         from rfmanta_b200 import scenes
-        self.specs = scenes.query_batches()
+        self.specs = scenes.query_batches(scale=scale)
         self.meshes = [scenes.query_scene(i) for i in range(8)]
         self.sc = None
+        self.scale = scale
+        self.plan_config = plan_config  # None: autotuned
 
     def config(self):
         return {"workload": self.name, "scenes": [int(m.n_tris) for m in self.meshes],
                 "batches": len(self.specs), "rays": int(sum(n for _, n, _ in self.specs)),
+                "batch_scale": self.scale,
                 "anyhit_batches": int(sum(a for _, _, a in self.specs)),
                 "triangle_kind": "wald", "tree": "gpu binned SAH",
                 "l2": "flushed before every timed step (256 MiB write); inputs exceed L2"}
@@ -600,8 +603,8 @@ class BatchedQueriesWL:
             lo, hi = self.meshes[si].bounds()
             o, d, tm = scenes.query_rays_torch(n, lo, hi, anyhit, seed=1000 + k, device=dev)
             self.batches.append(QueryBatch(si, o, d, tm, anyhit))
-        self.bq = BatchedQueries(self.bvhs, self.batches)
-        self.tuned = self.bq.autotune(reps=1)
+        self.bq = BatchedQueries(self.bvhs, self.batches, self.plan_config)
+        self.tuned = self.bq.autotune(reps=1) if self.plan_config is None else self.bq.config
         self.n_events = 0
         self.launches = 1
         self.total = self.bq.total_rays
@@ -690,23 +693,46 @@ class BatchedQueriesWL:
         """The plain per-call GPU form (one rq_trace_device launch per batch,
         timed like the batched leg) and Manta's per-packet form (rq_trace on
         64-ray host packets)."""
-        from rfmanta_b200.dynbvh import RayBatch
         legs = self.legs(dev)
-        b = self.batches[0]
-        o = b.org[:, :64 * 500].cpu().numpy()
-        d = b.dir[:, :64 * 500].cpu().numpy()
-        tm = b.tmax[:64 * 500].cpu().numpy()
-        npk = o.shape[1] // 64
-        t0 = time.perf_counter()
-        for k in range(npk):
-            r = RayBatch(o[:, 64 * k:64 * k + 64], d[:, 64 * k:64 * k + 64],
-                         tm[64 * k:64 * k + 64], flags=RayBatch.AnyHit if b.anyhit else 0)
-            self.bvhs[b.scene].intersect(r)
-        per_packet = npk * 64 / (time.perf_counter() - t0) / 1e6
         return {"plain_gpu_per_batch_mrays": round(legs["plain"], 1),
                 "batched_vs_plain": round(legs["batched"] / legs["plain"], 3),
-                "manta_per_packet_dropin_mrays": round(per_packet, 3),
+                "per_packet_calls_mrays": round(self.per_packet_rate(), 2),
+                "per_packet_calls": "64-ray rq_trace calls (host arrays) from 16 host threads "
+                                    "at once, rays of the first batch",
                 "autotuned": self.tuned, "build_ms_total": round(self.build_s * 1e3, 1)}
+
+    def per_packet_rate(self, threads=16, packets_per_thread=400):
+        """The per-call drop-in form as Manta's workers use it: every host
+        thread traces 64-ray packets from host arrays with rq_trace, one
+        call at a time; Mrays/s over all threads (ctypes releases the
+        interpreter lock during each call)."""
+        from rfmanta_b200 import _lib
+        b = self.batches[0]
+        n = 64 * packets_per_thread
+        o = np.ascontiguousarray(b.org[:, :n].cpu().numpy())
+        d = np.ascontiguousarray(b.dir[:, :n].cpu().numpy())
+        tm = np.ascontiguousarray(b.tmax[:n].cpu().numpy())
+        npk = o.shape[1] // 64
+        pk = [(np.ascontiguousarray(o[:, 64 * k:64 * k + 64]),
+               np.ascontiguousarray(d[:, 64 * k:64 * k + 64]),
+               np.ascontiguousarray(tm[64 * k:64 * k + 64])) for k in range(npk)]
+        h = self.bvhs[b.scene].handle
+        flags = _lib.RQ_ANYHIT if b.anyhit else _lib.RQ_CLOSEST
+
+        def work():
+            t = np.zeros(64, np.float32)
+            p = np.zeros(64, np.int32)
+            for po, pd, pt in pk:
+                _lib.lib.rq_trace(h, 64, po.ctypes.data, pd.ctypes.data, pt.ctypes.data, flags,
+                                  t.ctypes.data, p.ctypes.data, None, None)
+
+        th = [threading.Thread(target=work) for _ in range(threads)]
+        t0 = time.perf_counter()
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        return threads * npk * 64 / (time.perf_counter() - t0) / 1e6
 
     def cpu_reference(self, seconds_budget, threads):
         """Reference DynBVH::intersect (64-ray packets, all host threads) on
@@ -904,6 +930,7 @@ def system_forms(dev, streams=3):
     out = {"batched_mrays": round(legs["batched"], 1),
            "plain_per_batch_mrays": round(legs["plain"], 1),
            "batched_vs_plain": round(legs["batched"] / legs["plain"], 3),
+           "per_packet_calls_mrays": round(wl.per_packet_rate(), 2),
            "batched_autotuned": wl.tuned,
            "batched_workload": "64 batches, 1k-4M rays, 8 scenes of 10k-5.12M triangles, "
                                "50% any hit; L2 flushed (256 MiB) before every rep of both legs"}
@@ -928,7 +955,13 @@ def system_forms(dev, streams=3):
 
 
 def make_workload(args):
-    wl = WORKLOADS[args.workload]()
+    if args.workload == "batched_queries":
+        wl = BatchedQueriesWL(args.batch_scale,
+                              json.loads(args.batch_config) if args.batch_config else None)
+    else:
+        if args.batch_scale != 1.0 or args.batch_config:
+            raise SystemExit("--batch-scale/--batch-config apply to batched_queries")
+        wl = WORKLOADS[args.workload]()
     sc = getattr(wl, "sc", None)
     if (args.res or args.spp) and sc is None:
         raise SystemExit(f"--res/--spp apply to frame workloads, not {args.workload}")
@@ -1289,6 +1322,11 @@ def main():
                     help="WxH override of a frame workload's resolution (small ncu cases)")
     ap.add_argument("--spp", type=int, default=None,
                     help="samples per pixel override of a frame workload")
+    ap.add_argument("--batch-scale", type=float, default=1.0,
+                    help="batched_queries: batch sizes scaled by this factor (small ncu cases)")
+    ap.add_argument("--batch-config", default=None,
+                    help="batched_queries: a fixed plan configuration (JSON) instead of the "
+                         "autotuner's")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

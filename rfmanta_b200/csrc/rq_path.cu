@@ -326,14 +326,25 @@ cudaError_t launch_ordered_compaction(const PathBuffers& B, int n, int depth, cu
 
 // Grid of a persistent stage: every SM filled once at the kernel's own
 // occupancy for this block size and stack (or blocks_per_sm if smaller).
+// With blocks_per_sm below the occupancy maximum, the shared memory the
+// resident blocks do not need is left to L1 (the carveout preference is set
+// to what those blocks use), so the node and triangle records get more L1.
 static int stage_grid(const void* f, int block, int blocks_per_sm, size_t smem) {
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int b = 0, dev = 0, sms = 0;
+  cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutDefault);
+  int b = 0, dev = 0, sms = 0, per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, block, smem);
-  if (blocks_per_sm > 0) b = std::min(b, blocks_per_sm);
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (blocks_per_sm > 0 && blocks_per_sm < b && per_sm > 0) {
+    b = blocks_per_sm;
+    const size_t need = (size_t)b * (smem + 1024);  // + the per-block reservation
+    const int pct = (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / per_sm);
+    cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  }
   return std::max(1, b * sms);
 }
 

@@ -265,7 +265,9 @@ RQ_API int rq_queue_destroy(rq_queue* queue);
  * the builder's depth-first pre-order, breadth-first from the root, or the
  * top 16,384 records breadth-first followed by the rest depth-first.  Batch
  * plans (rq_batch_config) and the path stages (rq_launch_config) use a
- * reordered copy the scene keeps until its tree changes. */
+ * reordered copy the scene keeps until its tree changes; the copy is made
+ * on the device by the first call that needs it, which then synchronises
+ * the device once. */
 #define RQ_LAYOUT_DFS 0
 #define RQ_LAYOUT_BFS 1
 #define RQ_LAYOUT_BFS_TOP 2

@@ -185,3 +185,19 @@ def test_node_layouts_do_not_change_results(tiny, restatement, layout):
     exp = restatement.render_path(tree, sc, tri_kind=kind)
     assert out["rays"] == exp["rays"] and out["shadow_rays"] == exp["shadow_rays"]
     assert np.array_equal(_bits(out["rgb"]), _bits(exp["rgb"]))
+
+
+def test_path_image_into_page_locked_host_memory(tiny):
+    """An image given in page-locked host memory equals the image copied
+    to pageable memory, with the same ray counts."""
+    import ctypes as C
+    import torch
+    from rfmanta_b200 import _lib
+    kind, sc, bvh, tree = tiny
+    want = bvh.render_path(sc)
+    rgb = torch.empty((sc.xres * sc.yres, 3), pin_memory=True)
+    counts = (C.c_uint64 * 2)()
+    p = bvh.path_params(sc)
+    _lib.check(_lib.lib.rq_render_path(bvh.handle, C.byref(p), C.c_void_p(rgb.data_ptr()), counts))
+    assert counts[0] == want["rays"] and counts[1] == want["shadow_rays"]
+    assert np.array_equal(rgb.numpy().view(np.uint32), want["rgb"].view(np.uint32))

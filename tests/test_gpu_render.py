@@ -81,3 +81,46 @@ def test_render_device_path_matches_host_path(golden):
         torch.cuda.synchronize()
         assert int(ns.item()) == int(g["img_shadow_rays"])
         assert np.array_equal(_bits(rgb.cpu().numpy().reshape(-1, 3)), _bits(g["img_rgb"]))
+
+
+def test_frames_into_page_locked_host_memory():
+    """Frame outputs given in page-locked host memory (as the bench's
+    end-to-end runs give them) equal those written to pageable memory bit
+    for bit, for the Whitted frame and the supersampled frame, with and
+    without the optional t / prim outputs."""
+    import ctypes as C
+    import torch
+    from rfmanta_b200 import _lib, scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    sc = scenes.small_frame_scene(level=4, grid=40, xres=200, yres=150)
+    bvh = GpuDynBVH()
+    bvh.setGroup(sc.mesh)
+    bvh.rebuild()
+    npx = sc.xres * sc.yres
+    want = bvh.render_whitted(sc)
+    rgb = torch.empty((npx, 3), pin_memory=True)
+    t = torch.empty(npx, pin_memory=True)
+    prim = torch.empty(npx, dtype=torch.int32, pin_memory=True)
+    ns = C.c_uint64()
+    p = bvh.whitted_params(sc)
+    _lib.check(_lib.lib.rq_render_whitted(bvh.handle, C.byref(p), C.c_void_p(rgb.data_ptr()),
+                                          C.c_void_p(t.data_ptr()), C.c_void_p(prim.data_ptr()),
+                                          C.byref(ns)))
+    assert ns.value == want["shadow_rays"]
+    assert np.array_equal(prim.numpy(), want["prim"])
+    assert np.array_equal(t.numpy().view(np.uint32), want["t"].view(np.uint32))
+    assert np.array_equal(rgb.numpy().view(np.uint32), want["rgb"].view(np.uint32))
+    # only the image pinned, t and prim not wanted
+    rgb2 = torch.empty((npx, 3), pin_memory=True)
+    _lib.check(_lib.lib.rq_render_whitted(bvh.handle, C.byref(p), C.c_void_p(rgb2.data_ptr()),
+                                          None, None, None))
+    assert np.array_equal(rgb2.numpy().view(np.uint32), want["rgb"].view(np.uint32))
+    # the supersampled frame
+    sc.spp, sc.seed = 4, 11
+    fw = bvh.render_frame(sc, sc.mesh.materials)
+    fp = bvh.frame_params(sc, sc.mesh.materials)
+    rgb3 = torch.empty((npx, 3), pin_memory=True)
+    _lib.check(_lib.lib.rq_render_frame(bvh.handle, C.byref(fp), C.c_void_p(rgb3.data_ptr()),
+                                        C.byref(ns)))
+    assert ns.value == fw["shadow_rays"]
+    assert np.array_equal(rgb3.numpy().view(np.uint32), fw["rgb"].view(np.uint32))

@@ -9,7 +9,8 @@
 // DynBVH.cc:1804-1857), and a single object is always a leaf.
 //
 // Algorithm: level-synchronous top-down build, one CTA per node of the
-// current level.
+// current level (nodes of more than kBigNode primitives in a level of few
+// nodes: one CTA per slice of the node, see below).
 //   * n <= 32: the reference's own rule - an exact sweep over the centroid
 //     order on every axis (DynBVH::buildEvents, DynBVH.cc:2372-2440), one
 //     lane per candidate split;
@@ -414,6 +415,365 @@ __global__ void __launch_bounds__(kBuildThreads) build_level_kernel(BuildBufs B)
   }
 }
 
+// ---- large nodes: many CTAs per node --------------------------------------
+//
+// The top levels hold few nodes with many primitives each; one CTA per node
+// would leave most SMs idle.  Nodes with more than kBigNode primitives are
+// cut into slices of kSlice primitives and processed by one CTA per slice:
+// bounds (global atomic min/max), binning (shared-memory bins merged into
+// the node's global bins), one CTA per node for the SAH decision (the same
+// scans and rules as build_level_kernel), then a stable partition: per-slice
+// left counts, their prefix per node, and a scatter that keeps each slice's
+// order.  Bin counts and min/max bounds do not depend on the order of the
+// atomics and the partition is stable, so a node gets the same split and the
+// same child ranges as the one-CTA path would give it.
+constexpr int kBigNode = 1 << 16;
+constexpr int kSlice = 8192;
+
+struct BigAcc {
+  int nb[6];  // ordered-int node bounds: min xyz, max xyz
+  int cb[6];  // ordered-int centroid bounds
+  int bcount[3][kBins];
+  int bbox[3][kBins][6];
+  // decision (written by big_decide_kernel)
+  int axis, split, nl, median;
+  float cb_f[6];
+};
+
+struct BigSlice {
+  int node;  // index into the level's big nodes
+  int begin, end;
+  int offl, offr;  // left / right elements of earlier slices of the node
+  int nleft;
+};
+
+__global__ void big_init_kernel(BigAcc* acc, int n_big) {
+  const int k = blockIdx.x;
+  if (k >= n_big) return;
+  BigAcc& A = acc[k];
+  for (int i = threadIdx.x; i < 3 * kBins; i += blockDim.x) {
+    const int a = i / kBins, bin = i % kBins;
+    A.bcount[a][bin] = 0;
+    for (int c = 0; c < 3; ++c) {
+      A.bbox[a][bin][c] = f2o(INFINITY);
+      A.bbox[a][bin][3 + c] = f2o(-INFINITY);
+    }
+  }
+  if (threadIdx.x < 3) {
+    A.nb[threadIdx.x] = f2o(INFINITY);
+    A.nb[3 + threadIdx.x] = f2o(-INFINITY);
+    A.cb[threadIdx.x] = f2o(INFINITY);
+    A.cb[3 + threadIdx.x] = f2o(-INFINITY);
+  }
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    big_bounds_kernel(BuildBufs B, const BigSlice* slices, BigAcc* acc) {
+  __shared__ float red[kBuildThreads / 32][12];
+  const BigSlice sl = slices[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float v[12];
+  for (int c = 0; c < 3; ++c) {
+    v[c] = INFINITY;
+    v[3 + c] = -INFINITY;
+    v[6 + c] = INFINITY;
+    v[9 + c] = -INFINITY;
+  }
+  for (int i = sl.begin + tid; i < sl.end; i += blockDim.x) {
+    const int p = B.idx_in[i];
+    for (int c = 0; c < 3; ++c) {
+      v[c] = fminf(v[c], B.pbox[6 * (size_t)p + c]);
+      v[3 + c] = fmaxf(v[3 + c], B.pbox[6 * (size_t)p + 3 + c]);
+      const float cc = B.pcen[3 * (size_t)p + c];
+      v[6 + c] = fminf(v[6 + c], cc);
+      v[9 + c] = fmaxf(v[9 + c], cc);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int c = 0; c < 3; ++c) {
+      v[c] = fminf(v[c], __shfl_xor_sync(0xffffffffu, v[c], o));
+      v[3 + c] = fmaxf(v[3 + c], __shfl_xor_sync(0xffffffffu, v[3 + c], o));
+      v[6 + c] = fminf(v[6 + c], __shfl_xor_sync(0xffffffffu, v[6 + c], o));
+      v[9 + c] = fmaxf(v[9 + c], __shfl_xor_sync(0xffffffffu, v[9 + c], o));
+    }
+  if (lane == 0)
+    for (int k = 0; k < 12; ++k) red[warp][k] = v[k];
+  __syncthreads();
+  if (tid < 12) {
+    float x = red[0][tid];
+    for (int w = 1; w < (int)(blockDim.x / 32); ++w) {
+      const bool mn = (tid % 6) < 3;
+      x = mn ? fminf(x, red[w][tid]) : fmaxf(x, red[w][tid]);
+    }
+    BigAcc& A = acc[sl.node];
+    int* dst = tid < 6 ? &A.nb[tid] : &A.cb[tid - 6];
+    if ((tid % 6) < 3)
+      atomicMin(dst, f2o(x));
+    else
+      atomicMax(dst, f2o(x));
+  }
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    big_bin_kernel(BuildBufs B, const BigSlice* slices, BigAcc* acc) {
+  __shared__ int bcount[3][kBins];
+  __shared__ int bbox[3][kBins][6];
+  const BigSlice sl = slices[blockIdx.x];
+  BigAcc& A = acc[sl.node];
+  const int tid = threadIdx.x;
+  for (int k = tid; k < 3 * kBins; k += blockDim.x) {
+    const int a = k / kBins, bin = k % kBins;
+    bcount[a][bin] = 0;
+    for (int c = 0; c < 3; ++c) {
+      bbox[a][bin][c] = f2o(INFINITY);
+      bbox[a][bin][3 + c] = f2o(-INFINITY);
+    }
+  }
+  float cb[6], scale[3];
+  for (int k = 0; k < 6; ++k) cb[k] = o2f(A.cb[k]);
+  for (int a = 0; a < 3; ++a) {
+    const float ext = cb[3 + a] - cb[a];
+    scale[a] = ext > 0.f ? (float)kBins / ext : 0.f;
+  }
+  __syncthreads();
+  for (int i = sl.begin + tid; i < sl.end; i += blockDim.x) {
+    const int p = B.idx_in[i];
+    float pb[6];
+    for (int k = 0; k < 6; ++k) pb[k] = B.pbox[6 * (size_t)p + k];
+    for (int a = 0; a < 3; ++a) {
+      if (scale[a] == 0.f) continue;
+      const int bin = min(kBins - 1, (int)((B.pcen[3 * (size_t)p + a] - cb[a]) * scale[a]));
+      atomicAdd(&bcount[a][bin], 1);
+      for (int c = 0; c < 3; ++c) {
+        atomicMin(&bbox[a][bin][c], f2o(pb[c]));
+        atomicMax(&bbox[a][bin][3 + c], f2o(pb[3 + c]));
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = tid; k < 3 * kBins; k += blockDim.x) {
+    const int a = k / kBins, bin = k % kBins;
+    if (bcount[a][bin] == 0) continue;
+    atomicAdd(&A.bcount[a][bin], bcount[a][bin]);
+    for (int c = 0; c < 3; ++c) {
+      atomicMin(&A.bbox[a][bin][c], bbox[a][bin][c]);
+      atomicMax(&A.bbox[a][bin][3 + c], bbox[a][bin][3 + c]);
+    }
+  }
+}
+
+// One CTA (3 warps used) per large node: the binned SAH sweep and the split
+// decision of build_level_kernel, from the node's merged bins.
+__global__ void big_decide_kernel(BuildBufs B, const BuildItem* items, BigAcc* acc) {
+  __shared__ float best_cost[3];
+  __shared__ int best_split[3], best_nl[3];
+  const BuildItem it = items[blockIdx.x];
+  BigAcc& A = acc[blockIdx.x];
+  const int n = it.end - it.begin;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float nb[6], cb[6];
+  for (int k = 0; k < 6; ++k) {
+    nb[k] = o2f(A.nb[k]);
+    cb[k] = o2f(A.cb[k]);
+  }
+  const float parea = area6(nb);
+  if (warp < 3) {
+    const int a = warp;
+    const float ext = cb[3 + a] - cb[a];
+    const bool usable = ext > 0.f;
+    float cost = INFINITY;
+    int nl = 0;
+    if (usable) {
+      const int cnt = A.bcount[a][lane];
+      float bx[6];
+      for (int k = 0; k < 6; ++k) bx[k] = o2f(A.bbox[a][lane][k]);
+      int lc = cnt, rc = cnt;
+      float lb[6], rb[6];
+      for (int k = 0; k < 6; ++k) lb[k] = rb[k] = bx[k];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int tl = __shfl_up_sync(0xffffffffu, lc, o);
+        const int tr = __shfl_down_sync(0xffffffffu, rc, o);
+        float ul[6], dr[6];
+        for (int k = 0; k < 6; ++k) {
+          ul[k] = __shfl_up_sync(0xffffffffu, lb[k], o);
+          dr[k] = __shfl_down_sync(0xffffffffu, rb[k], o);
+        }
+        if (lane >= o) {
+          lc += tl;
+          for (int c = 0; c < 3; ++c) {
+            lb[c] = fminf(lb[c], ul[c]);
+            lb[3 + c] = fmaxf(lb[3 + c], ul[3 + c]);
+          }
+        }
+        if (lane + o < 32) {
+          rc += tr;
+          for (int c = 0; c < 3; ++c) {
+            rb[c] = fminf(rb[c], dr[c]);
+            rb[3 + c] = fmaxf(rb[3 + c], dr[3 + c]);
+          }
+        }
+      }
+      const int rcn = __shfl_down_sync(0xffffffffu, rc, 1);
+      float rbn[6];
+      for (int k = 0; k < 6; ++k) rbn[k] = __shfl_down_sync(0xffffffffu, rb[k], 1);
+      if (lane < 31 && lc > 0 && rcn > 0) {
+        cost = 1.f + ((float)lc * area6(lb) + (float)rcn * area6(rbn)) / parea;
+        nl = lc;
+      }
+    }
+    float bc = cost;
+    int bl = lane, bn = nl;
+    for (int o = 16; o > 0; o >>= 1) {
+      const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+      const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+      const int on = __shfl_xor_sync(0xffffffffu, bn, o);
+      if (oc < bc || (oc == bc && ol < bl)) {
+        bc = oc;
+        bl = ol;
+        bn = on;
+      }
+    }
+    if (lane == 0) {
+      best_cost[a] = usable ? bc : INFINITY;
+      best_split[a] = bl;
+      best_nl[a] = bn;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ba = -1;
+    float bc = INFINITY;
+    for (int a = 0; a < 3; ++a)
+      if (best_cost[a] < bc) {
+        bc = best_cost[a];
+        ba = a;
+      }
+    // n > kForceSplit always holds here: the node is split, by SAH when a
+    // plane exists, else at the object median
+    if (ba >= 0) {
+      A.axis = ba;
+      A.split = best_split[ba];
+      A.nl = best_nl[ba];
+      A.median = 0;
+    } else {
+      A.axis = 0;
+      A.split = -1;
+      A.nl = n / 2;
+      A.median = 1;
+    }
+    for (int k = 0; k < 6; ++k) {
+      A.cb_f[k] = cb[k];
+      B.nbounds[6 * (size_t)it.node + k] = nb[k];
+    }
+  }
+}
+
+__device__ __forceinline__ bool big_left(const BuildBufs& B, const BigAcc& A, int b, int i,
+                                         int p, float scale_a) {
+  if (A.median) return (i - b) < A.nl;
+  return min(kBins - 1, (int)((B.pcen[3 * (size_t)p + A.axis] - A.cb_f[A.axis]) * scale_a)) <=
+         A.split;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    big_count_kernel(BuildBufs B, const BuildItem* items, BigSlice* slices, const BigAcc* acc) {
+  __shared__ int wsum[kBuildThreads / 32];
+  BigSlice& sl = slices[blockIdx.x];
+  const BigAcc& A = acc[sl.node];
+  const int b = items[sl.node].begin;
+  const float scale_a = A.median ? 0.f : (float)kBins / (A.cb_f[3 + A.axis] - A.cb_f[A.axis]);
+  int c = 0;
+  for (int i = sl.begin + threadIdx.x; i < sl.end; i += blockDim.x)
+    c += big_left(B, A, b, i, B.idx_in[i], scale_a) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += wsum[w];
+    sl.nleft = t;
+  }
+}
+
+// Per large node (one thread each): offsets of its slices, then the child
+// pair and the next level's two items.
+__global__ void big_offsets_kernel(BuildBufs B, const BuildItem* items, BigSlice* slices,
+                                   int n_slices, const BigAcc* acc, int n_big) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_big) return;
+  int offl = 0, offr = 0;
+  for (int j = 0; j < n_slices; ++j) {
+    if (slices[j].node != k) continue;
+    slices[j].offl = offl;
+    slices[j].offr = offr;
+    offl += slices[j].nleft;
+    offr += (slices[j].end - slices[j].begin) - slices[j].nleft;
+  }
+  const BuildItem it = items[k];
+  const int nl = acc[k].nl;
+  const int c = atomicAdd(B.node_counter, 2);
+  B.nchild[it.node] = c;
+  B.nchildren[it.node] = 0;
+  B.naxis[it.node] = (unsigned char)acc[k].axis;
+  const int q = atomicAdd(B.n_next, 2);
+  B.next[q] = BuildItem{c, it.begin, it.begin + nl};
+  B.next[q + 1] = BuildItem{c + 1, it.begin + nl, it.end};
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    big_scatter_kernel(BuildBufs B, const BuildItem* items, const BigSlice* slices,
+                       const BigAcc* acc) {
+  __shared__ int wsum[kBuildThreads / 32][2];
+  __shared__ int base[2];
+  const BigSlice sl = slices[blockIdx.x];
+  const BigAcc& A = acc[sl.node];
+  const int b = items[sl.node].begin, e = items[sl.node].end;
+  const int nl = A.nl;
+  const float scale_a = A.median ? 0.f : (float)kBins / (A.cb_f[3 + A.axis] - A.cb_f[A.axis]);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    base[0] = sl.offl;
+    base[1] = sl.offr;
+  }
+  __syncthreads();
+  for (int start = sl.begin; start < sl.end; start += blockDim.x) {
+    const int i = start + tid;
+    int p = 0;
+    bool left = false;
+    if (i < sl.end) {
+      p = B.idx_in[i];
+      left = big_left(B, A, b, i, p, scale_a);
+    }
+    const unsigned ml = __ballot_sync(0xffffffffu, i < sl.end && left);
+    const unsigned mr = __ballot_sync(0xffffffffu, i < sl.end && !left);
+    if (lane == 0) {
+      wsum[warp][0] = __popc(ml);
+      wsum[warp][1] = __popc(mr);
+    }
+    __syncthreads();
+    int offl = base[0], offr = base[1];
+    for (int w = 0; w < warp; ++w) {
+      offl += wsum[w][0];
+      offr += wsum[w][1];
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    if (i < sl.end) {
+      // the node's left count nl comes from the same bin rule, so every
+      // destination lies in [b, e); the guard keeps a write inside the node
+      // even if it did not
+      const int d = left ? b + offl + __popc(ml & lt) : b + nl + offr + __popc(mr & lt);
+      if (d >= b && d < e) B.idx_out[d] = p;
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+        base[0] += wsum[w][0];
+        base[1] += wsum[w][1];
+      }
+    __syncthreads();
+  }
+}
+
 template <class T>
 static cudaError_t dalloc(T** p, size_t n) {
   return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
@@ -427,6 +787,13 @@ int gpu_build(Scene* s, HostTree& out, double* seconds) {
   int *counters = nullptr;
   unsigned char* naxis = nullptr;
   BuildItem *items_a = nullptr, *items_b = nullptr;
+  // large-node path: per-node accumulators, slice table, item lists
+  const int max_big = n / kBigNode + 1;
+  const int max_slices = n / kSlice + max_big + 1;
+  constexpr int kHostItems = 512;  // levels this small are split on the host
+  BigAcc* acc = nullptr;
+  BigSlice* slices = nullptr;
+  BuildItem *big_items = nullptr, *small_items = nullptr;
   const size_t max_nodes = 2 * (size_t)n;
   cudaError_t e = cudaSuccess;
   cudaEvent_t t0, t1;
@@ -436,6 +803,7 @@ int gpu_build(Scene* s, HostTree& out, double* seconds) {
     cudaFree(pbox); cudaFree(pcen); cudaFree(nb); cudaFree(ia); cudaFree(ib); cudaFree(ids);
     cudaFree(nchild); cudaFree(nchildren); cudaFree(counters); cudaFree(naxis);
     cudaFree(items_a); cudaFree(items_b);
+    cudaFree(acc); cudaFree(slices); cudaFree(big_items); cudaFree(small_items);
     cudaEventDestroy(t0); cudaEventDestroy(t1);
   };
 #define BCHK(x)                                                         \
@@ -459,6 +827,10 @@ int gpu_build(Scene* s, HostTree& out, double* seconds) {
   BCHK(dalloc(&counters, 4));
   BCHK(dalloc(&items_a, n));
   BCHK(dalloc(&items_b, n));
+  BCHK(dalloc(&acc, max_big));
+  BCHK(dalloc(&slices, max_slices));
+  BCHK(dalloc(&big_items, max_big));
+  BCHK(dalloc(&small_items, kHostItems));
   BCHK(cudaEventRecord(t0, 0));
   prim_bounds_kernel<<<(n + 255) / 256, 256>>>(s->d_verts, s->d_idx, n, pbox, pcen);
   BCHK(cudaGetLastError());
@@ -477,11 +849,48 @@ int gpu_build(Scene* s, HostTree& out, double* seconds) {
   BuildItem* cur = items_a;
   BuildItem* nxt = items_b;
   int levels = 0;
+  std::vector<BuildItem> h_items, h_big, h_small;
+  std::vector<BigSlice> h_slices;
   while (n_items > 0) {
     BCHK(cudaMemsetAsync(counters + 1, 0, sizeof(int), 0));
     BuildBufs B{pbox, pcen, idx_in, idx_out, ids, cur, nxt, counters + 1, counters,
                 nb, nchild, nchildren, naxis};
-    build_level_kernel<<<n_items, kBuildThreads>>>(B);
+    // a level of few nodes: nodes above kBigNode primitives go to the
+    // many-CTA path, the rest to build_level_kernel
+    h_big.clear();
+    h_small.clear();
+    if (n_items <= kHostItems) {
+      h_items.resize(n_items);
+      BCHK(cudaMemcpy(h_items.data(), cur, sizeof(BuildItem) * n_items, cudaMemcpyDeviceToHost));
+      for (const BuildItem& it : h_items)
+        (it.end - it.begin > kBigNode ? h_big : h_small).push_back(it);
+    }
+    if (!h_big.empty()) {
+      h_slices.clear();
+      for (int k = 0; k < (int)h_big.size(); ++k)
+        for (int b0 = h_big[k].begin; b0 < h_big[k].end; b0 += kSlice)
+          h_slices.push_back(BigSlice{k, b0, std::min(b0 + kSlice, h_big[k].end), 0, 0, 0});
+      const int nbig = (int)h_big.size(), nsl = (int)h_slices.size();
+      BCHK(cudaMemcpy(big_items, h_big.data(), sizeof(BuildItem) * nbig, cudaMemcpyHostToDevice));
+      BCHK(cudaMemcpy(slices, h_slices.data(), sizeof(BigSlice) * nsl, cudaMemcpyHostToDevice));
+      big_init_kernel<<<nbig, 128>>>(acc, nbig);
+      big_bounds_kernel<<<nsl, kBuildThreads>>>(B, slices, acc);
+      big_bin_kernel<<<nsl, kBuildThreads>>>(B, slices, acc);
+      big_decide_kernel<<<nbig, 96>>>(B, big_items, acc);
+      big_count_kernel<<<nsl, kBuildThreads>>>(B, big_items, slices, acc);
+      big_offsets_kernel<<<(nbig + 31) / 32, 32>>>(B, big_items, slices, nsl, acc, nbig);
+      big_scatter_kernel<<<nsl, kBuildThreads>>>(B, big_items, slices, acc);
+      BCHK(cudaGetLastError());
+      if (!h_small.empty()) {
+        BCHK(cudaMemcpy(small_items, h_small.data(), sizeof(BuildItem) * h_small.size(),
+                        cudaMemcpyHostToDevice));
+        BuildBufs Bs = B;
+        Bs.items = small_items;
+        build_level_kernel<<<(int)h_small.size(), kBuildThreads>>>(Bs);
+      }
+    } else {
+      build_level_kernel<<<n_items, kBuildThreads>>>(B);
+    }
     BCHK(cudaGetLastError());
     BCHK(cudaMemcpy(&n_items, counters + 1, sizeof(int), cudaMemcpyDeviceToHost));
     std::swap(idx_in, idx_out);

@@ -249,7 +249,10 @@ RQ_API int rq_trace_device(rq_scene* scene, int n, const float* d_org,
  * are back.  Packets of up to max_rays rays are batched (larger ones go
  * through rq_trace); closest-hit and any-hit packets form separate batches.
  * The scene must outlive the queue, and must not be updated while queued
- * traces run.
+ * traces run; rq_queue_destroy must not overlap calls on the queue.
+ * Measured under Manta's Raytracer on a 16-core host the queue is slower
+ * than per-packet rq_trace calls (waking the waiting workers costs more
+ * than the launches it saves); it is kept for callers with cheaper waits.
  */
 typedef struct rq_queue rq_queue;
 RQ_API int rq_queue_create(rq_scene* scene, int max_rays, rq_queue** out);

@@ -449,8 +449,33 @@ RQ_API int rq_server_create(rq_scene* const* scenes, int n_scenes,
 /* Queues a request (admitted by a later rq_server_step). */
 RQ_API int rq_server_submit(rq_server* server, const rq_serve_request* request,
                             int* request_id);
+
+/*
+ * Ray-query requests beside the render requests: n rays of one of the
+ * server's scenes (SoA host arrays as in rq_trace, copied on submit),
+ * closest or any hit.  Admitted in arrival order against the same HBM
+ * budget (36 bytes per ray: the rays and their results stay on the device
+ * until release), then traced in chunks of at most 1Mi rays, at most 8Mi
+ * rays per step, by one persistent launch of the batched traversal kernel
+ * inside the step that also runs the path chunks.  rq_server_poll reports
+ * them like renders; rq_server_query_result copies t and triangle id
+ * (either may be NULL) - equal, bit for bit, to rq_trace on the same rays.
+ */
+typedef struct {
+  int scene;
+  int n;
+  int flags;          /* RQ_CLOSEST or RQ_ANYHIT */
+  const float* org;   /* host, 3n */
+  const float* dir;   /* host, 3n */
+  const float* tmax;  /* host, n */
+} rq_serve_query;
+RQ_API int rq_server_submit_query(rq_server* server, const rq_serve_query* query,
+                                  int* request_id);
+RQ_API int rq_server_query_result(rq_server* server, int request_id, float* t, int32_t* prim,
+                                  double* latency_s, double* queue_s);
 /* Admits what fits, enqueues one step; *scheduled_paths = its path count
- * (0 when nothing was waiting).  Blocks only to keep two steps in flight. */
+ * plus its ray-query rays (0 when nothing was waiting).  Blocks only to
+ * keep two steps in flight. */
 RQ_API int rq_server_step(rq_server* server, int* scheduled_paths);
 /* Ids of requests finished on the device since the last poll. */
 RQ_API int rq_server_poll(rq_server* server, int* done_ids, int max_ids, int* n_done);
@@ -460,6 +485,8 @@ RQ_API int rq_server_result(rq_server* server, int request_id, float* rgb,
                             double* latency_s, double* queue_s);
 /* Frees a request's image and returns its bytes to the budget. */
 RQ_API int rq_server_release(rq_server* server, int request_id);
+/* ray_counts[0]: extension rays of paths plus ray-query rays; [1]: shadow
+ * rays. */
 RQ_API int rq_server_stats(rq_server* server, uint64_t* ray_counts, long long* steps,
                            int* pending, int* active, size_t* bytes_in_use);
 RQ_API int rq_server_destroy(rq_server* server);

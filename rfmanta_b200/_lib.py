@@ -119,6 +119,11 @@ class ServerStepRecord(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServeQuery(C.Structure):
+    _fields_ = [("scene", C.c_int), ("n", C.c_int), ("flags", C.c_int),
+                ("org", C.c_void_p), ("dir", C.c_void_p), ("tmax", C.c_void_p)]
+
+
 class ServeRequest(C.Structure):
     _fields_ = [("scene", C.c_int), ("eye", C.c_float * 3), ("lookat", C.c_float * 3),
                 ("up", C.c_float * 3), ("hfov", C.c_float), ("vfov", C.c_float),
@@ -188,6 +193,9 @@ def _load():
         "rq_queue_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                             C.POINTER(C.c_longlong)], i),
         "rq_queue_destroy": ([vp], i),
+        "rq_server_submit_query": ([vp, C.POINTER(ServeQuery), C.POINTER(i)], i),
+        "rq_server_query_result": ([vp, i, vp, vp, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)], i),
         "rq_server_run_stream": ([vp, vp, vp, i, vp, vp, vp, C.POINTER(C.c_double), C.c_double],
                                  i),
         "rq_server_set_profile": ([vp, i], i),

@@ -25,39 +25,11 @@
 #include <vector>
 
 #include "../../include/rfmanta_b200.h"
+#include "rq_batch.h"
 #include "rq_scene.h"
 #include "rq_traverse.cuh"
 
 namespace rq {
-
-constexpr int kMaxBatchScenes = 32;
-
-struct BatchDesc {
-  int scene;
-  int n;
-  int any;
-  int chunk0;  // first chunk index of this batch
-  const float* org;
-  const float* dir;
-  const float* tmax;
-  float* t;
-  int32_t* prim;
-  float* u;
-  float* v;
-};
-
-struct BatchArgs {
-  const DevScene* scenes;
-  int n_scenes;
-  const BatchDesc* batches;
-  int n_batches;
-  int total_chunks;
-  int chunk_rays;
-  int refill;
-  int stack_depth;  // shared-memory entries per thread
-  int* counter;
-  unsigned long long* stats;  // STATS kernels: box tests, triangle tests
-};
 
 template <int KIND, int R, bool STATS>
 __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
@@ -111,7 +83,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
           my_ray = w_next + (int)__popc(need & lt);
           my_scene = B.scene;
           my_any = B.any != 0;
-          const int n = B.n;
+          const int n = B.stride ? B.stride : B.n;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             r.o[c] = __ldg(B.org + (size_t)c * n + my_ray);
@@ -185,6 +157,27 @@ static cudaError_t batch_dispatch(int kind, int reg, bool stats, bool launch, in
   if (kind == kWald)
     return batch_dispatch_kind<kWald>(reg, stats, launch, grid, block, smem, A, st, fn);
   return batch_dispatch_kind<kKS>(reg, stats, launch, grid, block, smem, A, st, fn);
+}
+
+cudaError_t launch_batch(int tri_kind, int reg_stack, const BatchArgs& A, int grid, int block,
+                         size_t smem, cudaStream_t st) {
+  const void* f = nullptr;
+  batch_dispatch(tri_kind, reg_stack, A.stats != nullptr, false, 0, 0, 0, A, nullptr, &f);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return batch_dispatch(tri_kind, reg_stack, A.stats != nullptr, true, grid, block, smem, A, st,
+                        nullptr);
+}
+
+int batch_blocks_per_sm(int tri_kind, int reg_stack, int block, size_t smem) {
+  const void* f = nullptr;
+  BatchArgs A{};
+  batch_dispatch(tri_kind, reg_stack, false, false, 0, 0, 0, A, nullptr, &f);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, block, smem) != cudaSuccess) b = 1;
+  return std::max(1, b);
 }
 
 }  // namespace rq
@@ -355,6 +348,7 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
     d.prim = q.d_prim;
     d.u = q.d_u;
     d.v = q.d_v;
+    d.stride = 0;
     const long long c = ((long long)q.n + cfg.chunk_rays - 1) / cfg.chunk_rays;
     if (chunks + c > (1LL << 30)) return bfail(RQ_ERR_CAPACITY, "too many chunks");
     chunks += (int)c;

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../../include/rfmanta_b200.h"
+#include "rq_batch.h"
 #include "rq_pathcore.cuh"
 #include "rq_render.h"
 #include "rq_scene.h"
@@ -315,6 +316,15 @@ int sfail(int code, const std::string& m) {
 
 struct HostReq {
   int id = 0;
+  // a ray-query request: n_rays rays of one scene, closest or any hit,
+  // copied to the device on admission and traced in chunks of the steps
+  bool query = false;
+  int n_rays = 0;
+  int flags = 0;
+  std::vector<float> rays;    // host copy: org 3n, dir 3n, tmax n
+  float* d_rays = nullptr;    // the same on the device
+  float* d_res = nullptr;     // t n, prim n
+  int next_ray = 0;
   rq_serve_request spec{};
   std::vector<float> materials;
   rq::ServeReq dev{};  // parameters as the kernels see them (out, materials set on admission)
@@ -382,6 +392,14 @@ struct rq_server {
   // again before the next step
   std::vector<uint64_t> generations;
   std::vector<rq::DevScene> host_scenes;
+  // ray-query chunks of a step: descriptors for the batched traversal
+  // kernel (pinned staging per ring slot, one device table) and its counter
+  static const int kMaxQueryDescs = 1024;
+  rq::BatchDesc* h_qdesc[kRing] = {};
+  rq::BatchDesc* d_qdesc = nullptr;
+  int* d_qcounter = nullptr;
+  int qgrid = 1;
+  unsigned long long query_rays = 0;
   // per-step records (rq_server_set_profile): timing events around each
   // step's kernels, the record of the step in each ring slot until its end
   // event has been seen, finished records
@@ -413,8 +431,14 @@ struct rq_server {
       HostReq& r = *kv.second;
       if (r.d_out) cudaFreeAsync(r.d_out, stream);
       if (r.d_mat) cudaFreeAsync(r.d_mat, stream);
+      if (r.d_rays) cudaFreeAsync(r.d_rays, stream);
+      if (r.d_res) cudaFreeAsync(r.d_res, stream);
       if (r.done_ev) cudaEventDestroy(r.done_ev);
     }
+    if (stream) cudaStreamSynchronize(stream);
+    cudaFree(d_qdesc);
+    cudaFree(d_qcounter);
+    for (int i = 0; i < kRing; ++i) cudaFreeHost(h_qdesc[i]);
     cudaFree(B.o); cudaFree(B.d); cudaFree(B.imp); cudaFree(B.rad); cudaFree(B.rng);
     cudaFree(B.t); cudaFree(B.pos); cudaFree(B.prim); cudaFree(B.queue[0]); cudaFree(B.queue[1]);
     cudaFree(B.counters); cudaFree(B.alive); cudaFree(B.tile_counts);
@@ -434,6 +458,7 @@ struct rq_server {
   }
 
   bool admit(HostReq& r) {
+    if (r.query) return admit_query(r);
     const size_t need = r.bytes + r.materials.size() * sizeof(float);
     if ((int)active.size() >= max_active || used + need > budget) return false;
     // stream-ordered allocation: no device-wide synchronisation while
@@ -450,6 +475,27 @@ struct rq_server {
     cudaEventCreateWithFlags(&r.done_ev, cudaEventDisableTiming);
     r.dev.P.materials = r.d_mat;
     r.dev.out = r.d_out;
+    used += need;
+    r.admitted = true;
+    r.t_admit = now_s();
+    active.push_back(r.id);
+    return true;
+  }
+
+  // A ray query holds its rays (28 B each) and results (8 B each) on the
+  // device from admission to release.
+  bool admit_query(HostReq& r) {
+    const size_t need = r.bytes;
+    if ((int)active.size() >= max_active || used + need > budget) return false;
+    const size_t n = (size_t)r.n_rays;
+    if (cudaMallocFromPoolAsync(&r.d_rays, 28 * n, pool, stream) != cudaSuccess) return false;
+    if (cudaMallocFromPoolAsync(&r.d_res, 8 * n, pool, stream) != cudaSuccess) {
+      cudaFreeAsync(r.d_rays, stream);
+      r.d_rays = nullptr;
+      return false;
+    }
+    cudaMemcpyAsync(r.d_rays, r.rays.data(), 28 * n, cudaMemcpyHostToDevice, stream);
+    cudaEventCreateWithFlags(&r.done_ev, cudaEventDisableTiming);
     used += need;
     r.admitted = true;
     r.t_admit = now_s();
@@ -543,8 +589,12 @@ int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capac
             cudaMalloc(&s->d_reqs, sizeof(ServeReq) * s->max_active) == cudaSuccess &&
             cudaMalloc(&s->d_chunks, sizeof(ServeChunk) * s->max_chunks) == cudaSuccess &&
             cudaMalloc(&s->d_scenes, sizeof(DevScene) * n_scenes) == cudaSuccess;
+  ok = ok && cudaMalloc(&s->d_qdesc, sizeof(BatchDesc) * rq_server::kMaxQueryDescs) == cudaSuccess &&
+       cudaMalloc(&s->d_qcounter, sizeof(int)) == cudaSuccess;
   for (int i = 0; ok && i < rq_server::kRing; ++i)
-    ok = cudaMallocHost(&s->h_reqs[i], sizeof(ServeReq) * s->max_active) == cudaSuccess &&
+    ok = cudaMallocHost(&s->h_qdesc[i], sizeof(BatchDesc) * rq_server::kMaxQueryDescs) ==
+             cudaSuccess &&
+         cudaMallocHost(&s->h_reqs[i], sizeof(ServeReq) * s->max_active) == cudaSuccess &&
          cudaMallocHost(&s->h_chunks[i], sizeof(ServeChunk) * s->max_chunks) == cudaSuccess &&
          cudaEventCreateWithFlags(&s->ring_ev[i], cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&s->end_ev[i], cudaEventDisableTiming) == cudaSuccess;
@@ -577,6 +627,7 @@ int rq_server_create(rq_scene* const* scenes, int n_scenes, long long path_capac
   }
   s->smem = (size_t)s->depth * 128 * sizeof(int2);
   s->grid = std::max(1, serve_blocks_per_sm(s->tri_kind, s->smem) * s->num_sms);
+  s->qgrid = std::max(1, batch_blocks_per_sm(s->tri_kind, 0, 128, s->smem) * s->num_sms);
   s->table.assign(s->max_active, 0);
   s->host_scenes = ds;
   for (Scene* sc : s->scenes) s->generations.push_back(sc->generation);
@@ -618,6 +669,55 @@ int rq_server_submit(rq_server* s, const rq_serve_request* q, int* request_id) {
   return RQ_OK;
 }
 
+int rq_server_submit_query(rq_server* s, const rq_serve_query* q, int* request_id) {
+  if (!s || !q || !request_id) return sfail(RQ_ERR_ARG, "NULL argument");
+  if (q->scene < 0 || q->scene >= s->n_scenes) return sfail(RQ_ERR_ARG, "scene index out of range");
+  if (q->n <= 0 || q->n > (1 << 30)) return sfail(RQ_ERR_ARG, "ray count in [1, 2^30]");
+  if (!q->org || !q->dir || !q->tmax) return sfail(RQ_ERR_ARG, "NULL ray arrays");
+  if (q->flags != RQ_CLOSEST && q->flags != RQ_ANYHIT) return sfail(RQ_ERR_ARG, "bad flags");
+  const size_t n = (size_t)q->n;
+  const size_t bytes = 36 * n;
+  if (bytes > s->budget) return sfail(RQ_ERR_CAPACITY, "query larger than the server's HBM budget");
+  std::unique_ptr<HostReq> r(new HostReq());
+  r->id = s->next_id++;
+  r->query = true;
+  r->n_rays = q->n;
+  r->flags = q->flags;
+  r->spec.scene = q->scene;
+  r->rays.resize(7 * n);
+  std::memcpy(r->rays.data(), q->org, 12 * n);
+  std::memcpy(r->rays.data() + 3 * n, q->dir, 12 * n);
+  std::memcpy(r->rays.data() + 6 * n, q->tmax, 4 * n);
+  r->bytes = bytes;
+  r->t_submit = now_s();
+  *request_id = r->id;
+  s->pending.push_back(r->id);
+  s->reqs[r->id] = std::move(r);
+  return RQ_OK;
+}
+
+int rq_server_query_result(rq_server* s, int request_id, float* t, int32_t* prim,
+                           double* latency_s, double* queue_s) {
+  if (!s) return sfail(RQ_ERR_ARG, "NULL server");
+  auto it = s->reqs.find(request_id);
+  if (it == s->reqs.end()) return sfail(RQ_ERR_ARG, "unknown request");
+  HostReq& r = *it->second;
+  if (!r.query) return sfail(RQ_ERR_ARG, "a render request: use rq_server_result");
+  if (!r.done) return sfail(RQ_ERR_STATE, "request not finished");
+  if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
+  const size_t n = (size_t)r.n_rays;
+  cudaError_t e = cudaStreamWaitEvent(s->copy_stream, r.done_ev, 0);
+  if (e == cudaSuccess && t)
+    e = cudaMemcpyAsync(t, r.d_res, 4 * n, cudaMemcpyDeviceToHost, s->copy_stream);
+  if (e == cudaSuccess && prim)
+    e = cudaMemcpyAsync(prim, r.d_res + n, 4 * n, cudaMemcpyDeviceToHost, s->copy_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->copy_stream);
+  if (e != cudaSuccess) return sfail(RQ_ERR_CUDA, "query result copy failed");
+  if (latency_s) *latency_s = r.t_done - r.t_submit;
+  if (queue_s) *queue_s = r.t_admit - r.t_submit;
+  return RQ_OK;
+}
+
 int rq_server_step(rq_server* s, int* scheduled_paths) {
   using namespace rq;
   if (!s) return sfail(RQ_ERR_ARG, "NULL server");
@@ -645,6 +745,7 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
       s->depth = depth;
       s->smem = (size_t)depth * 128 * sizeof(int2);
       s->grid = std::max(1, serve_blocks_per_sm(s->tri_kind, s->smem) * s->num_sms);
+      s->qgrid = std::max(1, batch_blocks_per_sm(s->tri_kind, 0, 128, s->smem) * s->num_sms);
     }
   }
   // admission in arrival order while the budget allows
@@ -653,11 +754,14 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
     if (!s->admit(r)) break;
     s->pending.pop_front();
   }
-  // requests with pixels left, round-robin from the cursor
-  std::vector<int> cand;
-  for (int id : s->active)
-    if (!s->reqs[id]->scheduled_all) cand.push_back(id);
-  if (cand.empty()) return RQ_OK;
+  // requests with work left, in admission order: renders and ray queries
+  std::vector<int> cand, qcand;
+  for (int id : s->active) {
+    const HostReq& r = *s->reqs[id];
+    if (r.scheduled_all) continue;
+    (r.query ? qcand : cand).push_back(id);
+  }
+  if (cand.empty() && qcand.empty()) return RQ_OK;
   const int slot = (int)(s->steps % rq_server::kRing);
   if (s->ring_used[slot] && cudaEventSynchronize(s->ring_ev[slot]) != cudaSuccess)
     return sfail(RQ_ERR_CUDA, "staging ring wait failed");
@@ -701,11 +805,57 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
   for (int id : cand)
     while (take(*s->reqs[id])) {
     }
-  if (n_chunks == 0) return RQ_OK;
+  // Ray-query chunks, oldest request first, up to kStepQueryRays rays per
+  // step: each chunk is one descriptor of the batched traversal kernel
+  // over a consecutive range of the request's rays (row stride = the
+  // request's ray count).
+  constexpr int kQueryChunk = 1 << 20;
+  constexpr long long kStepQueryRays = 8LL << 20;
+  constexpr int kQueryWarpRays = 128;
+  BatchDesc* hq = s->h_qdesc[slot];
+  int n_qdesc = 0, q_warp_chunks = 0;
+  long long qrays = 0;
+  std::vector<int> qstep;  // query requests with rays in this step
+  for (int id : qcand) {
+    HostReq& r = *s->reqs[id];
+    bool any_here = false;
+    while (r.next_ray < r.n_rays && qrays < kStepQueryRays &&
+           n_qdesc < rq_server::kMaxQueryDescs) {
+      const int cnt = (int)std::min<long long>(
+          {(long long)kQueryChunk, (long long)(r.n_rays - r.next_ray), kStepQueryRays - qrays});
+      const size_t n = (size_t)r.n_rays, r0 = (size_t)r.next_ray;
+      BatchDesc& d = hq[n_qdesc++];
+      d.scene = r.spec.scene;
+      d.n = cnt;
+      d.any = r.flags == RQ_ANYHIT;
+      d.chunk0 = q_warp_chunks;
+      d.org = r.d_rays + r0;
+      d.dir = r.d_rays + 3 * n + r0;
+      d.tmax = r.d_rays + 6 * n + r0;
+      d.t = r.d_res + r0;
+      d.prim = reinterpret_cast<int32_t*>(r.d_res + n) + r0;
+      d.u = nullptr;
+      d.v = nullptr;
+      d.stride = r.n_rays;
+      q_warp_chunks += (cnt + kQueryWarpRays - 1) / kQueryWarpRays;
+      qrays += cnt;
+      r.next_ray += cnt;
+      any_here = true;
+    }
+    if (r.next_ray >= r.n_rays) r.scheduled_all = true;
+    if (any_here) qstep.push_back(id);
+  }
+  if (n_chunks == 0 && n_qdesc == 0) return RQ_OK;
   cudaStream_t st = s->stream;
-  cudaError_t e = cudaMemcpyAsync(s->d_reqs, hreq, sizeof(ServeReq) * n_req, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s->d_chunks, hch, sizeof(ServeChunk) * n_chunks, cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaSuccess;
+  if (n_chunks > 0) {
+    e = cudaMemcpyAsync(s->d_reqs, hreq, sizeof(ServeReq) * n_req, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->d_chunks, hch, sizeof(ServeChunk) * n_chunks, cudaMemcpyHostToDevice,
+                          st);
+  }
+  if (e == cudaSuccess && n_qdesc > 0)
+    e = cudaMemcpyAsync(s->d_qdesc, hq, sizeof(BatchDesc) * n_qdesc, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaEventRecord(s->ring_ev[slot], st);
   s->ring_used[slot] = true;
   if (s->profile) {
@@ -725,28 +875,52 @@ int rq_server_step(rq_server* s, int* scheduled_paths) {
     s->prof_open[slot] = true;
     if (e == cudaSuccess) e = cudaEventRecord(s->prof_start[slot], st);
   }
-  ServeArgs A;
-  A.scenes = s->d_scenes;
-  A.n_scenes = s->n_scenes;
-  A.reqs = s->d_reqs;
-  A.chunks = s->d_chunks;
-  A.n_chunks = n_chunks;
-  A.n_slots = (int)slots;
-  A.n_pix = (int)pix;
-  A.slot_req = s->slot_req;
-  A.slot_g = s->slot_g;
-  if (e == cudaSuccess)
+  // the step's ray queries: one persistent launch of the batched kernel
+  if (e == cudaSuccess && n_qdesc > 0) {
+    BatchArgs Q{};
+    Q.scenes = s->d_scenes;
+    Q.n_scenes = s->n_scenes;
+    Q.batches = s->d_qdesc;
+    Q.n_batches = n_qdesc;
+    Q.total_chunks = q_warp_chunks;
+    Q.chunk_rays = kQueryWarpRays;
+    Q.refill = 8;
+    Q.stack_depth = s->depth;
+    Q.counter = s->d_qcounter;
+    Q.stats = nullptr;
+    e = cudaMemsetAsync(s->d_qcounter, 0, sizeof(int), st);
+    const int qg = std::max(1, std::min(s->qgrid, (q_warp_chunks * 32 + 127) / 128));
+    if (e == cudaSuccess) e = launch_batch(s->tri_kind, 0, Q, qg, 128, s->smem, st);
+    s->query_rays += (unsigned long long)qrays;
+  }
+  // the step's path chunks: one wavefront over all of them
+  if (e == cudaSuccess && n_chunks > 0) {
+    ServeArgs A;
+    A.scenes = s->d_scenes;
+    A.n_scenes = s->n_scenes;
+    A.reqs = s->d_reqs;
+    A.chunks = s->d_chunks;
+    A.n_chunks = n_chunks;
+    A.n_slots = (int)slots;
+    A.n_pix = (int)pix;
+    A.slot_req = s->slot_req;
+    A.slot_g = s->slot_g;
     e = s->tri_kind == kWald ? serve_launch_step<kWald>(A, s->B, max_depth, s->grid, s->smem, st)
                              : serve_launch_step<kKS>(A, s->B, max_depth, s->grid, s->smem, st);
+  }
   if (e != cudaSuccess) return sfail(RQ_ERR_CUDA, std::string("serve step: ") + cudaGetErrorString(e));
   for (auto& kv : tidx) {
     HostReq& r = *s->reqs[kv.first];
     if (r.scheduled_all) cudaEventRecord(r.done_ev, st);
   }
+  for (int id : qstep) {
+    HostReq& r = *s->reqs[id];
+    if (r.scheduled_all) cudaEventRecord(r.done_ev, st);
+  }
   cudaEventRecord(s->end_ev[slot], st);
   if (s->profile) cudaEventRecord(s->prof_end[slot], st);
   ++s->steps;
-  if (scheduled_paths) *scheduled_paths = (int)slots;
+  if (scheduled_paths) *scheduled_paths = (int)std::min<long long>(slots + qrays, 1LL << 30);
   // keep at most two steps in flight: wait for the end of the step before
   // the one just enqueued
   if (s->steps >= 2) {
@@ -785,6 +959,7 @@ int rq_server_result(rq_server* s, int request_id, float* rgb, double* latency_s
   auto it = s->reqs.find(request_id);
   if (it == s->reqs.end()) return sfail(RQ_ERR_ARG, "unknown request");
   HostReq& r = *it->second;
+  if (r.query) return sfail(RQ_ERR_ARG, "a ray-query request: use rq_server_query_result");
   if (!r.done) return sfail(RQ_ERR_STATE, "request not finished");
   if (cudaSetDevice(s->device) != cudaSuccess) return sfail(RQ_ERR_CUDA, "cudaSetDevice");
   if (rgb && (cudaStreamWaitEvent(s->copy_stream, r.done_ev, 0) != cudaSuccess ||
@@ -807,6 +982,8 @@ int rq_server_release(rq_server* s, int request_id) {
   if (r.admitted) s->used -= r.bytes + r.materials.size() * sizeof(float);
   if (r.d_out) cudaFreeAsync(r.d_out, s->stream);
   if (r.d_mat) cudaFreeAsync(r.d_mat, s->stream);
+  if (r.d_rays) cudaFreeAsync(r.d_rays, s->stream);
+  if (r.d_res) cudaFreeAsync(r.d_res, s->stream);
   if (r.done_ev) cudaEventDestroy(r.done_ev);
   if (!r.admitted) {
     for (auto p = s->pending.begin(); p != s->pending.end(); ++p)
@@ -827,6 +1004,7 @@ int rq_server_stats(rq_server* s, uint64_t* ray_counts, long long* steps, int* p
     cudaStreamSynchronize(s->stream);
     if (cudaMemcpy(ray_counts, s->counts, 16, cudaMemcpyDeviceToHost) != cudaSuccess)
       return sfail(RQ_ERR_CUDA, "counter copy failed");
+    ray_counts[0] += s->query_rays;  // ray-query rays count as traced rays
   }
   if (steps) *steps = s->steps;
   if (pending) *pending = (int)s->pending.size();

@@ -78,6 +78,27 @@ class RenderServer:
         check(lib.rq_server_submit(self._h, C.byref(q), C.byref(rid)))
         return rid.value
 
+    def submit_query(self, scene: int, org, dir, tmax, anyhit: bool = False) -> int:
+        """A ray-query request: host arrays (3, n), (3, n), (n,) float32,
+        copied on submit; traced by the server's steps beside the renders."""
+        o = np.ascontiguousarray(org, np.float32)
+        d = np.ascontiguousarray(dir, np.float32)
+        tm = np.ascontiguousarray(tmax, np.float32)
+        q = _lib.ServeQuery(scene, int(tm.shape[0]), _lib.RQ_ANYHIT if anyhit else _lib.RQ_CLOSEST,
+                            o.ctypes.data, d.ctypes.data, tm.ctypes.data)
+        rid = C.c_int()
+        check(lib.rq_server_submit_query(self._h, C.byref(q), C.byref(rid)))
+        return rid.value
+
+    def query_result(self, rid: int, n: int):
+        """(t, triangle id, latency s, admission wait s) of a finished query."""
+        t = np.empty(n, np.float32)
+        prim = np.empty(n, np.int32)
+        lat, qs = C.c_double(), C.c_double()
+        check(lib.rq_server_query_result(self._h, rid, t.ctypes.data, prim.ctypes.data,
+                                         C.byref(lat), C.byref(qs)))
+        return t, prim, lat.value, qs.value
+
     def step(self) -> int:
         n = C.c_int()
         check(lib.rq_server_step(self._h, C.byref(n)))

@@ -134,3 +134,86 @@ def test_server_follows_scene_updates():
                               r.seed)
         assert np.array_equal(_bits(img), _bits(bvh.render_path(ps)["rgb"]))
     srv.close()
+
+
+def test_ray_queries_beside_renders(scenes3):
+    """Ray-query requests (closest and any hit, 1 to 2.5M rays, beyond one
+    step's 8Mi-ray budget in total) are served in the same steps as render
+    requests: every query's t and triangle ids equal rq_trace on the same
+    rays, and every render equals the same request rendered alone."""
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.dynbvh import RayBatch
+    from rfmanta_b200.serve import RenderServer
+    meshes, bvhs = scenes3
+    reqs = _requests(meshes)[:4]
+    queries = []
+    for k, (si, n, anyhit) in enumerate([(0, 1, False), (1, 5000, True), (2, 2_500_000, False),
+                                         (0, 300_000, True), (1, 2_600_000, False),
+                                         (2, 3_100_000, True)]):
+        lo, hi = meshes[si].bounds()
+        o, d, tm, _ = scenes.random_rays(n, lo - 0.2, hi + 0.2, seed=900 + k,
+                                         anyhit_fraction=1.0 if anyhit else 0.0)
+        if not anyhit:
+            tm = np.full(n, 1e19, np.float32)
+        queries.append((si, o, d, tm, anyhit))
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000)
+    alone = _run(srv, reqs)
+    srv.close()
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000)
+    rids, qids = [], []
+    for i in range(max(len(reqs), len(queries))):
+        if i < len(queries):
+            si, o, d, tm, anyhit = queries[i]
+            qids.append(srv.submit_query(si, o, d, tm, anyhit))
+        if i < len(reqs):
+            rids.append(srv.submit(reqs[i]))
+    imgs, qres = {}, {}
+    for _ in range(100000):
+        srv.step()
+        for rid in srv.poll():
+            if rid in qids:
+                k = qids.index(rid)
+                t, prim, lat, _ = srv.query_result(rid, queries[k][3].shape[0])
+                qres[k] = (t, prim)
+            else:
+                k = rids.index(rid)
+                imgs[k], _, _ = srv.result(rid, reqs[k].xres, reqs[k].yres)
+            srv.release(rid)
+        if len(imgs) == len(reqs) and len(qres) == len(queries):
+            break
+    st = srv.stats()
+    srv.close()
+    assert len(imgs) == len(reqs) and len(qres) == len(queries)
+    for k in range(len(reqs)):
+        assert np.array_equal(_bits(imgs[k]), _bits(alone[k])), k
+    for k, (si, o, d, tm, anyhit) in enumerate(queries):
+        r = RayBatch(o, d, tm, flags=RayBatch.AnyHit if anyhit else 0)
+        bvhs[si].intersect(r)
+        t, prim = qres[k]
+        if anyhit:
+            assert np.array_equal(prim >= 0, r.wasHit()), k
+        else:
+            assert np.array_equal(prim, r.hitPrim), k
+            assert np.array_equal(_bits(t), _bits(r.minT)), k
+    assert st["rays"] >= sum(q[1].shape[1] for q in queries)
+
+
+def test_query_errors(scenes3):
+    import ctypes as C
+    from rfmanta_b200 import _lib
+    from rfmanta_b200.serve import RenderServer
+    meshes, bvhs = scenes3
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000)
+    o = np.zeros((3, 4), np.float32)
+    q = _lib.ServeQuery(7, 4, 0, o.ctypes.data, o.ctypes.data, o[0].ctypes.data)
+    rid = C.c_int()
+    assert _lib.lib.rq_server_submit_query(srv._h, C.byref(q), C.byref(rid)) == _lib.RQ_ERR_ARG
+    q.scene, q.flags = 0, 5
+    assert _lib.lib.rq_server_submit_query(srv._h, C.byref(q), C.byref(rid)) == _lib.RQ_ERR_ARG
+    q.flags = 0
+    _lib.check(_lib.lib.rq_server_submit_query(srv._h, C.byref(q), C.byref(rid)))
+    # a query's result is not an image, and not ready before it ran
+    assert _lib.lib.rq_server_result(srv._h, rid.value, None, None, None) == _lib.RQ_ERR_ARG
+    assert _lib.lib.rq_server_query_result(srv._h, rid.value, None, None, None,
+                                           None) == _lib.RQ_ERR_STATE
+    srv.close()

@@ -217,3 +217,34 @@ def test_query_errors(scenes3):
     assert _lib.lib.rq_server_query_result(srv._h, rid.value, None, None, None,
                                            None) == _lib.RQ_ERR_STATE
     srv.close()
+
+
+def test_run_stream_in_the_library(scenes3):
+    """rq_server_run_stream: a timed arrival stream submitted, stepped and
+    collected inside the library; every image equals the request rendered
+    alone by rq_render_path, every request has a latency, and the per-step
+    records account for every step and path."""
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.serve import RenderServer
+    meshes, bvhs = scenes3
+    reqs = _requests(meshes)
+    stream = [(0.002 * i, r) for i, r in enumerate(reqs)]
+    srv = RenderServer(bvhs, path_capacity=1 << 16, chunk_pixels=1000)
+    srv.set_profile(True)
+    b0 = srv.stats()
+    out = srv.run_stream(stream, keep_images=True, timeout_s=120.0)
+    st = srv.stats()
+    prof = srv.profile()
+    srv.close()
+    assert len(out["info"]) == len(reqs) and out["wall_s"] > 0
+    for i, r in enumerate(reqs):
+        ps = scenes.PathScene(meshes[r.scene], scenes.Camera(r.eye, r.lookat, r.up, r.hfov, r.vfov),
+                              scenes.AreaLightSpec(r.light_anchor, r.light_v1, r.light_v2,
+                                                   r.light_color),
+                              r.background, r.xres, r.yres, r.spp, r.max_depth, r.rr_depth, r.seed)
+        want = bvhs[r.scene].render_path(ps)["rgb"]
+        assert np.array_equal(_bits(out["info"][i]["image"]), _bits(want)), i
+        assert out["info"][i]["latency"] > 0
+    assert len(prof) == st["steps"] - b0["steps"]
+    assert sum(p["paths"] for p in prof) == sum(r.xres * r.yres * r.spp for r in reqs)
+    assert all(p["gpu_ms"] > 0 for p in prof)

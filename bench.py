@@ -197,7 +197,9 @@ class PathFrame:
         for d in range(self.sc.max_depth):
             self.stage_names += [f"path_extend_persistent_kernel[{d}]", f"path_shade_persistent_kernel[{d}]"]
         self.stage_names.append("path_resolve_kernel")
-        self.launches = 1 + 3 * self.sc.max_depth + 1
+        # per frame: generate and resolve, and per bounce the ray count,
+        # extension, shade and the three ordered-compaction kernels
+        self.launches = 2 + 6 * self.sc.max_depth
 
     def frame(self, stream_ptr):
         self.bvh.render_path_device(self.params, self.rgb.data_ptr(), self.counts.data_ptr(),

@@ -102,9 +102,22 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
       }
     }
     if (exhausted && __all_sync(0xffffffffu, my_ray < 0)) break;
+    // Work is ordered scene by scene, closest-hit batches before any-hit
+    // ones, so a warp's busy lanes almost always share the query kind: the
+    // step is then compiled for that kind (the per-lane form only where
+    // kinds meet).
+    const bool stepping = my_ray >= 0 && ref != kDone;
+    const unsigned any_m = __ballot_sync(0xffffffffu, stepping && my_any);
+    const unsigned clo_m = __ballot_sync(0xffffffffu, stepping && !my_any);
     if (my_ray >= 0) {
-      if (ref != kDone)
-        step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, my_any, &cnt);
+      if (stepping) {
+        if (any_m == 0u)
+          step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, false, &cnt);
+        else if (clo_m == 0u)
+          step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, true, &cnt);
+        else
+          step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, my_any, &cnt);
+      }
       if (ref == kDone) {
         const BatchDesc& B = A.batches[my_batch];
         if (B.t) B.t[my_ray] = h.t;

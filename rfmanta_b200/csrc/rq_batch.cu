@@ -111,12 +111,18 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
     const unsigned clo_m = __ballot_sync(0xffffffffu, stepping && !my_any);
     if (my_ray >= 0) {
       if (stepping) {
+        // the lane's scene descriptor copied to registers: the step's stack
+        // stores go to shared memory too, and a descriptor read from there
+        // would be read again after every store
+        DevScene S;
+        S.nodes = sm_scenes[my_scene].nodes;
+        S.tris = sm_scenes[my_scene].tris;
         if (any_m == 0u)
-          step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, false, &cnt);
+          step_dyn<KIND, R, STATS>(S, r, h, ref, st, false, &cnt);
         else if (clo_m == 0u)
-          step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, true, &cnt);
+          step_dyn<KIND, R, STATS>(S, r, h, ref, st, true, &cnt);
         else
-          step_dyn<KIND, R, STATS>(sm_scenes[my_scene], r, h, ref, st, my_any, &cnt);
+          step_dyn<KIND, R, STATS>(S, r, h, ref, st, my_any, &cnt);
       }
       if (ref == kDone) {
         const BatchDesc& B = A.batches[my_batch];

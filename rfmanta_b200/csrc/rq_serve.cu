@@ -143,7 +143,14 @@ __global__ void __launch_bounds__(128) serve_extend_kernel(ServeArgs A, PathBuff
     }
     if (__all_sync(0xffffffffu, exhausted)) break;
     if (p >= 0) {
-      if (ref != kDone) step<KIND, false>(sm_scenes[scene], r, h, ref, sp, stk, stride);
+      if (ref != kDone) {
+        // scene pointers in registers: the stack stores would otherwise make
+        // every node visit read them from shared memory again
+        DevScene S;
+        S.nodes = sm_scenes[scene].nodes;
+        S.tris = sm_scenes[scene].tris;
+        step<KIND, false>(S, r, h, ref, sp, stk, stride);
+      }
       if (ref == kDone) {
         store_extension(R->P, B, depth, p, r, h);
         p = -1;
@@ -205,7 +212,12 @@ __global__ void __launch_bounds__(128) serve_shade_kernel(ServeArgs A, PathBuffe
     if (__all_sync(0xffffffffu, exhausted)) break;
     bool fin = false;
     if (p >= 0) {
-      if (ref != kDone) step<KIND, true>(sm_scenes[scene], sr, sh, ref, sp, stk, stride);
+      if (ref != kDone) {
+        DevScene S;
+        S.nodes = sm_scenes[scene].nodes;
+        S.tris = sm_scenes[scene].tris;
+        step<KIND, true>(S, sr, sh, ref, sp, stk, stride);
+      }
       if (ref == kDone) {
         if (traced && sh.id < 0) shade_finish(B, p, contrib);
         fin = true;

@@ -387,6 +387,11 @@ typedef struct {
   int refill_threshold; /* idle lanes before a warp refills, 1..32 */
   int reg_stack;        /* traversal-stack entries kept in registers: 0, 1, 2, 4 */
   int node_layout;      /* order of the node records in HBM (RQ_LAYOUT_*) */
+  int smem_entries;     /* 0 = the whole traversal stack in shared memory;
+                           k in 1..64 = the first k entries of each thread in
+                           shared memory and deeper ones in a global-memory
+                           area the plan owns, with registers held to 48 per
+                           thread, so more warps fit on an SM (reg_stack 0) */
 } rq_batch_config;
 
 
@@ -409,8 +414,9 @@ RQ_API int rq_batch_plan_destroy(rq_batch_plan* plan);
  * search: block size x rays per warp chunk x refill threshold (the
  * compaction threshold of the persistent loop) with the stack in shared
  * memory and depth-first records, then register-stack entries (0, 1, 2, 4)
- * x node layout (RQ_LAYOUT_*) at the best of those, then chunk x refill
- * again at the best stack and layout. */
+ * x node layout (RQ_LAYOUT_*) at the best of those, then a short shared
+ * stack column with an overflow area (smem_entries 8, 12, 16), then chunk x
+ * refill again at the best stack and layout. */
 RQ_API int rq_batch_autotune(rq_scene* const* scenes, int n_scenes,
                              const rq_batch* batches, int n_batches,
                              const rq_batch_config* candidates, int n_candidates,

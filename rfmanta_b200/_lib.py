@@ -104,7 +104,7 @@ class Batch(C.Structure):
 class BatchConfig(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int),
                 ("chunk_rays", C.c_int), ("refill_threshold", C.c_int), ("reg_stack", C.c_int),
-                ("node_layout", C.c_int)]
+                ("node_layout", C.c_int), ("smem_entries", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

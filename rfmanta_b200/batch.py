@@ -62,6 +62,7 @@ class BatchedQueries:
         c.refill_threshold = config.get("refill_threshold", 8)
         c.reg_stack = config.get("reg_stack", 0)
         c.node_layout = config.get("node_layout", 0)
+        c.smem_entries = config.get("smem_entries", 0)
         return c
 
     def make_plan(self, config: dict | None = None) -> None:

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/rfmanta_b200.h"
@@ -31,22 +32,37 @@
 
 namespace rq {
 
-template <int KIND, int R, bool STATS>
-__global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
+// Resets a lane's traversal stack: a RegStack over the thread's shared
+// column, or a SplitStack whose first A.stack_depth entries sit there and
+// whose deeper ones go to the thread's entries of the overflow area.
+template <int R>
+__device__ __forceinline__ void reset_stack(RegStack<R>& st, int2* smem, const BatchArgs&) {
+  st.init(smem + threadIdx.x, blockDim.x);
+}
+__device__ __forceinline__ void reset_stack(SplitStack& st, int2* smem, const BatchArgs& A) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  st.init(smem + threadIdx.x, A.stack_depth, A.ovf + g);
+}
+
+// SPLIT: the stack is a SplitStack with a short shared column, and
+// registers are held to 48 per thread (five 256-thread blocks per SM), so
+// more warps are resident to hide the traversal's dependent loads.
+template <int KIND, int R, bool STATS, bool SPLIT>
+__global__ void __launch_bounds__(256, SPLIT ? 5 : 1) batch_kernel(BatchArgs A) {
   extern __shared__ int2 smem[];
   __shared__ DevScene sm_scenes[kMaxBatchScenes];
   for (int i = threadIdx.x; i < A.n_scenes; i += blockDim.x) sm_scenes[i] = A.scenes[i];
   __syncthreads();
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
-  RegStack<R> st;
-  st.init(smem + threadIdx.x, blockDim.x);
+  typename std::conditional<SPLIT, SplitStack, RegStack<R>>::type st;
+  reset_stack(st, smem, A);
   // warp-uniform chunk state
   int w_batch = 0, w_next = 0, w_end = 0;
   bool exhausted = false;
   // lane state
-  int my_ray = -1, my_batch = 0, my_scene = 0;
-  bool my_any = false;
+  int my_ray = -1;
+  int my_tag = 0;  // batch << 6 | scene << 1 | any hit (one register for the three)
   Ray r;
   Hit h;
   int ref = kDone;
@@ -79,10 +95,8 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
         const bool take = ((need >> lane) & 1u) && (int)__popc(need & lt) < k;
         if (take) {
           const BatchDesc& B = A.batches[w_batch];
-          my_batch = w_batch;
           my_ray = w_next + (int)__popc(need & lt);
-          my_scene = B.scene;
-          my_any = B.any != 0;
+          my_tag = (w_batch << 6) | (B.scene << 1) | (B.any != 0);
           const int n = B.stride ? B.stride : B.n;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
@@ -92,8 +106,8 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
           }
           r.minT = __ldg(B.tmax + my_ray);
           int sp0;
-          start_ray(sm_scenes[my_scene], r, h, ref, sp0);
-          st.init(smem + threadIdx.x, blockDim.x);
+          start_ray(sm_scenes[B.scene], r, h, ref, sp0);
+          reset_stack(st, smem, A);
           if (STATS) cnt.boxes += 1;
         }
         const unsigned taken = __ballot_sync(0xffffffffu, take);
@@ -107,6 +121,8 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
     // step is then compiled for that kind (the per-lane form only where
     // kinds meet).
     const bool stepping = my_ray >= 0 && ref != kDone;
+    const bool my_any = (my_tag & 1) != 0;
+    const int my_scene = (my_tag >> 1) & 31;
     const unsigned any_m = __ballot_sync(0xffffffffu, stepping && my_any);
     const unsigned clo_m = __ballot_sync(0xffffffffu, stepping && !my_any);
     if (my_ray >= 0) {
@@ -125,7 +141,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
           step_dyn<KIND, R, STATS>(S, r, h, ref, st, my_any, &cnt);
       }
       if (ref == kDone) {
-        const BatchDesc& B = A.batches[my_batch];
+        const BatchDesc& B = A.batches[my_tag >> 6];
         if (B.t) B.t[my_ray] = h.t;
         if (B.prim) B.prim[my_ray] = h.id;
         if (B.u) B.u[my_ray] = h.u;
@@ -140,21 +156,26 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs A) {
   }
 }
 
-template <int KIND, int R, bool STATS>
+template <int KIND, int R, bool STATS, bool SPLIT = false>
 static cudaError_t batch_go(bool launch, int grid, int block, size_t smem, const BatchArgs& A,
                             cudaStream_t st, const void** fn) {
-  if (fn) *fn = (const void*)batch_kernel<KIND, R, STATS>;
-  if (launch) batch_kernel<KIND, R, STATS><<<grid, block, smem, st>>>(A);
+  if (fn) *fn = (const void*)batch_kernel<KIND, R, STATS, SPLIT>;
+  if (launch) batch_kernel<KIND, R, STATS, SPLIT><<<grid, block, smem, st>>>(A);
   return launch ? cudaGetLastError() : cudaSuccess;
 }
 
 // Resolves (triangle kind, register stack, statistics) to one kernel and
-// either returns its address or launches it.
+// either returns its address or launches it; reg = kSplitStack selects the
+// split-stack kernel.
+constexpr int kSplitStack = -1;
 template <int KIND>
 static cudaError_t batch_dispatch_kind(int reg, bool stats, bool launch, int grid, int block,
                                        size_t smem, const BatchArgs& A, cudaStream_t st,
                                        const void** fn) {
   switch (reg) {
+    case kSplitStack:
+      return stats ? batch_go<KIND, 0, true, true>(launch, grid, block, smem, A, st, fn)
+                   : batch_go<KIND, 0, false, true>(launch, grid, block, smem, A, st, fn);
     case 1:
       return stats ? batch_go<KIND, 1, true>(launch, grid, block, smem, A, st, fn)
                    : batch_go<KIND, 1, false>(launch, grid, block, smem, A, st, fn);
@@ -182,7 +203,9 @@ cudaError_t launch_batch(int tri_kind, int reg_stack, const BatchArgs& A, int gr
                          size_t smem, cudaStream_t st) {
   const void* f = nullptr;
   batch_dispatch(tri_kind, reg_stack, A.stats != nullptr, false, 0, 0, 0, A, nullptr, &f);
-  if (smem > 48 * 1024)
+  // static shared memory (the scene table) counts against the default 48 KB
+  // too, so the dynamic size is always declared
+  if (smem > 0)
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return batch_dispatch(tri_kind, reg_stack, A.stats != nullptr, true, grid, block, smem, A, st,
                         nullptr);
@@ -192,7 +215,7 @@ int batch_blocks_per_sm(int tri_kind, int reg_stack, int block, size_t smem) {
   const void* f = nullptr;
   BatchArgs A{};
   batch_dispatch(tri_kind, reg_stack, false, false, 0, 0, 0, A, nullptr, &f);
-  if (smem > 48 * 1024)
+  if (smem > 0)
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int b = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, block, smem) != cudaSuccess) b = 1;
@@ -209,6 +232,8 @@ struct rq_batch_plan {
   rq::DevScene* d_scenes = nullptr;
   rq::BatchDesc* d_batches = nullptr;
   int* d_counter = nullptr;
+  int2* d_ovf = nullptr;  // split-stack overflow area
+  size_t ovf_bytes = 0;
   int grid = 1;
   size_t smem = 0;
   long long total_rays = 0;
@@ -230,6 +255,7 @@ struct rq_batch_plan {
     cudaFree(d_scenes);
     cudaFree(d_batches);
     cudaFree(d_counter);
+    cudaFree(d_ovf);
   }
 };
 
@@ -248,6 +274,7 @@ rq_batch_config default_batch_config() {
   c.refill_threshold = 8;
   c.reg_stack = 0;
   c.node_layout = RQ_LAYOUT_DFS;
+  c.smem_entries = 0;
   return c;
 }
 
@@ -258,14 +285,18 @@ int capture_plan(rq_batch_plan* p) {
   using namespace rq;
   const rq_batch_config& cfg = p->cfg;
   BatchArgs& A = p->args;
-  A.stack_depth = p->stack_depth;
+  // split stack: the first smem_entries entries in shared memory, the rest
+  // of the deepest tree's entries in the overflow area
+  const bool split = cfg.smem_entries > 0;
+  const int reg = split ? kSplitStack : cfg.reg_stack;
+  A.stack_depth = split ? std::min(cfg.smem_entries, p->stack_depth) : p->stack_depth;
   // the shared-memory column holds what the register entries do not
-  p->smem = (size_t)std::max(1, p->stack_depth - cfg.reg_stack) * cfg.block_threads *
-            sizeof(int2);
+  p->smem = (size_t)std::max(1, A.stack_depth - (split ? 0 : cfg.reg_stack)) *
+            cfg.block_threads * sizeof(int2);
   const bool stats = A.stats != nullptr;
   const void* f = nullptr;
-  batch_dispatch(p->tri_kind, cfg.reg_stack, stats, false, 0, 0, 0, A, nullptr, &f);
-  if (p->smem > 48 * 1024 &&
+  batch_dispatch(p->tri_kind, reg, stats, false, 0, 0, 0, A, nullptr, &f);
+  if (p->smem > 0 &&
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem) !=
           cudaSuccess)
     return bfail(RQ_ERR_CAPACITY, "traversal stack does not fit in shared memory");
@@ -280,6 +311,21 @@ int capture_plan(rq_batch_plan* p) {
   const long long max_blocks =
       std::max(1LL, (warps_needed * 32 + cfg.block_threads - 1) / cfg.block_threads);
   p->grid = (int)std::max(1LL, std::min((long long)bps * p->num_sms, max_blocks));
+  if (split) {
+    const size_t need =
+        (size_t)(p->stack_depth - A.stack_depth) * p->grid * cfg.block_threads * sizeof(int2);
+    if (need > p->ovf_bytes) {
+      // launches of the graph captured before may still use the old area
+      cudaDeviceSynchronize();
+      cudaFree(p->d_ovf);
+      p->d_ovf = nullptr;
+      p->ovf_bytes = 0;
+      if (cudaMalloc(&p->d_ovf, need) != cudaSuccess)
+        return bfail(RQ_ERR_OOM, "traversal stack overflow area");
+      p->ovf_bytes = need;
+    }
+    A.ovf = p->d_ovf;
+  }
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
   p->exec = nullptr;
@@ -287,9 +333,35 @@ int capture_plan(rq_batch_plan* p) {
   cudaError_t e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     cudaMemsetAsync(p->d_counter, 0, sizeof(int), p->cap_stream);
-    batch_dispatch(p->tri_kind, cfg.reg_stack, stats, true, p->grid, cfg.block_threads, p->smem,
-                   A, p->cap_stream, nullptr);
+    batch_dispatch(p->tri_kind, reg, stats, true, p->grid, cfg.block_threads, p->smem, A,
+                   p->cap_stream, nullptr);
     e = cudaStreamEndCapture(p->cap_stream, &p->graph);
+  }
+  if (e == cudaSuccess && split) {
+    // split stack: the shared-memory carveout is set to what the resident
+    // blocks use (column + scene table + the per-block reservation), so the
+    // rest of the SM's L1/shared storage caches node and triangle records
+    int dev = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, f);
+    const size_t need = (size_t)bps * (p->smem + fa.sharedSizeBytes + 1024);
+    if (per_sm > 0) {
+      cudaLaunchAttributeValue v{};
+      v.sharedMemCarveout =
+          (unsigned)std::min<size_t>(100, (need * 100 + per_sm - 1) / per_sm);
+      size_t n = 0;
+      cudaGraphGetNodes(p->graph, nullptr, &n);
+      std::vector<cudaGraphNode_t> nodes(n);
+      cudaGraphGetNodes(p->graph, nodes.data(), &n);
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+          e = cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePreferredSharedMemoryCarveout,
+                                              &v);
+      }
+    }
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
   if (e != cudaSuccess) return bfail(RQ_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
@@ -308,6 +380,7 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
   if (!scenes || n_scenes <= 0 || n_scenes > kMaxBatchScenes)
     return bfail(RQ_ERR_ARG, "1..32 scenes");
   if (!batches || n_batches <= 0) return bfail(RQ_ERR_ARG, "no batches");
+  if (n_batches > (1 << 24)) return bfail(RQ_ERR_CAPACITY, "more than 2^24 batches");
   rq_batch_config cfg = cfg_in ? *cfg_in : default_batch_config();
   if (cfg.block_threads < 32 || cfg.block_threads > 256 || cfg.block_threads % 32)
     return bfail(RQ_ERR_ARG, "block_threads must be a multiple of 32 in [32, 256]");
@@ -319,6 +392,10 @@ int rq_batch_plan_create(rq_scene* const* scenes, int n_scenes, const rq_batch* 
     return bfail(RQ_ERR_ARG, "reg_stack is 0, 1, 2 or 4");
   if (cfg.node_layout < RQ_LAYOUT_DFS || cfg.node_layout > RQ_LAYOUT_BFS_TOP)
     return bfail(RQ_ERR_ARG, "node_layout is one of RQ_LAYOUT_*");
+  if (cfg.smem_entries < 0 || cfg.smem_entries > 64)
+    return bfail(RQ_ERR_ARG, "smem_entries must be in [0, 64]");
+  if (cfg.smem_entries > 0 && cfg.reg_stack != 0)
+    return bfail(RQ_ERR_ARG, "smem_entries > 0 takes reg_stack 0");
   const Scene* s0 = reinterpret_cast<const Scene*>(scenes[0]);
   if (!s0) return bfail(RQ_ERR_ARG, "NULL scene");
   if (cudaSetDevice(s0->device) != cudaSuccess) return bfail(RQ_ERR_CUDA, "cudaSetDevice");
@@ -530,6 +607,16 @@ int rq_batch_autotune(rq_scene* const* scenes, int n_scenes, const rq_batch* bat
         c.node_layout = nl;
         rc = time_one(c);
       }
+    // 2b. a short shared column with a global overflow area (more resident
+    //     warps) at the best shape and layout
+    const rq_batch_config lay = *best;
+    for (int se : {8, 12, 16}) {
+      if (rc != RQ_OK) break;
+      rq_batch_config c = lay;
+      c.reg_stack = 0;
+      c.smem_entries = se;
+      rc = time_one(c);
+    }
     // 3. chunk and refill again at the best stack and layout
     const rq_batch_config mid = *best;
     for (int cr : {64, 128, 256, 512})

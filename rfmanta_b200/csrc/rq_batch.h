@@ -39,6 +39,7 @@ struct BatchArgs {
   int chunk_rays;
   int refill;
   int stack_depth;  // shared-memory entries per thread
+  int2* ovf;        // split-stack kernels: overflow area (entry-major over the grid's threads)
   int* counter;
   unsigned long long* stats;  // STATS kernels: box tests, triangle tests
 };

@@ -305,7 +305,7 @@ static int serve_blocks_per_sm(int kind, size_t smem) {
                                      : (const void*)serve_shade_kernel<kKS>};
   int a = 1, b = 1;
   for (const void* f : fs)
-    if (smem > 48 * 1024)
+    if (smem > 0)  // the static scene table counts against the default 48 KB too
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, fs[0], 128, smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fs[1], 128, smem);

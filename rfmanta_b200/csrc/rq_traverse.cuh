@@ -210,12 +210,42 @@ struct RegStack {
   }
 };
 
+// Traversal stack split between shared memory and global memory: the first
+// `cap` entries of a thread live in its shared-memory column, deeper ones in
+// a global-memory area laid out entry-major over all threads of the launch
+// (entry k >= cap of thread g at ovf[(k - cap) * ostride + g]).  A kernel can
+// then keep a short shared column, so more blocks fit on an SM, and still
+// take trees of any depth.  LIFO order as in RegStack.
+struct SplitStack {
+  int2* col;  // this thread's shared column (stride blockDim.x)
+  int cap;
+  int2* ovf;  // this thread's first overflow entry (stride = threads of the grid)
+  int sp;
+  __device__ __forceinline__ void init(int2* c, int k, int2* o) {
+    col = c;
+    cap = k;
+    ovf = o;
+    sp = 0;
+  }
+  __device__ __forceinline__ void push(int2 e) {
+    if (sp < cap) col[sp * blockDim.x] = e;
+    else ovf[(size_t)(sp - cap) * (gridDim.x * blockDim.x)] = e;
+    ++sp;
+  }
+  __device__ __forceinline__ bool pop(int2& e) {
+    if (sp == 0) return false;
+    --sp;
+    e = sp < cap ? col[sp * blockDim.x] : ovf[(size_t)(sp - cap) * (gridDim.x * blockDim.x)];
+    return true;
+  }
+};
+
 // The while-while step with the any-hit flag decided per ray at run time
 // (a warp of the batched kernel may hold closest-hit and any-hit rays of
-// different batches and scenes at once) and a RegStack.
-template <int KIND, int R, bool STATS = false>
+// different batches and scenes at once) and a RegStack (or a SplitStack).
+template <int KIND, int R, bool STATS = false, class Stack = RegStack<R>>
 __device__ __forceinline__ void step_dyn(const DevScene& S, Ray& r, Hit& h, int& ref,
-                                         RegStack<R>& st, bool any, Counts* cnt = nullptr) {
+                                         Stack& st, bool any, Counts* cnt = nullptr) {
   const bool fast = inv_finite(r);
   while (ref >= 0 && ref != kDone) {
     if (STATS) cnt->boxes += 2;

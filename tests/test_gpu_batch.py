@@ -1,6 +1,7 @@
 """Batched multi-scene queries in one persistent, graph-captured launch:
 every configuration (block size, rays per warp chunk, refill threshold,
-register stack entries, node-record layout) and the autotuned one give, for
+register stack entries, node-record layout, split shared/global stack) and
+the autotuned one give, for
 every batch, the same bits as tracing that batch alone (rq_trace), which the
 other tests tie to the reference."""
 import numpy as np
@@ -71,7 +72,15 @@ def _check(bq, exp):
                                  dict(block_threads=128, chunk_rays=64, refill_threshold=8, reg_stack=4,
                                       node_layout=1),
                                  dict(block_threads=64, chunk_rays=128, refill_threshold=16, reg_stack=1,
-                                      node_layout=2)])
+                                      node_layout=2),
+                                 # split stack: 2 shared entries, the rest in the overflow area
+                                 dict(block_threads=256, chunk_rays=128, refill_threshold=8,
+                                      smem_entries=2),
+                                 dict(block_threads=96, chunk_rays=64, refill_threshold=4,
+                                      smem_entries=5, node_layout=1),
+                                 # split-stack kernel with a column deeper than every tree
+                                 dict(block_threads=128, chunk_rays=256, refill_threshold=16,
+                                      smem_entries=64, node_layout=2)])
 def test_batches_match_single_queries(setup, cfg):
     from rfmanta_b200.batch import BatchedQueries
     bvhs, batches, host = setup
@@ -123,6 +132,13 @@ def test_plan_errors(setup):
     assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, None, C.byref(plan)) == _lib.RQ_ERR_ARG
     arr[0].scene = 0
     assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, None, C.byref(plan)) == _lib.RQ_ERR_ARG
+    b = batches[0]
+    arr[0].n = int(b.tmax.shape[0])
+    arr[0].d_org, arr[0].d_dir, arr[0].d_tmax = b.org.data_ptr(), b.dir.data_ptr(), b.tmax.data_ptr()
+    for bad in (dict(smem_entries=65), dict(smem_entries=-1), dict(smem_entries=8, reg_stack=2)):
+        cfg = _lib.BatchConfig(block_threads=128, chunk_rays=128, refill_threshold=8, **bad)
+        assert _lib.lib.rq_batch_plan_create(scenes, 1, arr, 1, C.byref(cfg),
+                                             C.byref(plan)) == _lib.RQ_ERR_ARG, bad
 
 
 def test_plan_follows_scene_updates():
@@ -147,13 +163,15 @@ def test_plan_follows_scene_updates():
     bq.launch()
     # a plan over a breadth-first copy of the records follows the updates too
     bq2 = BatchedQueries([bvh], [batch], dict(reg_stack=2, node_layout=1))
+    # and a split-stack plan, whose overflow area grows with a deeper tree
+    bq3 = BatchedQueries([bvh], [batch], dict(smem_entries=3))
     v0 = mesh.vertices.copy()
     for k, rotate in ((1, True), (2, False), (3, True)):
         mesh.vertices = scenes.animated_vertices(v0, k, amplitude=0.05)
         bvh.update(rotate=rotate)
-        bq.launch()
-        _check(bq, _expected([bvh], [(0, o, d, tm, False)]))
-        bq2.launch()
-        _check(bq2, _expected([bvh], [(0, o, d, tm, False)]))
+        for p in (bq, bq2, bq3):
+            p.launch()
+            _check(p, _expected([bvh], [(0, o, d, tm, False)]))
     bq.close()
     bq2.close()
+    bq3.close()

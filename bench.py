@@ -439,6 +439,52 @@ class SmallFrame:
                 f"of the scene took {build_s:.2f} s")
         return rays / secs / 1e6, threads, text, secs
 
+    def dropin_rates(self, threads, seconds=1.5):
+        """The reference's own renderer on the host cores with the drop-in
+        swapped in: Manta's Raytracer + Lambertian + HardShadows (the
+        reference's classes compiled here in the MANTA_SSE build the CPU
+        baseline uses, oracle/_ref/libmanta_dropin_sse.so) tracing every
+        64-ray packet through
+        GpuDynBVH, one packet per call, on `threads` render workers.  Packets
+        reach the device per call (rq_trace: a launch and a synchronise
+        each), through the resident packet channel (rq_channel_*), and
+        through the channel with GpuHardShadows for the shadow rays.
+        Mrays/s of whole frames (primary + shadow rays)."""
+        from oracle.pyoracle import DROPIN_SO, DROPIN_SSE_SO, Reference
+        path = DROPIN_SSE_SO if os.path.exists(DROPIN_SSE_SO) else DROPIN_SO
+        if not os.path.exists(path):
+            return None
+        ref = Reference(path=path)
+        rs = ref.scene(self.sc.mesh, 0)
+        rs.use_gpu(0, 0)  # the drop-in's own GPU-built tree
+        npx = self.sc.xres * self.sc.yres
+        build = "MANTA_SSE" if path == DROPIN_SSE_SO else "scalar"
+        out = {"threads": threads,
+               "frame": f"{self.sc.xres}x{self.sc.yres}, 1 spp, Raytracer/Lambertian/"
+                        f"HardShadows of the reference ({build} build) over GpuDynBVH"}
+        def rate(workers):
+            rs.render(self.sc, nthreads=workers, want_ids=False)  # warm-up
+            secs, rays, frames = 0.0, 0, 0
+            while frames < 2 or secs < seconds:
+                o = rs.render(self.sc, nthreads=workers, want_ids=False)
+                secs += o["seconds"]
+                rays += npx + o["shadow_rays"]
+                frames += 1
+            return round(rays / secs / 1e6, 2)
+
+        for name, mode, gpu_shadows in (("per_call", 0, False), ("resident", 2, False),
+                                        ("resident_gpu_shadows", 2, True)):
+            rs.gpu_options(mode=mode, gpu_shadows=gpu_shadows)
+            out[f"{name}_mrays"] = rate(threads)
+        # more render workers than cores: a worker waiting on its packet
+        # yields the core to one that shades
+        rs.gpu_options(mode=2, gpu_shadows=True)
+        out["resident_gpu_shadows_workers_mrays"] = {str(w): rate(w) for w in
+                                                     (2 * threads, 4 * threads, 8 * threads)}
+        rs.gpu_options(mode=0)
+        rs.close()
+        return out
+
 
 class CoherentFrame:
     """1920x1080, 4 spp jittered primary + hard-shadow rays from two point
@@ -985,6 +1031,7 @@ class AnimatedFrame(SmallFrame):
     device) and updates the tree as DynBVH::update does (refit, leaf
     re-splits, tree rotations), then renders."""
     name = "animated_frame"
+    dropin_rates = None  # measured on the small frame itself
     PERIOD = 8
 
     def __init__(self):
@@ -1223,6 +1270,8 @@ def run_ours(args):
                                     "kind": "reference", "sample": text}
             if hasattr(wl, "image_check"):
                 line["image_error"] = wl.image_check()
+            if getattr(wl, "dropin_rates", None):
+                line["manta_dropin"] = wl.dropin_rates(threads)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

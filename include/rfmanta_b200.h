@@ -264,6 +264,49 @@ RQ_API int rq_queue_stats(const rq_queue* queue, long long* batches, long long* 
                           long long* rays);
 RQ_API int rq_queue_destroy(rq_queue* queue);
 
+/*
+ * Resident packet channel: the per-packet form of rq_trace without a launch,
+ * copy or stream synchronisation per call.  A persistent kernel keeps one
+ * CTA per slot resident and polls the slots, which live in mapped pinned
+ * host memory; a calling thread takes a free slot, writes its rays there,
+ * publishes a sequence number and spins until the device posts the hits
+ * back.  rq_channel_trace has rq_trace's arguments and results and may be
+ * called from any number of threads at once (up to `slots` at a time are
+ * served concurrently; more wait for a slot).  Packets of more than
+ * `max_rays` rays go through rq_trace.  This is the round trip Manta's
+ * workers make per packet in DynBVH::intersect (Model/Groups/DynBVH.cc:
+ * 101-130, called from Engine/Control/RTRT.cc:984-990).
+ *
+ * The kernel starts on the first packet and exits after idle_ms without a
+ * packet (default 20 ms) or after life_s in all (default 10 s; the next
+ * packet starts it again), or when asked (rq_channel_stop, and before any
+ * entry point changes the scene's tree).  While it runs it occupies `slots`
+ * CTAs of 128 threads, and device-wide synchronisation in the process
+ * (cudaDeviceSynchronize, cudaFree) waits until the channel goes idle.
+ * Every wait is bounded: a packet not answered within timeout_s (default
+ * 10 s) returns RQ_ERR_TIMEOUT and its slot is retired.  Statistics mode
+ * (rq_set_stats) does not count channel packets.  The scene must not be
+ * updated while channel traces run; destroy channels before their scene
+ * (a destroyed scene leaves its channels returning RQ_ERR_STATE).
+ * slots <= 0 = 64 (at most 1024); max_rays <= 0 = 1024 (at most 65536).
+ */
+typedef struct rq_channel rq_channel;
+RQ_API int rq_channel_create(rq_scene* scene, int slots, int max_rays, rq_channel** out);
+RQ_API int rq_channel_trace(rq_channel* channel, int n, const float* org, const float* dir,
+                            const float* tmax, int flags, float* t, int32_t* prim, float* u,
+                            float* v);
+RQ_API int rq_channel_set_timing(rq_channel* channel, double idle_ms, double life_s,
+                                 double timeout_s);
+/* Packets and rays traced through the channel, kernel launches so far, and
+ * per packet on average: device time from the slot's CTA seeing the packet to
+ * posting its hits, and the caller's wait from publishing it to seeing the
+ * hits (any pointer may be NULL). */
+RQ_API int rq_channel_stats(const rq_channel* channel, long long* packets, long long* rays,
+                            long long* launches, double* device_us, double* round_trip_us);
+/* Stops the kernel now (it starts again on the next packet). */
+RQ_API int rq_channel_stop(rq_channel* channel);
+RQ_API int rq_channel_destroy(rq_channel* channel);
+
 /* Node-record orders a traversal can read (same records, same results):
  * the builder's depth-first pre-order, breadth-first from the root, or the
  * top 16,384 records breadth-first followed by the rest depth-first.  Batch

@@ -23,6 +23,7 @@ ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmanta_ref.so")
 REF_SSE_SO = os.path.join(HERE, "_ref", "libmanta_ref_sse.so")
 DROPIN_SO = os.path.join(HERE, "_ref", "libmanta_dropin.so")
+DROPIN_SSE_SO = os.path.join(HERE, "_ref", "libmanta_dropin_sse.so")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
@@ -626,10 +627,13 @@ class RefScene:
         if self.ref.lib.mref_scene_gpu_as_primitive(self.h) != 0:
             raise RuntimeError("mref_scene_gpu_as_primitive: the scene is not on the drop-in")
 
-    def gpu_options(self, batching=True, gpu_shadows=False):
-        """Drop-in library only: packets through the submission queue or one
-        round trip each; GpuHardShadows instead of HardShadows."""
-        if self.ref.lib.mref_scene_gpu_options(self.h, int(batching), int(gpu_shadows)) != 0:
+    def gpu_options(self, batching=True, gpu_shadows=False, mode=None):
+        """Drop-in library only: packets through the submission queue
+        (batching) or one round trip each, or `mode` 0 / 1 / 2 = per call /
+        queue / resident packet channel; GpuHardShadows instead of
+        HardShadows."""
+        m = int(batching) if mode is None else int(mode)
+        if self.ref.lib.mref_scene_gpu_options(self.h, m, int(gpu_shadows)) != 0:
             raise RuntimeError("mref_scene_gpu_options: the scene is not on the drop-in")
 
     def close(self):

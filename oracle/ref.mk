@@ -102,7 +102,7 @@ all: $(OUT)/libmanta_ref.so $(OUT)/libmanta_ref_sse.so
 # The same checker with this project's C++ drop-in (rfmanta_b200/manta/
 # GpuDynBVH) compiled against the reference headers and linked to the CUDA
 # library: the reference's renderers running on the device path.
-dropin: $(OUT)/libmanta_dropin.so
+dropin: $(OUT)/libmanta_dropin.so $(OUT)/libmanta_dropin_sse.so
 
 # ---- generated config headers (one set per SSE variant) -------------------
 define GEN_HEADERS
@@ -188,6 +188,26 @@ DROPIN_OBJ := $(OUT)/obj_nosse/harness_dropin.o $(OUT)/obj_nosse/GpuDynBVH.o \
 
 $(OUT)/libmanta_dropin.so: $(OBJ_NOSSE) $(DROPIN_OBJ) $(REPO)/rfmanta_b200/librfmanta_b200.so
 	$(CXX) -shared -pthread -o $@ $(OBJ_NOSSE) $(DROPIN_OBJ) -L$(REPO)/rfmanta_b200 -lrfmanta_b200 -Wl,-rpath,'$$ORIGIN/../../rfmanta_b200' -Wl,--no-as-needed -lstdc++ -lm
+
+# The drop-in over the MANTA_SSE build of the reference classes (the build
+# the CPU baseline is timed in), for timing the reference's renderer with
+# GpuDynBVH swapped in.
+DROPIN_HDRS := $(REPO)/rfmanta_b200/manta/GpuDynBVH.h $(REPO)/rfmanta_b200/manta/GpuHardShadows.h \
+  $(REPO)/rfmanta_b200/manta/GpuMeshPrimitive.h $(REPO)/include/rfmanta_b200.h
+
+$(OUT)/obj_sse/harness_dropin.o: $(HERE)ref_harness.cc $(DROPIN_HDRS) $(OUT)/gen_sse/include/.stamp
+	@mkdir -p $(dir $@)
+	$(CXX) $(COMMON_FLAGS) -msse4.1 -DMREF_DROPIN $(INC_SSE) -I$(REPO) -c $< -o $@
+
+$(OUT)/obj_sse/Gpu%.o: $(REPO)/rfmanta_b200/manta/Gpu%.cc $(DROPIN_HDRS) $(OUT)/gen_sse/include/.stamp
+	@mkdir -p $(dir $@)
+	$(CXX) $(COMMON_FLAGS) -msse4.1 $(INC_SSE) -I$(REPO) -c $< -o $@
+
+DROPIN_SSE_OBJ := $(OUT)/obj_sse/harness_dropin.o $(OUT)/obj_sse/GpuDynBVH.o \
+  $(OUT)/obj_sse/GpuHardShadows.o $(OUT)/obj_sse/GpuMeshPrimitive.o
+
+$(OUT)/libmanta_dropin_sse.so: $(OBJ_SSE) $(DROPIN_SSE_OBJ) $(REPO)/rfmanta_b200/librfmanta_b200.so
+	$(CXX) -shared -pthread -o $@ $(OBJ_SSE) $(DROPIN_SSE_OBJ) -L$(REPO)/rfmanta_b200 -lrfmanta_b200 -Wl,-rpath,'$$ORIGIN/../../rfmanta_b200' -Wl,--no-as-needed -lstdc++ -lm
 
 $(OUT)/libmanta_ref.so: $(OBJ_NOSSE) $(OUT)/obj_nosse/harness.o
 	$(CXX) -shared -pthread -o $@ $^ -Wl,--no-as-needed -lstdc++ -lm

@@ -1206,8 +1206,9 @@ int mref_scene_use_gpu(void* h, int device, int tri_kind, const char* tree_file)
   return 0;
 }
 
-// Options of a scene already swapped to the drop-in: batching of concurrent
-// packets through the submission queue (GpuDynBVH::setBatching), and
+// Options of a scene already swapped to the drop-in: how packets reach the
+// device (GpuDynBVH::setPacketMode: 0 one round trip per call, 1 the
+// submission queue, 2 the resident packet channel), and
 // GpuHardShadows for Whitted renders.
 int mref_scene_gpu_options(void* h, int batching, int gpu_shadows) {
   RefScene* s = static_cast<RefScene*>(h);
@@ -1219,7 +1220,7 @@ int mref_scene_gpu_options(void* h, int batching, int gpu_shadows) {
     g = p ? p->bvh() : 0;
   }
   if (!g) return 1;
-  g->setBatching(batching != 0);
+  g->setPacketMode(batching);
   s->gpu_shadows = gpu_shadows;
   return 0;
 }

@@ -193,6 +193,14 @@ def _load():
         "rq_queue_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                             C.POINTER(C.c_longlong)], i),
         "rq_queue_destroy": ([vp], i),
+        "rq_channel_create": ([vp, i, i, C.POINTER(vp)], i),
+        "rq_channel_trace": ([vp, i, vp, vp, vp, i, vp, vp, vp, vp], i),
+        "rq_channel_set_timing": ([vp, C.c_double, C.c_double, C.c_double], i),
+        "rq_channel_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                              C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                              C.POINTER(C.c_double)], i),
+        "rq_channel_stop": ([vp], i),
+        "rq_channel_destroy": ([vp], i),
         "rq_server_submit_query": ([vp, C.POINTER(ServeQuery), C.POINTER(i)], i),
         "rq_server_query_result": ([vp, i, vp, vp, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)], i),

@@ -972,6 +972,7 @@ extern "C" int rq_scene_build(rq_scene* scene, int bins) {
     rq::set_error("cudaSetDevice failed");
     return RQ_ERR_CUDA;
   }
+  rq::park_channels(s);  // the build's allocations would wait for a running channel
   rq::HostTree t;
   double secs = 0;
   int rc = rq::gpu_build(s, t, &secs);

@@ -188,6 +188,7 @@ int update_begin(Scene* s, const void* vertices, int n_vertices, int mode) {
     set_error("NULL argument");
     return RQ_ERR_ARG;
   }
+  park_channels(s);
   if (mode != RQ_UPDATE_REFIT && mode != RQ_UPDATE_ROTATE) {
     set_error("unknown update mode");
     return RQ_ERR_ARG;

@@ -54,6 +54,7 @@ Staging::~Staging() {
 }
 
 Scene::~Scene() {
+  detach_channels(this);
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
@@ -219,6 +220,7 @@ int layout_tree(const HostTree& t, int n_objects, TreeLayout& L) {
 
 int Scene::set_tree(const HostTree& t) {
   if (instanced) return set_instance_tree(this, t);
+  park_channels(this);
   TreeLayout L;
   const int rc = layout_tree(t, n_tris, L);
   if (rc != RQ_OK) return rc;

@@ -163,6 +163,11 @@ struct Scene {
   int n_stage_events = 0;
   std::mutex frame_mu;
 
+  // resident packet channels over this scene (rq_channel.cu); their kernels
+  // are stopped before the tree changes and detached when the scene goes
+  std::mutex chan_mu;
+  std::vector<rq_channel*> channels;
+
   // node records in another order (rq_layout.cu), per RQ_LAYOUT_*, made on
   // first use and kept until the tree changes
   struct AltLayout {
@@ -192,6 +197,12 @@ struct Scene {
                    bool anyhit, float* t, int32_t* prim, float* u, float* v,
                    cudaStream_t st, int* counter, int stride = 0, bool one_per_ray = false);
 };
+
+// Stops the kernels of the scene's channels (they start again on their next
+// packet, with the scene's new descriptor); detach_channels also cuts the
+// channels off the scene, which is going away.
+void park_channels(Scene* s);
+void detach_channels(Scene* s);
 
 int rotate_update(Scene* s);
 int sync_layout_host(Scene* s);

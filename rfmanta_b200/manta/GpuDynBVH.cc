@@ -20,15 +20,24 @@ using namespace Manta;
 static const int kQueueRays = 256 * RayPacket::MaxSize;
 
 GpuDynBVH::GpuDynBVH(int device_, int tri_kind_)
-    : group(0), mesh(0), scene(0), queue(0), device(device_), tri_kind(tri_kind_), dirty(false),
-      batching(false) {}
+    : group(0), mesh(0), scene(0), queue(0), channel(0), device(device_), tri_kind(tri_kind_),
+      dirty(false), mode(PerCall) {}
 
 GpuDynBVH::~GpuDynBVH() {
+  if (channel) rq_channel_destroy(channel);
   if (queue) rq_queue_destroy(queue);
   if (scene) rq_scene_destroy(scene);
 }
 
-void GpuDynBVH::setBatching(bool on) { batching = on; }
+void GpuDynBVH::setPacketMode(int m) {
+  if (m != PerCall && m != Queue && m != Resident)
+    throw InternalError("GpuDynBVH::setPacketMode: PerCall, Queue or Resident");
+  mode = m;
+  // an idle channel's kernel is stopped at once rather than at its idle limit
+  if (mode != Resident && channel) rq_channel_stop(channel);
+}
+
+void GpuDynBVH::setBatching(bool on) { setPacketMode(on ? Queue : PerCall); }
 
 void GpuDynBVH::check(int rc, const char* what) const {
   if (rc != RQ_OK)
@@ -58,6 +67,10 @@ Interpolable::InterpErr GpuDynBVH::parallelInterpolate(const std::vector<keyfram
 // Mesh::vertices / vertex_indices / face_material (Model/Groups/Mesh.h:27-50).
 void GpuDynBVH::upload() {
   if (!mesh) throw InternalError("GpuDynBVH needs a Mesh group");
+  if (channel) {
+    rq_channel_destroy(channel);
+    channel = 0;
+  }
   if (queue) {
     rq_queue_destroy(queue);
     queue = 0;
@@ -71,11 +84,19 @@ void GpuDynBVH::upload() {
   for (size_t i = 0; i < nv; ++i)
     for (int c = 0; c < 3; ++c) v[3 * i + c] = mesh->vertices[i][c];
   const int nt = (int)(mesh->vertex_indices.size() / 3);
+  texmap.resize(mesh->size());
+  for (size_t i = 0; i < texmap.size(); ++i)
+    texmap[i] = dynamic_cast<const TexCoordMapper*>(mesh->get(i));
   check(rq_scene_create(&v[0], (int)nv, &mesh->vertex_indices[0], nt,
                         mesh->face_material.empty() ? 0 : &mesh->face_material[0], tri_kind,
                         device, &scene),
         "scene upload");
   check(rq_queue_create(scene, kQueueRays, &queue), "submission queue");
+  // 128 slots: one per render worker up to 128 at a time (workers may
+  // outnumber the cores, so some shade while others wait); 1024-ray packets
+  // hold GpuHardShadows' shadow packets of up to 16 lights (larger ones take
+  // the per-call path)
+  check(rq_channel_create(scene, 128, 16 * RayPacket::MaxSize, &channel), "packet channel");
   dirty = false;
 }
 
@@ -160,7 +181,9 @@ void GpuDynBVH::packRays(const RayPacket& rays, const int* map, int n, int strid
 void GpuDynBVH::traceRays(int n, const float* org, const float* dir, const float* tmax, bool any,
                           float* t, int* prim, float* u, float* v) const {
   const int flags = any ? RQ_ANYHIT : RQ_CLOSEST;
-  if (batching && queue)
+  if (mode == Resident && channel)
+    check(rq_channel_trace(channel, n, org, dir, tmax, flags, t, prim, u, v), "channel trace");
+  else if (mode == Queue && queue)
     check(rq_queue_trace(queue, n, org, dir, tmax, flags, t, prim, u, v), "queued trace");
   else
     check(rq_trace(scene, n, org, dir, tmax, flags, t, prim, u, v), "trace");
@@ -169,25 +192,45 @@ void GpuDynBVH::traceRays(int n, const float* org, const float* dir, const float
 void GpuDynBVH::applyHits(const RenderContext& context, RayPacket& rays, bool any,
                           const int* map, int n, const float* t, const int* prim,
                           const float* u, const float* v) const {
+  Real oldT[RayPacket::MaxSize];
+  bool hit[RayPacket::MaxSize];
   for (int k = 0; k < n; ++k) {
+    hit[k] = false;
     if (prim[k] < 0) continue;
     const int i = map[k];
     const MeshTriangle* tri = mesh->get(prim[k]);
     const Material* matl = mesh->materials[mesh->face_material[prim[k]]];
-    const TexCoordMapper* tex = dynamic_cast<const TexCoordMapper*>(tri);
-    const Real oldT = rays.getMinT(i);
+    const TexCoordMapper* tex = (size_t)prim[k] < texmap.size()
+                                    ? texmap[prim[k]]
+                                    : dynamic_cast<const TexCoordMapper*>(tri);
+    oldT[k] = rays.getMinT(i);
     if (rays.hit(i, t[k], matl, tri, tex)) {
+      hit[k] = true;
       rays.getScratchpad<Real>(WaldTriangle::SCRATCH_U)[i] = u[k];
       rays.getScratchpad<Real>(WaldTriangle::SCRATCH_V)[i] = v[k];
-      if (any) {
-        RayPacket one(rays, i, i + 1);
-        matl->attenuateShadows(context, one);
-        if (one.getColor(i) != Color::black())
-          rays.resetHit(i, oldT);
-        else
-          rays.overrideMinT(i, T_EPSILON);
-      }
     }
+  }
+  if (!any) return;
+  // occluded rays: the material attenuates them, over runs of adjacent rays
+  // with the same hit material as DynBVH does (DynBVH.cc:320-345); an
+  // attenuated ray is released again, an opaque one keeps its hit with
+  // minT = T_EPSILON
+  for (int k = 0; k < n; ++k) {
+    if (!hit[k]) continue;
+    const int i = map[k];
+    const Material* matl = rays.getHitMaterial(i);
+    int e = k + 1;
+    while (e < n && hit[e] && map[e] == map[e - 1] + 1 && rays.getHitMaterial(map[e]) == matl)
+      ++e;
+    RayPacket run(rays, i, map[e - 1] + 1);
+    matl->attenuateShadows(context, run);
+    for (int q = k; q < e; ++q) {
+      if (run.getColor(map[q]) != Color::black())
+        rays.resetHit(map[q], oldT[q]);
+      else
+        rays.overrideMinT(map[q], T_EPSILON);
+    }
+    k = e - 1;
   }
 }
 

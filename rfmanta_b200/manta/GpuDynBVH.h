@@ -10,12 +10,14 @@
 #include <Interface/RayPacket.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/rfmanta_b200.h"
 
 namespace Manta {
 class Group;
 class Mesh;
+class TexCoordMapper;
 
 class GpuDynBVH : public AccelerationStructure {
  public:
@@ -43,14 +45,19 @@ class GpuDynBVH : public AccelerationStructure {
 
   rq_scene* handle() const { return scene; }
 
-  // How a packet reaches the device.  Off (the default): every call is its
-  // own round trip (rq_trace: one launch on a private stream, rays read from
-  // and hits written to mapped host memory, one synchronise).  On: calls go
-  // through one submission queue (rq_queue_*), where packets that arrive
-  // while the device is busy are sent together as one batch.  On the
-  // measured host (16 cores, Manta's Raytracer, 16-256 workers) the queue
-  // is slower: waking the waiting workers costs more than the launches it
-  // saves.
+  // How a packet reaches the device (setPacketMode):
+  //   PerCall   every call is its own round trip (rq_trace: one launch on a
+  //             private stream, rays read from and hits written to mapped
+  //             host memory, one synchronise);
+  //   Queue     calls go through one submission queue (rq_queue_*), where
+  //             packets that arrive while the device is busy are sent
+  //             together as one batch;
+  //   Resident  calls go through a resident packet channel (rq_channel_*):
+  //             a persistent kernel polls mapped host memory, so a packet
+  //             costs no launch and no synchronise.
+  // setBatching(true) is Queue, setBatching(false) PerCall.
+  enum PacketMode { PerCall = 0, Queue = 1, Resident = 2 };
+  void setPacketMode(int mode);
   void setBatching(bool on);
 
   // Packet plumbing shared with GpuHardShadows.  selectRays lists the rays
@@ -77,10 +84,14 @@ class GpuDynBVH : public AccelerationStructure {
   Mesh* mesh;
   rq_scene* scene;
   rq_queue* queue;
+  rq_channel* channel;
+  // each triangle's TexCoordMapper side (a cross-cast resolved once per
+  // upload instead of once per hit)
+  std::vector<const TexCoordMapper*> texmap;
   int device;
   int tri_kind;
   bool dirty;
-  bool batching;
+  int mode;
 };
 
 }  // namespace Manta

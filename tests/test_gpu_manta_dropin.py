@@ -50,11 +50,12 @@ def test_raytracer_through_gpu_dynbvh(kind, tmp_path):
 @pytest.mark.parametrize("kind", [0, 1])
 def test_gpu_hard_shadows_and_batched_packets(kind, tmp_path):
     """GpuHardShadows (all lights' shadow rays of a packet in one
-    submission) and the submission queue (concurrent workers' packets
-    gathered into batches) under the reference's own Raytracer and
-    Lambertian, with three point lights and 32 worker threads: the frame,
-    the per-pixel hits and the shadow-ray count equal the reference's
-    DynBVH + HardShadows render bit for bit, with batching on and off."""
+    submission), the submission queue (concurrent workers' packets gathered
+    into batches) and the resident packet channel under the reference's own
+    Raytracer and Lambertian, with three point lights and 32 worker threads:
+    the frame, the per-pixel hits and the shadow-ray count equal the
+    reference's DynBVH + HardShadows render bit for bit in every packet
+    mode."""
     from rfmanta_b200 import scenes
     sc = scenes.small_frame_scene(xres=192, yres=160)
     sc.lights = list(sc.lights) + [scenes.PointLightSpec((-2.5, 2.0, 1.0), (0.3, 0.35, 0.4)),
@@ -64,12 +65,13 @@ def test_gpu_hard_shadows_and_batched_packets(kind, tmp_path):
     want = cpu.render(sc, nthreads=8)
     gpu = ref.scene(sc.mesh, kind)
     gpu.use_gpu(0, kind, tree_file=str(tmp_path / "tree.bvh"))
-    for batching, gpu_shadows in ((True, True), (False, True), (True, False)):
-        gpu.gpu_options(batching=batching, gpu_shadows=gpu_shadows)
+    # packet modes: 0 one round trip per call, 1 submission queue, 2 resident channel
+    for mode, gpu_shadows in ((1, True), (0, True), (1, False), (2, True), (2, False)):
+        gpu.gpu_options(mode=mode, gpu_shadows=gpu_shadows)
         got = gpu.render(sc, nthreads=32)
-        assert got["shadow_rays"] == want["shadow_rays"], (batching, gpu_shadows)
-        assert np.array_equal(got["prim"], want["prim"]), (batching, gpu_shadows)
-        assert np.array_equal(_bits(got["rgb"]), _bits(want["rgb"])), (batching, gpu_shadows)
+        assert got["shadow_rays"] == want["shadow_rays"], (mode, gpu_shadows)
+        assert np.array_equal(got["prim"], want["prim"]), (mode, gpu_shadows)
+        assert np.array_equal(_bits(got["rgb"]), _bits(want["rgb"])), (mode, gpu_shadows)
 
 
 def test_gpu_mesh_as_primitive_in_a_group(tmp_path):

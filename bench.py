@@ -1031,7 +1031,6 @@ class AnimatedFrame(SmallFrame):
     device) and updates the tree as DynBVH::update does (refit, leaf
     re-splits, tree rotations), then renders."""
     name = "animated_frame"
-    dropin_rates = None  # measured on the small frame itself
     PERIOD = 8
 
     def __init__(self):
@@ -1270,8 +1269,11 @@ def run_ours(args):
                                     "kind": "reference", "sample": text}
             if hasattr(wl, "image_check"):
                 line["image_error"] = wl.image_check()
-            if getattr(wl, "dropin_rates", None):
-                line["manta_dropin"] = wl.dropin_rates(threads)
+            if wl.name in ("path_frame", "small_frame"):
+                # the per-packet drop-in form under the reference's own
+                # renderer (512x512 small frame scene), beside the baseline
+                line["manta_dropin"] = (wl if wl.name == "small_frame"
+                                        else SmallFrame()).dropin_rates(threads)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

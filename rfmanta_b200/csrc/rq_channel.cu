@@ -266,7 +266,7 @@ struct rq_channel {
   cudaStream_t stream = nullptr;
   std::unique_ptr<std::atomic<int>[]> busy;  // slot owned by a host thread
   std::vector<unsigned> seq;                 // last request per slot (owner only)
-  std::vector<char> poisoned;                // slots given up after a timeout
+  std::atomic<int> retired{0};               // slots given up after a timeout (kept busy)
   // launches
   std::mutex launch_mu;
   std::atomic<unsigned> epoch{0};
@@ -357,11 +357,11 @@ int take_slot(rq_channel* ch) {
   int start = hint >= 0 && hint < n ? hint : (int)(std::hash<std::thread::id>()(
                                                        std::this_thread::get_id()) % n);
   for (unsigned spin = 0;; ++spin) {
-    if (std::count(ch->poisoned.begin(), ch->poisoned.end(), 1) == n) return -1;
+    if (ch->retired.load(std::memory_order_relaxed) == n) return -1;
     for (int k = 0; k < n; ++k) {
       const int i = (start + k) % n;
       int zero = 0;
-      if (!ch->poisoned[i] && ch->busy[i].load(std::memory_order_relaxed) == 0 &&
+      if (ch->busy[i].load(std::memory_order_relaxed) == 0 &&
           ch->busy[i].compare_exchange_strong(zero, 1, std::memory_order_acquire)) {
         hint = i;
         return i;
@@ -454,7 +454,6 @@ int rq_channel_create(rq_scene* scene, int slots, int max_rays, rq_channel** out
   ch->busy.reset(new std::atomic<int>[slots]);
   for (int i = 0; i < slots; ++i) ch->busy[i].store(0);
   ch->seq.assign(slots, 0u);
-  ch->poisoned.assign(slots, 0);
   ch->scene = s;
   {
     std::lock_guard<std::mutex> g(s->chan_mu);
@@ -541,8 +540,8 @@ int rq_channel_trace(rq_channel* ch, int n, const float* org, const float* dir,
     }
   }
   if (rc != RQ_OK) {
-    // the request may still be served later: this slot is not used again
-    ch->poisoned[k] = 1;
+    // the request may still be served later: the slot stays taken for good
+    ch->retired.fetch_add(1);
     return rc;
   }
   for (int i = 0; i < n; ++i) {

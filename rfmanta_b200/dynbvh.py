@@ -87,12 +87,29 @@ class SceneInfo:
 class GpuDynBVH:
     """AccelerationStructure over one triangle Mesh, on one GPU."""
 
+    # how intersect() reaches the device (GpuDynBVH::setPacketMode in the
+    # C++ drop-in): one rq_trace call each, or the resident packet channel
+    PerCall, Resident = 0, 2
+
     def __init__(self, tri_kind: int = RQ_TRI_WALD, device: int = 0):
         self.tri_kind = tri_kind
         self.device = device
         self._h = C.c_void_p()
+        self._ch = C.c_void_p()
+        self._mode = self.PerCall
         self._group: Mesh | None = None
         self._dirty = False
+
+    def setPacketMode(self, mode: int) -> None:
+        """PerCall: every intersect() is an rq_trace call (one launch and one
+        synchronise); Resident: calls of up to 1,024 rays go through a
+        resident packet channel (rq_channel_*: a persistent kernel polls
+        mapped host memory, no launch per call), made on first use."""
+        if mode not in (self.PerCall, self.Resident):
+            raise ValueError("PerCall or Resident")
+        self._mode = mode
+        if mode != self.Resident and self._ch:
+            check(lib.rq_channel_stop(self._ch))
 
     # -- AccelerationStructure surface -------------------------------------
     def setGroup(self, group: Mesh) -> None:
@@ -216,8 +233,13 @@ class GpuDynBVH:
         n = len(rays)
         flags = RQ_ANYHIT if rays.getFlag(RQ_ANYHIT) else RQ_CLOSEST
         t = np.empty(n, np.float32)
-        check(lib.rq_trace(self._h, n, _p(rays.org), _p(rays.dir), _p(rays.minT), flags,
-                           _p(t), _p(rays.hitPrim), _p(rays.u), _p(rays.v)))
+        fn, h = lib.rq_trace, self._h
+        if self._mode == self.Resident:
+            if not self._ch:
+                check(lib.rq_channel_create(self._h, 0, 0, C.byref(self._ch)))
+            fn, h = lib.rq_channel_trace, self._ch
+        check(fn(h, n, _p(rays.org), _p(rays.dir), _p(rays.minT), flags,
+                 _p(t), _p(rays.hitPrim), _p(rays.u), _p(rays.v)))
         rays.minT[:] = t
 
     def intersect_device(self, n: int, org_ptr: int, dir_ptr: int, tmax_ptr: int,
@@ -420,6 +442,9 @@ class GpuDynBVH:
         return self._h
 
     def close(self) -> None:
+        if self._ch:
+            lib.rq_channel_destroy(self._ch)
+            self._ch = C.c_void_p()
         if self._h:
             lib.rq_scene_destroy(self._h)
             self._h = C.c_void_p()

@@ -21,7 +21,7 @@ static const int kQueueRays = 256 * RayPacket::MaxSize;
 
 GpuDynBVH::GpuDynBVH(int device_, int tri_kind_)
     : group(0), mesh(0), scene(0), queue(0), channel(0), device(device_), tri_kind(tri_kind_),
-      dirty(false), mode(PerCall) {}
+      dirty(false), mode(Resident) {}
 
 GpuDynBVH::~GpuDynBVH() {
   if (channel) rq_channel_destroy(channel);

@@ -220,3 +220,47 @@ def test_channel_arguments(scene):
     assert _lib.lib.rq_channel_set_timing(ch, 0.0, 1.0, 1.0) == _lib.RQ_ERR_ARG
     assert _stats(ch)[2] == 0  # nothing traced: no kernel was started
     _lib.check(_lib.lib.rq_channel_destroy(ch))
+
+
+def test_python_mirror_resident_mode(scene):
+    """GpuDynBVH.setPacketMode(Resident) (the mirror of the C++ drop-in's
+    packet mode) gives intersect() the same results as per-call tracing,
+    from several threads at once."""
+    import threading
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.dynbvh import GpuDynBVH, RayBatch
+    sc, _ = scene
+    bvh = GpuDynBVH()
+    bvh.setGroup(sc.mesh)
+    bvh.rebuild()
+    lo, hi = sc.mesh.bounds()
+    batches = []
+    for k in range(32):
+        o, d, tm, _ = scenes.random_rays(64 if k % 4 else 2000, lo - 0.3, hi + 0.3,
+                                         seed=700 + k, anyhit_fraction=1.0 if k % 2 else 0.0)
+        batches.append((o, d, tm if k % 2 else np.full(tm.shape, 1e19, np.float32), k % 2))
+    want = []
+    for o, d, tm, a in batches:
+        r = RayBatch(o, d, tm, flags=RayBatch.AnyHit if a else 0)
+        bvh.intersect(r)
+        want.append(r)
+    bvh.setPacketMode(GpuDynBVH.Resident)
+    got = [None] * len(batches)
+
+    def worker(w):
+        for k in range(w, len(batches), 4):
+            o, d, tm, a = batches[k]
+            r = RayBatch(o, d, tm, flags=RayBatch.AnyHit if a else 0)
+            bvh.intersect(r)
+            got[k] = r
+
+    th = [threading.Thread(target=worker, args=(w,)) for w in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for g, w in zip(got, want):
+        assert np.array_equal(g.hitPrim, w.hitPrim)
+        assert np.array_equal(g.minT.view(np.uint32), w.minT.view(np.uint32))
+    bvh.setPacketMode(GpuDynBVH.PerCall)
+    bvh.close()

@@ -350,6 +350,29 @@ class PathFrame:
         return rays / secs / 1e6, threads, text, secs
 
 
+def scenes_camera_rays(sc):
+    """Primary rays of a WhittedScene's pinhole camera in pixel order (row
+    by row), as 3 x n origin and direction arrays (pixel centres; the
+    library's own frame uses the reference's camera on the device)."""
+    cam = sc.camera
+    eye = np.asarray(cam.eye, np.float64)
+    look = np.asarray(cam.lookat, np.float64) - eye
+    up = np.asarray(cam.up, np.float64)
+    w = look / np.linalg.norm(look)
+    u = np.cross(w, up)
+    u /= np.linalg.norm(u)
+    v = np.cross(u, w)
+    tu = np.tan(np.radians(cam.hfov) / 2)
+    tv = np.tan(np.radians(cam.vfov) / 2)
+    ys, xs = np.mgrid[0:sc.yres, 0:sc.xres]
+    px = ((xs + 0.5) / sc.xres * 2 - 1).ravel() * tu
+    py = ((ys + 0.5) / sc.yres * 2 - 1).ravel() * tv
+    d = (w[:, None] + u[:, None] * px[None, :] + v[:, None] * py[None, :])
+    d /= np.linalg.norm(d, axis=0)
+    o = np.repeat(eye[:, None], d.shape[1], axis=1)
+    return o.astype(np.float32), d.astype(np.float32)
+
+
 class SmallFrame:
     name = "small_frame"
 
@@ -438,6 +461,50 @@ class SmallFrame:
                 f"({'MANTA_SSE' if sse else 'scalar'} build); the reference's DynBVH::rebuild "
                 f"of the scene took {build_s:.2f} s")
         return rays / secs / 1e6, threads, text, secs
+
+    def extra(self, dev):
+        """Per-packet latency of the frame's own camera rays: 64-ray packets
+        (one image row segment each, as Manta's workers make them) traced
+        one at a time from host arrays through rq_trace (a launch and a
+        synchronise per packet) and through the resident packet channel;
+        the channel's own records split its round trip into device time and
+        the rest (PCIe signalling and host wait)."""
+        from rfmanta_b200 import _lib
+        sc = self.sc
+        cam = scenes_camera_rays(sc)
+        o, d = cam
+        npk = 512
+        pk = [(np.ascontiguousarray(o[:, 64 * k:64 * k + 64]),
+               np.ascontiguousarray(d[:, 64 * k:64 * k + 64]),
+               np.full(64, 1e19, np.float32)) for k in range(npk)]
+        t = np.zeros(64, np.float32)
+        pr = np.zeros(64, np.int32)
+        ch = C.c_void_p()
+        _lib.check(_lib.lib.rq_channel_create(self.bvh.handle, 16, 1024, C.byref(ch)))
+
+        def run(fn, h):
+            for oo, dd, tm in pk[:32]:  # warm-up
+                _lib.check(fn(h, 64, oo.ctypes.data, dd.ctypes.data, tm.ctypes.data,
+                              _lib.RQ_CLOSEST, t.ctypes.data, pr.ctypes.data, None, None))
+            t0 = time.perf_counter()
+            for oo, dd, tm in pk:
+                _lib.check(fn(h, 64, oo.ctypes.data, dd.ctypes.data, tm.ctypes.data,
+                              _lib.RQ_CLOSEST, t.ctypes.data, pr.ctypes.data, None, None))
+            return (time.perf_counter() - t0) / npk * 1e6
+
+        per_call = run(_lib.lib.rq_trace, self.bvh.handle)
+        resident = run(_lib.lib.rq_channel_trace, ch)
+        p_, r_, n_ = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        dev_us, rt_us = C.c_double(), C.c_double()
+        _lib.check(_lib.lib.rq_channel_stats(ch, C.byref(p_), C.byref(r_), C.byref(n_),
+                                             C.byref(dev_us), C.byref(rt_us)))
+        _lib.lib.rq_channel_destroy(ch)
+        return {"packet_latency_us": {
+            "packet": "64 camera rays of one image row, closest hit, one caller thread",
+            "per_call_rq_trace": round(per_call, 2),
+            "resident_channel": round(resident, 2),
+            "resident_channel_device": round(dev_us.value, 2),
+            "resident_channel_round_trip": round(rt_us.value, 2)}}
 
     def dropin_rates(self, threads, seconds=1.5):
         """The reference's own renderer on the host cores with the drop-in

@@ -1069,6 +1069,50 @@ def system_forms(dev, streams=3):
     return out
 
 
+def quick_rate(wl, dev, steps=5, warmup=3):
+    """Device and end-to-end Mrays/s of one frame workload, timed like the
+    main line (L2 flushed before every timed frame, CUDA events on the
+    launching stream; e2e through the host-buffer call), for the compact
+    record of the other workloads on the default line."""
+    import torch
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    if hasattr(wl, "build"):
+        bvh = wl.build(dev)
+    else:
+        bvh = GpuDynBVH(tri_kind=0, device=dev.index or 0)
+        bvh.setGroup(wl.sc.mesh)
+        bvh.rebuild()
+    wl.setup(bvh, dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        wl.frame(stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    rays = sum(wl.rays())
+    ms = 0.0
+    for k in range(steps):
+        flush.fill_(k & 0xff)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        wl.frame(stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms += a.elapsed_time(b)
+    e2e = 0.0
+    for k in range(warmup + steps):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        wl.host_frame()
+        if k >= warmup:
+            e2e += time.perf_counter() - t0
+    del flush
+    return {"value": round(rays * steps / (ms * 1e-3) / 1e6, 1),
+            "e2e": round(rays * steps / e2e / 1e6, 1),
+            "ms_per_step": round(ms / steps, 4), "rays_per_step": int(rays),
+            "steps": steps, "warmup": warmup}
+
+
 def make_workload(args):
     if args.workload == "batched_queries":
         wl = BatchedQueriesWL(args.batch_scale,
@@ -1293,8 +1337,15 @@ def run_ours(args):
     else:
         achieved, basis = alg_gbs, "algorithmic (cache-inclusive)"
     forms = None
+    others = None
     if rank == 0 and args.system_forms and wl.name == "path_frame":
         forms = system_forms(dev)
+        # the other frame workloads, compactly, so one run records all of them
+        others = {}
+        for cls in (SmallFrame, CoherentFrame, AnimatedFrame):
+            w = cls()
+            others[w.name] = quick_rate(w, dev)
+            del w
 
     if rank == 0:
         line = {
@@ -1330,6 +1381,8 @@ def run_ours(args):
         }
         if forms:
             line["system_forms"] = forms
+        if others:
+            line["other_workloads"] = others
         if not args.no_cpu_baseline:
             v, threads, text, _ = wl.cpu_reference(args.cpu_seconds, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mrays/s", "cores": threads,

@@ -530,13 +530,12 @@ int rq_channel_trace(rq_channel* ch, int n, const float* org, const float* dir,
     if (it < 16) {
       cpu_relax();
     } else {
-      std::this_thread::yield();
-      if ((it & 255u) == 0 &&
-          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >
-              ch->timeout_s) {
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >
+          ch->timeout_s) {
         rc = cfail(RQ_ERR_TIMEOUT, "channel: no answer from the device");
         break;
       }
+      std::this_thread::yield();
     }
   }
   if (rc != RQ_OK) {

@@ -361,8 +361,14 @@ __global__ void __launch_bounds__(128)
                          SampleBufs B, int n_items, unsigned long long* stats) {
   extern __shared__ int2 smem_stack[];
   const unsigned lane = threadIdx.x & 31u;
-  for (int base = blockIdx.x * blockDim.x; base < n_items; base += gridDim.x * blockDim.x) {
-    const int it = base + threadIdx.x;
+  // each warp claims 32 consecutive samples at a time (one per lane), so
+  // warps that finish early take more instead of a fixed share
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&B.counters[1], 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n_items) break;
+    const int it = base + (int)lane;
     bool hit = false;
     Counts cnt;
     if (it < n_items) {
@@ -498,8 +504,12 @@ __global__ void __launch_bounds__(128)
   const unsigned lane = threadIdx.x & 31u;
   int2* stk = smem_stack + threadIdx.x;
   const int stride = blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < nq; base += gridDim.x * blockDim.x) {
-    const int qi = base + threadIdx.x;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&B.counters[2], 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= nq) break;
+    const int qi = base + (int)lane;
     int nshadow = 0;
     Counts cnt;
     if (qi < nq) {

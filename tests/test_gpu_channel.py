@@ -264,3 +264,30 @@ def test_python_mirror_resident_mode(scene):
         assert np.array_equal(g.minT.view(np.uint32), w.minT.view(np.uint32))
     bvh.setPacketMode(GpuDynBVH.PerCall)
     bvh.close()
+
+
+def test_channel_wait_is_bounded(scene):
+    """The host's wait for a packet is bounded: with a timeout far below a
+    PCIe round trip the call returns RQ_ERR_TIMEOUT and retires its slot
+    (the device may still answer into it later); once every slot is
+    retired the channel reports RQ_ERR_STATE, and a new channel traces
+    normally.  No device wait is involved: the kernel itself exits on its
+    idle limit."""
+    from rfmanta_b200 import _lib
+    sc, bvh = scene
+    ch = C.c_void_p()
+    _lib.check(_lib.lib.rq_channel_create(bvh.handle, 2, 64, C.byref(ch)))
+    o, d, tm, fl = _packets(sc.mesh, 1, [64], seed0=900)[0]
+    rc, _ = _trace(_lib.lib.rq_channel_trace, ch, o, d, tm, fl)  # kernel up
+    assert rc == _lib.RQ_OK
+    _lib.check(_lib.lib.rq_channel_set_timing(ch, 20.0, 10.0, 1e-9))
+    for _ in range(2):
+        rc, _ = _trace(_lib.lib.rq_channel_trace, ch, o, d, tm, fl)
+        assert rc == _lib.RQ_ERR_TIMEOUT
+    rc, _ = _trace(_lib.lib.rq_channel_trace, ch, o, d, tm, fl)
+    assert rc == _lib.RQ_ERR_STATE
+    _lib.check(_lib.lib.rq_channel_destroy(ch))
+    _lib.check(_lib.lib.rq_channel_create(bvh.handle, 2, 64, C.byref(ch)))
+    rc, got = _trace(_lib.lib.rq_channel_trace, ch, o, d, tm, fl)
+    assert rc == _lib.RQ_OK and _same(got, _trace(_lib.lib.rq_trace, bvh.handle, o, d, tm, fl)[1])
+    _lib.check(_lib.lib.rq_channel_destroy(ch))

@@ -291,6 +291,8 @@ struct SampleBufs {
   int32_t* queue;
   int32_t* counters;
   unsigned long long* shadow;
+  uint8_t* hit;     // per sample: the primary ray hit something
+  int32_t* tiles;   // compaction scratch
 };
 
 __device__ __forceinline__ void sample_ray(const FrameParams& P, const SampleParams& Q,
@@ -389,14 +391,10 @@ __global__ void __launch_bounds__(128)
         for (int c = 0; c < 3; ++c) B.col[3 * (size_t)it + c] = bg[c];
       }
     }
-    const unsigned m = __ballot_sync(0xffffffffu, hit);
-    if (m) {
-      const int leader = __ffs(m) - 1;
-      int q = 0;
-      if ((int)lane == leader) q = atomicAdd(&B.counters[0], __popc(m));
-      q = __shfl_sync(0xffffffffu, q, leader);
-      if (hit) B.queue[q + __popc(m & ((1u << lane) - 1u))] = it;
-    }
+    // the shade queue is compacted in sample order afterwards, so that the
+    // shade stage's warps take neighbouring samples whatever order the
+    // primary warps finished in
+    if (it < n_items) B.hit[it] = hit ? 1 : 0;
     if (STATS) add_counts(stats, cnt.boxes, cnt.tris);
   }
 }
@@ -622,6 +620,8 @@ static cudaError_t frame_go(const Scene& s, const FrameParams& P, const SamplePa
   frame_primary_kernel<KIND, TWO, STATS>
       <<<std::max(1, std::min(grid, (n_items + bs - 1) / bs)), bs, smem, st>>>(
           S, s.d_blas, P, Q, B, n_items, s.stats);
+  e = launch_flag_compaction(B.hit, n_items, B.tiles, &B.counters[0], B.queue, st);
+  if (e != cudaSuccess) return e;
   if (nev > 1) cudaEventRecord(ev[1], st);
   if (refl)
     frame_shade_kernel<KIND, TWO, STATS, true><<<grid, bs, smem, st>>>(S, s.d_blas, P, Q, B,
@@ -660,8 +660,11 @@ struct SampleScratch {
   void free_items() {
     cudaFree(B.t); cudaFree(B.prim); cudaFree(B.pos); cudaFree(B.blas); cudaFree(B.col);
     cudaFree(B.queue);
+    cudaFree(B.hit);
+    cudaFree(B.tiles);
     B.t = B.col = nullptr;
-    B.prim = B.pos = B.blas = B.queue = nullptr;
+    B.prim = B.pos = B.blas = B.queue = B.tiles = nullptr;
+    B.hit = nullptr;
     items = 0;
   }
   ~SampleScratch() {
@@ -725,7 +728,9 @@ int frame_prepare(rq::Scene* s, const rq_frame_params* fp, rq::FrameParams& P,
     SampleBufs& B = x->B;
     if (cudaMalloc(&B.t, 4 * items) != cudaSuccess || cudaMalloc(&B.prim, 4 * items) != cudaSuccess ||
         cudaMalloc(&B.pos, 4 * items) != cudaSuccess || cudaMalloc(&B.blas, 4 * items) != cudaSuccess ||
-        cudaMalloc(&B.col, 12 * items) != cudaSuccess || cudaMalloc(&B.queue, 4 * items) != cudaSuccess) {
+        cudaMalloc(&B.col, 12 * items) != cudaSuccess || cudaMalloc(&B.queue, 4 * items) != cudaSuccess ||
+        cudaMalloc(&B.hit, items) != cudaSuccess ||
+        cudaMalloc(&B.tiles, 4 * (size_t)flag_compaction_tiles((int)items)) != cudaSuccess) {
       x->free_items();
       return ifail(RQ_ERR_OOM, "frame sample buffers");
     }

@@ -43,6 +43,13 @@ cudaError_t launch_tri_setup(int tri_kind, const float* d_verts,
                              const uint32_t* d_idx, const int32_t* d_perm,
                              int n, float4* d_tris, cudaStream_t st);
 
+// Ordered stream compaction (rq_path.cu): the indices i < n with flags[i]
+// != 0, in increasing order, into qout, and their count into *total_out;
+// tile_counts holds flag_compaction_tiles(n) ints of scratch.
+int flag_compaction_tiles(int n);
+cudaError_t launch_flag_compaction(const uint8_t* flags, int n, int* tile_counts, int* total_out,
+                                   int* qout, cudaStream_t st);
+
 void set_error(const std::string& msg);
 
 }  // namespace rq

@@ -315,6 +315,17 @@ __global__ void __launch_bounds__(kCompactThreads)
     if (base + k < n && alive[base + k]) qout[o++] = base + k;
 }
 
+int flag_compaction_tiles(int n) { return std::max(1, (n + kCompactTile - 1) / kCompactTile); }
+
+cudaError_t launch_flag_compaction(const uint8_t* flags, int n, int* tile_counts, int* total_out,
+                                   int* qout, cudaStream_t st) {
+  const int tiles = flag_compaction_tiles(n);
+  compact_count_kernel<<<tiles, kCompactThreads, 0, st>>>(flags, n, tile_counts);
+  compact_scan_kernel<<<1, 1024, 0, st>>>(tile_counts, tiles, total_out);
+  compact_scatter_kernel<<<tiles, kCompactThreads, 0, st>>>(flags, n, tile_counts, qout);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ordered_compaction(const PathBuffers& B, int n, int depth, cudaStream_t st) {
   const int tiles = std::max(1, (n + kCompactTile - 1) / kCompactTile);
   compact_count_kernel<<<tiles, kCompactThreads, 0, st>>>(B.alive, n, B.tile_counts);

@@ -719,7 +719,7 @@ class BatchedQueriesWL:
             o, d, tm = scenes.query_rays_torch(n, lo, hi, anyhit, seed=1000 + k, device=dev)
             self.batches.append(QueryBatch(si, o, d, tm, anyhit))
         self.bq = BatchedQueries(self.bvhs, self.batches, self.plan_config)
-        self.tuned = self.bq.autotune(reps=1) if self.plan_config is None else self.bq.config
+        self.tuned = self.bq.autotune(reps=3) if self.plan_config is None else self.bq.config
         self.n_events = 0
         self.launches = 1
         self.total = self.bq.total_rays

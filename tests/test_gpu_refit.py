@@ -9,8 +9,9 @@ shape.  Checked here:
   * every refitted box is the exact union of its children / triangles;
   * closest-hit and any-hit queries and the shaded frame on the refitted
     tree agree with the reference's own updated tree on every ray except
-    near-ties (two candidate hits within 1e-6 relative, the north star's
-    exemption, found with the restatement's top-2 pass);
+    near-ties (two candidate hits within 1e-6 relative in t, where the
+    traversal order may pick either; found with the restatement's top-2
+    pass);
   * a GPU-built tree refitted to moved vertices replays bit for bit in the
     restatement.
 """

@@ -175,3 +175,41 @@ def test_plan_follows_scene_updates():
     bq.close()
     bq2.close()
     bq3.close()
+
+
+@pytest.mark.parametrize("cfg", [dict(block_threads=128, chunk_rays=64, refill_threshold=8),
+                                 dict(block_threads=256, chunk_rays=128, refill_threshold=16,
+                                      smem_entries=3, node_layout=1)])
+def test_kensler_shirley_batches_match_single_queries(cfg):
+    """The same check with Kensler-Shirley triangle records (the plan's
+    kernels are compiled per triangle kind), whole stack in shared memory
+    and split."""
+    import torch
+    from rfmanta_b200 import scenes
+    from rfmanta_b200.batch import BatchedQueries, QueryBatch
+    from rfmanta_b200.dynbvh import GpuDynBVH
+    meshes = [scenes.sphere_set(2, 3, seed=4), scenes.heightfield(30, 30, seed=5, extent=3.0)]
+    bvhs = []
+    for m in meshes:
+        b = GpuDynBVH(tri_kind=1)
+        b.setGroup(m)
+        b.rebuild()
+        bvhs.append(b)
+    batches, host = [], []
+    for k, n in enumerate([700, 33, 5000, 1]):
+        si = k % 2
+        lo, hi = meshes[si].bounds()
+        anyhit = bool(k % 2)
+        o, d, tm, _ = scenes.random_rays(n, lo - 0.3, hi + 0.3, seed=300 + k,
+                                         anyhit_fraction=1.0 if anyhit else 0.0)
+        if not anyhit:
+            tm = np.full(n, 1e19, np.float32)
+        host.append((si, o, d, tm, anyhit))
+        batches.append(QueryBatch(si, torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda(),
+                                  torch.from_numpy(tm).cuda(), anyhit, want_uv=True))
+    bq = BatchedQueries(bvhs, batches, cfg)
+    bq.launch()
+    _check(bq, _expected(bvhs, host))
+    bq.close()
+    for b in bvhs:
+        b.close()

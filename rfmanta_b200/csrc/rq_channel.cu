@@ -264,15 +264,23 @@ struct rq_channel {
   float4* data = nullptr;
   rq::ChanDev* d_dev = nullptr;
   cudaStream_t stream = nullptr;
-  std::unique_ptr<std::atomic<int>[]> busy;  // slot owned by a host thread
-  std::vector<unsigned> seq;                 // last request per slot (owner only)
   std::atomic<int> retired{0};               // slots given up after a timeout (kept busy)
   // launches
   std::mutex launch_mu;
   std::atomic<unsigned> epoch{0};
   bool launched = false;
   uint64_t launched_gen = ~0ull;
-  std::atomic<long long> packets{0}, rays{0}, launches{0}, device_ns{0}, wait_ns{0};
+  std::atomic<long long> launches{0};
+  // host-side state of each slot on its own cache line, so callers on
+  // different slots share no line: the owner flag, the last request's
+  // sequence number and counters written only by the slot's current owner
+  // (summed when read)
+  struct alignas(64) Slot {
+    std::atomic<int> busy{0};
+    unsigned seq = 0;
+    std::atomic<long long> packets{0}, rays{0}, device_ns{0}, wait_ns{0};
+  };
+  std::unique_ptr<Slot[]> slot;
 
   ~rq_channel();
 };
@@ -361,8 +369,8 @@ int take_slot(rq_channel* ch) {
     for (int k = 0; k < n; ++k) {
       const int i = (start + k) % n;
       int zero = 0;
-      if (ch->busy[i].load(std::memory_order_relaxed) == 0 &&
-          ch->busy[i].compare_exchange_strong(zero, 1, std::memory_order_acquire)) {
+      if (ch->slot[i].busy.load(std::memory_order_relaxed) == 0 &&
+          ch->slot[i].busy.compare_exchange_strong(zero, 1, std::memory_order_acquire)) {
         hint = i;
         return i;
       }
@@ -451,9 +459,7 @@ int rq_channel_create(rq_scene* scene, int slots, int max_rays, rq_channel** out
     return cfail(RQ_ERR_OOM, "channel control block");
   if (cudaStreamCreateWithFlags(&ch->stream, cudaStreamNonBlocking) != cudaSuccess)
     return cfail(RQ_ERR_CUDA, "channel stream");
-  ch->busy.reset(new std::atomic<int>[slots]);
-  for (int i = 0; i < slots; ++i) ch->busy[i].store(0);
-  ch->seq.assign(slots, 0u);
+  ch->slot.reset(new rq_channel::Slot[slots]);
   ch->scene = s;
   {
     std::lock_guard<std::mutex> g(s->chan_mu);
@@ -511,7 +517,7 @@ int rq_channel_trace(rq_channel* ch, int n, const float* org, const float* dir,
   h->n = n;
   h->flags = flags;
   h->serve_ns = 0;
-  const unsigned seq = ++ch->seq[k];
+  const unsigned seq = ++ch->slot[k].seq;
   const auto t0 = std::chrono::steady_clock::now();
   __atomic_store_n(&h->req, seq, __ATOMIC_SEQ_CST);
   int rc = RQ_OK;
@@ -550,26 +556,35 @@ int rq_channel_trace(rq_channel* ch, int n, const float* org, const float* dir,
     if (u) u[i] = r.z;
     if (v) v[i] = r.w;
   }
-  ch->device_ns.fetch_add(h->serve_ns, std::memory_order_relaxed);
-  ch->wait_ns.fetch_add(std::chrono::duration_cast<std::chrono::nanoseconds>(
-                            std::chrono::steady_clock::now() - t0)
-                            .count(),
-                        std::memory_order_relaxed);
-  ch->busy[k].store(0, std::memory_order_release);
-  ch->packets.fetch_add(1, std::memory_order_relaxed);
-  ch->rays.fetch_add(n, std::memory_order_relaxed);
+  rq_channel::Slot& ss = ch->slot[k];
+  ss.device_ns.store(ss.device_ns.load(std::memory_order_relaxed) + h->serve_ns,
+                     std::memory_order_relaxed);
+  ss.wait_ns.store(ss.wait_ns.load(std::memory_order_relaxed) +
+                       std::chrono::duration_cast<std::chrono::nanoseconds>(
+                           std::chrono::steady_clock::now() - t0)
+                           .count(),
+                   std::memory_order_relaxed);
+  ss.packets.store(ss.packets.load(std::memory_order_relaxed) + 1, std::memory_order_relaxed);
+  ss.rays.store(ss.rays.load(std::memory_order_relaxed) + n, std::memory_order_relaxed);
+  ss.busy.store(0, std::memory_order_release);
   return RQ_OK;
 }
 
 int rq_channel_stats(const rq_channel* ch, long long* packets, long long* rays,
                      long long* launches, double* device_us, double* round_trip_us) {
   if (!ch) return rq::cfail(RQ_ERR_ARG, "NULL channel");
-  const long long p = ch->packets.load();
+  long long p = 0, r = 0, dn = 0, wn = 0;
+  for (int k = 0; k < ch->slots; ++k) {
+    p += ch->slot[k].packets.load(std::memory_order_relaxed);
+    r += ch->slot[k].rays.load(std::memory_order_relaxed);
+    dn += ch->slot[k].device_ns.load(std::memory_order_relaxed);
+    wn += ch->slot[k].wait_ns.load(std::memory_order_relaxed);
+  }
   if (packets) *packets = p;
-  if (rays) *rays = ch->rays.load();
+  if (rays) *rays = r;
   if (launches) *launches = ch->launches.load();
-  if (device_us) *device_us = p ? ch->device_ns.load() * 1e-3 / p : 0.0;
-  if (round_trip_us) *round_trip_us = p ? ch->wait_ns.load() * 1e-3 / p : 0.0;
+  if (device_us) *device_us = p ? dn * 1e-3 / p : 0.0;
+  if (round_trip_us) *round_trip_us = p ? wn * 1e-3 / p : 0.0;
   return RQ_OK;
 }
 

@@ -28,6 +28,10 @@ struct ShadowSet {
   int begin[GpuHardShadows::kMaxLights], end[GpuHardShadows::kMaxLights];
   int depth[GpuHardShadows::kMaxLights], flags[GpuHardShadows::kMaxLights];
   bool valid[GpuHardShadows::kMaxLights];
+  // the one submission's rows (origin, direction, minT in; t, u, v out) and
+  // hit ids, kept with the set so a shade call allocates nothing
+  float rows[11 * GpuHardShadows::kMaxLights * RayPacket::MaxSize];
+  int prim[GpuHardShadows::kMaxLights * RayPacket::MaxSize];
 };
 
 // Per-thread free list of ShadowSets (a shade call on a worker takes one
@@ -147,9 +151,8 @@ void GpuHardShadows::computeShadows(const RenderContext& context, StateBuffer& s
     }
     // all lights' shadow rays in one submission
     if (total > 0) {
-      std::vector<float> buf(11 * (size_t)total);
-      std::vector<int> prim(total);
-      float* org = &buf[0];
+      float* org = set->rows;
+      int* prim = set->prim;
       float* dir = org + 3 * (size_t)total;
       float* tmax = dir + 3 * (size_t)total;
       float* t = tmax + total;
@@ -163,7 +166,7 @@ void GpuHardShadows::computeShadows(const RenderContext& context, StateBuffer& s
         GpuDynBVH::packRays(p, map[l], count[l], total, base, org, dir, tmax);
         base += count[l];
       }
-      bvh->traceRays(total, org, dir, tmax, true, t, &prim[0], u, v);
+      bvh->traceRays(total, org, dir, tmax, true, t, prim, u, v);
       base = 0;
       for (int l = 0; l < nlights; ++l) {
         if (!count[l]) continue;

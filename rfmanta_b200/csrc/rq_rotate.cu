@@ -546,8 +546,9 @@ __global__ void relocate_kernel(DynView V, Scratch S, const int32_t* __restrict_
 //
 // Nodes are handed between threads on different SMs, so every node field is
 // read through volatile pointers (L2, never a stale L1 line) and each hand-
-// over is fenced: writes, __threadfence, arrival counter; counter,
-// __threadfence, reads.
+// over is one acquire-release atomic on the node's arrival counter: the
+// first arrival's writes below the node are released by its increment and
+// acquired by the second arrival's, which then reads them.
 
 struct VNodes {
   volatile float* bounds;
@@ -793,9 +794,14 @@ __global__ void rotate_kernel(DynView D, const float4* __restrict__ recs,
   volatile int32_t* parent = D.parent;
   int node = rec_node[i >> 1];
   while (node >= 0) {
-    __threadfence();
-    if (atomicAdd(D.arrive + node, 1) == 0) return;
-    __threadfence();
+    // one acquire-release arrival: releases this thread's writes below
+    // `node` and, for the second arrival, acquires the sibling's
+    int first;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                 : "=r"(first)
+                 : "l"(D.arrive + node)
+                 : "memory");
+    if (first == 0) return;
     rotate_node(V, node);
     node = parent[node];
   }

@@ -10,11 +10,13 @@
 // memory served by one resident CTA:
 //
 //   host (slot owner)                      device (CTA of the slot)
-//   write rays, n, flags                   poll req (ld.acquire.sys)
-//   req = seq        (seq_cst store)       req != last: load rays (ld.cv),
-//   load state       (seq_cst)               trace, store hits,
-//   spin until done == seq                   fence.sys, done = req (release)
-//   read hits
+//   write rays, n, flags                   poll the slot's first 16 bytes
+//   req = seq        (seq_cst store)         (req, stop, n, flags; one
+//   load state       (seq_cst)               relaxed system-scope load)
+//   spin, then yield, until done == seq    req != last: acquire fence, load
+//   read hits                                rays (ld.cv), trace, store hits,
+//                                            CTA barrier, done = req
+//                                            (system-scope release)
 //
 // Lifetime.  The kernel exits when the host asks (stop), after `idle_ns`
 // without a packet on any slot, or after `life_ns` in all; every device wait

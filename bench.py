@@ -1338,7 +1338,7 @@ def run_ours(args):
         achieved, basis = alg_gbs, "algorithmic (cache-inclusive)"
     forms = None
     others = None
-    if rank == 0 and args.system_forms and wl.name == "path_frame":
+    if rank == 0 and world == 1 and args.system_forms and wl.name == "path_frame":
         forms = system_forms(dev)
         # the other frame workloads, compactly, so one run records all of them
         others = {}
@@ -1383,7 +1383,7 @@ def run_ours(args):
             line["system_forms"] = forms
         if others:
             line["other_workloads"] = others
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the host baseline: rank 0 at N=1
             v, threads, text, _ = wl.cpu_reference(args.cpu_seconds, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mrays/s", "cores": threads,
                                     "kind": "reference", "sample": text}
@@ -1422,7 +1422,7 @@ def run_custom(args, wl, dev, world, rank):
             "gpu_launches": None,
             "roofline": None,
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the host baseline: rank 0 at N=1
             v, threads, text, _ = wl.cpu_reference(args.cpu_seconds, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mrays/s", "cores": threads,
                                     "kind": "reference", "sample": text}

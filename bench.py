@@ -773,6 +773,32 @@ class BatchedQueriesWL:
     def group_stages(self, frame_ms):
         return ["batch_kernel"], [frame_ms]
 
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per ray of
+    # batch_kernel: one ncu capture of the same 64 batches scaled by 1/4
+    # (7,080,009 rays; 1,275.7 MB read, 75.7 MB written) with the autotuned
+    # kind of configuration (split stack, 8 shared entries), scaled to a
+    # full launch by its rays (the batches and scenes are the same, so the
+    # re-read pattern per ray carries over).
+    DRAM_BYTES_PER_RAY = 190.9
+
+    # What bounds batch_kernel, from one `ncu --set full` capture at 1/4 of
+    # the batch sizes (split stack, 8 shared entries, 48 registers).
+    LIMITER = {"limiter": "dependent-load latency and SIMT efficiency on uniformly random rays, "
+                          "not HBM bandwidth",
+               "lanes_per_warp_instruction": 8.67, "warps_active_pct": 55.2,
+               "warps_active_theoretical_pct": 62.5, "issue_active_pct": 61.5,
+               "long_scoreboard_stalls_per_issue": 7.88, "l1_hit_pct": 60.3,
+               "l2_hit_pct": 61.4}
+
+    def limiter(self):
+        return dict(self.LIMITER)
+
+    def traffic(self, rays):
+        n = rays[0]
+        return self.DRAM_BYTES_PER_RAY * n, (
+            f"ncu DRAM bytes per ray of batch_kernel at 1/4 of the batch sizes "
+            f"({self.DRAM_BYTES_PER_RAY} B) x rays of the launch")
+
     def legs(self, dev, reps=5):
         """Device time of the batched plan and of the plain per-call form
         (one rq_trace_device launch per batch, in batch order) over the same

@@ -253,7 +253,7 @@ inline void cpu_relax() {
 }  // namespace rq
 
 struct rq_channel {
-  rq::Scene* scene = nullptr;  // NULL once the scene is gone
+  std::atomic<rq::Scene*> scene{nullptr};  // NULL once the scene is gone
   int device = 0;
   int slots = 0;
   int max_rays = 0;
@@ -314,7 +314,7 @@ int stop_locked(rq_channel* ch) {
 int relaunch(rq_channel* ch, unsigned seen_epoch) {
   std::lock_guard<std::mutex> g(ch->launch_mu);
   if (ch->epoch.load(std::memory_order_acquire) != seen_epoch) return RQ_OK;
-  if (!ch->scene) return cfail(RQ_ERR_STATE, "channel: its scene was destroyed");
+  if (!ch->scene.load()) return cfail(RQ_ERR_STATE, "channel: its scene was destroyed");
   if (cudaSetDevice(ch->device) != cudaSuccess) return cfail(RQ_ERR_CUDA, "cudaSetDevice");
   if (ch->launched) {
     const cudaError_t e = cudaStreamSynchronize(ch->stream);
@@ -322,7 +322,7 @@ int relaunch(rq_channel* ch, unsigned seen_epoch) {
     if (e != cudaSuccess)
       return cfail(RQ_ERR_CUDA, std::string("channel: ") + cudaGetErrorString(e));
   }
-  Scene* s = ch->scene;
+  Scene* s = ch->scene.load();
   if (!s->has_tree) return cfail(RQ_ERR_STATE, "scene has no tree");
   ChanArgs A;
   A.S = s->dev();
@@ -397,7 +397,7 @@ void detach_channels(Scene* s) {
   for (rq_channel* ch : s->channels) {
     std::lock_guard<std::mutex> l(ch->launch_mu);
     stop_locked(ch);
-    ch->scene = nullptr;
+    ch->scene.store(nullptr);
   }
   s->channels.clear();
 }
@@ -409,9 +409,9 @@ rq_channel::~rq_channel() {
     std::lock_guard<std::mutex> l(launch_mu);
     if (ctl) rq::stop_locked(this);
   }
-  if (scene) {
-    std::lock_guard<std::mutex> g(scene->chan_mu);
-    auto& v = scene->channels;
+  if (rq::Scene* s = scene.load()) {
+    std::lock_guard<std::mutex> g(s->chan_mu);
+    auto& v = s->channels;
     v.erase(std::remove(v.begin(), v.end(), this), v.end());
   }
   cudaSetDevice(device);
@@ -462,7 +462,7 @@ int rq_channel_create(rq_scene* scene, int slots, int max_rays, rq_channel** out
   if (cudaStreamCreateWithFlags(&ch->stream, cudaStreamNonBlocking) != cudaSuccess)
     return cfail(RQ_ERR_CUDA, "channel stream");
   ch->slot.reset(new rq_channel::Slot[slots]);
-  ch->scene = s;
+  ch->scene.store(s);
   {
     std::lock_guard<std::mutex> g(s->chan_mu);
     s->channels.push_back(ch.get());
@@ -492,7 +492,7 @@ int rq_channel_trace(rq_channel* ch, int n, const float* org, const float* dir,
   if (n < 0 || (n > 0 && (!org || !dir || !tmax))) return cfail(RQ_ERR_ARG, "bad ray arrays");
   if (flags != RQ_CLOSEST && flags != RQ_ANYHIT) return cfail(RQ_ERR_ARG, "bad flags");
   if (n == 0) return RQ_OK;
-  Scene* s = ch->scene;
+  Scene* s = ch->scene.load();
   if (!s) return cfail(RQ_ERR_STATE, "channel: its scene was destroyed");
   if (n > ch->max_rays)  // larger packets take the per-call path
     return rq_trace(static_cast<rq_scene*>(s), n, org, dir, tmax, flags, t, prim, u, v);
